@@ -1,0 +1,516 @@
+/*
+ * cf_oracle.c -- CPU restatement of Cosmic-Fields-Lite's lattice time-stepping
+ * hot path, in plain C, FP64.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity checker: only tests/, the smoke
+ * check and bench.py's CPU-baseline leg load the library built from this file
+ * (oracle/liboracle.so).  The product (libcfb200.so) never links or calls it.
+ *
+ * Each function cites the reference file:line it restates.  Arithmetic follows
+ * the reference's operation order where that is cheap to keep, so the restatement
+ * agrees with the reference build (oracle/_ref) to rounding; the parity tests
+ * check that agreement and pin both against the reference's published outputs
+ * (output/Growth_and_FS/*_0.dat).
+ *
+ * Layout conventions (reference src/fdm3d.hpp:16,24):
+ *   state  : 2N^3 doubles [phi | dphi], site (a,b,c) at N*N*a + N*b + c;
+ *   HC     : half-complex 2*N*N*(N/2+1) doubles, mode (a,b,c<=N/2) at
+ *            2*(N*(N/2+1)*a + (N/2+1)*b + c) (real, imag);
+ *   S2 bins: 3*(N/2)^2+1 doubles indexed by s^2 = i^2+j^2+k^2.
+ *
+ * Equation codes: 0 = KleinGordonEquation (flat), 1 = KleinGordonEquationInFRW,
+ * 2 = ComovingCurvatureEquationInFRW.  Stencil: 7 (reference) or 13 (fourth
+ * order; no reference counterpart, restated from the standard 5-point
+ * second-derivative formula per axis).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fftw3.h"
+
+#define IDX(N, a, b, c) ((N) * (N) * (a) + (N) * (b) + (c))
+
+static const double CFO_PI = 3.14159265358979323846;
+
+typedef struct {
+  int64_t N;
+  double L, m;
+  double a1, H1, t1, p; /* StaticEOSCosmology, src/physics.hpp:15-56 */
+  int eq;
+  int stencil;
+} cfo_params;
+
+/* ---- cosmology: src/physics.hpp:34-55 ---------------------------------- */
+double cfo_a(const cfo_params *P, double t) {
+  return P->a1 * pow(1 + (1 + 1 / P->p) * P->H1 * (t - P->t1), P->p / (1 + P->p));
+}
+double cfo_H(const cfo_params *P, double t) {
+  return P->H1 * pow(1 + (1 + 1 / P->p) * P->H1 * (t - P->t1), -1);
+}
+double cfo_eta(const cfo_params *P, double t) {
+  return (P->p / (P->a1 * P->H1)) * pow(1 + (1 + 1 / P->p) * P->H1 * (t - P->t1), 1 / (1 + P->p));
+}
+
+/* ---- Psi / dPsi/dt transfer functions: src/equations.cpp:141-183 --------- */
+void cfo_psi_dpsidt_fft(int64_t N, const double *R_fft, double *Psi_fft, double *dPsidt_fft,
+                        double factor, double H_t) {
+  const int64_t nh = N / 2 + 1;
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < nh; ++c) {
+        int64_t as = (a <= N / 2) ? a : (N - a);
+        int64_t bs = (b <= N / 2) ? b : (N - b);
+        int64_t s2 = as * as + bs * bs + c * c;
+        int64_t o = 2 * (N * nh * a + nh * b + c);
+        if (s2 == 0) {
+          Psi_fft[o] = Psi_fft[o + 1] = 0;
+          if (dPsidt_fft) dPsidt_fft[o] = dPsidt_fft[o + 1] = 0;
+          continue;
+        }
+        double x = sqrt((double)s2) * factor;
+        double sv = sin(x), cv = cos(x);
+        double common = 2.0 / (x * x * x) / (double)(N * N * N);
+        double tp = (sv - x * cv) * common;
+        Psi_fft[o] = R_fft[o] * tp;
+        Psi_fft[o + 1] = R_fft[o + 1] * tp;
+        if (dPsidt_fft) {
+          double td = H_t * (3 * x * cv + (x * x - 3.0) * sv) * common;
+          dPsidt_fft[o] = R_fft[o] * td;
+          dPsidt_fft[o + 1] = R_fft[o + 1] * td;
+        }
+      }
+}
+
+/* Psi(x,t) and (optionally) dPsi/dt(x,t) on the lattice, N^3 each.  The
+ * reference computes them with FFTW c2r into dense arrays
+ * (src/equations.cpp:215-233 via fftwWrapper::execute_z2d). */
+void cfo_psi_fields(const cfo_params *P, const double *R_fft, double t, double *Psi, double *dPsidt) {
+  const int64_t N = P->N;
+  const size_t hc = (size_t)(2 * N * N * (N / 2 + 1));
+  double eta_t = cfo_eta(P, t), H_t = cfo_H(P, t);
+  double factor = (2 * CFO_PI / P->L) * eta_t / sqrt(3);
+  double *pf = (double *)malloc(sizeof(double) * hc);
+  double *df = dPsidt ? (double *)malloc(sizeof(double) * hc) : NULL;
+  cfo_psi_dpsidt_fft(N, R_fft, pf, df, factor, H_t);
+  fftw_plan pl = fftw_plan_dft_c2r_3d((int)N, (int)N, (int)N, (fftw_complex *)pf, Psi, FFTW_ESTIMATE);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)pf, Psi);
+  if (dPsidt) fftw_execute_dft_c2r(pl, (fftw_complex *)df, dPsidt);
+  fftw_destroy_plan(pl);
+  free(pf);
+  free(df);
+}
+
+/* Lattice Laplacian times h^2 at site (a,b,c): 7-point (reference
+ * src/equations.cpp:94-101 summation order) or 13-point fourth order. */
+static inline double lap_h2(const double *f, int64_t N, int64_t a, int64_t b, int64_t c, int stencil) {
+  int64_t ap = (a + 1) % N, am = (a + N - 1) % N, bp = (b + 1) % N, bm = (b + N - 1) % N;
+  int64_t cp = (c + 1) % N, cm = (c + N - 1) % N;
+  double f0 = f[IDX(N, a, b, c)];
+  if (stencil != 13) {
+    double s = -6.0 * f0 + f[IDX(N, ap, b, c)] + f[IDX(N, am, b, c)] + f[IDX(N, a, bp, c)] +
+               f[IDX(N, a, bm, c)];
+    return s + (f[IDX(N, a, b, cp)] + f[IDX(N, a, b, cm)]);
+  }
+  int64_t a2p = (a + 2) % N, a2m = (a + 2 * N - 2) % N, b2p = (b + 2) % N, b2m = (b + 2 * N - 2) % N;
+  int64_t c2p = (c + 2) % N, c2m = (c + 2 * N - 2) % N;
+  double s1 = f[IDX(N, ap, b, c)] + f[IDX(N, am, b, c)] + f[IDX(N, a, bp, c)] + f[IDX(N, a, bm, c)] +
+              f[IDX(N, a, b, cp)] + f[IDX(N, a, b, cm)];
+  double s2 = f[IDX(N, a2p, b, c)] + f[IDX(N, a2m, b, c)] + f[IDX(N, a, b2p, c)] +
+              f[IDX(N, a, b2m, c)] + f[IDX(N, a, b, c2p)] + f[IDX(N, a, b, c2m)];
+  return (16.0 * s1 - s2 - 90.0 * f0) / 12.0;
+}
+
+/* dxdt = Equation(x, t).
+ *   eq 0: src/equations.cpp:8-36   dphi' = -m^2 phi + h^-2 lap phi
+ *   eq 1: src/equations.cpp:71-104 dphi' = -3H dphi - m^2 phi + a^-2 h^-2 lap phi
+ *   eq 2: src/equations.cpp:186-261
+ *         dphi' = (-3H + 4 dPsi/dt) dphi - e^{2Psi} m^2 phi + e^{4Psi} a^-2 h^-2 lap phi
+ * R_fft is used for eq 2 only. */
+void cfo_rhs(const cfo_params *P, const double *x, const double *R_fft, double t, double *dxdt) {
+  const int64_t N = P->N, N3 = N * N * N;
+  const double m = P->m;
+  const double h = P->L / N;
+  double inv, H_t = 0;
+  if (P->eq == 0) {
+    inv = 1.0 / (h * h);
+  } else {
+    double a_t = cfo_a(P, t);
+    H_t = cfo_H(P, t);
+    inv = 1.0 / (h * h) / (a_t * a_t);
+  }
+  double *Psi = NULL, *dPsi = NULL;
+  if (P->eq == 2) {
+    Psi = (double *)malloc(sizeof(double) * N3);
+    dPsi = (double *)malloc(sizeof(double) * N3);
+    cfo_psi_fields(P, R_fft, t, Psi, dPsi);
+  }
+  const double *phi = x, *pi = x + N3;
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < N; ++c) {
+        int64_t i = IDX(N, a, b, c);
+        double lap = lap_h2(phi, N, a, b, c, P->stencil);
+        dxdt[i] = pi[i];
+        if (P->eq == 0) {
+          dxdt[N3 + i] = (-1.0) * m * m * phi[i] + inv * lap;
+        } else if (P->eq == 1) {
+          dxdt[N3 + i] = (-3.0) * H_t * pi[i] - m * m * phi[i] + inv * lap;
+        } else {
+          dxdt[N3 + i] = (-3.0 * H_t + 4.0 * dPsi[i]) * pi[i] - exp(2 * Psi[i]) * m * m * phi[i] +
+                         exp(4 * Psi[i]) * inv * lap;
+        }
+      }
+  free(Psi);
+  free(dPsi);
+}
+
+/* One classic RK4 step in place, exactly the stage structure of
+ * boost/numeric/odeint/stepper/runge_kutta4_classic.hpp:88-138 with the
+ * Eigen scale_sum2 / scale_sum5 of src/odeint_eigen/eigen_operations.hpp:33-101:
+ *   k1 = f(x,t); y = x + dt/2 k1; k2 = f(y, t+dt/2); y = x + dt/2 k2;
+ *   k3 = f(y, t+dt/2); y = x + dt k3; k4 = f(y, t+dt);
+ *   x = x + dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4. */
+void cfo_rk4_step(const cfo_params *P, double *x, const double *R_fft, double t, double dt) {
+  const size_t n = (size_t)(2 * P->N * P->N * P->N);
+  double *k1 = (double *)malloc(sizeof(double) * n * 5);
+  double *k2 = k1 + n, *k3 = k2 + n, *k4 = k3 + n, *y = k4 + n;
+  const double dh = dt / 2.0, th = t + dh;
+  cfo_rhs(P, x, R_fft, t, k1);
+  for (size_t i = 0; i < n; ++i) y[i] = 1.0 * x[i] + dh * k1[i];
+  cfo_rhs(P, y, R_fft, th, k2);
+  for (size_t i = 0; i < n; ++i) y[i] = 1.0 * x[i] + dh * k2[i];
+  cfo_rhs(P, y, R_fft, th, k3);
+  for (size_t i = 0; i < n; ++i) y[i] = 1.0 * x[i] + dt * k3[i];
+  cfo_rhs(P, y, R_fft, t + dt, k4);
+  const double dt6 = dt / 6.0, dt3 = dt / 3.0;
+  for (size_t i = 0; i < n; ++i)
+    x[i] = 1.0 * x[i] + dt6 * k1[i] + dt3 * k2[i] + dt3 * k3[i] + dt6 * k4[i];
+  free(k1);
+}
+
+/* `nsteps` steps of integrate_const's loop body
+ * (integrate/detail/integrate_const.hpp:55-64): step j runs at
+ * t = t0 + (step0 + j) * dt (direct, not accumulated). */
+void cfo_rk4_steps(const cfo_params *P, double *x, const double *R_fft, double t0, double dt,
+                   int64_t step0, int64_t nsteps) {
+  for (int64_t j = 0; j < nsteps; ++j) {
+    double t = t0 + (double)(step0 + j) * dt;
+    cfo_rk4_step(P, x, R_fft, t, dt);
+  }
+}
+
+/* Energy density rho (N^3):
+ *   eq 0: src/equations.cpp:38-69, eq 1: :106-138 (inv = h^-2 a^-2),
+ *   eq 2: :265-322 (e^{-2Psi} kinetic, e^{2Psi} gradient weights).
+ *   rho = 1/2 dphi^2 + 1/2 m^2 phi^2 + 1/8 inv sum_axes (phi_{+1}-phi_{-1})^2 */
+void cfo_energy_density(const cfo_params *P, const double *x, const double *R_fft, double t, double *rho) {
+  const int64_t N = P->N, N3 = N * N * N;
+  const double m = P->m, h = P->L / N;
+  double inv = 1.0 / (h * h);
+  if (P->eq != 0) {
+    double a_t = cfo_a(P, t);
+    inv = inv / (a_t * a_t);
+  }
+  double *Psi = NULL;
+  if (P->eq == 2) {
+    Psi = (double *)malloc(sizeof(double) * N3);
+    cfo_psi_fields(P, R_fft, t, Psi, NULL);
+  }
+  const double *phi = x, *pi = x + N3;
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < N; ++c) {
+        int64_t i = IDX(N, a, b, c);
+        double dx = phi[IDX(N, (a + 1) % N, b, c)] - phi[IDX(N, (a + N - 1) % N, b, c)];
+        double dy = phi[IDX(N, a, (b + 1) % N, c)] - phi[IDX(N, a, (b + N - 1) % N, c)];
+        double dz = phi[IDX(N, a, b, (c + 1) % N)] - phi[IDX(N, a, b, (c + N - 1) % N)];
+        double grad = dx * dx + dy * dy + dz * dz;
+        if (P->eq != 2) {
+          rho[i] = 0.5 * (pi[i] * pi[i] + m * m * phi[i] * phi[i] + 0.25 * inv * grad);
+        } else {
+          rho[i] = 0.5 * (exp(-2 * Psi[i]) * pi[i] * pi[i] + m * m * phi[i] * phi[i] +
+                          exp(2 * Psi[i]) * 0.25 * inv * grad);
+        }
+      }
+  free(Psi);
+}
+
+/* r2c of one N^3 field into HC (fftwWrapper::execute_d2z, src/fftw_wrapper.cpp:24-34). */
+void cfo_d2z(int64_t N, const double *f, double *hc) {
+  fftw_plan pl = fftw_plan_dft_r2c_3d((int)N, (int)N, (int)N, (double *)f, (fftw_complex *)hc, FFTW_ESTIMATE);
+  fftw_execute_dft_r2c(pl, (double *)f, (fftw_complex *)hc);
+  fftw_destroy_plan(pl);
+}
+
+/* out[s^2] = sum over all N^3 modes |f_k|^2 (src/fdm3d.cpp:7-34); length 3(N/2)^2+1. */
+void cfo_power_spectrum(int64_t N, const double *f, double *out) {
+  const int64_t nh = N / 2 + 1, nb = 3 * (N / 2) * (N / 2) + 1;
+  double *hc = (double *)malloc(sizeof(double) * 2 * N * N * nh);
+  cfo_d2z(N, f, hc);
+  memset(out, 0, sizeof(double) * nb);
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < N; ++c) {
+        int64_t as = (a <= N / 2) ? a : (N - a), bs = (b <= N / 2) ? b : (N - b), cs = (c <= N / 2) ? c : (N - c);
+        int64_t s2 = as * as + bs * bs + cs * cs;
+        int64_t o = 2 * (N * nh * a + nh * b + cs);
+        out[s2] += hc[o] * hc[o] + hc[o + 1] * hc[o + 1];
+      }
+  free(hc);
+}
+
+/* out[s^2] = sum |phi_k|^2 + |dphi_k|^2 / (m^2 + (2 pi/L)^2 s^2 / a^2)
+ * (src/fdm3d.cpp:36-72). */
+void cfo_mode_power_spectrum(int64_t N, double L, double m, double a_t, const double *state, double *out) {
+  const int64_t nh = N / 2 + 1, nb = 3 * (N / 2) * (N / 2) + 1, N3 = N * N * N;
+  double *h1 = (double *)malloc(sizeof(double) * 4 * N * N * nh);
+  double *h2 = h1 + 2 * N * N * nh;
+  cfo_d2z(N, state, h1);
+  cfo_d2z(N, state + N3, h2);
+  memset(out, 0, sizeof(double) * nb);
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < N; ++c) {
+        int64_t as = (a <= N / 2) ? a : (N - a), bs = (b <= N / 2) ? b : (N - b), cs = (c <= N / 2) ? c : (N - c);
+        int64_t s2 = as * as + bs * bs + cs * cs;
+        int64_t o = 2 * (N * nh * a + nh * b + cs);
+        out[s2] += h1[o] * h1[o] + h1[o + 1] * h1[o + 1] +
+                   (h2[o] * h2[o] + h2[o + 1] * h2[o + 1]) /
+                       (m * m + (2 * CFO_PI / L) * (2 * CFO_PI / L) * s2 / (a_t * a_t));
+      }
+  free(h1);
+}
+
+/* Mode multiplicity per s^2 over the lattice momenta -N/2+1..N/2 on each axis
+ * (the rule of plot_util.py:53-58), exact integers. */
+void cfo_s2_counts(int64_t N, int64_t *counts) {
+  const int64_t nb = 3 * (N / 2) * (N / 2) + 1;
+  memset(counts, 0, sizeof(int64_t) * nb);
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < N; ++c) {
+        int64_t as = (a <= N / 2) ? a : (N - a), bs = (b <= N / 2) ? b : (N - b), cs = (c <= N / 2) ? c : (N - c);
+        counts[as * as + bs * bs + cs * cs] += 1;
+      }
+}
+
+/* Integer square root floor(sqrt(s2)). */
+int64_t cfo_isqrt(int64_t s2) {
+  int64_t r = (int64_t)sqrt((double)s2);
+  while (r * r > s2) --r;
+  while ((r + 1) * (r + 1) <= s2) ++r;
+  return r;
+}
+
+/* Unit-width |k| shells (no reference counterpart): shell i collects the S2
+ * bins s^2 in [i^2, (i+1)^2).  nshell = isqrt(3(N/2)^2)+1.  Sums are accumulated
+ * in s^2 order in long double, then rounded once. */
+void cfo_shells_from_s2(int64_t N, const double *s2bins, const int64_t *s2counts, double *shells,
+                        int64_t *shell_counts) {
+  const int64_t nb = 3 * (N / 2) * (N / 2) + 1;
+  const int64_t ns = cfo_isqrt(nb - 1) + 1;
+  long double *acc = (long double *)calloc((size_t)ns, sizeof(long double));
+  if (shell_counts) memset(shell_counts, 0, sizeof(int64_t) * ns);
+  for (int64_t s = 0; s < nb; ++s) {
+    int64_t i = cfo_isqrt(s);
+    if (s2bins) acc[i] += s2bins[s];
+    if (shell_counts) shell_counts[i] += s2counts[s];
+  }
+  if (shells)
+    for (int64_t i = 0; i < ns; ++i) shells[i] = (double)acc[i];
+  free(acc);
+}
+
+/* ---- seeded inputs as the reference makes them ---------------------------
+ * std::mt19937 (Matsumoto & Nishimura 1998) and libstdc++'s
+ * std::normal_distribution (Marsaglia polar method, one cached deviate, uniform
+ * deviates from generate_canonical<double,53> = two 32-bit draws / 2^64), as
+ * used by RandomNormal (src/random_field.cpp:13-33). */
+typedef struct {
+  uint32_t mt[624];
+  int idx;
+  int have_saved;
+  double saved;
+} cfo_rng;
+
+void cfo_rng_seed(cfo_rng *r, uint32_t seed) {
+  r->mt[0] = seed;
+  for (int i = 1; i < 624; ++i) r->mt[i] = 1812433253u * (r->mt[i - 1] ^ (r->mt[i - 1] >> 30)) + (uint32_t)i;
+  r->idx = 624;
+  r->have_saved = 0;
+}
+
+static uint32_t mt_next(cfo_rng *r) {
+  if (r->idx >= 624) {
+    for (int i = 0; i < 624; ++i) {
+      uint32_t y = (r->mt[i] & 0x80000000u) | (r->mt[(i + 1) % 624] & 0x7fffffffu);
+      uint32_t v = r->mt[(i + 397) % 624] ^ (y >> 1);
+      if (y & 1u) v ^= 0x9908b0dfu;
+      r->mt[i] = v;
+    }
+    r->idx = 0;
+  }
+  uint32_t y = r->mt[r->idx++];
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+static double canonical53(cfo_rng *r) {
+  double lo = (double)mt_next(r);
+  double hi = (double)mt_next(r);
+  double v = (lo + hi * 4294967296.0) / 18446744073709551616.0;
+  if (v >= 1.0) v = nextafter(1.0, 0.0);
+  return v;
+}
+
+double cfo_rng_normal(cfo_rng *r) {
+  if (r->have_saved) {
+    r->have_saved = 0;
+    return r->saved;
+  }
+  double x, y, r2;
+  do {
+    x = 2.0 * canonical53(r) - 1.0;
+    y = 2.0 * canonical53(r) - 1.0;
+    r2 = x * x + y * y;
+  } while (r2 > 1.0 || r2 == 0.0);
+  double mult = sqrt(-2 * log(r2) / r2);
+  r->saved = x * mult;
+  r->have_saved = 1;
+  return y * mult;
+}
+
+size_t cfo_rng_size(void) { return sizeof(cfo_rng); }
+
+/* Spectrum callback P(k) for the Gaussian random field. */
+typedef double (*cfo_spectrum_fn)(double k, const double *args);
+
+/* generate_inhomogeneous_gaussian_random_field (src/random_field.cpp:36-83):
+ * white noise / N^3, times exp(Psi) (Psi may be NULL = 0, scaled by psi_scale),
+ * r2c, times sqrt(P(|k|)) per half-complex mode, unnormalised c2r. */
+void cfo_grf(cfo_rng *r, int64_t N, double L, const double *Psi, double psi_scale, cfo_spectrum_fn P,
+             const double *args, double *out) {
+  const int64_t N3 = N * N * N, nh = N / 2 + 1;
+  for (int64_t i = 0; i < N3; ++i) out[i] = (1.0 / (double)N3) * cfo_rng_normal(r);
+  if (Psi)
+    for (int64_t i = 0; i < N3; ++i) out[i] = out[i] * exp(psi_scale * Psi[i]);
+  double *hc = (double *)malloc(sizeof(double) * 2 * N * N * nh);
+  cfo_d2z(N, out, hc);
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < nh; ++c) {
+        int64_t as = (a <= N / 2) ? a : (a - N), bs = (b <= N / 2) ? b : (b - N);
+        int64_t s2 = as * as + bs * bs + c * c;
+        double abs_k = sqrt((double)s2) * 2 * CFO_PI / L;
+        double sp = sqrt(P(abs_k, args));
+        int64_t o = 2 * (N * nh * a + nh * b + c);
+        hc[o] *= sp;
+        hc[o + 1] *= sp;
+      }
+  fftw_plan pl = fftw_plan_dft_c2r_3d((int)N, (int)N, (int)N, (fftw_complex *)hc, out, FFTW_ESTIMATE);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)hc, out);
+  fftw_destroy_plan(pl);
+  free(hc);
+}
+
+/* Spectra of src/random_field.cpp:92-121 and :128-134, args as listed. */
+/* args = {P_k_ast, k_ast, alpha}: power law with sharp cutoff. */
+static double sp_power_law_cutoff(double k, const double *args) {
+  return k == 0.0 ? 0.0 : (args[0] * (k <= args[1] ? pow(k / args[1], args[2]) : 0.0));
+}
+/* args = {P_k_ast, k_ast, alpha, m}: (k^2 + m^2) times the above. */
+static double sp_deriv_power_law_cutoff(double k, const double *args) {
+  return (k * k + args[3] * args[3]) * sp_power_law_cutoff(k, args);
+}
+/* args = {P_k0}: scale invariant with k0 = 1. */
+static double sp_scale_invariant(double k, const double *args) {
+  return k == 0.0 ? 0.0 : (args[0] * pow(k / 1.0, -3));
+}
+
+/* P_k_ast of power_law_with_cutoff_given_amplitude_3d (src/random_field.cpp:92-101). */
+double cfo_power_law_amplitude(int64_t N, double L, double sigma, double k_ast, double alpha) {
+  double P = alpha == -3.0
+                 ? 2 * CFO_PI * CFO_PI * sigma * sigma / (k_ast * k_ast * k_ast * log(k_ast * L / (2 * CFO_PI)))
+                 : (3 + alpha) * 2 * CFO_PI * CFO_PI * sigma * sigma * (L * L * L * pow(k_ast * L, alpha)) /
+                       (pow(k_ast * L, alpha + 3) - pow(2 * CFO_PI, alpha + 3));
+  P *= ((double)N / L) * ((double)N / L) * ((double)N / L);
+  return P;
+}
+
+/* Cosine integral Ci(x) = gamma + ln x + sum_{k>=1} (-x^2)^k / (2k (2k)!),
+ * the convergent power series (Abramowitz & Stegun 5.2.16), for 0 < x <= 4. */
+double cfo_ci(double x) {
+  double sum = 0.0, term = 1.0;
+  for (int k = 1; k < 60; ++k) {
+    term *= -x * x / ((2.0 * k - 1) * (2.0 * k));
+    double add = term / (2.0 * k);
+    sum += add;
+    if (fabs(add) < 1e-18 * fabs(sum)) break;
+  }
+  return 0.57721566490153286061 + log(x) + sum;
+}
+
+/* Rebuilds the initial state and R_fft of the reference driver
+ * (src/main.cpp:88-138 with perturbed_grf_and_comoving_curvature_fft,
+ * src/initializer.hpp:150-206): params of src/main.cpp:98-122 with N, L given.
+ * state: 2N^3, R_fft: HC.  The amplitude A_s follows initializer.hpp:156-166
+ * with Ci evaluated by the series above. */
+void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, double *R_fft) {
+  const double m = 1.0, k_ast = 1.0, varphi_std = 1.0, Psi_std = 0.02, a1 = 1.0, H1 = 0.05;
+  const double t1 = 1.0 / (2 * H1), t_start = t1;
+  cfo_params P = {N, L, m, a1, H1, t1, 1.0, 2, 7};
+  const int64_t N3 = N * N * N;
+  cfo_rng *r = (cfo_rng *)malloc(sizeof(cfo_rng));
+  cfo_rng_seed(r, seed);
+  const double pi = CFO_PI;
+  double eta_i = cfo_eta(&P, t_start);
+  double A_s = (-576 * pow(pi, 6) * pow(eta_i, 6) * pow(Psi_std, 2)) /
+               (-81 * pow(L, 4) * (pow(L, 2) + 2 * pow(pi, 2) * pow(eta_i, 2)) +
+                L * (81 * pow(L, 5) - 54 * pow(L, 3) * pow(pi, 2) * pow(eta_i, 2) + 48 * L * pow(pi, 4) * pow(eta_i, 4)) *
+                    cos((4 * pi * eta_i) / (sqrt(3) * L)) +
+                256 * pow(pi, 6) * pow(eta_i, 6) * cfo_ci((4 * pi * eta_i) / (sqrt(3) * L)) +
+                4 * sqrt(3) * L * pi * eta_i * (27 * pow(L, 4) + 6 * pow(L, 2) * pow(pi, 2) * pow(eta_i, 2) - 16 * pow(pi, 4) * pow(eta_i, 4)) *
+                    sin((4 * pi * eta_i) / (sqrt(3) * L)));
+  double P_k0 = A_s / ((1.0 * 1.0 * 1.0) / (2 * pi * pi));
+  P_k0 *= ((double)N / L) * ((double)N / L) * ((double)N / L);
+  double *R = (double *)malloc(sizeof(double) * N3);
+  cfo_grf(r, N, L, NULL, 0.0, sp_scale_invariant, &P_k0, R);
+  /* Psi = compute_field_with_scaled_fourier_modes(R, kernel) (src/fdm3d.cpp:76-102) */
+  const int64_t nh = N / 2 + 1;
+  double *hc = (double *)malloc(sizeof(double) * 2 * N * N * nh);
+  cfo_d2z(N, R, hc);
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < nh; ++c) {
+        int64_t as = (a <= N / 2) ? a : (N - a), bs = (b <= N / 2) ? b : (N - b);
+        int64_t s2 = as * as + bs * bs + c * c;
+        double k = sqrt((double)s2) * (2 * pi / L);
+        double kern = k == 0.0 ? 0.0
+                               : (6 * sqrt(3) * (-((k * eta_i * cos((k * eta_i) / sqrt(3))) / sqrt(3)) + sin((k * eta_i) / sqrt(3)))) /
+                                     (pow(k, 3) * pow(eta_i, 3));
+        double scale = kern / (double)(N * N * N);
+        int64_t o = 2 * (N * nh * a + nh * b + c);
+        hc[o] *= scale;
+        hc[o + 1] *= scale;
+      }
+  double *Psi = (double *)malloc(sizeof(double) * N3);
+  fftw_plan pl = fftw_plan_dft_c2r_3d((int)N, (int)N, (int)N, (fftw_complex *)hc, Psi, FFTW_ESTIMATE);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)hc, Psi);
+  fftw_destroy_plan(pl);
+  double v = k_ast / (a1 * m);
+  double alpha_phi = 0.5 * (-3 * pow(4 * pow(v, 2) + 5, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
+  double alpha_dphi = 0.5 * (25 - 20 * pow(v, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
+  double args[4] = {cfo_power_law_amplitude(N, L, varphi_std, k_ast, 0), k_ast, 0.0, m};
+  cfo_grf(r, N, L, Psi, alpha_phi, sp_power_law_cutoff, args, state);
+  cfo_grf(r, N, L, Psi, alpha_dphi, sp_deriv_power_law_cutoff, args, state + N3);
+  cfo_d2z(N, R, R_fft);
+  free(R);
+  free(hc);
+  free(Psi);
+  free(r);
+}
