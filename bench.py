@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""RK4 site-updates/s of the B200 lattice time stepper (libcfb200.so).
+
+Workload (the configuration the headline metric is quoted on): the
+comoving-curvature-coupled Klein-Gordon equation in radiation-dominated FRW
+(a1 = 1, H1 = 0.5, t1 = 1, so a = t^1/2), N = 512, L = 512, m = 1, FP32 hi+lo
+compensated state with FP64 arithmetic, 7-point Laplacian, RK4 dt = 0.05 from
+t = 1.  phi(0) is a Gaussian random field (k* = 0.25, <phi^2> = 1), dphi(0) = 0;
+R is a k^-3 field with cutoff k_max = 0.5 normalised to rms Psi = 1e-2.
+Seeded synthetic inputs; no dataset is involved.
+
+One bench step = one RK4 step of the whole lattice (4 fused stage kernels and
+the Psi / dPsi refreshes at the two new stage times).  The state (1 GB) and all
+RK4 buffers are far larger than the 126 MB L2, so no L2 flush is needed between
+steps.  Times are CUDA events on the stepping stream, max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cfb200|reference]
+
+With N > 1 (torchrun), every rank runs an independent replica on its own GPU
+(the path has no data-parallel exchange); value = total site updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cosmic-fields-lite_b200"))
+
+METRIC = "RK4 site-updates/s @N=512: FP32-comp vs FP64 at ≤1e-6 spectrum err; %HBM peak"
+UNIT = "site-updates/s"
+
+FRW = dict(a1=1.0, H1=0.5, t1=1.0)
+WORKLOAD = dict(workload="comoving-curvature KG, radiation FRW, N=512^3, L=512, m=1, FP32-comp, 7-point, "
+                         "RK4 dt=0.05 from t=1", N=512, L=512.0, m=1.0, dt=0.05, t0=1.0, k_star=0.25,
+                psi_rms=1e-2, k_max=0.5)
+
+# Algorithmic bytes per site and RK4 step of the four fused stage kernels:
+# words moved (state, RK4 accumulator, stage input) per stage 6 + 10 + 10 + 6
+# (FP64) or 6 + 10 + 10 + 12 (FP32-comp, hi + lo state), plus 2 words of
+# Psi, dPsi/dt per stage for the comoving-curvature equation.
+def stage_bytes_per_site(precision, comoving):
+    if precision == "fp64":
+        words, w = 32, 8
+    else:
+        words, w = 38, 4
+    if comoving:
+        words += 8
+    return words * w
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(name):
+    """DRAM bytes per site-update measured by ncu, from the committed summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_site_update:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.f:
+            return None
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x, pg):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ---------------------------------------------------------------- reference arm
+
+
+def cpu_reference_rate(N, steps, threads, comoving=True):
+    """The reference's own CPU path (oracle/_ref: src/equations.cpp + Eigen +
+    Boost.odeint RK4) on the same workload at lattice size N: site-updates/s."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from cfb200 import fields
+
+    os.environ["CF_FFT_THREADS"] = str(threads)
+    W = WORKLOAD
+    L = float(N)
+    x = fields.initial_state(N, L, W["k_star"], seed=2)
+    eta0 = 2.0 * W["t0"] ** 0.5
+    Rf = fields.curvature_R_fft(N, L, eta0, W["psi_rms"], W["k_max"], seed=3) if comoving else None
+    eq = 2 if comoving else 1
+    t_end = W["t0"] + (steps + 0.5) * W["dt"]
+    t = time.perf_counter()
+    O.ref_integrate(eq, N, L, W["m"], x, W["t0"], t_end, W["dt"], R_fft=Rf, **FRW)
+    el = time.perf_counter() - t
+    return N ** 3 * steps / el, el
+
+
+def run_reference_arm(args):
+    world, rank, local, pg = dist_setup()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) missing"}))
+        return
+    threads = os.cpu_count() or 1
+    N = 128
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, el = cpu_reference_rate(N, 1, threads)
+        if i >= args.warmup:
+            rates.append((r, el))
+    el = sum(e for _, e in rates)
+    value = N ** 3 * len(rates) / el
+    sample = (f"reference CPU path (src/equations.cpp ComovingCurvatureEquationInFRW + Eigen + Boost.odeint "
+              f"runge_kutta4_classic) at N=128 (the same workload at a lattice the CPU finishes in seconds), "
+              f"1 RK4 step per bench step, FFTs via the FFTW3 restatement on {threads} threads")
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                      "steps": len(rates), "warmup": args.warmup, "ms_per_step": 1e3 * el / len(rates),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": {k: v for k, v in WORKLOAD.items()},
+                      "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ---------------------------------------------------------------- product arm
+
+
+def make_case(N, L, precision, stencil, comoving, use_torch_inputs=True):
+    import torch
+
+    import cfb200
+    from cfb200 import fields
+    W = WORKLOAD
+    prec = cfb200.FP32_COMP if precision == "fp32comp" else cfb200.FP64
+    eq = cfb200.EQ_COMOVING_FRW if comoving else cfb200.EQ_KG_FRW
+    ctx = cfb200.Context(N, L, m=W["m"], equation=eq, precision=prec, stencil=stencil, **FRW)
+    x = fields.initial_state(N, L, W["k_star"], seed=2, use_torch=use_torch_inputs)
+    st = torch.empty(ctx.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    ctx.import_f64(st, x)
+    if comoving:
+        eta0 = 2.0 * W["t0"] ** 0.5
+        Rf = fields.curvature_R_fft(N, L, eta0, W["psi_rms"], W["k_max"], seed=3, use_torch=use_torch_inputs)
+        ctx.set_R_fft(Rf, on_device=True)
+        del Rf
+    del x
+    torch.cuda.synchronize()
+    return ctx, st
+
+
+def time_steps(ctx, st, steps, warmup, profile=False):
+    import torch
+    W = WORKLOAD
+    stream = torch.cuda.current_stream()
+    ctx.rk4_steps(st, W["t0"], W["dt"], warmup, step0=0)
+    torch.cuda.synchronize()
+    if profile:
+        ctx.profile(True)
+        ctx.profile_reset()
+    l0 = ctx.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.rk4_steps(st, W["t0"], W["dt"], steps, step0=warmup)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = ctx.profile_read() if profile else None
+    if profile:
+        ctx.profile(False)
+    return ms, ctx.launches - l0, prof
+
+
+def run_product(args):
+    import numpy as np
+    import torch
+
+    import cfb200
+    world, rank, local, pg = dist_setup()
+    torch.cuda.set_device(local)
+    W = WORKLOAD
+    N, L = W["N"], W["L"]
+    peak, peak_kind = load_peaks()
+
+    # ---- headline: FP32-comp comoving, 7-point
+    ctx, st = make_case(N, L, "fp32comp", 7, True)
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        ms, launches, prof = time_steps(ctx, st, args.steps, args.warmup, profile=True)
+    clocks = clk.summary()
+    ms = max_over_ranks(ms, pg)
+    value = world * N ** 3 * args.steps / (ms * 1e-3)
+
+    stage_ms = sum(prof[k][1] for k in ("stage1", "stage2", "stage3", "stage4"))
+    stage_launches = sum(prof[k][0] for k in ("stage1", "stage2", "stage3", "stage4"))
+    bps = stage_bytes_per_site("fp32comp", True)
+    achieved = bps * N ** 3 * args.steps / (stage_ms * 1e-3) / 1e9
+    traffic = traffic_from_profiles("stage_kernels_n512.md")
+    roofline = {"bound": "hbm", "kernel": "k_stage (RK4 stages 1-4, FP32-comp, comoving)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind,
+                "traffic": (traffic * N ** 3 * args.steps / stage_launches) if traffic else None,
+                "traffic_unit": "bytes per launch",
+                "algorithmic_bytes_per_site_update": bps,
+                "time_share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()
+                               if v[0]}}
+
+    # ---- accuracy of the FP32-comp state after the timed run, against the FP64 stepper
+    total_steps = args.warmup + args.steps
+    ctx64, st64 = make_case(N, L, "fp64", 7, True)
+    t64_ms, _, prof64 = time_steps(ctx64, st64, args.steps, args.warmup, profile=True)
+    t_end = W["t0"] + total_steps * W["dt"]
+    s32 = torch.empty(ctx.info.s2_bins, dtype=torch.float64, device="cuda")
+    s64 = torch.empty_like(s32)
+    ctx.density_spectrum_s2(st, t_end, s32)
+    ctx64.density_spectrum_s2(st64, t_end, s64)
+    torch.cuda.synchronize()
+    a, b = s32.cpu().numpy(), s64.cpu().numpy()
+    spec_err = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    big = np.abs(b) >= 1e-6 * np.abs(b).max()
+    spec_err_bin = float(np.max(np.abs(a - b)[big] / np.abs(b)[big]))
+    fp64_value = world * N ** 3 * args.steps / (max_over_ranks(t64_ms, pg) * 1e-3)
+    del ctx64, st64
+    torch.cuda.empty_cache()
+
+    # ---- secondary variants (same workload shape)
+    secondary = {"fp64_comoving_7pt": {"value": fp64_value, "ms_per_step": t64_ms / args.steps}}
+    ks = max(5, args.steps // 4)
+    for name, prec, stencil, com in (("fp32comp_comoving_13pt", "fp32comp", 13, True),
+                                     ("fp32comp_kgfrw_7pt", "fp32comp", 7, False),
+                                     ("fp64_kgfrw_7pt", "fp64", 7, False)):
+        c2, s2_ = make_case(N, L, prec, stencil, com)
+        t2, _, p2 = time_steps(c2, s2_, ks, args.warmup, profile=True)
+        sm = sum(p2[k][1] for k in ("stage1", "stage2", "stage3", "stage4"))
+        bb = stage_bytes_per_site(prec, com)
+        secondary[name] = {"value": world * N ** 3 * ks / (max_over_ranks(t2, pg) * 1e-3),
+                           "ms_per_step": t2 / ks,
+                           "stage_kernels_gbs": bb * N ** 3 * ks / (sm * 1e-3) / 1e9}
+        del c2, s2_
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with host buffers: one observer interval
+    # (dt_save = 5 -> 100 RK4 steps) per e2e step: upload the state from pinned
+    # host memory, step, density spectrum, download the spectrum.
+    n_inner = 100
+    host_state = torch.empty(2 * N ** 3, dtype=torch.float64).pin_memory()
+    tmp = torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
+    ctx.export_f64(tmp, st)
+    host_state.copy_(tmp.cpu())
+    del tmp
+    host_spec = torch.empty(ctx.info.s2_bins, dtype=torch.float64).pin_memory()
+    e2e_steps = 2
+    stream = torch.cuda.current_stream()
+
+    def e2e_step(k):
+        ctx.upload(st, host_state.data_ptr())
+        ctx.rk4_steps(st, W["t0"], W["dt"], n_inner, step0=k * n_inner)
+        ctx.density_spectrum_s2(st, W["t0"] + (k + 1) * n_inner * W["dt"], s32)
+        host_spec.copy_(s32, non_blocking=True)
+
+    e2e_step(0)
+    torch.cuda.synchronize()
+    barrier(pg)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(e2e_steps):
+        e2e_step(k + 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg)
+    e2e_value = world * N ** 3 * n_inner * e2e_steps / (e2e_ms * 1e-3)
+
+    # ---- CPU baseline: the reference's own CPU path, bounded sample, rank 0 at N=1
+    cpu = None
+    if world == 1 and rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if O.ref_available():
+            nb = 128
+            r, el = cpu_reference_rate(nb, 2, 1)
+            cpu = {"value": r, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference CPU path (ComovingCurvatureEquationInFRW, Eigen, Boost.odeint RK4) "
+                             f"on the same workload at N={nb}, 2 RK4 steps ({el:.1f} s), single thread as "
+                             f"shipped; FFTs through the FFTW3 restatement"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "storage": "f32 hi + f32 lo",
+                "data": "synthetic",
+                "config": dict(WORKLOAD, precision="fp32comp", stencil=7, parallelism=f"replicas x{world}",
+                               l2="inputs larger than L2 (state 1.07 GB, RK4 buffers 3.2 GB); no flush"),
+                "fp32comp_vs_fp64": value / fp64_value,
+                "density_spectrum_err_vs_fp64": {"normwise": spec_err, "max_bin_rel_ge_1e-6_max": spec_err_bin,
+                                                 "after_steps": total_steps},
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT,
+                        "h2d_bytes_per_step": int(host_state.numel() * 8),
+                        "d2h_bytes_per_step": int(host_spec.numel() * 8),
+                        "step": f"upload state + {n_inner} RK4 steps + density spectrum + download spectrum"},
+                "gpu_launches": launches, "clocks": clocks, "secondary": secondary}
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cfb200", choices=["cfb200", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,248 @@
+"""ctypes binding of libcfb200.so (the C ABI in include/cfb200.h).
+
+This is the harness the parity tests and bench.py use to drive the product
+through its C ABI; C++ callers use include/cfb200.h (and the odeint adapter
+include/cfb200_odeint.hpp) directly.  Device buffers are plain CUDA pointers;
+the helpers accept torch CUDA tensors for convenience (torch only provides the
+memory and the stream).
+
+There is no CPU fallback: if the library is missing or no GPU is usable, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libcfb200.so")
+HEADER = os.path.join(ROOT, "include", "cfb200.h")
+
+CF_OK = 0
+STATUS = {0: "CF_OK", -1: "CF_ERR_INVALID", -2: "CF_ERR_CUDA", -3: "CF_ERR_CUFFT", -4: "CF_ERR_NOMEM",
+          -5: "CF_ERR_NONFINITE", -6: "CF_ERR_TIMEOUT", -7: "CF_ERR_UNSUPPORTED"}
+EQ_KG, EQ_KG_FRW, EQ_COMOVING_FRW = 0, 1, 2
+FP64, FP32_COMP = 0, 1
+
+
+class CfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class cf_params(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int64), ("L", ctypes.c_double), ("m", ctypes.c_double),
+                ("a1", ctypes.c_double), ("H1", ctypes.c_double), ("t1", ctypes.c_double),
+                ("p", ctypes.c_double), ("equation", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("stencil", ctypes.c_int32), ("flags", ctypes.c_int32)]
+
+
+class cf_info(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int64), ("state_bytes", ctypes.c_int64), ("field_count", ctypes.c_int64),
+                ("hc_count", ctypes.c_int64), ("s2_bins", ctypes.c_int64), ("shells", ctypes.c_int64)]
+
+
+_vp = ctypes.c_void_p
+_d = ctypes.c_double
+_i64 = ctypes.c_int64
+_i = ctypes.c_int
+
+_SIGS = {
+    "cf_create": ([ctypes.POINTER(cf_params), ctypes.POINTER(_vp)], _i),
+    "cf_destroy": ([_vp], _i),
+    "cf_get_info": ([_vp, ctypes.POINTER(cf_info)], _i),
+    "cf_last_error": ([], ctypes.c_char_p),
+    "cf_launch_count": ([_vp], _i64),
+    "cf_state_upload": ([_vp, _vp, _vp, _vp], _i),
+    "cf_state_download": ([_vp, _vp, _vp, _vp], _i),
+    "cf_state_import": ([_vp, _vp, _vp, _vp], _i),
+    "cf_state_export": ([_vp, _vp, _vp, _vp], _i),
+    "cf_set_R_fft": ([_vp, _vp, _i, _vp], _i),
+    "cf_rk4_steps": ([_vp, _vp, _d, _d, _i64, _i64, _vp], _i),
+    "cf_rhs": ([_vp, _vp, _vp, _d, _vp], _i),
+    "cf_scale_sum": ([_vp, _vp, _i, _vp, _vp, _i64, _vp], _i),
+    "cf_energy_density": ([_vp, _vp, _d, _vp, _vp], _i),
+    "cf_power_spectrum_s2": ([_vp, _vp, _vp, _vp], _i),
+    "cf_mode_power_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
+    "cf_density_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
+    "cf_s2_to_shells": ([_vp, _vp, _vp, _vp], _i),
+    "cf_s2_counts": ([_vp, _vp, _vp], _i),
+    "cf_check_finite": ([_vp, _vp, ctypes.POINTER(_i64), _vp], _i),
+    "cf_profile_enable": ([_vp, _i], _i),
+    "cf_profile_read": ([_vp, _vp], _i),
+    "cf_profile_reset": ([_vp], _i),
+}
+
+PROF_KINDS = ["stage1", "stage2", "stage3", "stage4", "psi_transfer", "psi_fft", "spectrum", "other"]
+
+
+class cf_profile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64 * 8), ("ms", ctypes.c_double * 8)]
+
+_lib = None
+
+
+def header_symbols():
+    """Every function name declared in include/cfb200.h."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*(cf_\w+)\s*\(", txt, re.M)))
+
+
+def lib():
+    """Loads libcfb200.so (built by `make -C cosmic-fields-lite_b200`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C cosmic-fields-lite_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(code):
+    if code != CF_OK:
+        msg = lib().cf_last_error()
+        raise CfError(code, msg.decode() if msg else "")
+    return code
+
+
+def _ptr(x):
+    """Device/host pointer of a torch tensor, numpy array or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    if hasattr(x, "data_ptr"):
+        return ctypes.c_void_p(x.data_ptr())
+    if hasattr(x, "ctypes"):
+        return ctypes.c_void_p(x.ctypes.data)
+    raise TypeError(type(x))
+
+
+def _stream(stream):
+    if stream is None:
+        try:
+            import torch
+            return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            return None
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Context:
+    """One cf_ctx: a lattice, an equation, a precision and a stencil."""
+
+    def __init__(self, N, L, m=1.0, equation=EQ_KG_FRW, precision=FP64, stencil=7, a1=1.0, H1=0.0,
+                 t1=0.0, p=1.0):
+        self.params = cf_params(int(N), float(L), float(m), float(a1), float(H1), float(t1), float(p),
+                                int(equation), int(precision), int(stencil), 0)
+        h = ctypes.c_void_p()
+        check(lib().cf_create(ctypes.byref(self.params), ctypes.byref(h)))
+        self.h = h
+        info = cf_info()
+        check(lib().cf_get_info(self.h, ctypes.byref(info)))
+        self.info = info
+        self.N = int(N)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def launches(self):
+        return int(lib().cf_launch_count(self.h))
+
+    # ---- state
+    def upload(self, d_state, h_xy, stream=None):
+        check(lib().cf_state_upload(self.h, _ptr(d_state), _ptr(h_xy), _stream(stream)))
+
+    def download(self, h_xy, d_state, stream=None):
+        check(lib().cf_state_download(self.h, _ptr(h_xy), _ptr(d_state), _stream(stream)))
+
+    def import_f64(self, d_state, d_xy, stream=None):
+        check(lib().cf_state_import(self.h, _ptr(d_state), _ptr(d_xy), _stream(stream)))
+
+    def export_f64(self, d_xy, d_state, stream=None):
+        check(lib().cf_state_export(self.h, _ptr(d_xy), _ptr(d_state), _stream(stream)))
+
+    def set_R_fft(self, R_fft, on_device, stream=None):
+        check(lib().cf_set_R_fft(self.h, _ptr(R_fft), int(on_device), _stream(stream)))
+
+    # ---- hot path
+    def rk4_steps(self, d_state, t0, dt, nsteps, step0=0, stream=None):
+        check(lib().cf_rk4_steps(self.h, _ptr(d_state), float(t0), float(dt), int(step0), int(nsteps),
+                                 _stream(stream)))
+
+    def rhs(self, d_x, d_dxdt, t, stream=None):
+        check(lib().cf_rhs(self.h, _ptr(d_x), _ptr(d_dxdt), float(t), _stream(stream)))
+
+    def scale_sum(self, d_out, d_ins, alphas, length, stream=None):
+        n = len(d_ins)
+        arr = (ctypes.c_void_p * n)(*[_ptr(x).value for x in d_ins])
+        al = (ctypes.c_double * n)(*[float(a) for a in alphas])
+        check(lib().cf_scale_sum(self.h, _ptr(d_out), n, ctypes.cast(arr, ctypes.c_void_p),
+                                 ctypes.cast(al, ctypes.c_void_p), int(length), _stream(stream)))
+
+    # ---- observers
+    def energy_density(self, d_state, t, d_rho, stream=None):
+        check(lib().cf_energy_density(self.h, _ptr(d_state), float(t), _ptr(d_rho), _stream(stream)))
+
+    def power_spectrum_s2(self, d_f, d_out, stream=None):
+        check(lib().cf_power_spectrum_s2(self.h, _ptr(d_f), _ptr(d_out), _stream(stream)))
+
+    def mode_power_spectrum_s2(self, d_state, a_t, d_out, stream=None):
+        check(lib().cf_mode_power_spectrum_s2(self.h, _ptr(d_state), float(a_t), _ptr(d_out), _stream(stream)))
+
+    def density_spectrum_s2(self, d_state, t, d_out, stream=None):
+        check(lib().cf_density_spectrum_s2(self.h, _ptr(d_state), float(t), _ptr(d_out), _stream(stream)))
+
+    def s2_to_shells(self, d_shells, d_counts=None, stream=None):
+        check(lib().cf_s2_to_shells(self.h, _ptr(d_shells), _ptr(d_counts), _stream(stream)))
+
+    def s2_counts(self, d_counts, stream=None):
+        check(lib().cf_s2_counts(self.h, _ptr(d_counts), _stream(stream)))
+
+    # ---- profiling
+    def profile(self, on=True):
+        check(lib().cf_profile_enable(self.h, int(on)))
+
+    def profile_reset(self):
+        check(lib().cf_profile_reset(self.h))
+
+    def profile_read(self):
+        p = cf_profile()
+        check(lib().cf_profile_read(self.h, ctypes.byref(p)))
+        return {k: (int(p.launches[i]), float(p.ms[i])) for i, k in enumerate(PROF_KINDS)}
+
+    def check_finite(self, d_state, stream=None):
+        bad = _i64(0)
+        code = lib().cf_check_finite(self.h, _ptr(d_state), ctypes.byref(bad), _stream(stream))
+        return code, int(bad.value)
+
+
+def a_of_t(a1, H1, t1, t, p=1.0):
+    """StaticEOSCosmology::a (reference src/physics.hpp:34-36) on the host."""
+    return a1 * (1 + (1 + 1 / p) * H1 * (t - t1)) ** (p / (1 + p))

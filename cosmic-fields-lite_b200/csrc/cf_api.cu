@@ -1,0 +1,469 @@
+// cf_api.cu -- the C ABI (include/cfb200.h): context, state transfer, dispatch.
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+
+#include "cf_internal.cuh"
+
+namespace cfb {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+const char *get_error() { return g_err; }
+
+// StaticEOSCosmology::a / H / eta (src/physics.hpp:34-55), same expressions.
+double cosmo_a(const cf_params &p, double t) {
+  return p.a1 * pow(1 + (1 + 1 / p.p) * p.H1 * (t - p.t1), p.p / (1 + p.p));
+}
+double cosmo_H(const cf_params &p, double t) { return p.H1 * pow(1 + (1 + 1 / p.p) * p.H1 * (t - p.t1), -1); }
+double cosmo_eta(const cf_params &p, double t) {
+  return (p.p / (p.a1 * p.H1)) * pow(1 + (1 + 1 / p.p) * p.H1 * (t - p.t1), 1 / (1 + p.p));
+}
+
+void stage_coeffs(const cf_params &p, double t, double *inv_ah2, double *H) {
+  const double h = p.L / (double)p.N;
+  if (p.equation == CF_EQ_KG) {
+    *inv_ah2 = 1.0 / (h * h);  // src/equations.cpp:14
+    *H = 0.0;
+    return;
+  }
+  const double a_t = cosmo_a(p, t);
+  *H = cosmo_H(p, t);
+  *inv_ah2 = 1.0 / (h * h) / (a_t * a_t);  // src/equations.cpp:80
+}
+
+int ensure_rk4_scratch(cf_ctx *ctx) {
+  if (ctx->acc) return CF_OK;
+  const size_t bytes = 2 * (size_t)ctx->N3 * ctx->word;
+  void *p = nullptr;
+  if (cudaMalloc(&p, 3 * bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMalloc of the RK4 temporaries (%zu bytes) failed", 3 * bytes);
+    return CF_ERR_NOMEM;
+  }
+  ctx->acc = p;
+  ctx->ya = (char *)p + bytes;
+  ctx->yb = (char *)p + 2 * bytes;
+  return CF_OK;
+}
+
+// defined in the other translation units
+int rk4_steps(cf_ctx *, void *, double, double, int64_t, int64_t, cudaStream_t);
+int rhs(cf_ctx *, const double *, double *, double, cudaStream_t);
+int scale_sum(cf_ctx *, double *, int, const double *const *, const double *, int64_t, cudaStream_t);
+int set_R_fft(cf_ctx *, const double *, int, cudaStream_t);
+int energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
+int power_spectrum_s2(cf_ctx *, const double *, double *, cudaStream_t);
+int mode_power_spectrum_s2(cf_ctx *, const void *, double, double *, cudaStream_t);
+int density_spectrum_s2(cf_ctx *, const void *, double, double *, cudaStream_t);
+int s2_to_shells(cf_ctx *, double *, int64_t *, cudaStream_t);
+int s2_counts(cf_ctx *, int64_t *, cudaStream_t);
+int state_export(cf_ctx *, double *, const void *, cudaStream_t);
+int state_import(cf_ctx *, void *, const double *, cudaStream_t);
+int check_finite(cf_ctx *, const void *, int64_t *, cudaStream_t);
+
+ProfScope::ProfScope(cf_ctx *c, int k, cudaStream_t s) : ctx(c), kind(k), st(s) {
+  if (!ctx->prof_on) return;
+  if (ctx->prof_pool.empty()) {
+    if (cudaEventCreate(&a) != cudaSuccess) {
+      a = nullptr;
+      return;
+    }
+  } else {
+    a = ctx->prof_pool.back();
+    ctx->prof_pool.pop_back();
+  }
+  cudaEventRecord(a, st);
+}
+
+static void prof_drain(cf_ctx *ctx) {
+  for (auto &r : ctx->prof_pending) {
+    cudaEventSynchronize(r.b);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      ctx->prof_ms[r.kind] += ms;
+      ctx->prof_launches[r.kind] += 1;
+    }
+    ctx->prof_pool.push_back(r.a);
+    ctx->prof_pool.push_back(r.b);
+  }
+  ctx->prof_pending.clear();
+}
+
+ProfScope::~ProfScope() {
+  if (!a) return;
+  cudaEvent_t b = nullptr;
+  if (ctx->prof_pool.empty()) {
+    if (cudaEventCreate(&b) != cudaSuccess) return;
+  } else {
+    b = ctx->prof_pool.back();
+    ctx->prof_pool.pop_back();
+  }
+  cudaEventRecord(b, st);
+  ctx->prof_pending.push_back({kind, a, b});
+  if (ctx->prof_pending.size() > 8192) prof_drain(ctx);
+}
+
+static long long isqrt_host(long long s) {
+  long long r = (long long)std::sqrt((double)s);
+  while (r * r > s) --r;
+  while ((r + 1) * (r + 1) <= s) ++r;
+  return r;
+}
+
+static int check_ctx(const cf_ctx *ctx) {
+  if (!ctx) {
+    set_error("NULL context");
+    return CF_ERR_INVALID;
+  }
+  return CF_OK;
+}
+
+static int check_ptr(const void *p, const char *what, size_t align = 16) {
+  if (!p) {
+    set_error("%s is NULL", what);
+    return CF_ERR_INVALID;
+  }
+  if (((uintptr_t)p) % align) {
+    set_error("%s is not %zu-byte aligned", what, align);
+    return CF_ERR_INVALID;
+  }
+  return CF_OK;
+}
+
+static int use_device(const cf_ctx *ctx) {
+  CF_TRY_CUDA(cudaSetDevice(ctx->device));
+  return CF_OK;
+}
+
+}  // namespace cfb
+
+using namespace cfb;
+
+extern "C" {
+
+const char *cf_last_error(void) { return get_error(); }
+
+int cf_create(const cf_params *params, cf_ctx **out) {
+  if (!params || !out) {
+    set_error("cf_create: NULL argument");
+    return CF_ERR_INVALID;
+  }
+  *out = nullptr;
+  const cf_params &p = *params;
+  if (p.N < 8 || p.N > 2048 || p.N % 8 != 0) {
+    set_error("N = %lld unsupported: need N %% 8 == 0 and 8 <= N <= 2048", (long long)p.N);
+    return CF_ERR_INVALID;
+  }
+  if (!(p.L > 0) || !std::isfinite(p.L) || !std::isfinite(p.m)) {
+    set_error("L must be positive and finite, m finite");
+    return CF_ERR_INVALID;
+  }
+  if (p.equation < CF_EQ_KG || p.equation > CF_EQ_COMOVING_FRW) {
+    set_error("unknown equation %d", p.equation);
+    return CF_ERR_INVALID;
+  }
+  if (p.precision != CF_FP64 && p.precision != CF_FP32_COMP) {
+    set_error("unknown precision %d", p.precision);
+    return CF_ERR_INVALID;
+  }
+  if (p.stencil != 7 && p.stencil != 13) {
+    set_error("stencil must be 7 or 13, got %d", p.stencil);
+    return CF_ERR_INVALID;
+  }
+  if (p.equation != CF_EQ_KG && (!(p.p > 0) || !std::isfinite(p.a1) || !std::isfinite(p.H1) || !std::isfinite(p.t1))) {
+    set_error("FRW parameters must be finite with p > 0");
+    return CF_ERR_INVALID;
+  }
+  if (p.equation == CF_EQ_COMOVING_FRW && (p.H1 == 0.0 || p.a1 == 0.0)) {
+    set_error("the comoving-curvature equation needs a1 != 0 and H1 != 0 (conformal time)");
+    return CF_ERR_INVALID;
+  }
+  int dev = 0;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_error("no usable CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "device count is 0");
+    return CF_ERR_CUDA;
+  }
+  CF_TRY_CUDA(cudaGetDevice(&dev));
+  cf_ctx *ctx = new (std::nothrow) cf_ctx();
+  if (!ctx) {
+    set_error("host allocation failed");
+    return CF_ERR_NOMEM;
+  }
+  ctx->p = p;
+  ctx->N = p.N;
+  ctx->N3 = p.N * p.N * p.N;
+  ctx->nh = p.N / 2 + 1;
+  ctx->hc_count = 2 * p.N * p.N * (p.N / 2 + 1);
+  ctx->s2_bins = 3 * (p.N / 2) * (p.N / 2) + 1;
+  ctx->shells = isqrt_host(ctx->s2_bins - 1) + 1;
+  ctx->device = dev;
+  ctx->word = p.precision == CF_FP32_COMP ? 4 : 8;
+  *out = ctx;
+  return CF_OK;
+}
+
+int cf_destroy(cf_ctx *ctx) {
+  if (!ctx) return CF_OK;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  prof_drain(ctx);
+  for (auto e : ctx->prof_pool) cudaEventDestroy(e);
+  cudaFree(ctx->acc);
+  cudaFree(ctx->R_fft);
+  cudaFree(ctx->psi_hc);
+  for (auto &s : ctx->slot) cudaFree(s.psi);
+  if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
+  if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);
+  if (ctx->have_d2z2) cufftDestroy(ctx->plan_d2z2);
+  cudaFree(ctx->spec_hc);
+  cudaFree(ctx->spec_field);
+  cudaFree(ctx->bins);
+  cudaFree(ctx->maxbits);
+  cudaFree(ctx->s2_counts);
+  delete ctx;
+  return CF_OK;
+}
+
+int cf_get_info(const cf_ctx *ctx, cf_info *info) {
+  CF_TRY(check_ctx(ctx));
+  if (!info) {
+    set_error("info is NULL");
+    return CF_ERR_INVALID;
+  }
+  info->N = ctx->N;
+  info->state_bytes = 16 * ctx->N3;  // 2N^3 doubles, or 4N^3 floats
+  info->field_count = ctx->N3;
+  info->hc_count = ctx->hc_count;
+  info->s2_bins = ctx->s2_bins;
+  info->shells = ctx->shells;
+  return CF_OK;
+}
+
+int64_t cf_launch_count(const cf_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int cf_state_upload(cf_ctx *ctx, void *d_state, const double *h_xy, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(h_xy, "h_xy", 8));
+  CF_TRY(use_device(ctx));
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t bytes = 2 * (size_t)ctx->N3 * sizeof(double);
+  if (ctx->p.precision == CF_FP64) {
+    CF_TRY_CUDA(cudaMemcpyAsync(d_state, h_xy, bytes, cudaMemcpyHostToDevice, st));
+    return CF_OK;
+  }
+  double *tmp = nullptr;
+  if (cudaMallocAsync((void **)&tmp, bytes, st) != cudaSuccess) {
+    set_error("cudaMallocAsync staging buffer failed");
+    return CF_ERR_NOMEM;
+  }
+  CF_TRY_CUDA(cudaMemcpyAsync(tmp, h_xy, bytes, cudaMemcpyHostToDevice, st));
+  int s = state_import(ctx, d_state, tmp, st);
+  CF_TRY_CUDA(cudaFreeAsync(tmp, st));
+  return s;
+}
+
+int cf_state_download(cf_ctx *ctx, double *h_xy, const void *d_state, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(h_xy, "h_xy", 8));
+  CF_TRY(use_device(ctx));
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t bytes = 2 * (size_t)ctx->N3 * sizeof(double);
+  if (ctx->p.precision == CF_FP64) {
+    CF_TRY_CUDA(cudaMemcpyAsync(h_xy, d_state, bytes, cudaMemcpyDeviceToHost, st));
+    return CF_OK;
+  }
+  double *tmp = nullptr;
+  if (cudaMallocAsync((void **)&tmp, bytes, st) != cudaSuccess) {
+    set_error("cudaMallocAsync staging buffer failed");
+    return CF_ERR_NOMEM;
+  }
+  int s = state_export(ctx, tmp, d_state, st);
+  if (s == CF_OK) CF_TRY_CUDA(cudaMemcpyAsync(h_xy, tmp, bytes, cudaMemcpyDeviceToHost, st));
+  CF_TRY_CUDA(cudaFreeAsync(tmp, st));
+  return s;
+}
+
+int cf_state_import(cf_ctx *ctx, void *d_state, const double *d_xy, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(d_xy, "d_xy", 8));
+  CF_TRY(use_device(ctx));
+  return state_import(ctx, d_state, d_xy, (cudaStream_t)stream);
+}
+
+int cf_state_export(cf_ctx *ctx, double *d_xy, const void *d_state, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(d_xy, "d_xy", 8));
+  CF_TRY(use_device(ctx));
+  return state_export(ctx, d_xy, d_state, (cudaStream_t)stream);
+}
+
+int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(R_fft, "R_fft", 8));
+  CF_TRY(use_device(ctx));
+  return set_R_fft(ctx, R_fft, on_device, (cudaStream_t)stream);
+}
+
+int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  if (nsteps < 0 || !std::isfinite(t0) || !std::isfinite(dt)) {
+    set_error("nsteps must be >= 0 and t0, dt finite");
+    return CF_ERR_INVALID;
+  }
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW && !ctx->R_fft) {
+    set_error("comoving-curvature equation: call cf_set_R_fft first");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  return rk4_steps(ctx, d_state, t0, dt, step0, nsteps, (cudaStream_t)stream);
+}
+
+int cf_rhs(cf_ctx *ctx, const double *d_x, double *d_dxdt, double t, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_x, "d_x"));
+  CF_TRY(check_ptr(d_dxdt, "d_dxdt"));
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
+    if (ctx->p.precision != CF_FP64) {
+      set_error("cf_rhs of the comoving-curvature equation needs a CF_FP64 context");
+      return CF_ERR_UNSUPPORTED;
+    }
+    if (!ctx->R_fft) {
+      set_error("comoving-curvature equation: call cf_set_R_fft first");
+      return CF_ERR_INVALID;
+    }
+  }
+  CF_TRY(use_device(ctx));
+  return rhs(ctx, d_x, d_dxdt, t, (cudaStream_t)stream);
+}
+
+int cf_scale_sum(cf_ctx *ctx, double *d_out, int n, const double *const *d_in, const double *alpha, int64_t len,
+                 void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_out, "d_out", 8));
+  if (n < 1 || n > 14 || !d_in || !alpha || len < 0) {
+    set_error("cf_scale_sum: need 1 <= n <= 14, non-NULL inputs, len >= 0");
+    return CF_ERR_INVALID;
+  }
+  for (int k = 0; k < n; ++k) CF_TRY(check_ptr(d_in[k], "d_in[k]", 8));
+  CF_TRY(use_device(ctx));
+  return scale_sum(ctx, d_out, n, d_in, alpha, len, (cudaStream_t)stream);
+}
+
+int cf_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(d_rho, "d_rho", 8));
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW && !ctx->R_fft) {
+    set_error("comoving-curvature equation: call cf_set_R_fft first");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  return energy_density(ctx, d_state, t, d_rho, (cudaStream_t)stream);
+}
+
+int cf_power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_f, "d_f"));
+  CF_TRY(check_ptr(d_out, "d_out", 8));
+  CF_TRY(use_device(ctx));
+  return power_spectrum_s2(ctx, d_f, d_out, (cudaStream_t)stream);
+}
+
+int cf_mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(d_out, "d_out", 8));
+  if (!std::isfinite(a_t) || a_t == 0.0) {
+    set_error("a_t must be finite and non-zero");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  return mode_power_spectrum_s2(ctx, d_state, a_t, d_out, (cudaStream_t)stream);
+}
+
+int cf_density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(d_out, "d_out", 8));
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW && !ctx->R_fft) {
+    set_error("comoving-curvature equation: call cf_set_R_fft first");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  return density_spectrum_s2(ctx, d_state, t, d_out, (cudaStream_t)stream);
+}
+
+int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_shells, "d_shells", 8));
+  CF_TRY(use_device(ctx));
+  return s2_to_shells(ctx, d_shells, d_counts, (cudaStream_t)stream);
+}
+
+int cf_s2_counts(cf_ctx *ctx, int64_t *d_counts, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_counts, "d_counts", 8));
+  CF_TRY(use_device(ctx));
+  return s2_counts(ctx, d_counts, (cudaStream_t)stream);
+}
+
+int cf_profile_enable(cf_ctx *ctx, int on) {
+  CF_TRY(check_ctx(ctx));
+  ctx->prof_on = on != 0;
+  return CF_OK;
+}
+
+int cf_profile_read(cf_ctx *ctx, cf_profile *out) {
+  CF_TRY(check_ctx(ctx));
+  if (!out) {
+    set_error("out is NULL");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  prof_drain(ctx);
+  for (int k = 0; k < CF_PROF_KINDS; ++k) {
+    out->launches[k] = ctx->prof_launches[k];
+    out->ms[k] = ctx->prof_ms[k];
+  }
+  return CF_OK;
+}
+
+int cf_profile_reset(cf_ctx *ctx) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(use_device(ctx));
+  prof_drain(ctx);
+  for (int k = 0; k < CF_PROF_KINDS; ++k) {
+    ctx->prof_launches[k] = 0;
+    ctx->prof_ms[k] = 0.0;
+  }
+  return CF_OK;
+}
+
+int cf_check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(use_device(ctx));
+  return check_finite(ctx, d_state, h_bad, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+// cf_internal.cuh -- shared definitions of libcfb200 (context, errors, helpers).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "cfb200.h"
+
+namespace cfb {
+
+// Thread-local last error message (cf_last_error()).
+void set_error(const char *fmt, ...);
+const char *get_error();
+
+#define CF_TRY_CUDA(expr)                                                                      \
+  do {                                                                                         \
+    cudaError_t e_ = (expr);                                                                   \
+    if (e_ != cudaSuccess) {                                                                   \
+      ::cfb::set_error("%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return CF_ERR_CUDA;                                                                      \
+    }                                                                                          \
+  } while (0)
+
+#define CF_TRY_CUFFT(expr)                                                                     \
+  do {                                                                                         \
+    cufftResult r_ = (expr);                                                                   \
+    if (r_ != CUFFT_SUCCESS) {                                                                 \
+      ::cfb::set_error("%s failed: cufftResult %d (%s:%d)", #expr, (int)r_, __FILE__, __LINE__); \
+      return CF_ERR_CUFFT;                                                                     \
+    }                                                                                          \
+  } while (0)
+
+#define CF_TRY(...)             \
+  do {                          \
+    int s_ = (__VA_ARGS__);     \
+    if (s_ != CF_OK) return s_; \
+  } while (0)
+
+// Checks the launch that was just enqueued.
+#define CF_LAUNCHED(ctx)                                                                       \
+  do {                                                                                         \
+    cudaError_t e_ = cudaGetLastError();                                                       \
+    if (e_ != cudaSuccess) {                                                                   \
+      ::cfb::set_error("kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return CF_ERR_CUDA;                                                                      \
+    }                                                                                          \
+    (ctx)->launches++;                                                                         \
+  } while (0)
+
+// One cached Psi / dPsi/dt pair at a stage time (comoving-curvature equation).
+struct PsiSlot {
+  double t = 0;
+  bool valid = false;
+  void *psi = nullptr;   // N^3 of the storage type
+  void *dpsi = nullptr;  // N^3 of the storage type
+  uint64_t stamp = 0;
+};
+
+}  // namespace cfb
+
+struct cf_ctx {
+  cf_params p;
+  int64_t N = 0, N3 = 0, nh = 0, hc_count = 0, s2_bins = 0, shells = 0;
+  int device = 0;
+  int64_t launches = 0;
+  size_t word = 8;  // bytes of the storage type (8 FP64, 4 FP32_COMP)
+
+  // RK4 temporaries (storage type): acc and ping-pong stage inputs, 2N^3 words each.
+  void *acc = nullptr, *ya = nullptr, *yb = nullptr;
+
+  // Comoving curvature: R_fft in the storage type's complex HC, the transfer
+  // outputs (2 HC arrays) and three cached (Psi, dPsi) slots.
+  void *R_fft = nullptr;
+  void *psi_hc = nullptr;  // 2 consecutive HC arrays (Psi_k, dPsi_k), storage type
+  cfb::PsiSlot slot[3];
+  uint64_t slot_clock = 0;
+  cufftHandle plan_psi = 0;  // batched (2) C2R/Z2D into dense N^3
+  bool have_plan_psi = false;
+
+  // Spectra: FP64 R2C plans and scratch.
+  cufftHandle plan_d2z1 = 0, plan_d2z2 = 0;
+  bool have_d2z1 = false, have_d2z2 = false;
+  double *spec_hc = nullptr;    // 2 HC arrays (FP64)
+  double *spec_field = nullptr; // N^3 FP64 (energy density scratch)
+  unsigned long long *bins = nullptr;   // 2 * s2_bins words: (lo, hi) fixed point
+  unsigned long long *maxbits = nullptr;
+  int64_t *s2_counts = nullptr;
+
+  // Profiling (cf_profile_enable): pending event pairs and per-kind totals.
+  bool prof_on = false;
+  struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof_pending;
+  std::vector<cudaEvent_t> prof_pool;
+  int64_t prof_launches[CF_PROF_KINDS] = {};
+  double prof_ms[CF_PROF_KINDS] = {};
+};
+
+namespace cfb {
+
+// Lazily allocated scratch.
+int ensure_rk4_scratch(cf_ctx *ctx);
+int ensure_spectrum_scratch(cf_ctx *ctx, int nfields);
+int ensure_psi(cf_ctx *ctx);
+
+// Returns the cached Psi / dPsi/dt slot for stage time t, refreshing one slot
+// (transfer kernel + batched C2R on `stream`) if t is not cached.
+int psi_at(cf_ctx *ctx, double t, cudaStream_t stream, const void **psi, const void **dpsi);
+
+// Host-side StaticEOSCosmology (reference src/physics.hpp:34-55), bit-identical
+// to the reference's host code: same expressions, same libm.
+double cosmo_a(const cf_params &p, double t);
+double cosmo_H(const cf_params &p, double t);
+double cosmo_eta(const cf_params &p, double t);
+
+// 1/h^2/a(t)^2 and H(t) exactly as the reference host code forms them
+// (src/equations.cpp:199-202, src/equations_cuda.cu:526-529).
+void stage_coeffs(const cf_params &p, double t, double *inv_ah2, double *H);
+
+inline unsigned ceil_div(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Brackets the launches made between begin and end with profiling events
+// (no-op unless profiling is on).
+struct ProfScope {
+  cf_ctx *ctx;
+  int kind;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  ProfScope(cf_ctx *c, int k, cudaStream_t s);
+  ~ProfScope();
+};
+
+}  // namespace cfb

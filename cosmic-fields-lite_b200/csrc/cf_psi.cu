@@ -1,0 +1,185 @@
+// cf_psi.cu -- Psi(x,t), dPsi/dt(x,t) for the comoving-curvature equation.
+//
+// The reference recomputes both fields inside every right-hand-side call: a
+// transfer-function kernel over the half-complex grid followed by two in-place
+// cuFFT Z2D, with the two HC buffers allocated and freed per call
+// (src/equations_cuda.cu:678-731, kernel :210-253).  RK4 evaluates the
+// right-hand side at only three distinct times per step (t, t+dt/2 twice, t+dt)
+// and t+dt is the next step's t, so here the fields are cached per stage time
+// in three persistent slots and refreshed -- transfer kernel + ONE batched
+// C2R of both fields -- only when a stage asks for a time no slot holds.
+//
+// Storage follows the context precision: FP64 (Z2D) or FP32 (C2R); the
+// transfer function is always evaluated in FP64.
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+
+#include "cf_internal.cuh"
+
+namespace cfb {
+
+// Psi_k = R_k * 2 (sin x - x cos x) / x^3 / N^3,
+// dPsi_k = R_k * 2 H (3 x cos x + (x^2 - 3) sin x) / x^3 / N^3,  x = sqrt(s^2) * factor
+// (src/equations_cuda.cu:210-253; src/equations.cpp:141-183).  Output: two HC
+// arrays of the storage complex type, consecutive.
+template <typename S>
+__global__ void k_transfer(const S *__restrict__ R, S *__restrict__ out, int N, long long hc_pairs,
+                           double factor, double H_t) {
+  const int nh = N / 2 + 1;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < hc_pairs; i += stride) {
+    const int c = (int)(i % nh);
+    const long long ab = i / nh;
+    const int b = (int)(ab % N);
+    const int a = (int)(ab / N);
+    const int as = (a <= N / 2) ? a : N - a;
+    const int bs = (b <= N / 2) ? b : N - b;
+    const long long s2 = (long long)as * as + (long long)bs * bs + (long long)c * c;
+    double rr = (double)R[2 * i], ri = (double)R[2 * i + 1];
+    double tp = 0.0, td = 0.0;
+    if (s2 != 0) {
+      const double x = sqrt((double)s2) * factor;
+      double sv, cv;
+      sincos(x, &sv, &cv);
+      const double common = 2.0 / (x * x * x) * inv_n3;
+      tp = (sv - x * cv) * common;
+      td = H_t * (3 * x * cv + (x * x - 3.0) * sv) * common;
+    }
+    out[2 * i] = (S)(rr * tp);
+    out[2 * i + 1] = (S)(ri * tp);
+    out[2 * hc_pairs + 2 * i] = (S)(rr * td);
+    out[2 * hc_pairs + 2 * i + 1] = (S)(ri * td);
+  }
+}
+
+template <typename S>
+__global__ void k_copy_convert(const double *__restrict__ in, S *__restrict__ out, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (S)in[i];
+}
+
+int ensure_psi(cf_ctx *ctx) {
+  if (ctx->have_plan_psi) return CF_OK;
+  const int N = (int)ctx->N;
+  const size_t w = ctx->word;
+  const size_t hc_bytes = (size_t)ctx->hc_count * w;
+  if (!ctx->R_fft) {
+    if (cudaMalloc(&ctx->R_fft, hc_bytes) != cudaSuccess) {
+      set_error("cudaMalloc R_fft (%zu bytes) failed", hc_bytes);
+      return CF_ERR_NOMEM;
+    }
+    CF_TRY_CUDA(cudaMemset(ctx->R_fft, 0, hc_bytes));
+  }
+  if (cudaMalloc(&ctx->psi_hc, 2 * hc_bytes) != cudaSuccess) {
+    set_error("cudaMalloc Psi transfer buffers (%zu bytes) failed", 2 * hc_bytes);
+    return CF_ERR_NOMEM;
+  }
+  for (auto &s : ctx->slot) {
+    if (cudaMalloc(&s.psi, 2 * (size_t)ctx->N3 * w) != cudaSuccess) {
+      set_error("cudaMalloc Psi slot failed");
+      return CF_ERR_NOMEM;
+    }
+    s.dpsi = (char *)s.psi + (size_t)ctx->N3 * w;
+    s.valid = false;
+  }
+  long long n[3] = {N, N, N};
+  long long inembed[3] = {N, N, N / 2 + 1};
+  long long onembed[3] = {N, N, N};
+  const long long idist = ctx->hc_count / 2;  // complex elements per HC array
+  const long long odist = ctx->N3;
+  CF_TRY_CUFFT(cufftCreate(&ctx->plan_psi));
+  size_t work = 0;
+  CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_psi, 3, n, inembed, 1, idist, onembed, 1, odist,
+                                   w == 8 ? CUFFT_Z2D : CUFFT_C2R, 2, &work));
+  ctx->have_plan_psi = true;
+  return CF_OK;
+}
+
+int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void **dpsi) {
+  CF_TRY(ensure_psi(ctx));
+  for (auto &s : ctx->slot) {
+    if (s.valid && s.t == t) {
+      s.stamp = ++ctx->slot_clock;
+      *psi = s.psi;
+      *dpsi = s.dpsi;
+      return CF_OK;
+    }
+  }
+  // refresh the least recently used slot
+  PsiSlot *v = &ctx->slot[0];
+  for (auto &s : ctx->slot)
+    if (!s.valid || s.stamp < v->stamp) v = &s;
+  const double eta_t = cosmo_eta(ctx->p, t);
+  const double H_t = cosmo_H(ctx->p, t);
+  const double factor = (2 * 3.14159265358979323846 / ctx->p.L) * eta_t / sqrt(3);
+  const long long pairs = ctx->hc_count / 2;
+  unsigned blocks = (unsigned)std::min<long long>((pairs + 255) / 256, 148LL * 32);
+  CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+    if (ctx->word == 8)
+      k_transfer<double><<<blocks, 256, 0, st>>>((const double *)ctx->R_fft, (double *)ctx->psi_hc, (int)ctx->N,
+                                                 pairs, factor, H_t);
+    else
+      k_transfer<float><<<blocks, 256, 0, st>>>((const float *)ctx->R_fft, (float *)ctx->psi_hc, (int)ctx->N,
+                                                pairs, factor, H_t);
+    CF_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    if (ctx->word == 8)
+      CF_TRY_CUFFT(cufftExecZ2D(ctx->plan_psi, (cufftDoubleComplex *)ctx->psi_hc, (cufftDoubleReal *)v->psi));
+    else
+      CF_TRY_CUFFT(cufftExecC2R(ctx->plan_psi, (cufftComplex *)ctx->psi_hc, (cufftReal *)v->psi));
+  }
+  v->t = t;
+  v->valid = true;
+  v->stamp = ++ctx->slot_clock;
+  *psi = v->psi;
+  *dpsi = v->dpsi;
+  return CF_OK;
+}
+
+int set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, cudaStream_t st) {
+  const size_t hc = (size_t)ctx->hc_count;
+  const size_t w = ctx->word;
+  if (!ctx->R_fft) {
+    if (cudaMalloc(&ctx->R_fft, hc * w) != cudaSuccess) {
+      set_error("cudaMalloc R_fft failed");
+      return CF_ERR_NOMEM;
+    }
+  }
+  const double *src = R_fft;
+  double *tmp = nullptr;
+  if (!on_device) {
+    if (w == 8) {
+      CF_TRY_CUDA(cudaMemcpyAsync(ctx->R_fft, R_fft, hc * 8, cudaMemcpyHostToDevice, st));
+      src = nullptr;
+    } else {
+      if (cudaMallocAsync((void **)&tmp, hc * 8, st) != cudaSuccess) {
+        set_error("cudaMallocAsync R_fft staging failed");
+        return CF_ERR_NOMEM;
+      }
+      CF_TRY_CUDA(cudaMemcpyAsync(tmp, R_fft, hc * 8, cudaMemcpyHostToDevice, st));
+      src = tmp;
+    }
+  }
+  if (src) {
+    unsigned blocks = (unsigned)std::min<size_t>((hc + 255) / 256, 148 * 32);
+    if (w == 8) {
+      CF_TRY_CUDA(cudaMemcpyAsync(ctx->R_fft, src, hc * 8, cudaMemcpyDeviceToDevice, st));
+    } else {
+      k_copy_convert<float><<<blocks, 256, 0, st>>>(src, (float *)ctx->R_fft, (long long)hc);
+      CF_LAUNCHED(ctx);
+    }
+  }
+  if (tmp) CF_TRY_CUDA(cudaFreeAsync(tmp, st));
+  for (auto &s : ctx->slot) s.valid = false;
+  return CF_OK;
+}
+
+}  // namespace cfb

@@ -1,0 +1,419 @@
+// cf_spectrum.cu -- energy density, deterministic spectrum binning, spectra.
+//
+// The reference bins |f_k|^2 into s^2 bins with FP64 atomicAdd, whose result
+// depends on the order the atomics land in (src/fdm3d_cuda.cu:3-27, comment at
+// :25).  Here every mode value is converted to a 128-bit fixed-point integer
+// whose scale is a power of two chosen from the (order-independent) maximum
+// mode value, and the bins accumulate those integers with 64-bit integer
+// atomics (carry propagated to the high word).  Integer addition is
+// associative, so the bins are bit-reproducible, and the sums are exact up to
+// the fixed-point resolution (2^-126 of an upper bound on any bin).
+// Unit-width |k| shells are then exact integer regroupings of the s^2 bins.
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+
+#include "cf_internal.cuh"
+
+namespace cfb {
+
+// ---- energy density -----------------------------------------------------
+// rho = 1/2 (e^{-2Psi} pi^2 + m^2 phi^2 + e^{2Psi} 1/4 h^-2 a^-2 sum_axes (phi_{+1} - phi_{-1})^2)
+// with Psi = 0 for the uncoupled equations (src/equations_cuda.cu:332-369, :451-473;
+// src/equations.cpp:38-69, :106-138, :265-322).
+template <typename S, bool COMOV>
+__global__ void k_energy(const S *__restrict__ x, const S *__restrict__ xlo, const S *__restrict__ psi,
+                         double *__restrict__ rho, int N, double m2, double inv) {
+  const long long N3 = (long long)N * N * N;
+  const long long NN = (long long)N * N;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  auto phi = [&](long long i) -> double {
+    double v = (double)x[i];
+    if (xlo) v += (double)xlo[i];
+    return v;
+  };
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N3; i += stride) {
+    const int c = (int)(i % N);
+    const int b = (int)((i / N) % N);
+    const int a = (int)(i / NN);
+    const long long ap = NN * ((a + 1) % N) + (long long)N * b + c, am = NN * ((a + N - 1) % N) + (long long)N * b + c;
+    const long long bp = NN * a + (long long)N * ((b + 1) % N) + c, bm = NN * a + (long long)N * ((b + N - 1) % N) + c;
+    const long long cp = NN * a + (long long)N * b + (c + 1) % N, cm = NN * a + (long long)N * b + (c + N - 1) % N;
+    const double dx = phi(ap) - phi(am), dy = phi(bp) - phi(bm), dz = phi(cp) - phi(cm);
+    const double grad = dx * dx + dy * dy + dz * dz;
+    const double f = phi(i);
+    double p = (double)x[N3 + i];
+    if (xlo) p += (double)xlo[N3 + i];
+    if constexpr (COMOV) {
+      const double ps = (double)psi[i];
+      rho[i] = 0.5 * (exp(-2 * ps) * p * p + m2 * f * f + exp(2 * ps) * 0.25 * inv * grad);
+    } else {
+      rho[i] = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad);
+    }
+  }
+}
+
+// FP32_COMP state -> FP64 [phi | pi] (hi + lo).
+__global__ void k_export_f32(const float *__restrict__ s, double *__restrict__ out, long long n2) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride)
+    out[i] = (double)s[i] + (double)s[n2 + i];
+}
+
+// FP64 [phi | pi] -> FP32_COMP state.
+__global__ void k_import_f32(const double *__restrict__ in, float *__restrict__ s, long long n2) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
+    const double v = in[i];
+    const float h = (float)v;
+    s[i] = h;
+    s[n2 + i] = (float)(v - (double)h);
+  }
+}
+
+__global__ void k_count_nonfinite(const void *__restrict__ s, long long n, int is_f32,
+                                  unsigned long long *__restrict__ bad) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  unsigned long long local = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double v = is_f32 ? (double)((const float *)s)[i] : ((const double *)s)[i];
+    if (!isfinite(v)) ++local;
+  }
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(bad, local);
+}
+
+// ---- binning --------------------------------------------------------------
+struct SpecIn {
+  const double *f;  // HC of the field (or phi)
+  const double *g;  // HC of dphi (mode spectrum) or nullptr
+  int N;
+  double k2;   // (2 pi / L)^2
+  double m2;   // m^2
+  double a2;   // a_t^2
+};
+
+// weighted mode value of HC entry (a, b, c): weight 2 for 0 < c < N/2 (the
+// entry stands for the conjugate pair c and N - c of the full grid).
+__device__ __forceinline__ double mode_value(const SpecIn &A, long long i, int c, long long s2) {
+  const double fr = A.f[2 * i], fi = A.f[2 * i + 1];
+  double v = fr * fr + fi * fi;
+  if (A.g) {
+    const double gr = A.g[2 * i], gi = A.g[2 * i + 1];
+    v += (gr * gr + gi * gi) / (A.m2 + A.k2 * (double)s2 / A.a2);
+  }
+  return (c == 0 || 2 * c == A.N) ? v : 2.0 * v;
+}
+
+__device__ __forceinline__ void decode_mode(int N, long long i, int &c, long long &s2) {
+  const int nh = N / 2 + 1;
+  c = (int)(i % nh);
+  const long long ab = i / nh;
+  const int b = (int)(ab % N);
+  const int a = (int)(ab / N);
+  const long long as = (a <= N / 2) ? a : N - a;
+  const long long bs = (b <= N / 2) ? b : N - b;
+  s2 = as * as + bs * bs + (long long)c * c;
+}
+
+__global__ void k_spec_max(const SpecIn A, long long pairs, unsigned long long *maxbits) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+    int c;
+    long long s2;
+    decode_mode(A.N, i, c, s2);
+    m = fmax(m, mode_value(A, i, c, s2));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  // non-negative doubles order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(m));
+}
+
+// Power-of-two exponent e with (max * entries) * 2^e <= 2^126.
+__device__ __forceinline__ int fixed_exponent(unsigned long long maxbits, long long pairs) {
+  const double m = __longlong_as_double((long long)maxbits);
+  if (!(m > 0.0)) return 0;
+  int ex;
+  frexp(m * (double)pairs, &ex);  // m*pairs < 2^ex
+  return 126 - ex;
+}
+
+__global__ void k_spec_bin(const SpecIn A, long long pairs, const unsigned long long *maxbits,
+                           unsigned long long *bins) {
+  const int e = fixed_exponent(*maxbits, pairs);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+    int c;
+    long long s2;
+    decode_mode(A.N, i, c, s2);
+    const double y = ldexp(mode_value(A, i, c, s2), e);
+    const unsigned long long hi = __double2ull_rz(ldexp(y, -64));
+    const unsigned long long lo = __double2ull_rz(y - ldexp((double)hi, 64));
+    unsigned long long carry = 0;
+    if (lo) {
+      const unsigned long long old = atomicAdd(&bins[2 * s2], lo);
+      carry = (old + lo < old) ? 1ull : 0ull;
+    }
+    if (hi + carry) atomicAdd(&bins[2 * s2 + 1], hi + carry);
+  }
+}
+
+__device__ __forceinline__ double fixed_to_double(unsigned long long lo, unsigned long long hi, int e) {
+  return ldexp(ldexp(__ull2double_rn(hi), 64) + __ull2double_rn(lo), -e);
+}
+
+__global__ void k_spec_final(const unsigned long long *bins, const unsigned long long *maxbits, long long pairs,
+                             double *out, long long nb) {
+  const int e = fixed_exponent(*maxbits, pairs);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += stride)
+    out[s] = fixed_to_double(bins[2 * s], bins[2 * s + 1], e);
+}
+
+__device__ __forceinline__ long long isqrt_ll(long long s) {
+  long long r = (long long)sqrt((double)s);
+  while (r * r > s) --r;
+  while ((r + 1) * (r + 1) <= s) ++r;
+  return r;
+}
+
+__global__ void k_shells(const unsigned long long *bins, const unsigned long long *maxbits, long long pairs,
+                         const long long *s2counts, double *shells, long long *counts, long long nb, long long ns) {
+  const int e = fixed_exponent(*maxbits, pairs);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    unsigned long long lo = 0, hi = 0;
+    long long cnt = 0;
+    const long long s_end = min((i + 1) * (i + 1), nb);
+    for (long long s = i * i; s < s_end; ++s) {
+      const unsigned long long l = bins[2 * s];
+      const unsigned long long nl = lo + l;
+      hi += bins[2 * s + 1] + (nl < lo ? 1ull : 0ull);
+      lo = nl;
+      cnt += s2counts[s];
+    }
+    if (shells) shells[i] = fixed_to_double(lo, hi, e);
+    if (counts) counts[i] = cnt;
+  }
+}
+
+__global__ void k_s2_counts(int N, long long pairs, unsigned long long *counts) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+    int c;
+    long long s2;
+    decode_mode(N, i, c, s2);
+    atomicAdd(&counts[s2], (c == 0 || 2 * c == N) ? 1ull : 2ull);
+  }
+}
+
+static unsigned grid_for(long long n, int per = 256) {
+  long long b = (n + per - 1) / per;
+  if (b > 148LL * 32) b = 148LL * 32;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+int ensure_spectrum_scratch(cf_ctx *ctx, int nfields) {
+  const size_t hc = (size_t)ctx->hc_count;
+  if (!ctx->spec_hc) {
+    if (cudaMalloc(&ctx->spec_hc, 2 * hc * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc spectrum HC scratch failed");
+      return CF_ERR_NOMEM;
+    }
+    if (cudaMalloc(&ctx->spec_field, 2 * (size_t)ctx->N3 * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc spectrum field scratch failed");
+      return CF_ERR_NOMEM;
+    }
+    if (cudaMalloc(&ctx->bins, 2 * (size_t)ctx->s2_bins * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&ctx->maxbits, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&ctx->s2_counts, (size_t)ctx->s2_bins * sizeof(int64_t)) != cudaSuccess) {
+      set_error("cudaMalloc spectrum bins failed");
+      return CF_ERR_NOMEM;
+    }
+    CF_TRY_CUDA(cudaMemset(ctx->s2_counts, 0, (size_t)ctx->s2_bins * sizeof(int64_t)));
+    k_s2_counts<<<grid_for(hc / 2), 256>>>((int)ctx->N, (long long)(hc / 2), (unsigned long long *)ctx->s2_counts);
+    CF_LAUNCHED(ctx);
+    CF_TRY_CUDA(cudaMemset(ctx->bins, 0, 2 * (size_t)ctx->s2_bins * sizeof(unsigned long long)));
+    CF_TRY_CUDA(cudaMemset(ctx->maxbits, 0, sizeof(unsigned long long)));
+    CF_TRY_CUDA(cudaDeviceSynchronize());
+  }
+  const int N = (int)ctx->N;
+  if (nfields >= 1 && !ctx->have_d2z1) {
+    CF_TRY_CUFFT(cufftPlan3d(&ctx->plan_d2z1, N, N, N, CUFFT_D2Z));
+    ctx->have_d2z1 = true;
+  }
+  if (nfields >= 2 && !ctx->have_d2z2) {
+    long long n[3] = {N, N, N};
+    long long inembed[3] = {N, N, N};
+    long long onembed[3] = {N, N, N / 2 + 1};
+    size_t work = 0;
+    CF_TRY_CUFFT(cufftCreate(&ctx->plan_d2z2));
+    CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_d2z2, 3, n, inembed, 1, ctx->N3, onembed, 1, ctx->hc_count / 2,
+                                     CUFFT_D2Z, 2, &work));
+    ctx->have_d2z2 = true;
+  }
+  return CF_OK;
+}
+
+// Bins the HC data already in ctx->spec_hc (1 field, or phi/dphi for the mode spectrum).
+static int bin_spectrum(cf_ctx *ctx, bool mode, double a_t, double *d_out, cudaStream_t st) {
+  const long long pairs = ctx->hc_count / 2;
+  SpecIn A{};
+  A.f = ctx->spec_hc;
+  A.g = mode ? ctx->spec_hc + ctx->hc_count : nullptr;
+  A.N = (int)ctx->N;
+  const double kir = 2 * 3.14159265358979323846 / ctx->p.L;
+  A.k2 = kir * kir;
+  A.m2 = ctx->p.m * ctx->p.m;
+  A.a2 = a_t * a_t;
+  ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
+  CF_TRY_CUDA(cudaMemsetAsync(ctx->maxbits, 0, sizeof(unsigned long long), st));
+  CF_TRY_CUDA(cudaMemsetAsync(ctx->bins, 0, 2 * (size_t)ctx->s2_bins * sizeof(unsigned long long), st));
+  k_spec_max<<<grid_for(pairs), 256, 0, st>>>(A, pairs, ctx->maxbits);
+  CF_LAUNCHED(ctx);
+  k_spec_bin<<<grid_for(pairs), 256, 0, st>>>(A, pairs, ctx->maxbits, ctx->bins);
+  CF_LAUNCHED(ctx);
+  if (d_out) {
+    k_spec_final<<<grid_for(ctx->s2_bins), 256, 0, st>>>(ctx->bins, ctx->maxbits, pairs, d_out, ctx->s2_bins);
+    CF_LAUNCHED(ctx);
+  }
+  return CF_OK;
+}
+
+int power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, cudaStream_t st) {
+  CF_TRY(ensure_spectrum_scratch(ctx, 1));
+  CF_TRY_CUFFT(cufftSetStream(ctx->plan_d2z1, st));
+  {
+    ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
+    CF_TRY_CUFFT(cufftExecD2Z(ctx->plan_d2z1, (cufftDoubleReal *)d_f, (cufftDoubleComplex *)ctx->spec_hc));
+  }
+  return bin_spectrum(ctx, false, 1.0, d_out, st);
+}
+
+static const double *state_as_f64(cf_ctx *ctx, const void *d_state, cudaStream_t st, int *err) {
+  *err = CF_OK;
+  if (ctx->p.precision == CF_FP64) return (const double *)d_state;
+  const long long n2 = 2 * ctx->N3;
+  k_export_f32<<<grid_for(n2), 256, 0, st>>>((const float *)d_state, ctx->spec_field, n2);
+  if (cudaGetLastError() != cudaSuccess) {
+    set_error("state export launch failed");
+    *err = CF_ERR_CUDA;
+  }
+  ctx->launches++;
+  return ctx->spec_field;
+}
+
+int mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double *d_out, cudaStream_t st) {
+  CF_TRY(ensure_spectrum_scratch(ctx, 2));
+  int err;
+  const double *x = state_as_f64(ctx, d_state, st, &err);
+  CF_TRY(err);
+  CF_TRY_CUFFT(cufftSetStream(ctx->plan_d2z2, st));
+  {
+    ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
+    CF_TRY_CUFFT(cufftExecD2Z(ctx->plan_d2z2, (cufftDoubleReal *)x, (cufftDoubleComplex *)ctx->spec_hc));
+  }
+  return bin_spectrum(ctx, true, a_t, d_out, st);
+}
+
+int energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, cudaStream_t st) {
+  double inv, H;
+  stage_coeffs(ctx->p, t, &inv, &H);
+  const int N = (int)ctx->N;
+  const double m2 = ctx->p.m * ctx->p.m;
+  const long long N3 = ctx->N3;
+  const bool f32 = ctx->p.precision == CF_FP32_COMP;
+  unsigned g = grid_for(N3);
+  const void *ps = nullptr, *dps = nullptr;
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW) CF_TRY(psi_at(ctx, t, st, &ps, &dps));
+  ProfScope prof(ctx, CF_PROF_SPECTRUM, st);
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
+    if (f32)
+      k_energy<float, true><<<g, 256, 0, st>>>((const float *)d_state, (const float *)d_state + 2 * N3,
+                                               (const float *)ps, d_rho, N, m2, inv);
+    else
+      k_energy<double, true><<<g, 256, 0, st>>>((const double *)d_state, nullptr, (const double *)ps, d_rho, N,
+                                                m2, inv);
+  } else {
+    if (f32)
+      k_energy<float, false><<<g, 256, 0, st>>>((const float *)d_state, (const float *)d_state + 2 * N3, nullptr,
+                                                d_rho, N, m2, inv);
+    else
+      k_energy<double, false><<<g, 256, 0, st>>>((const double *)d_state, nullptr, nullptr, d_rho, N, m2, inv);
+  }
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+int density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d_out, cudaStream_t st) {
+  CF_TRY(ensure_spectrum_scratch(ctx, 1));
+  CF_TRY(energy_density(ctx, d_state, t, ctx->spec_field, st));
+  return power_spectrum_s2(ctx, ctx->spec_field, d_out, st);
+}
+
+int s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, cudaStream_t st) {
+  CF_TRY(ensure_spectrum_scratch(ctx, 0));
+  k_shells<<<grid_for(ctx->shells, 128), 128, 0, st>>>(ctx->bins, ctx->maxbits, ctx->hc_count / 2,
+                                                       (const long long *)ctx->s2_counts, d_shells,
+                                                       (long long *)d_counts, ctx->s2_bins, ctx->shells);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+int s2_counts(cf_ctx *ctx, int64_t *d_counts, cudaStream_t st) {
+  CF_TRY(ensure_spectrum_scratch(ctx, 0));
+  CF_TRY_CUDA(cudaMemcpyAsync(d_counts, ctx->s2_counts, (size_t)ctx->s2_bins * sizeof(int64_t),
+                              cudaMemcpyDeviceToDevice, st));
+  return CF_OK;
+}
+
+int state_export(cf_ctx *ctx, double *d_xy, const void *d_state, cudaStream_t st) {
+  const long long n2 = 2 * ctx->N3;
+  if (ctx->p.precision == CF_FP64) {
+    CF_TRY_CUDA(cudaMemcpyAsync(d_xy, d_state, n2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return CF_OK;
+  }
+  k_export_f32<<<grid_for(n2), 256, 0, st>>>((const float *)d_state, d_xy, n2);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+int state_import(cf_ctx *ctx, void *d_state, const double *d_xy, cudaStream_t st) {
+  const long long n2 = 2 * ctx->N3;
+  if (ctx->p.precision == CF_FP64) {
+    CF_TRY_CUDA(cudaMemcpyAsync(d_state, d_xy, n2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return CF_OK;
+  }
+  k_import_f32<<<grid_for(n2), 256, 0, st>>>(d_xy, (float *)d_state, n2);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+int check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, cudaStream_t st) {
+  unsigned long long *d_bad = nullptr;
+  if (cudaMallocAsync((void **)&d_bad, sizeof(unsigned long long), st) != cudaSuccess) {
+    set_error("cudaMallocAsync failed");
+    return CF_ERR_NOMEM;
+  }
+  CF_TRY_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), st));
+  const bool f32 = ctx->p.precision == CF_FP32_COMP;
+  const long long n = (f32 ? 4 : 2) * ctx->N3;
+  k_count_nonfinite<<<grid_for(n), 256, 0, st>>>(d_state, n, f32 ? 1 : 0, d_bad);
+  CF_LAUNCHED(ctx);
+  unsigned long long h = 0;
+  CF_TRY_CUDA(cudaMemcpyAsync(&h, d_bad, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CF_TRY_CUDA(cudaFreeAsync(d_bad, st));
+  CF_TRY_CUDA(cudaStreamSynchronize(st));
+  if (h_bad) *h_bad = (int64_t)h;
+  if (h) {
+    set_error("state holds %llu non-finite values", h);
+    return CF_ERR_NONFINITE;
+  }
+  return CF_OK;
+}
+
+}  // namespace cfb

@@ -1,0 +1,193 @@
+/*
+ * cfb200.h -- C ABI of the B200 lattice time-stepping library (libcfb200.so).
+ *
+ * Scope: the hot path of Cosmic-Fields-Lite -- RK4 time stepping of the
+ * Klein-Gordon family on a periodic N^3 lattice (flat, FRW, comoving-curvature
+ * coupled), the energy density, and the field / density power spectra that the
+ * observers save.  Everything runs on one CUDA device; there is no CPU fallback:
+ * every call that needs the GPU fails with CF_ERR_CUDA if none is usable.
+ *
+ * Conventions
+ *   - Every function returns int status: CF_OK (0) or a negative cf_status code;
+ *     cf_last_error() then returns a message (thread-local).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls enqueue work and return; there are no hidden device-wide syncs unless
+ *     a function says so.
+ *   - Device pointers are plain CUDA device addresses owned by the caller.
+ *   - Field layout (reference src/fdm3d.hpp:16): site (a,b,c) of an N^3 field at
+ *     N*N*a + N*b + c; a "state" in FP64 is 2N^3 doubles [phi | dphi].
+ *   - Half-complex (HC) arrays: 2*N*N*(N/2+1) doubles, mode (a,b,c<=N/2) at
+ *     2*(N*(N/2+1)*a + (N/2+1)*b + c) (real, imag) -- the FFTW/cuFFT r2c layout.
+ *   - S2 spectra: 3*(N/2)^2+1 doubles indexed by s^2 = i^2+j^2+k^2 with lattice
+ *     momenta i,j,k in -N/2+1..N/2 (reference src/fdm3d.hpp:27-40).
+ *   - Shell spectra: isqrt(3*(N/2)^2)+1 unit-width |k| shells; shell i holds the
+ *     s^2 bins in [i^2, (i+1)^2).
+ *   - Requirements: N % 8 == 0 and 8 <= N <= 2048 (the reference's own spectra
+ *     assert N % 8 == 0, src/fdm3d_cuda.cu:148,165).
+ *   - A context is not thread-safe; separate contexts are independent.
+ */
+#ifndef CFB200_H
+#define CFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFB200_ABI_VERSION 1
+
+typedef enum cf_status {
+  CF_OK = 0,
+  CF_ERR_INVALID = -1,     /* bad argument (size, alignment, enum, NULL) */
+  CF_ERR_CUDA = -2,        /* CUDA runtime error (message has the CUDA error string) */
+  CF_ERR_CUFFT = -3,       /* cuFFT error */
+  CF_ERR_NOMEM = -4,       /* device allocation failed */
+  CF_ERR_NONFINITE = -5,   /* a NaN/Inf was found in the state */
+  CF_ERR_TIMEOUT = -6,     /* a bounded device wait gave up */
+  CF_ERR_UNSUPPORTED = -7  /* combination of options not built */
+} cf_status;
+
+typedef enum cf_equation {
+  CF_EQ_KG = 0,           /* KleinGordonEquation (src/equations.hpp:36-59) */
+  CF_EQ_KG_FRW = 1,       /* KleinGordonEquationInFRW / CudaKleinGordonEquationInFRW */
+  CF_EQ_COMOVING_FRW = 2  /* ComovingCurvatureEquationInFRW / CudaComovingCurvatureEquationInFRW */
+} cf_equation;
+
+typedef enum cf_precision {
+  CF_FP64 = 0,      /* state stored and stepped in FP64 */
+  CF_FP32_COMP = 1  /* state stored as FP32 hi + FP32 compensation, arithmetic in FP64 */
+} cf_precision;
+
+/* Flat parameter block (replaces the reference's POD Param + WorkspaceGeneric
+ * field copy, src/workspace.hpp:81-93).  a1, H1, t1, p describe
+ * StaticEOSCosmology (src/physics.hpp:15-56); CF_EQ_KG ignores them. */
+typedef struct cf_params {
+  int64_t N;
+  double L;
+  double m;
+  double a1;
+  double H1;
+  double t1;
+  double p;          /* a ~ eta^p; 1 = radiation (the reference's param constructor) */
+  int32_t equation;  /* cf_equation */
+  int32_t precision; /* cf_precision */
+  int32_t stencil;   /* 7 (reference) or 13 (fourth-order Laplacian) */
+  int32_t flags;     /* reserved, 0 */
+} cf_params;
+
+typedef struct cf_ctx cf_ctx;
+
+/* Sizes a caller needs to allocate buffers. */
+typedef struct cf_info {
+  int64_t N;
+  int64_t state_bytes;  /* bytes of one device state in this context's precision */
+  int64_t field_count;  /* N^3 */
+  int64_t hc_count;     /* doubles in one HC array: 2*N*N*(N/2+1) */
+  int64_t s2_bins;      /* 3*(N/2)^2+1 */
+  int64_t shells;       /* isqrt(3*(N/2)^2)+1 */
+} cf_info;
+
+/* ---- context --------------------------------------------------------------
+ * Replaces WorkspaceGeneric's tools (FFT wrapper, Psi buffers) and the odeint
+ * stepper's temporaries: the context owns cuFFT plans and all device scratch
+ * (allocated on first use of the function that needs it). */
+int cf_create(const cf_params *params, cf_ctx **out);
+int cf_destroy(cf_ctx *ctx);
+int cf_get_info(const cf_ctx *ctx, cf_info *info);
+const char *cf_last_error(void);
+/* Number of this library's own kernels the context has launched (cuFFT calls not counted). */
+int64_t cf_launch_count(const cf_ctx *ctx);
+
+/* ---- state ----------------------------------------------------------------
+ * A device state is cf_info.state_bytes bytes, 16-byte aligned, caller owned.
+ * CF_FP64: 2N^3 doubles [phi | dphi] -- identical to the reference State
+ *   (thrust::device_vector<double>, src/equations_cuda.cuh:22-23).
+ * CF_FP32_COMP: four N^3 float planes [phi_hi | dphi_hi | phi_lo | dphi_lo]
+ *   with value = (double)hi + (double)lo. */
+int cf_state_upload(cf_ctx *ctx, void *d_state, const double *h_xy, void *stream);
+int cf_state_download(cf_ctx *ctx, double *h_xy, const void *d_state, void *stream);
+int cf_state_import(cf_ctx *ctx, void *d_state, const double *d_xy, void *stream);
+int cf_state_export(cf_ctx *ctx, double *d_xy, const void *d_state, void *stream);
+
+/* R_fft: HC array of the comoving curvature perturbation (the reference's
+ * workspace.R_fft, src/initializer.hpp:200-205), host or device pointer. */
+int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream);
+
+/* ---- the hot path -----------------------------------------------------------
+ * nsteps classic RK4 steps in place; step j runs at t = t0 + (step0 + j) * dt
+ * (integrate_const's direct time, integrate/detail/integrate_const.hpp:63) with
+ * stage times t, t+dt/2, t+dt/2, t+dt (stepper/runge_kutta4_classic.hpp:88-138).
+ * Replaces 4 x Equation::operator() + 3 x scale_sum2 + scale_sum5 per step
+ * (src/equations_cuda.cu:522-534, :678-731; src/odeint_thrust/thrust_operations.cu:238-313)
+ * by four fused stage kernels, one HBM pass each. */
+int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
+                 void *stream);
+
+/* ---- odeint building blocks (FP64 device arrays of 2N^3) --------------------
+ * cf_rhs: dxdt = Equation(x, t)  (Equation::operator(), src/equations_cuda.cu:522-534,
+ * :678-731).  cf_scale_sum: out = sum_i alpha_i * in_i over len doubles
+ * (thrust_operations::scale_sum1..14, src/odeint_thrust/thrust_operations.cuh:24-353);
+ * d_in is a HOST array of n device pointers, 1 <= n <= 14; out may alias in[0]. */
+int cf_rhs(cf_ctx *ctx, const double *d_x, double *d_dxdt, double t, void *stream);
+int cf_scale_sum(cf_ctx *ctx, double *d_out, int n, const double *const *d_in, const double *alpha,
+                 int64_t len, void *stream);
+
+/* ---- observers --------------------------------------------------------------
+ * cf_energy_density: Equation::compute_energy_density (src/equations_cuda.cu:537-553,
+ *   :733-760) of a device state at time t into d_rho (N^3 doubles).
+ * cf_power_spectrum_s2: compute_power_spectrum (src/fdm3d_cuda.cu:161-176) of an N^3
+ *   FP64 field: R2C + deterministic binning into S2 bins.
+ * cf_mode_power_spectrum_s2: compute_mode_power_spectrum (src/fdm3d_cuda.cu:144-159)
+ *   of a state: |phi_k|^2 + |dphi_k|^2/(m^2 + (2 pi/L)^2 s^2/a_t^2) per S2 bin.
+ * cf_density_spectrum_s2: energy density at t followed by cf_power_spectrum_s2 (the
+ *   observer's rho spectrum, src/observer.hpp:102-108), without a caller buffer.
+ * cf_s2_to_shells: exact regrouping of an S2 spectrum computed by this context
+ *   (most recent call) into unit shells, with mode counts; d_counts may be NULL.
+ * Sums are exact fixed-point integer sums (order independent, bit-reproducible)
+ * converted to FP64 once. */
+int cf_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, void *stream);
+int cf_power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, void *stream);
+int cf_mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double *d_out,
+                              void *stream);
+int cf_density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d_out, void *stream);
+int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stream);
+
+/* Mode multiplicity per S2 bin (exact, the rule of plot_util.py:53-58). */
+int cf_s2_counts(cf_ctx *ctx, int64_t *d_counts, void *stream);
+
+/* Scans a state for NaN/Inf; synchronises `stream` and sets *h_bad to the number
+ * of non-finite entries found (0 if clean).  Returns CF_ERR_NONFINITE if any. */
+int cf_check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, void *stream);
+
+/* ---- profiling ----------------------------------------------------------------
+ * When enabled, every kernel (or cuFFT call) the context launches is bracketed by
+ * a pair of CUDA events on its stream and its device time is accumulated per
+ * kind.  cf_profile_read synchronises on the recorded events. */
+typedef enum cf_prof_kind {
+  CF_PROF_STAGE1 = 0,  /* RK4 stage kernels 1..4 */
+  CF_PROF_STAGE2 = 1,
+  CF_PROF_STAGE3 = 2,
+  CF_PROF_STAGE4 = 3,
+  CF_PROF_PSI_TRANSFER = 4, /* Psi / dPsi transfer-function kernel */
+  CF_PROF_PSI_FFT = 5,      /* batched C2R of Psi / dPsi (cuFFT) */
+  CF_PROF_SPECTRUM = 6,     /* energy density, R2C, binning */
+  CF_PROF_OTHER = 7,
+  CF_PROF_KINDS = 8
+} cf_prof_kind;
+
+typedef struct cf_profile {
+  int64_t launches[CF_PROF_KINDS];
+  double ms[CF_PROF_KINDS];
+} cf_profile;
+
+int cf_profile_enable(cf_ctx *ctx, int on);
+int cf_profile_read(cf_ctx *ctx, cf_profile *out);
+int cf_profile_reset(cf_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFB200_H */

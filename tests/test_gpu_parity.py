@@ -1,0 +1,291 @@
+"""GPU parity: libcfb200.so (called through its C ABI) against the oracle.
+
+Tolerances (written per test): FP64 paths agree with the FP64 oracle to
+<= 1e-12 relative (fields, spectra; the stencil sums are ordered like the
+reference, so the difference is rounding of a few operations per step);
+FP32-compensated paths are compared against the FP64 oracle with the error
+budget of FP32 stage storage; mode counts are exact.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import cfb200  # noqa: E402
+from cfb200 import fields  # noqa: E402
+
+FRW = dict(a1=1.0, H1=0.5, t1=1.0)
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def make_inputs(N, L, eq, seed):
+    x = fields.initial_state(N, L, 0.5, seed)
+    x[N ** 3:] = 0.3 * fields.gaussian_field(N, L, 0.5, seed + 1)  # non-zero dphi exercises every term
+    Rf = fields.curvature_R_fft(N, L, eta_start=2.0, psi_rms=1e-2, k_max=0.5 * 2 * np.pi * 8 / L, seed=seed + 2) \
+        if eq == 2 else None
+    return x, Rf
+
+
+def ctx_for(N, L, eq, prec=cfb200.FP64, stencil=7, m=1.0):
+    cos = FRW if eq else {}
+    return cfb200.Context(N, L, m=m, equation=eq, precision=prec, stencil=stencil, **cos)
+
+
+@pytest.mark.parametrize("stencil", [7, 13])
+@pytest.mark.parametrize("eq", [0, 1, 2])
+@pytest.mark.parametrize("N", [16, 24, 40])
+def test_rhs_matches_oracle(N, eq, stencil):
+    L = 0.8 * N
+    x, Rf = make_inputs(N, L, eq, 10 + N)
+    c = ctx_for(N, L, eq, stencil=stencil)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    dx, dd = dev(x), torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
+    t = 1.37
+    c.rhs(dx, dd, t)
+    got = dd.cpu().numpy()
+    P = O.make_params(N, L, 1.0, eq=eq, stencil=stencil, **(FRW if eq else {}))
+    want = O.rhs(P, x, t, Rf)
+    assert rel(got[: N ** 3], want[: N ** 3]) <= 1e-15
+    assert rel(got[N ** 3:], want[N ** 3:]) <= 1e-13
+
+
+@pytest.mark.parametrize("stencil", [7, 13])
+@pytest.mark.parametrize("eq", [0, 1, 2])
+def test_rk4_fp64_matches_oracle(eq, stencil):
+    N, L, nsteps, dt = 32, 28.0, 12, 0.1
+    x, Rf = make_inputs(N, L, eq, 3 + eq)
+    t0 = 1.0 if eq else 0.0
+    c = ctx_for(N, L, eq, stencil=stencil)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    d = dev(x)
+    c.rk4_steps(d, t0, dt, nsteps)
+    got = d.cpu().numpy()
+    P = O.make_params(N, L, 1.0, eq=eq, stencil=stencil, **(FRW if eq else {}))
+    want = O.rk4_steps(P, x, t0, dt, nsteps, R_fft=Rf)
+    assert rel(got[: N ** 3], want[: N ** 3]) <= 1e-12
+    assert rel(got[N ** 3:], want[N ** 3:]) <= 1e-12
+
+
+@pytest.mark.parametrize("eq", [0, 1, 2])
+def test_rk4_split_calls_equal_one_call(eq):
+    """step0 offsets reproduce integrate_const's direct time t0 + step*dt."""
+    N, L, dt = 16, 16.0, 0.05
+    x, Rf = make_inputs(N, L, eq, 21)
+    t0 = 1.0 if eq else 0.0
+    c = ctx_for(N, L, eq)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    a, b = dev(x), dev(x)
+    c.rk4_steps(a, t0, dt, 10)
+    c.rk4_steps(b, t0, dt, 4)
+    c.rk4_steps(b, t0, dt, 6, step0=4)
+    assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("eq", [1, 2])
+def test_rk4_fp32_comp_error_budget(eq):
+    """FP32 hi+lo state, FP32 stage buffers, FP64 arithmetic: after 40 steps the
+    fields stay within 2e-6 (relative, norm-wise) of the FP64 oracle, and the
+    density spectrum within 1e-5."""
+    N, L, nsteps, dt = 32, 32.0, 40, 0.05
+    x, Rf = make_inputs(N, L, eq, 40 + eq)
+    c = ctx_for(N, L, eq, prec=cfb200.FP32_COMP)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    c.upload(st, x)
+    c.rk4_steps(st, 1.0, dt, nsteps)
+    got = np.empty(2 * N ** 3)
+    c.download(got, st)
+    torch.cuda.synchronize()
+    P = O.make_params(N, L, 1.0, eq=eq, **FRW)
+    want = O.rk4_steps(P, x, 1.0, dt, nsteps, R_fft=Rf)
+    assert rel(got[: N ** 3], want[: N ** 3]) <= 2e-6
+    assert rel(got[N ** 3:], want[N ** 3:]) <= 2e-6
+    t_end = 1.0 + nsteps * dt
+    spec = torch.empty(O.n_s2(N), dtype=torch.float64, device="cuda")
+    c.density_spectrum_s2(st, t_end, spec)
+    want_s = O.power_spectrum(O.energy_density(P, want, t_end, Rf))
+    assert rel(spec.cpu().numpy(), want_s) <= 1e-5
+
+
+def test_fp32_comp_state_roundtrip_is_exact_to_fp48():
+    N, L = 16, 16.0
+    x, _ = make_inputs(N, L, 1, 77)
+    c = ctx_for(N, L, 1, prec=cfb200.FP32_COMP)
+    st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    c.upload(st, x)
+    back = np.empty_like(x)
+    c.download(back, st)
+    torch.cuda.synchronize()
+    assert np.abs(back - x).max() <= 2.0 ** -46 * np.abs(x).max()
+
+
+@pytest.mark.parametrize("eq", [0, 1, 2])
+@pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
+def test_energy_density_matches_oracle(eq, prec):
+    N, L = 24, 20.0
+    x, Rf = make_inputs(N, L, eq, 55)
+    c = ctx_for(N, L, eq, prec=prec)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    c.upload(st, x)
+    rho = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
+    t = 2.5
+    c.energy_density(st, t, rho)
+    P = O.make_params(N, L, 1.0, eq=eq, **(FRW if eq else {}))
+    xs = x
+    if prec == cfb200.FP32_COMP:  # the oracle sees the same (hi+lo) state
+        xs = np.empty_like(x)
+        c.download(xs, st)
+        torch.cuda.synchronize()
+    want = O.energy_density(P, xs, t, Rf)
+    tol = 1e-13 if (prec == cfb200.FP64 or eq != 2) else 1e-7  # FP32 Psi in the coupled FP32 mode
+    assert rel(rho.cpu().numpy(), want) <= tol
+
+
+@pytest.mark.parametrize("N", [8, 16, 24, 48])
+def test_power_spectrum_s2_matches_oracle_and_reference(N):
+    L = float(N)
+    f = fields.gaussian_field(N, L, 0.7, 100 + N) ** 2  # a density-like positive field
+    c = ctx_for(N, L, 1)
+    out = torch.empty(O.n_s2(N), dtype=torch.float64, device="cuda")
+    c.power_spectrum_s2(dev(f), out)
+    got = out.cpu().numpy()
+    want = O.power_spectrum(f)
+    big = np.abs(want) >= 1e-10 * np.abs(want).max()
+    assert np.max(np.abs(got - want)[big] / np.abs(want)[big]) <= 1e-12
+    if O.ref_available():
+        assert rel(got, O.ref_power_spectrum(f)) <= 1e-12
+
+
+def test_mode_power_spectrum_matches_oracle():
+    N, L, m, a_t = 32, 25.6, 1.3, 1.7
+    x, _ = make_inputs(N, L, 1, 9)
+    c = cfb200.Context(N, L, m=m, equation=1, **FRW)
+    out = torch.empty(O.n_s2(N), dtype=torch.float64, device="cuda")
+    c.mode_power_spectrum_s2(dev(x), a_t, out)
+    want = O.mode_power_spectrum(N, L, m, a_t, x)
+    got = out.cpu().numpy()
+    big = np.abs(want) >= 1e-10 * np.abs(want).max()
+    assert np.max(np.abs(got - want)[big] / np.abs(want)[big]) <= 1e-12
+
+
+def test_spectrum_is_bit_reproducible_and_shells_are_exact():
+    N, L = 32, 32.0
+    x, _ = make_inputs(N, L, 1, 12)
+    c = ctx_for(N, L, 1)
+    d = dev(x)
+    s1 = torch.empty(O.n_s2(N), dtype=torch.float64, device="cuda")
+    s2 = torch.empty_like(s1)
+    c.density_spectrum_s2(d, 1.5, s1)
+    sh = torch.empty(O.n_shells(N), dtype=torch.float64, device="cuda")
+    cnt = torch.empty(O.n_shells(N), dtype=torch.int64, device="cuda")
+    c.s2_to_shells(sh, cnt)
+    c.density_spectrum_s2(d, 1.5, s2)
+    assert torch.equal(s1, s2)  # bit-identical: order-independent integer sums
+    want_sh, want_cnt = O.shells_from_s2(N, s1.cpu().numpy())
+    assert np.array_equal(cnt.cpu().numpy(), want_cnt)
+    assert np.max(np.abs(sh.cpu().numpy() - want_sh) / np.maximum(np.abs(want_sh), 1e-300)) <= 1e-15
+    counts = torch.empty(O.n_s2(N), dtype=torch.int64, device="cuda")
+    c.s2_counts(counts)
+    assert np.array_equal(counts.cpu().numpy(), O.s2_counts(N))
+
+
+def test_scale_sum_matches_numpy():
+    N = 16
+    c = ctx_for(N, 16.0, 1)
+    rng = np.random.default_rng(0)
+    n = 2 * N ** 3
+    ins = [rng.standard_normal(n) for _ in range(5)]
+    al = [1.0, 0.05 / 6, 0.05 / 3, 0.05 / 3, 0.05 / 6]
+    dins = [dev(v) for v in ins]
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    c.scale_sum(out, dins, al, n)
+    want = al[0] * ins[0] + al[1] * ins[1] + al[2] * ins[2] + al[3] * ins[3] + al[4] * ins[4]
+    assert np.abs(out.cpu().numpy() - want).max() <= 1e-15 * np.abs(want).max()
+
+
+def test_plain_odeint_path_equals_fused_stepper():
+    """cf_rhs + cf_scale_sum composed as runge_kutta4_classic does
+    (stepper/runge_kutta4_classic.hpp:88-138) equals the fused cf_rk4_steps."""
+    N, L, dt, t = 16, 16.0, 0.1, 1.3
+    x, _ = make_inputs(N, L, 1, 31)
+    c = ctx_for(N, L, 1)
+    n = 2 * N ** 3
+    X = dev(x)
+    k = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(4)]
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    c.rhs(X, k[0], t)
+    c.scale_sum(y, [X, k[0]], [1.0, dt / 2], n)
+    c.rhs(y, k[1], t + dt / 2)
+    c.scale_sum(y, [X, k[1]], [1.0, dt / 2], n)
+    c.rhs(y, k[2], t + dt / 2)
+    c.scale_sum(y, [X, k[2]], [1.0, dt], n)
+    c.rhs(y, k[3], t + dt)
+    c.scale_sum(X, [X] + k, [1.0, dt / 6, dt / 3, dt / 3, dt / 6], n)
+    F = dev(x)
+    c.rk4_steps(F, t, dt, 1)
+    assert rel(X.cpu().numpy(), F.cpu().numpy()) <= 1e-15
+
+
+def test_check_finite_reports_planted_nan():
+    N, L = 16, 16.0
+    x, _ = make_inputs(N, L, 1, 2)
+    x[1234] = np.nan  # planted on the host
+    c = ctx_for(N, L, 1)
+    code, bad = c.check_finite(dev(x))
+    assert code == -5 and bad == 1
+    x[1234] = 0.0
+    assert c.check_finite(dev(x)) == (0, 0)
+
+
+def test_config0_observer_run_matches_reference():
+    """Config 0 (flat KG, N=64, L=64, m=1, dt=0.1, 100 steps, spectra every
+    unit time): the GPU stepper + observers reproduce the reference's own CPU run
+    (oracle/_ref, its ConstIntervalObserver files) within 1e-12."""
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    N, L, m, dt = 64, 64.0, 1.0, 0.1
+    x = fields.initial_state(N, L, 0.5, 0)
+    final_ref, obs = O.ref_integrate(0, N, L, m, x, 0.0, 10.05, dt, t_interval=0.999, observe=True)
+    c = cfb200.Context(N, L, m=m, equation=0)
+    d = dev(x)
+    spec = torch.empty(O.n_s2(N), dtype=torch.float64, device="cuda")
+    step = 0
+    for i, t_save in enumerate(obs["t_list"]):
+        target = int(round(t_save / dt))
+        c.rk4_steps(d, 0.0, dt, target - step, step0=step)
+        step = target
+        c.mode_power_spectrum_s2(d, 1.0, spec)
+        assert rel(spec.cpu().numpy(), obs["varphi_plus"][i]) <= 1e-12
+        c.density_spectrum_s2(d, t_save, spec)
+        assert rel(spec.cpu().numpy(), obs["rho"][i]) <= 1e-12
+    assert rel(d.cpu().numpy(), final_ref) <= 1e-12
+
+
+def test_linearity_at_full_size_n256():
+    """KG-FRW is linear in the state, so one RK4 step commutes with linear
+    combinations up to rounding: step(x + 2y) = step(x) + 2 step(y).  Checked at
+    the N=256 configuration size, where the oracle is too slow to run."""
+    N, L = 256, 256.0
+    c = ctx_for(N, L, 1)
+    x = fields.initial_state(N, L, 0.25, 1, use_torch=True)
+    y = fields.initial_state(N, L, 0.25, 2, use_torch=True)
+    z = x + 2 * y
+    for s in (x, y, z):
+        c.rk4_steps(s, 1.0, 0.05, 3)
+    assert float(torch.linalg.norm(z - (x + 2 * y)) / torch.linalg.norm(z)) <= 1e-14
