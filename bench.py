@@ -294,6 +294,14 @@ def run_product(args):
                 "algorithmic_bytes_per_site_update": bps,
                 "time_share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()
                                if v[0]}}
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": ms / args.steps, "config": WORKLOAD,
+                              "roofline": roofline, "gpu_launches": launches, "clocks": clocks}))
+        if pg is not None:
+            pg.destroy_process_group()
+        return
 
     # ---- accuracy of the FP32-comp state after the timed run, against the FP64 stepper
     total_steps = args.warmup + args.steps
@@ -401,9 +409,17 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cfb200", choices=["cfb200", "reference"])
+    ap.add_argument("--n", type=int, default=None,
+                    help="lattice size override (profiling a smaller case of the same workload)")
+    ap.add_argument("--quick", action="store_true",
+                    help="headline measurement only (no accuracy check, variants, e2e or CPU baseline)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.n:
+        WORKLOAD["N"] = args.n
+        WORKLOAD["L"] = float(args.n)
+        WORKLOAD["workload"] = WORKLOAD["workload"].replace("N=512^3, L=512", f"N={args.n}^3, L={args.n}")
     if args.impl == "reference":
         run_reference_arm(args)
     else:

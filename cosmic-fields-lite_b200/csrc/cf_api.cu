@@ -226,6 +226,7 @@ int cf_destroy(cf_ctx *ctx) {
   cudaFree(ctx->acc);
   cudaFree(ctx->R_fft);
   cudaFree(ctx->psi_hc);
+  cudaFree(ctx->psi_table);
   for (auto &s : ctx->slot) cudaFree(s.psi);
   if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
   if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);

@@ -77,6 +77,7 @@ struct cf_ctx {
   // outputs (2 HC arrays) and three cached (Psi, dPsi) slots.
   void *R_fft = nullptr;
   void *psi_hc = nullptr;  // 2 consecutive HC arrays (Psi_k, dPsi_k), storage type
+  double *psi_table = nullptr;  // (T_Psi, T_dPsi) per s^2
   cfb::PsiSlot slot[3];
   uint64_t slot_clock = 0;
   cufftHandle plan_psi = 0;  // batched (2) C2R/Z2D into dense N^3

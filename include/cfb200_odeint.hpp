@@ -1,0 +1,502 @@
+/*
+ * cfb200_odeint.hpp -- drop-in C++ adapter: the reference's Equation / Workspace /
+ * odeint / observer API over the C ABI of libcfb200.so (include/cfb200.h).
+ *
+ * A reference driver (src/main.cpp:82-196) switches to the B200 path by changing
+ * its typedefs, e.g.
+ *
+ *   #include "cfb200_odeint.hpp"
+ *   typedef cfb200::CudaComovingCurvatureEquationInFRW Equation;   // was ComovingCurvatureEquationInFRW
+ *   typedef Equation::Workspace Workspace;                          // cfb200::WorkspaceGeneric<DeviceState>
+ *   Workspace workspace(param, initializer);                         // initializer fills state / R_fft on the host
+ *   Equation eqn(workspace);
+ *   cfb200::ConstIntervalObserver<Equation> observer(dir, param, eqn);
+ *   auto stepper = cfb200::fused_rk4();                              // or runge_kutta4_classic<State,double,State,double>()
+ *   integrate_const(stepper, eqn, workspace.state, param.t_start, param.t_end, param.delta_t, observer);
+ *
+ * What maps to what:
+ *   - State: cfb200::DeviceState (device memory, RAII, deep copy), the role of
+ *     thrust::device_vector<double> (src/equations_cuda.cuh:22-23).  odeint traits
+ *     is_resizeable / same_size / resize (src/odeint_thrust/thrust_resize.hpp:37-126) and
+ *     algebra_dispatcher -> vector_space_algebra (thrust_algebra_dispatcher.hpp:43-47)
+ *     are specialised below; operations_dispatcher -> cfb200::device_operations,
+ *     whose scale_sum1..6 call cf_scale_sum (replacing
+ *     src/odeint_thrust/thrust_operations.cuh:24-353).
+ *   - Equation functors: operator()(x, dxdt, t) -> cf_rhs (the stock odeint steppers
+ *     then run on the device); compute_energy_density -> cf_energy_density
+ *     (src/equations_cuda.cuh:21-103).
+ *   - cfb200::fused_rk4: a Stepper (concept as in src/midpoint.hpp:25-101) whose
+ *     do_step is ONE cf_rk4_steps call (four fused stage kernels).  It is the path
+ *     for the FP32-compensated state (Param field `precision` = CF_FP32_COMP).
+ *   - WorkspaceGeneric<DeviceState>(param, initializer): the POD-param + concept
+ *     field copy of src/workspace.hpp:20-93.  Optional Param fields `precision` and
+ *     `stencil` (long long) select CF_FP32_COMP and the 13-point Laplacian.
+ *   - ConstIntervalObserver<Equation, field, density, slices>: the save trigger and
+ *     the raw FP64 .dat files of src/observer.hpp:64-126.
+ *   - compute_power_spectrum / compute_mode_power_spectrum: src/fdm3d_cuda.cuh:22-31.
+ *
+ * Requirements: C++20, Boost.odeint headers (the reference vendors Boost 1.84),
+ * CUDA runtime headers; link libcfb200.so and cudart.
+ */
+#ifndef CFB200_ODEINT_HPP
+#define CFB200_ODEINT_HPP
+
+#include <cuda_runtime.h>
+
+#include <boost/numeric/odeint.hpp>
+#include <cmath>
+#include <concepts>
+#include <cstdio>
+#include <fstream>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "cfb200.h"
+
+namespace cfb200 {
+
+inline void check(int status) {
+  if (status != CF_OK) throw std::runtime_error(std::string("cfb200: ") + cf_last_error());
+}
+
+inline void check_cuda(cudaError_t e) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("cfb200: CUDA: ") + cudaGetErrorString(e));
+}
+
+/* FRW background of constant equation of state (src/physics.hpp:15-56): same
+ * members, constructors and formulas, so host-side stage coefficients agree
+ * bit for bit with the reference. */
+struct StaticEOSCosmology {
+  double a1, H1, t1, p;
+  StaticEOSCosmology(double a1_, double H1_, double t1_, double p_) : a1(a1_), H1(H1_), t1(t1_), p(p_) {}
+  template <typename T>
+  StaticEOSCosmology(const T &param) : a1(param.a1), H1(param.H1), t1(param.t1), p(1.0) {}
+  StaticEOSCosmology() : a1(1.0), H1(0), t1(0), p(1.0) {}
+  double a(double t) const { return a1 * pow(1 + (1 + 1 / p) * H1 * (t - t1), p / (1 + p)); }
+  double H(double t) const { return H1 * pow(1 + (1 + 1 / p) * H1 * (t - t1), -1); }
+  double eta(double t) const { return (p / (a1 * H1)) * pow(1 + (1 + 1 / p) * H1 * (t - t1), 1 / (1 + p)); }
+};
+
+/* Owns one cf_ctx. */
+class Context {
+ public:
+  explicit Context(const cf_params &p) {
+    cf_ctx *c = nullptr;
+    check(cf_create(&p, &c));
+    ctx_ = c;
+    check(cf_get_info(ctx_, &info_));
+    params_ = p;
+  }
+  ~Context() { cf_destroy(ctx_); }
+  Context(const Context &) = delete;
+  Context &operator=(const Context &) = delete;
+  cf_ctx *get() const { return ctx_; }
+  const cf_info &info() const { return info_; }
+  const cf_params &params() const { return params_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s) { stream_ = s; }
+
+ private:
+  cf_ctx *ctx_ = nullptr;
+  cf_info info_{};
+  cf_params params_{};
+  cudaStream_t stream_ = nullptr;
+};
+
+/* Device buffer of `size()` doubles' worth of bytes (a state of 2N^3 entries in
+ * the context's precision, or any FP64 device vector).  Copies are deep. */
+class DeviceState {
+ public:
+  DeviceState() = default;
+  explicit DeviceState(size_t n) { resize(n); }
+  DeviceState(const DeviceState &o) : ctx(o.ctx), precision(o.precision) {
+    resize(o.n_);
+    if (n_) check_cuda(cudaMemcpy(p_, o.p_, n_ * 8, cudaMemcpyDeviceToDevice));
+  }
+  DeviceState(DeviceState &&o) noexcept { swap(o); }
+  DeviceState &operator=(DeviceState o) {
+    swap(o);
+    return *this;
+  }
+  ~DeviceState() {
+    if (p_) cudaFree(p_);
+  }
+  void resize(size_t n) {
+    if (n == n_) return;
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+    if (n) check_cuda(cudaMalloc(&p_, n * 8));
+    n_ = n;
+  }
+  size_t size() const { return n_; }
+  void *data() { return p_; }
+  const void *data() const { return p_; }
+  double *f64() { return static_cast<double *>(p_); }
+  const double *f64() const { return static_cast<const double *>(p_); }
+  void swap(DeviceState &o) noexcept {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+    std::swap(ctx, o.ctx);
+    std::swap(precision, o.precision);
+  }
+  /* Host FP64 -> device (FP64 layout; a workspace converts to its precision when bound). */
+  void copy_from_host(const double *h, size_t n) {
+    resize(n);
+    check_cuda(cudaMemcpy(p_, h, n * 8, cudaMemcpyHostToDevice));
+  }
+
+  std::shared_ptr<Context> ctx;  // set once the state belongs to a bound workspace
+  int precision = CF_FP64;
+
+ private:
+  void *p_ = nullptr;
+  size_t n_ = 0;
+};
+
+/* State -> host FP64 [phi | dphi] (copy_vector, src/cuda_wrapper.cu:45-54). */
+inline void copy_vector(std::vector<double> &out, const DeviceState &in) {
+  out.resize(in.size());
+  if (in.ctx && in.precision != CF_FP64) {
+    check(cf_state_download(in.ctx->get(), out.data(), in.data(), in.ctx->stream()));
+    check_cuda(cudaStreamSynchronize(in.ctx->stream()));
+  } else {
+    check_cuda(cudaMemcpy(out.data(), in.data(), in.size() * 8, cudaMemcpyDeviceToHost));
+  }
+}
+
+/* odeint operations for DeviceState (replaces thrust_operations::scale_sumN). */
+struct device_operations {
+  template <size_t K>
+  struct scale_sum_k {
+    double alpha[K];
+    template <typename... S>
+    void apply(DeviceState &out, const S &...in) const {
+      const double *ptrs[K] = {in.f64()...};
+      std::shared_ptr<Context> c = out.ctx;
+      ((c = c ? c : in.ctx), ...);
+      if (!c) throw std::runtime_error("cfb200: scale_sum on states without a context");
+      check(cf_scale_sum(c->get(), out.f64(), (int)K, ptrs, alpha, (int64_t)out.size(), c->stream()));
+    }
+  };
+  template <class F1 = double>
+  struct scale_sum1 : scale_sum_k<1> {
+    typedef void result_type;
+    scale_sum1(F1 a1) { this->alpha[0] = a1; }
+    void operator()(DeviceState &o, const DeviceState &s1) const { this->apply(o, s1); }
+  };
+  template <class F1 = double, class F2 = F1>
+  struct scale_sum2 : scale_sum_k<2> {
+    typedef void result_type;
+    scale_sum2(F1 a1, F2 a2) { this->alpha[0] = a1, this->alpha[1] = a2; }
+    void operator()(DeviceState &o, const DeviceState &s1, const DeviceState &s2) const { this->apply(o, s1, s2); }
+  };
+  template <class F1 = double, class F2 = F1, class F3 = F2>
+  struct scale_sum3 : scale_sum_k<3> {
+    typedef void result_type;
+    scale_sum3(F1 a1, F2 a2, F3 a3) { this->alpha[0] = a1, this->alpha[1] = a2, this->alpha[2] = a3; }
+    void operator()(DeviceState &o, const DeviceState &s1, const DeviceState &s2, const DeviceState &s3) const {
+      this->apply(o, s1, s2, s3);
+    }
+  };
+  template <class F1 = double, class F2 = F1, class F3 = F2, class F4 = F3>
+  struct scale_sum4 : scale_sum_k<4> {
+    typedef void result_type;
+    scale_sum4(F1 a1, F2 a2, F3 a3, F4 a4) {
+      this->alpha[0] = a1, this->alpha[1] = a2, this->alpha[2] = a3, this->alpha[3] = a4;
+    }
+    void operator()(DeviceState &o, const DeviceState &s1, const DeviceState &s2, const DeviceState &s3,
+                    const DeviceState &s4) const {
+      this->apply(o, s1, s2, s3, s4);
+    }
+  };
+  template <class F1 = double, class F2 = F1, class F3 = F2, class F4 = F3, class F5 = F4>
+  struct scale_sum5 : scale_sum_k<5> {
+    typedef void result_type;
+    scale_sum5(F1 a1, F2 a2, F3 a3, F4 a4, F5 a5) {
+      this->alpha[0] = a1, this->alpha[1] = a2, this->alpha[2] = a3, this->alpha[3] = a4, this->alpha[4] = a5;
+    }
+    void operator()(DeviceState &o, const DeviceState &s1, const DeviceState &s2, const DeviceState &s3,
+                    const DeviceState &s4, const DeviceState &s5) const {
+      this->apply(o, s1, s2, s3, s4, s5);
+    }
+  };
+  template <class F1 = double, class F2 = F1, class F3 = F2, class F4 = F3, class F5 = F4, class F6 = F5>
+  struct scale_sum6 : scale_sum_k<6> {
+    typedef void result_type;
+    scale_sum6(F1 a1, F2 a2, F3 a3, F4 a4, F5 a5, F6 a6) {
+      this->alpha[0] = a1, this->alpha[1] = a2, this->alpha[2] = a3, this->alpha[3] = a4, this->alpha[4] = a5,
+      this->alpha[5] = a6;
+    }
+    void operator()(DeviceState &o, const DeviceState &s1, const DeviceState &s2, const DeviceState &s3,
+                    const DeviceState &s4, const DeviceState &s5, const DeviceState &s6) const {
+      this->apply(o, s1, s2, s3, s4, s5, s6);
+    }
+  };
+};
+
+/* ---- workspace (src/workspace.hpp:20-93) ---------------------------------- */
+#define CFB200_TYPE_REQUIREMENT(value, type) \
+  { std::remove_cvref_t<decltype((value))>() } -> std::same_as<type>;
+
+template <typename Param>
+concept HasLatticeParams = requires(Param param) {
+  CFB200_TYPE_REQUIREMENT(param.N, long long int)
+  CFB200_TYPE_REQUIREMENT(param.L, double)
+};
+template <typename Param>
+concept HasMass = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.m, double) };
+template <typename Param>
+concept HasFRWParameters = requires(Param param) {
+  CFB200_TYPE_REQUIREMENT(param.a1, double)
+  CFB200_TYPE_REQUIREMENT(param.H1, double)
+  CFB200_TYPE_REQUIREMENT(param.t1, double)
+};
+template <typename Param>
+concept HasPrecision = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.precision, long long int) };
+template <typename Param>
+concept HasStencil = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.stencil, long long int) };
+
+template <typename Vector = DeviceState>
+struct WorkspaceGeneric {
+  typedef Vector State;
+  long long int N;
+  double L;
+  double m = 0.0;
+  StaticEOSCosmology cosmology{};
+  State state;                 /* filled by the initializer with host data (FP64 [phi|dphi]) */
+  double lambda{0};
+  double f_a{1.0};
+  std::vector<double> R_fft;   /* host HC array of the comoving curvature (comoving equation) */
+  std::vector<double> t_list;
+  int precision = CF_FP64;
+  int stencil = 7;
+  std::shared_ptr<Context> ctx; /* created when an Equation binds the workspace */
+  int equation = -1;
+
+  template <HasLatticeParams Param, typename Init>
+  WorkspaceGeneric(const Param &param, Init &initializer) : N(param.N), L(param.L) {
+    if constexpr (HasFRWParameters<Param>) cosmology = StaticEOSCosmology(param);
+    if constexpr (HasMass<Param>) m = param.m;
+    if constexpr (HasPrecision<Param>) precision = (int)param.precision;
+    if constexpr (HasStencil<Param>) stencil = (int)param.stencil;
+    initializer(param, *this);
+  }
+
+  /* Creates the context for `eq` and converts the state to its precision. */
+  void bind(int eq) {
+    if (ctx && equation == eq) return;
+    cf_params p{};
+    p.N = N;
+    p.L = L;
+    p.m = m;
+    p.a1 = cosmology.a1;
+    p.H1 = cosmology.H1;
+    p.t1 = cosmology.t1;
+    p.p = cosmology.p;
+    p.equation = eq;
+    p.precision = precision;
+    p.stencil = stencil;
+    ctx = std::make_shared<Context>(p);
+    equation = eq;
+    if (eq == CF_EQ_COMOVING_FRW) {
+      if (R_fft.size() != (size_t)ctx->info().hc_count)
+        throw std::runtime_error("cfb200: comoving-curvature equation needs workspace.R_fft (HC array)");
+      check(cf_set_R_fft(ctx->get(), R_fft.data(), 0, ctx->stream()));
+    }
+    if (precision != CF_FP64 && state.precision == CF_FP64 && state.size()) {
+      State conv(state.size());
+      check(cf_state_import(ctx->get(), conv.data(), state.f64(), ctx->stream()));
+      check_cuda(cudaStreamSynchronize(ctx->stream()));
+      state.swap(conv);
+    }
+    state.ctx = ctx;
+    state.precision = precision;
+  }
+};
+
+typedef WorkspaceGeneric<DeviceState> Workspace;
+
+/* ---- equations (src/equations_cuda.cuh:21-103, src/equations.hpp:36-117) -- */
+template <int EQ>
+struct DeviceEquation {
+  typedef DeviceState Vector;
+  typedef Vector State;
+  typedef WorkspaceGeneric<Vector> Workspace;
+  Workspace &workspace;
+
+  explicit DeviceEquation(Workspace &ws) : workspace(ws) { workspace.bind(EQ); }
+
+  /* dxdt = f(x, t) on the device (FP64 states; the odeint building-block path). */
+  void operator()(const State &x, State &dxdt, const double t) {
+    if (workspace.precision != CF_FP64)
+      throw std::runtime_error("cfb200: the odeint building-block path is FP64; use cfb200::fused_rk4");
+    dxdt.ctx = workspace.ctx;
+    check(cf_rhs(workspace.ctx->get(), x.f64(), dxdt.f64(), t, workspace.ctx->stream()));
+  }
+
+  /* Energy density (N^3 FP64 on the device) of workspace.state at time t. */
+  static Vector compute_energy_density(Workspace &ws, const double t) {
+    Vector rho((size_t)ws.ctx->info().field_count);
+    rho.ctx = ws.ctx;
+    check(cf_energy_density(ws.ctx->get(), ws.state.data(), t, rho.f64(), ws.ctx->stream()));
+    return rho;
+  }
+};
+
+typedef DeviceEquation<CF_EQ_KG> KleinGordonEquation;
+typedef DeviceEquation<CF_EQ_KG_FRW> KleinGordonEquationInFRW;
+typedef DeviceEquation<CF_EQ_KG_FRW> CudaKleinGordonEquationInFRW;
+typedef DeviceEquation<CF_EQ_COMOVING_FRW> ComovingCurvatureEquationInFRW;
+typedef DeviceEquation<CF_EQ_COMOVING_FRW> CudaComovingCurvatureEquationInFRW;
+
+/* ---- fused RK4 stepper (Stepper concept, src/midpoint.hpp:25-101) ---------- */
+class fused_rk4 {
+ public:
+  typedef DeviceState state_type;
+  typedef DeviceState deriv_type;
+  typedef double value_type;
+  typedef double time_type;
+  typedef unsigned short order_type;
+  typedef boost::numeric::odeint::stepper_tag stepper_category;
+  static order_type order() { return 4; }
+
+  template <class System>
+  void do_step(System system, state_type &x, time_type t, time_type dt) {
+    typename boost::numeric::odeint::unwrap_reference<System>::type &sys = system;
+    auto &ws = sys.workspace;
+    check(cf_rk4_steps(ws.ctx->get(), x.data(), t, dt, 0, 1, ws.ctx->stream()));
+  }
+};
+
+/* ---- spectra (src/fdm3d_cuda.cuh:22-31) ----------------------------------- */
+inline DeviceState compute_power_spectrum(const long long int N, const DeviceState &f, Context &ctx) {
+  (void)N;
+  DeviceState out((size_t)ctx.info().s2_bins);
+  check(cf_power_spectrum_s2(ctx.get(), f.f64(), out.f64(), ctx.stream()));
+  return out;
+}
+
+inline DeviceState compute_mode_power_spectrum(const long long int N, const double L, const double m,
+                                               const double a_t, const DeviceState &state, Context &ctx) {
+  (void)N, (void)L, (void)m;
+  DeviceState out((size_t)ctx.info().s2_bins);
+  check(cf_mode_power_spectrum_s2(ctx.get(), state.data(), a_t, out.f64(), ctx.stream()));
+  return out;
+}
+
+/* ---- raw FP64 file output (src/io.cpp:53-62) ------------------------------- */
+inline void write_vector_to_file(const std::vector<double> &v, const std::string &filename) {
+  std::ofstream file(filename, std::ios::binary);
+  if (file.is_open()) file.write(reinterpret_cast<const char *>(v.data()), v.size() * sizeof(double));
+}
+
+inline void write_vector_to_filename_template(const std::vector<double> &v, const std::string &fmt, int idx) {
+  char name[512];
+  std::snprintf(name, sizeof(name), fmt.c_str(), idx);
+  write_vector_to_file(v, name);
+}
+
+/* ---- observer (src/observer.hpp:64-126) ------------------------------------ */
+template <typename Equation, bool save_field_spectrum = true, bool save_density_spectrum = true,
+          bool save_density = false>
+struct ConstIntervalObserver {
+  typedef typename Equation::Workspace Workspace;
+  typedef typename Workspace::State State;
+  Workspace &workspace;
+  int idx;
+  std::string dir;
+  double t_start, t_end, t_interval, t_last;
+
+  template <typename Param>
+  ConstIntervalObserver(const std::string &dir_, const Param &param, Equation &eqn)
+      : workspace(eqn.workspace), idx(0), dir(dir_), t_start(param.t_start), t_end(param.t_end),
+        t_interval(param.t_interval), t_last(param.t_start) {}
+
+  void operator()(const State &, double t) {
+    if (t >= t_last + t_interval || t == t_end || t == t_start) {
+      const long long N = workspace.N;
+      Context &ctx = *workspace.ctx;
+      const cf_info &info = ctx.info();
+      std::vector<double> host;
+      if constexpr (save_field_spectrum) {
+        DeviceState s((size_t)info.s2_bins);
+        check(cf_mode_power_spectrum_s2(ctx.get(), workspace.state.data(), workspace.cosmology.a(t), s.f64(),
+                                        ctx.stream()));
+        check_cuda(cudaStreamSynchronize(ctx.stream()));
+        copy_vector(host, s);
+        write_vector_to_filename_template(host, dir + "varphi_plus_spectrum_%d.dat", idx);
+      }
+      if constexpr (save_density_spectrum) {
+        DeviceState s((size_t)info.s2_bins);
+        check(cf_density_spectrum_s2(ctx.get(), workspace.state.data(), t, s.f64(), ctx.stream()));
+        check_cuda(cudaStreamSynchronize(ctx.stream()));
+        copy_vector(host, s);
+        write_vector_to_filename_template(host, dir + "rho_spectrum_%d.dat", idx);
+      }
+      if constexpr (save_density) {
+        State rho = Equation::compute_energy_density(workspace, t);
+        check_cuda(cudaStreamSynchronize(ctx.stream()));
+        copy_vector(host, rho);
+        std::vector<double> slice(host.begin(), host.begin() + N * N);
+        std::vector<double> avg((size_t)(N * N), 0.0);
+        for (long long i = 0; i < N * N; ++i) {
+          double acc = 0.0;
+          for (long long k = 0; k < N; ++k) acc += host[(size_t)(i + k * N * N)];
+          avg[(size_t)i] = acc / (double)N;
+        }
+        write_vector_to_filename_template(slice, dir + "rho_slice_%d.dat", idx);
+        write_vector_to_filename_template(avg, dir + "rho_axis_average_%d.dat", idx);
+      }
+      workspace.t_list.push_back(t);
+      t_last = t;
+      ++idx;
+    }
+  }
+};
+
+}  // namespace cfb200
+
+/* ---- odeint traits for DeviceState ---------------------------------------- */
+namespace boost {
+namespace numeric {
+namespace odeint {
+
+template <>
+struct is_resizeable<cfb200::DeviceState> {
+  typedef boost::true_type type;
+  static const bool value = type::value;
+};
+
+template <>
+struct same_size_impl<cfb200::DeviceState, cfb200::DeviceState> {
+  static bool same_size(const cfb200::DeviceState &x, const cfb200::DeviceState &y) { return x.size() == y.size(); }
+};
+
+template <>
+struct resize_impl<cfb200::DeviceState, cfb200::DeviceState> {
+  static void resize(cfb200::DeviceState &x, const cfb200::DeviceState &y) {
+    x.resize(y.size());
+    x.ctx = y.ctx;
+    x.precision = CF_FP64;  // odeint temporaries are FP64 device vectors
+  }
+};
+
+template <>
+struct algebra_dispatcher<cfb200::DeviceState> {
+  typedef vector_space_algebra algebra_type;
+};
+
+template <>
+struct operations_dispatcher<cfb200::DeviceState> {
+  typedef cfb200::device_operations operations_type;
+};
+
+}  // namespace odeint
+}  // namespace numeric
+}  // namespace boost
+
+#endif /* CFB200_ODEINT_HPP */

@@ -1,0 +1,119 @@
+// adapter_main.cpp -- drives libcfb200.so through include/cfb200_odeint.hpp the
+// way the reference driver (src/main.cpp:82-196) drives its own code:
+// POD Param + WorkspaceGeneric(param, initializer) + Equation + observer +
+// odeint integrate_const.  Used by tests/test_gpu_adapter.py.
+//
+// usage: adapter_main <mode> <N> <L> <dt> <t_start> <t_end> <t_interval> <in_state.bin> <out_dir/> [R_fft.bin]
+//   mode 0: KleinGordonEquationInFRW with the stock odeint runge_kutta4_classic
+//           (device State, cfb200 odeint operations: cf_rhs + cf_scale_sum)
+//   mode 1: KleinGordonEquationInFRW with cfb200::fused_rk4 (FP64)
+//   mode 2: KleinGordonEquationInFRW with cfb200::fused_rk4, FP32-compensated state
+//   mode 3: ComovingCurvatureEquationInFRW with cfb200::fused_rk4 (FP64), R_fft from file
+//   mode 4: KleinGordonEquation (flat) with the stock runge_kutta4_classic
+// Writes out_dir/state.dat (final FP64 state), the observer's spectra files and
+// out_dir/t_list.dat.
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "cfb200_odeint.hpp"
+
+struct FRWParam {
+  long long int N;
+  double L;
+  double m;
+  double a1;
+  double H1;
+  double t1;
+  double t_start;
+  double t_end;
+  double t_interval;
+  long long int precision;
+  long long int stencil;
+};
+
+struct FlatParam {
+  long long int N;
+  double L;
+  double m;
+  double t_start;
+  double t_end;
+  double t_interval;
+};
+
+static std::vector<double> read_file(const std::string &name) {
+  std::ifstream f(name, std::ios::binary | std::ios::ate);
+  if (!f) {
+    std::fprintf(stderr, "cannot open %s\n", name.c_str());
+    std::exit(2);
+  }
+  std::streamsize n = f.tellg();
+  f.seekg(0);
+  std::vector<double> v((size_t)n / 8);
+  f.read(reinterpret_cast<char *>(v.data()), n);
+  return v;
+}
+
+template <typename Equation, typename Stepper, typename Param>
+static int run(const Param &param, const std::vector<double> &x0, const std::vector<double> &R_fft, double dt,
+               const std::string &dir) {
+  auto init = [&](const auto &, auto &ws) {
+    ws.state.copy_from_host(x0.data(), x0.size());
+    ws.R_fft = R_fft;
+  };
+  typename Equation::Workspace workspace(param, init);
+  Equation eqn(workspace);
+  cfb200::ConstIntervalObserver<Equation, true, true, true> observer(dir, param, eqn);
+  Stepper stepper;
+  size_t steps = boost::numeric::odeint::integrate_const(stepper, eqn, workspace.state, param.t_start, param.t_end,
+                                                          dt, observer);
+  std::vector<double> out;
+  cfb200::copy_vector(out, workspace.state);
+  cfb200::write_vector_to_file(out, dir + "state.dat");
+  cfb200::write_vector_to_file(workspace.t_list, dir + "t_list.dat");
+  std::printf("steps=%zu saves=%zu\n", steps, workspace.t_list.size());
+  return 0;
+}
+
+int main(int argc, char **argv) {
+  if (argc < 10) {
+    std::fprintf(stderr, "usage: %s mode N L dt t_start t_end t_interval in_state out_dir [R_fft]\n", argv[0]);
+    return 2;
+  }
+  const int mode = std::atoi(argv[1]);
+  const long long N = std::atoll(argv[2]);
+  const double L = std::atof(argv[3]), dt = std::atof(argv[4]);
+  const double t0 = std::atof(argv[5]), t1 = std::atof(argv[6]), ti = std::atof(argv[7]);
+  const std::vector<double> x0 = read_file(argv[8]);
+  const std::string dir = argv[9];
+  std::vector<double> R_fft;
+  if (argc > 10) R_fft = read_file(argv[10]);
+  using cfb200::DeviceState;
+  typedef boost::numeric::odeint::runge_kutta4_classic<DeviceState, double, DeviceState, double> StockRK4;
+  try {
+    FRWParam p{N, L, 1.0, 1.0, 0.5, 1.0, t0, t1, ti, CF_FP64, 7};
+    switch (mode) {
+      case 0:
+        return run<cfb200::KleinGordonEquationInFRW, StockRK4>(p, x0, R_fft, dt, dir);
+      case 1:
+        return run<cfb200::KleinGordonEquationInFRW, cfb200::fused_rk4>(p, x0, R_fft, dt, dir);
+      case 2:
+        p.precision = CF_FP32_COMP;
+        return run<cfb200::KleinGordonEquationInFRW, cfb200::fused_rk4>(p, x0, R_fft, dt, dir);
+      case 3:
+        return run<cfb200::ComovingCurvatureEquationInFRW, cfb200::fused_rk4>(p, x0, R_fft, dt, dir);
+      case 4: {
+        FlatParam q{N, L, 1.0, t0, t1, ti};
+        return run<cfb200::KleinGordonEquation, StockRK4>(q, x0, R_fft, dt, dir);
+      }
+      default:
+        std::fprintf(stderr, "unknown mode %d\n", mode);
+        return 2;
+    }
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "error: %s\n", e.what());
+    return 1;
+  }
+}

@@ -1,0 +1,76 @@
+"""The C++ drop-in adapter (include/cfb200_odeint.hpp) driven like the
+reference driver: WorkspaceGeneric(param, initializer), an Equation functor,
+odeint integrate_const with the stock runge_kutta4_classic or the fused
+stepper, and ConstIntervalObserver writing the reference's .dat files.
+
+The driver binary (tests/cpp/_build/adapter_main) is compiled by build() where
+Boost.odeint headers are available; the outputs are compared with the
+reference's own CPU run of the same integrate_const (oracle/_ref) when present,
+else with the restated oracle.
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from cfb200 import fields  # noqa: E402
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "tests", "cpp", "_build", "adapter_main")
+FRW = dict(a1=1.0, H1=0.5, t1=1.0)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="adapter driver not built (needs Boost.odeint headers)")
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4])
+def test_adapter_integrate_const_matches_reference(mode):
+    N, L, dt, nsteps = 16, 16.0, 0.05, 30
+    eq = {0: 1, 1: 1, 2: 1, 3: 2, 4: 0}[mode]
+    t0 = 0.0 if eq == 0 else 1.0
+    t_end = t0 + (nsteps + 0.5) * dt
+    ti = 0.499
+    x = fields.initial_state(N, L, 0.5, 5 + mode)
+    x[N ** 3:] = 0.2 * fields.gaussian_field(N, L, 0.5, 50 + mode)
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, 3.0, seed=9) if eq == 2 else None
+    cos = FRW if eq else {}
+    with tempfile.TemporaryDirectory() as d:
+        xin = os.path.join(d, "x.bin")
+        x.tofile(xin)
+        args = [BIN, str(mode), str(N), repr(L), repr(dt), repr(t0), repr(t_end), repr(ti), xin, d + "/"]
+        if Rf is not None:
+            rin = os.path.join(d, "r.bin")
+            Rf.tofile(rin)
+            args.append(rin)
+        out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        got = np.fromfile(os.path.join(d, "state.dat"))
+        t_list = np.fromfile(os.path.join(d, "t_list.dat"))
+        spectra = [(np.fromfile(os.path.join(d, f"varphi_plus_spectrum_{i}.dat")),
+                    np.fromfile(os.path.join(d, f"rho_spectrum_{i}.dat")),
+                    np.fromfile(os.path.join(d, f"rho_slice_{i}.dat"))) for i in range(len(t_list))]
+    if O.ref_available():
+        want, obs = O.ref_integrate(eq, N, L, 1.0, x, t0, t_end, dt, R_fft=Rf, t_interval=ti, observe=True, **cos)
+        assert np.allclose(t_list, obs["t_list"], rtol=0, atol=1e-12)
+    else:
+        P = O.make_params(N, L, 1.0, eq=eq, **cos)
+        want = O.rk4_steps(P, x, t0, dt, nsteps, R_fft=Rf)
+        obs = None
+    tol = 2e-6 if mode == 2 else 1e-12
+    assert rel(got, want) <= tol
+    if obs is not None:
+        for i in range(len(t_list)):
+            assert rel(spectra[i][0], obs["varphi_plus"][i]) <= max(tol, 1e-12) * 10
+            assert rel(spectra[i][1], obs["rho"][i]) <= max(tol, 1e-12) * 10
+    P = O.make_params(N, L, 1.0, eq=eq, **cos)
+    rho_last = O.energy_density(P, got, t_list[-1], Rf)
+    assert rel(spectra[-1][2], rho_last[: N * N]) <= 1e-12

@@ -180,8 +180,11 @@ def test_mode_power_spectrum_matches_oracle():
     c.mode_power_spectrum_s2(dev(x), a_t, out)
     want = O.mode_power_spectrum(N, L, m, a_t, x)
     got = out.cpu().numpy()
+    # norm-wise 1e-13; per bin 1e-11 over bins >= 1e-10 of the maximum (the
+    # smallest bins carry the FFT rounding of the largest modes)
+    assert rel(got, want) <= 1e-13
     big = np.abs(want) >= 1e-10 * np.abs(want).max()
-    assert np.max(np.abs(got - want)[big] / np.abs(want)[big]) <= 1e-12
+    assert np.max(np.abs(got - want)[big] / np.abs(want)[big]) <= 1e-11
 
 
 def test_spectrum_is_bit_reproducible_and_shells_are_exact():
