@@ -72,6 +72,14 @@ _SIGS = {
     "cf_s2_to_shells": ([_vp, _vp, _vp, _vp], _i),
     "cf_s2_counts": ([_vp, _vp, _vp], _i),
     "cf_check_finite": ([_vp, _vp, ctypes.POINTER(_i64), _vp], _i),
+    "cf_adjoint_create": ([_vp, _i64, _i64, ctypes.POINTER(_vp)], _i),
+    "cf_adjoint_destroy": ([_vp], _i),
+    "cf_adjoint_forward": ([_vp, _vp, _d, _d, _vp], _i),
+    "cf_adjoint_shell_log_loss": ([_vp, _vp, _vp, ctypes.POINTER(_d), _vp], _i),
+    "cf_adjoint_set_lambda": ([_vp, _vp, _d, _vp], _i),
+    "cf_adjoint_backward": ([_vp, _vp, ctypes.POINTER(_d), _vp], _i),
+    "cf_field_from_shell_amplitudes": ([_vp, _vp, _vp, _vp, _i, _i, _vp, _vp], _i),
+    "cf_shell_amplitude_gradient": ([_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp], _i),
     "cf_profile_enable": ([_vp, _i], _i),
     "cf_profile_read": ([_vp, _vp], _i),
     "cf_profile_reset": ([_vp], _i),
@@ -241,6 +249,61 @@ class Context:
         bad = _i64(0)
         code = lib().cf_check_finite(self.h, _ptr(d_state), ctypes.byref(bad), _stream(stream))
         return code, int(bad.value)
+
+
+class Adjoint:
+    """cf_adjoint: checkpointed forward run, shell-spectrum log loss, reverse sweep."""
+
+    def __init__(self, ctx, nsteps, checkpoint_every):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        check(lib().cf_adjoint_create(ctx.h, int(nsteps), int(checkpoint_every), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cf_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, d_state, t0, dt, stream=None):
+        check(lib().cf_adjoint_forward(self.h, _ptr(d_state), float(t0), float(dt), _stream(stream)))
+
+    def shell_log_loss(self, d_state, target_shells, stream=None):
+        import numpy as np
+        tgt = np.ascontiguousarray(target_shells, dtype=np.float64)
+        loss = _d(0.0)
+        check(lib().cf_adjoint_shell_log_loss(self.h, _ptr(d_state), _ptr(tgt), ctypes.byref(loss), _stream(stream)))
+        return float(loss.value)
+
+    def set_lambda(self, d_lambda, dm_direct=0.0, stream=None):
+        check(lib().cf_adjoint_set_lambda(self.h, _ptr(d_lambda), float(dm_direct), _stream(stream)))
+
+    def backward(self, d_lambda0=None, stream=None):
+        dm = _d(0.0)
+        check(lib().cf_adjoint_backward(self.h, _ptr(d_lambda0), ctypes.byref(dm), _stream(stream)))
+        return float(dm.value)
+
+
+def field_from_shell_amplitudes(ctx, d_xi, d_sqrtP, theta, shells_per_group, d_phi, stream=None):
+    import numpy as np
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    check(lib().cf_field_from_shell_amplitudes(ctx.h, _ptr(d_xi), _ptr(d_sqrtP), _ptr(th), th.size,
+                                               int(shells_per_group), _ptr(d_phi), _stream(stream)))
+
+
+def shell_amplitude_gradient(ctx, d_lambda_phi, d_xi, d_sqrtP, theta, shells_per_group, stream=None):
+    import numpy as np
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    g = np.empty_like(th)
+    check(lib().cf_shell_amplitude_gradient(ctx.h, _ptr(d_lambda_phi), _ptr(d_xi), _ptr(d_sqrtP), _ptr(th), th.size,
+                                            int(shells_per_group), _ptr(g), _stream(stream)))
+    return g
 
 
 def a_of_t(a1, H1, t1, t, p=1.0):

@@ -70,6 +70,24 @@ def initial_state(N, L, k_star, seed, use_torch=False):
     return np.concatenate([phi, np.zeros_like(phi)])
 
 
+def white_noise_hc(N, seed):
+    """xi = r2c(w / N^3) of seeded white noise w (the first two steps of the
+    reference GRF, src/random_field.cpp:36-56), as an HC float64 array."""
+    w = np.random.default_rng(seed).standard_normal((N, N, N)) / N ** 3
+    return np.ascontiguousarray(np.fft.rfftn(w)).view(np.float64).ravel()
+
+
+def gaussian_sqrtP_by_s2(N, L, k_star):
+    """sqrt(P(k)) tabulated by s^2 = i^2+j^2+k^2 for the Gaussian spectrum of
+    gaussian_field (P(0) = 0, <phi^2> = 1): c2r(sqrtP * xi) is that field."""
+    A = gaussian_spectrum_amplitude(N, L, k_star)
+    s2 = np.arange(3 * (N // 2) ** 2 + 1, dtype=np.float64)
+    k2 = s2 * (2 * np.pi / L) ** 2
+    P = A * np.exp(-k2 / (2 * k_star ** 2))
+    P[0] = 0.0
+    return np.sqrt(P)
+
+
 def transfer_psi(x):
     """Psi_k / R_k at x = k eta / sqrt(3): 2 (sin x - x cos x) / x^3
     (src/equations.cpp:141-183 without the 1/N^3 of the unnormalised c2r)."""

@@ -73,6 +73,17 @@ int s2_counts(cf_ctx *, int64_t *, cudaStream_t);
 int state_export(cf_ctx *, double *, const void *, cudaStream_t);
 int state_import(cf_ctx *, void *, const double *, cudaStream_t);
 int check_finite(cf_ctx *, const void *, int64_t *, cudaStream_t);
+int adjoint_create(cf_ctx *, int64_t, int64_t, cf_adjoint **);
+void adjoint_destroy(cf_adjoint *);
+int adjoint_forward(cf_adjoint *, void *, double, double, cudaStream_t);
+int adjoint_shell_log_loss(cf_adjoint *, const void *, const double *, double *, cudaStream_t);
+int adjoint_set_lambda(cf_adjoint *, const double *, double, cudaStream_t);
+int adjoint_backward(cf_adjoint *, double *, double *, cudaStream_t);
+cf_ctx *adjoint_ctx(cf_adjoint *);
+int field_from_shell_amplitudes(cf_ctx *, const double *, const double *, const double *, int, int, double *,
+                                cudaStream_t);
+int shell_amplitude_gradient(cf_ctx *, const double *, const double *, const double *, const double *, int, int,
+                             double *, cudaStream_t);
 
 ProfScope::ProfScope(cf_ctx *c, int k, cudaStream_t s) : ctx(c), kind(k), st(s) {
   if (!ctx->prof_on) return;
@@ -426,6 +437,111 @@ int cf_s2_counts(cf_ctx *ctx, int64_t *d_counts, void *stream) {
   CF_TRY(check_ptr(d_counts, "d_counts", 8));
   CF_TRY(use_device(ctx));
   return s2_counts(ctx, d_counts, (cudaStream_t)stream);
+}
+
+int cf_adjoint_create(cf_ctx *ctx, int64_t nsteps, int64_t checkpoint_every, cf_adjoint **out) {
+  CF_TRY(check_ctx(ctx));
+  if (!out) {
+    set_error("out is NULL");
+    return CF_ERR_INVALID;
+  }
+  *out = nullptr;
+  CF_TRY(use_device(ctx));
+  cf_adjoint *a = nullptr;
+  int s = adjoint_create(ctx, nsteps, checkpoint_every, &a);
+  if (s != CF_OK) {
+    adjoint_destroy(a);
+    return s;
+  }
+  *out = a;
+  return CF_OK;
+}
+
+int cf_adjoint_destroy(cf_adjoint *adj) {
+  adjoint_destroy(adj);
+  return CF_OK;
+}
+
+int cf_adjoint_forward(cf_adjoint *adj, void *d_state, double t0, double dt, void *stream) {
+  if (!adj) {
+    set_error("NULL adjoint");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(use_device(adjoint_ctx(adj)));
+  return adjoint_forward(adj, d_state, t0, dt, (cudaStream_t)stream);
+}
+
+int cf_adjoint_shell_log_loss(cf_adjoint *adj, const void *d_state, const double *h_target_shells, double *h_loss,
+                              void *stream) {
+  if (!adj || !h_target_shells) {
+    set_error("NULL adjoint or target");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(use_device(adjoint_ctx(adj)));
+  return adjoint_shell_log_loss(adj, d_state, h_target_shells, h_loss, (cudaStream_t)stream);
+}
+
+int cf_adjoint_set_lambda(cf_adjoint *adj, const double *d_lambda, double dL_dm_direct, void *stream) {
+  if (!adj) {
+    set_error("NULL adjoint");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(check_ptr(d_lambda, "d_lambda"));
+  CF_TRY(use_device(adjoint_ctx(adj)));
+  return adjoint_set_lambda(adj, d_lambda, dL_dm_direct, (cudaStream_t)stream);
+}
+
+int cf_adjoint_backward(cf_adjoint *adj, double *d_lambda0, double *h_dL_dm, void *stream) {
+  if (!adj) {
+    set_error("NULL adjoint");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(adjoint_ctx(adj)));
+  return adjoint_backward(adj, d_lambda0, h_dL_dm, (cudaStream_t)stream);
+}
+
+int cf_field_from_shell_amplitudes(cf_ctx *ctx, const double *d_xi_hc, const double *d_sqrtP_s2,
+                                   const double *h_theta, int ngroups, int shells_per_group, double *d_phi,
+                                   void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_xi_hc, "d_xi_hc", 8));
+  CF_TRY(check_ptr(d_sqrtP_s2, "d_sqrtP_s2", 8));
+  CF_TRY(check_ptr(d_phi, "d_phi", 8));
+  if (!h_theta || ngroups < 1 || ngroups > 1024 || shells_per_group < 1) {
+    set_error("need theta, 1 <= ngroups <= 1024, shells_per_group >= 1");
+    return CF_ERR_INVALID;
+  }
+  for (int g = 0; g < ngroups; ++g)
+    if (!(h_theta[g] >= 0)) {
+      set_error("theta must be non-negative");
+      return CF_ERR_INVALID;
+    }
+  CF_TRY(use_device(ctx));
+  return field_from_shell_amplitudes(ctx, d_xi_hc, d_sqrtP_s2, h_theta, ngroups, shells_per_group, d_phi,
+                                     (cudaStream_t)stream);
+}
+
+int cf_shell_amplitude_gradient(cf_ctx *ctx, const double *d_lambda_phi, const double *d_xi_hc,
+                                const double *d_sqrtP_s2, const double *h_theta, int ngroups, int shells_per_group,
+                                double *h_grad, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_lambda_phi, "d_lambda_phi", 8));
+  CF_TRY(check_ptr(d_xi_hc, "d_xi_hc", 8));
+  CF_TRY(check_ptr(d_sqrtP_s2, "d_sqrtP_s2", 8));
+  if (!h_theta || !h_grad || ngroups < 1 || ngroups > 1024 || shells_per_group < 1) {
+    set_error("need theta, grad, 1 <= ngroups <= 1024, shells_per_group >= 1");
+    return CF_ERR_INVALID;
+  }
+  for (int g = 0; g < ngroups; ++g)
+    if (!(h_theta[g] > 0)) {
+      set_error("theta must be positive for the gradient");
+      return CF_ERR_INVALID;
+    }
+  CF_TRY(use_device(ctx));
+  return shell_amplitude_gradient(ctx, d_lambda_phi, d_xi_hc, d_sqrtP_s2, h_theta, ngroups, shells_per_group, h_grad,
+                                  (cudaStream_t)stream);
 }
 
 int cf_profile_enable(cf_ctx *ctx, int on) {

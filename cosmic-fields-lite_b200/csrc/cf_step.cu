@@ -400,6 +400,37 @@ static int rk4_steps_t(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t
   return CF_OK;
 }
 
+// One forward stage (1..3) with explicit buffers: the adjoint's recompute of
+// the stage inputs y2, y3, y4 of a step (same kernels as rk4_steps, so the
+// recomputed values are bit-identical to the forward sweep).
+template <typename S>
+static int forward_stage_t(cf_ctx *ctx, int stage, const void *yin, void *yout, void *x, void *xlo, double t,
+                           double cy, double dt6, cudaStream_t st) {
+  CF_TRY(ensure_rk4_scratch(ctx));
+  StageArgs<S> A{};
+  A.N = (int)ctx->N;
+  A.N3 = ctx->N3;
+  A.m2 = ctx->p.m * ctx->p.m;
+  A.x = (S *)x;
+  A.xlo = (S *)xlo;
+  A.acc = (S *)ctx->acc;
+  A.dt6 = dt6;
+  CF_TRY(fill_stage_coeffs(ctx, A, t, st));
+  A.yin = (const S *)yin;
+  A.yout = (S *)yout;
+  A.cy = cy;
+  if (stage == 1) return launch_stage<S, 1>(ctx, A, st);
+  if (stage == 2) return launch_stage<S, 2>(ctx, A, st);
+  if (stage == 3) return launch_stage<S, 3>(ctx, A, st);
+  return launch_stage<S, 4>(ctx, A, st);
+}
+
+int launch_forward_stage(cf_ctx *ctx, int stage, const void *yin, void *yout, void *x, void *xlo, double t, double cy,
+                         double dt6, cudaStream_t st) {
+  if (ctx->p.precision == CF_FP32_COMP) return forward_stage_t<float>(ctx, stage, yin, yout, x, xlo, t, cy, dt6, st);
+  return forward_stage_t<double>(ctx, stage, yin, yout, x, xlo, t, cy, dt6, st);
+}
+
 int rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, cudaStream_t st) {
   if (ctx->p.precision == CF_FP32_COMP) return rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st);
   return rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);

@@ -161,6 +161,39 @@ int cf_s2_counts(cf_ctx *ctx, int64_t *d_counts, void *stream);
  * of non-finite entries found (0 if clean).  Returns CF_ERR_NONFINITE if any. */
 int cf_check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, void *stream);
 
+/* ---- adjoint (gradients of a spectrum loss) -------------------------------------
+ * Discrete adjoint of cf_rk4_steps for CF_EQ_KG / CF_EQ_KG_FRW (7- or 13-point,
+ * either precision; adjoint variables are FP64).  No reference counterpart: the
+ * reference has no differentiation.
+ *   cf_adjoint_create: checkpoints every `checkpoint_every` of `nsteps` steps.
+ *   cf_adjoint_forward: runs the nsteps from d_state (in: x0, out: x_T), t_j = t0 + j dt,
+ *     storing checkpoints.
+ *   cf_adjoint_shell_log_loss: L = sum_s (log P_s - log T_s)^2 over unit shells s with
+ *     P_s, T_s > 0, where P_s is the shell density spectrum of x_T at t_T (as
+ *     cf_density_spectrum_s2 + cf_s2_to_shells); sets dL/dx_T as the adjoint seed.
+ *   cf_adjoint_set_lambda: sets the seed dL/dx_T (FP64 2N^3, device) directly, with the
+ *     part of dL/dm not carried by the state.
+ *   cf_adjoint_backward: reverse sweep (recomputing each segment from its checkpoint):
+ *     dL/dx_0 -> d_lambda0 (FP64 2N^3, device; may be NULL), dL/dm -> *h_dL_dm.
+ * Initial-field parameterisation by shell groups (group g holds unit shells
+ * [g*spg, (g+1)*spg), the last group everything beyond):
+ *   phi0 = c2r(sqrt(theta_g(k)) sqrtP(s^2) xi_k), xi an HC array, sqrtP indexed by s^2;
+ *   cf_shell_amplitude_gradient: dL/dtheta_g from dL/dphi0 (N^3 device, FP64). */
+typedef struct cf_adjoint cf_adjoint;
+int cf_adjoint_create(cf_ctx *ctx, int64_t nsteps, int64_t checkpoint_every, cf_adjoint **out);
+int cf_adjoint_destroy(cf_adjoint *adj);
+int cf_adjoint_forward(cf_adjoint *adj, void *d_state, double t0, double dt, void *stream);
+int cf_adjoint_shell_log_loss(cf_adjoint *adj, const void *d_state, const double *h_target_shells,
+                              double *h_loss, void *stream);
+int cf_adjoint_set_lambda(cf_adjoint *adj, const double *d_lambda, double dL_dm_direct, void *stream);
+int cf_adjoint_backward(cf_adjoint *adj, double *d_lambda0, double *h_dL_dm, void *stream);
+int cf_field_from_shell_amplitudes(cf_ctx *ctx, const double *d_xi_hc, const double *d_sqrtP_s2,
+                                   const double *h_theta, int ngroups, int shells_per_group, double *d_phi,
+                                   void *stream);
+int cf_shell_amplitude_gradient(cf_ctx *ctx, const double *d_lambda_phi, const double *d_xi_hc,
+                                const double *d_sqrtP_s2, const double *h_theta, int ngroups,
+                                int shells_per_group, double *h_grad, void *stream);
+
 /* ---- profiling ----------------------------------------------------------------
  * When enabled, every kernel (or cuFFT call) the context launches is bracketed by
  * a pair of CUDA events on its stream and its device time is accumulated per
