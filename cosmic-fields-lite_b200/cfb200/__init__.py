@@ -75,11 +75,21 @@ _SIGS = {
     "cf_adjoint_create": ([_vp, _i64, _i64, ctypes.POINTER(_vp)], _i),
     "cf_adjoint_destroy": ([_vp], _i),
     "cf_adjoint_forward": ([_vp, _vp, _d, _d, _vp], _i),
-    "cf_adjoint_shell_log_loss": ([_vp, _vp, _vp, ctypes.POINTER(_d), _vp], _i),
+    "cf_adjoint_shell_log_loss": ([_vp, _vp, _vp, _d, ctypes.POINTER(_d), _vp], _i),
     "cf_adjoint_set_lambda": ([_vp, _vp, _d, _vp], _i),
     "cf_adjoint_backward": ([_vp, _vp, ctypes.POINTER(_d), _vp], _i),
     "cf_field_from_shell_amplitudes": ([_vp, _vp, _vp, _vp, _i, _i, _vp, _vp], _i),
     "cf_shell_amplitude_gradient": ([_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp], _i),
+    "cf_ensemble_create": ([_vp, _i, ctypes.POINTER(_vp)], _i),
+    "cf_ensemble_destroy": ([_vp], _i),
+    "cf_ensemble_info": ([_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i),
+    "cf_ensemble_launch_count": ([_vp], _i64),
+    "cf_ensemble_state_upload": ([_vp, _i, _vp, _vp], _i),
+    "cf_ensemble_state_download": ([_vp, _i, _vp, _vp], _i),
+    "cf_ensemble_rk4_steps": ([_vp, _d, _d, _i64, _i64, _i, _vp], _i),
+    "cf_ensemble_density_spectra_s2": ([_vp, _d, _vp, _vp], _i),
+    "cf_ensemble_run_graph": ([_vp, _d, _d, _i64, _i64, _vp, _vp], _i),
+    "cf_ensemble_autotune": ([_vp, _d, _d, _i64, _vp, ctypes.POINTER(_i), ctypes.POINTER(_i)], _i),
     "cf_profile_enable": ([_vp, _i], _i),
     "cf_profile_read": ([_vp, _vp], _i),
     "cf_profile_reset": ([_vp], _i),
@@ -274,11 +284,12 @@ class Adjoint:
     def forward(self, d_state, t0, dt, stream=None):
         check(lib().cf_adjoint_forward(self.h, _ptr(d_state), float(t0), float(dt), _stream(stream)))
 
-    def shell_log_loss(self, d_state, target_shells, stream=None):
+    def shell_log_loss(self, d_state, target_shells, rel_floor=0.0, stream=None):
         import numpy as np
         tgt = np.ascontiguousarray(target_shells, dtype=np.float64)
         loss = _d(0.0)
-        check(lib().cf_adjoint_shell_log_loss(self.h, _ptr(d_state), _ptr(tgt), ctypes.byref(loss), _stream(stream)))
+        check(lib().cf_adjoint_shell_log_loss(self.h, _ptr(d_state), _ptr(tgt), float(rel_floor), ctypes.byref(loss),
+                                              _stream(stream)))
         return float(loss.value)
 
     def set_lambda(self, d_lambda, dm_direct=0.0, stream=None):
@@ -288,6 +299,74 @@ class Adjoint:
         dm = _d(0.0)
         check(lib().cf_adjoint_backward(self.h, _ptr(d_lambda0), ctypes.byref(dm), _stream(stream)))
         return float(dm.value)
+
+
+ENS_PERSISTENT, ENS_BATCHED, ENS_LOOP = 0, 1, 2
+
+
+class Ensemble:
+    """cf_ensemble: lattices of uneven N stepped together (one work list)."""
+
+    def __init__(self, members):
+        """members: list of dicts with N, L, m and the shared equation, precision,
+        stencil, a1, H1, t1, p."""
+        arr = (cf_params * len(members))()
+        for i, d in enumerate(members):
+            arr[i] = cf_params(int(d["N"]), float(d["L"]), float(d.get("m", 1.0)), float(d.get("a1", 1.0)),
+                               float(d.get("H1", 0.0)), float(d.get("t1", 0.0)), float(d.get("p", 1.0)),
+                               int(d.get("equation", EQ_KG_FRW)), int(d.get("precision", FP64)),
+                               int(d.get("stencil", 7)), 0)
+        self.members = members
+        h = ctypes.c_void_p()
+        check(lib().cf_ensemble_create(ctypes.cast(arr, ctypes.c_void_p), len(members), ctypes.byref(h)))
+        self.h = h
+        tot, items = _i64(0), _i64(0)
+        check(lib().cf_ensemble_info(self.h, ctypes.byref(tot), ctypes.byref(items)))
+        self.spectra_total = int(tot.value)
+        self.work_items = int(items.value)
+        self.offsets = []
+        off = 0
+        for d in members:
+            self.offsets.append(off)
+            off += 3 * (int(d["N"]) // 2) ** 2 + 1
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cf_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self):
+        return int(lib().cf_ensemble_launch_count(self.h))
+
+    def upload(self, member, h_xy, stream=None):
+        check(lib().cf_ensemble_state_upload(self.h, int(member), _ptr(h_xy), _stream(stream)))
+
+    def download(self, member, h_xy, stream=None):
+        check(lib().cf_ensemble_state_download(self.h, int(member), _ptr(h_xy), _stream(stream)))
+
+    def rk4_steps(self, t0, dt, nsteps, step0=0, mode=ENS_PERSISTENT, stream=None):
+        check(lib().cf_ensemble_rk4_steps(self.h, float(t0), float(dt), int(step0), int(nsteps), int(mode),
+                                          _stream(stream)))
+
+    def density_spectra_s2(self, t, d_out, stream=None):
+        check(lib().cf_ensemble_density_spectra_s2(self.h, float(t), _ptr(d_out), _stream(stream)))
+
+    def run_graph(self, t0, dt, steps_per_segment, nsegments, d_spectra=None, stream=None):
+        check(lib().cf_ensemble_run_graph(self.h, float(t0), float(dt), int(steps_per_segment), int(nsegments),
+                                          _ptr(d_spectra), _stream(stream)))
+
+    def autotune(self, t0, dt, steps=2, stream=None):
+        shape, chunk = _i(0), _i(0)
+        check(lib().cf_ensemble_autotune(self.h, float(t0), float(dt), int(steps), _stream(stream),
+                                         ctypes.byref(shape), ctypes.byref(chunk)))
+        return int(shape.value), int(chunk.value)
 
 
 def field_from_shell_amplitudes(ctx, d_xi, d_sqrtP, theta, shells_per_group, d_phi, stream=None):

@@ -432,8 +432,8 @@ int adjoint_forward(cf_adjoint *a, void *d_state, double t0, double dt, cudaStre
   return CF_OK;
 }
 
-int adjoint_shell_log_loss(cf_adjoint *a, const void *d_state, const double *h_target, double *h_loss,
-                           cudaStream_t st) {
+int adjoint_shell_log_loss(cf_adjoint *a, const void *d_state, const double *h_target, double rel_floor,
+                           double *h_loss, cudaStream_t st) {
   cf_ctx *ctx = a->ctx;
   const double tT = a->t0 + (double)a->nsteps * a->dt;
   const long long ns = ctx->shells;
@@ -444,9 +444,11 @@ int adjoint_shell_log_loss(cf_adjoint *a, const void *d_state, const double *h_t
   std::vector<double> P(ns), g(ns, 0.0);
   CF_TRY_CUDA(cudaMemcpyAsync(P.data(), d_sh, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
   CF_TRY_CUDA(cudaStreamSynchronize(st));
-  double loss = 0.0;
+  double loss = 0.0, tmax = 0.0;
+  for (long long s = 0; s < ns; ++s) tmax = std::max(tmax, h_target[s]);
+  const double floor_v = std::max(0.0, rel_floor) * tmax;
   for (long long s = 0; s < ns; ++s) {
-    if (P[s] > 0 && h_target[s] > 0) {
+    if (P[s] > 0 && h_target[s] > 0 && h_target[s] > floor_v) {
       const double d = std::log(P[s]) - std::log(h_target[s]);
       loss += d * d;
       g[s] = 2.0 * d / P[s];

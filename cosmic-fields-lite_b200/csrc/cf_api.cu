@@ -76,7 +76,7 @@ int check_finite(cf_ctx *, const void *, int64_t *, cudaStream_t);
 int adjoint_create(cf_ctx *, int64_t, int64_t, cf_adjoint **);
 void adjoint_destroy(cf_adjoint *);
 int adjoint_forward(cf_adjoint *, void *, double, double, cudaStream_t);
-int adjoint_shell_log_loss(cf_adjoint *, const void *, const double *, double *, cudaStream_t);
+int adjoint_shell_log_loss(cf_adjoint *, const void *, const double *, double, double *, cudaStream_t);
 int adjoint_set_lambda(cf_adjoint *, const double *, double, cudaStream_t);
 int adjoint_backward(cf_adjoint *, double *, double *, cudaStream_t);
 cf_ctx *adjoint_ctx(cf_adjoint *);
@@ -472,15 +472,15 @@ int cf_adjoint_forward(cf_adjoint *adj, void *d_state, double t0, double dt, voi
   return adjoint_forward(adj, d_state, t0, dt, (cudaStream_t)stream);
 }
 
-int cf_adjoint_shell_log_loss(cf_adjoint *adj, const void *d_state, const double *h_target_shells, double *h_loss,
-                              void *stream) {
+int cf_adjoint_shell_log_loss(cf_adjoint *adj, const void *d_state, const double *h_target_shells, double rel_floor,
+                              double *h_loss, void *stream) {
   if (!adj || !h_target_shells) {
     set_error("NULL adjoint or target");
     return CF_ERR_INVALID;
   }
   CF_TRY(check_ptr(d_state, "d_state"));
   CF_TRY(use_device(adjoint_ctx(adj)));
-  return adjoint_shell_log_loss(adj, d_state, h_target_shells, h_loss, (cudaStream_t)stream);
+  return adjoint_shell_log_loss(adj, d_state, h_target_shells, rel_floor, h_loss, (cudaStream_t)stream);
 }
 
 int cf_adjoint_set_lambda(cf_adjoint *adj, const double *d_lambda, double dL_dm_direct, void *stream) {

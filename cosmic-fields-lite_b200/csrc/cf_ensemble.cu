@@ -1,0 +1,796 @@
+// cf_ensemble.cu -- ensembles of FRW Klein-Gordon lattices of uneven N advanced
+// together.
+//
+// Every member is an independent lattice (its own N, L, m; a shared
+// cosmology, time grid, precision and stencil).  A step of the whole ensemble is
+// the same four fused RK4 stages as cf_rk4_steps (cf_stage_tile.cuh), applied to
+// a work list of (member, b-tile, c-tile, a-chunk) items.  Three schedules:
+//
+//   CF_ENS_PERSISTENT  one cooperative kernel for all steps: each CTA walks the
+//                      work list of a stage, then a grid barrier (bounded spin:
+//                      gives up with CF_ERR_TIMEOUT instead of hanging) before the
+//                      next stage.  Stage coefficients come from a per-step table
+//                      in device memory, so a captured graph replays it.
+//   CF_ENS_BATCHED     one launch per stage over the whole work list.
+//   CF_ENS_LOOP        one launch per stage per member (the single-instance path).
+//
+// cf_ensemble_run_graph captures one observer interval -- barrier reset, the
+// persistent kernel for S steps and the advance of a device step counter -- in a
+// CUDA graph and replays it once per interval; the members' density spectra at
+// each interval end are enqueued on the same stream after the replay.
+//
+// Tile shapes and a-chunk lengths are chosen per size class by cf_ensemble_autotune
+// (timing of the candidates on the members themselves).
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
+
+#include "cf_internal.cuh"
+#include "cf_stage_tile.cuh"
+
+namespace cfb {
+
+struct EnsMember {
+  void *x, *acc, *ya, *yb;  // storage type; x holds [hi | lo] in FP32_COMP
+  long long N3;
+  int N;
+  double m2;
+  double inv_scale;  // 1 / h^2 (h = L/N); divided by a^2 per stage
+};
+
+struct EnsItem {
+  int member, c0, b0, a_begin, a_end, shape;
+};
+
+struct EnsCoef {
+  double a2;     // a(t)^2 of the stage time (inv = (1/h^2) / a^2, the single-lattice order)
+  double hub3;   // 3 H(t)
+};
+
+struct EnsArgs {
+  const EnsMember *members;
+  const EnsItem *items;
+  int n_items;
+  const EnsCoef *coef;      // 4 per step, indexed by absolute step
+  const long long *step_counter;  // absolute index of the first step of this launch (device)
+  int nsteps;
+  double dt;
+  unsigned *bar_count;
+  unsigned *bar_gen;
+  int *err;
+};
+
+// Tile shapes compiled for the ensemble kernels (threads along c x along b).
+constexpr int ENS_SHAPES = 2;
+template <int SHAPE>
+struct EnsShape;
+template <>
+struct EnsShape<0> {
+  static constexpr int TX = 8, TY = 32;
+};
+template <>
+struct EnsShape<1> {
+  static constexpr int TX = 16, TY = 16;
+};
+
+template <typename S, int H, int SHAPE>
+__device__ __forceinline__ void ens_item_stage(const EnsArgs &E, const EnsItem &it, int stage, long long step,
+                                               S *sm) {
+  constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
+  const EnsMember mb = E.members[it.member];
+  StageArgs<S> A;
+  A.N = mb.N;
+  A.N3 = mb.N3;
+  A.m2 = mb.m2;
+  A.x = (S *)mb.x;
+  A.xlo = (sizeof(S) == 4) ? (S *)mb.x + 2 * mb.N3 : nullptr;
+  A.acc = (S *)mb.acc;
+  A.psi = A.dpsi = nullptr;
+  A.a_chunk = 0;
+  const EnsCoef cf = E.coef[4 * step + stage - 1];
+  A.inv = mb.inv_scale / cf.a2;
+  A.hub3 = cf.hub3;
+  A.dt6 = E.dt / 6.0;
+  switch (stage) {
+    case 1:
+      A.yin = (const S *)mb.x;
+      A.yout = (S *)mb.ya;
+      A.cy = E.dt / 2.0;
+      stage_tile<S, H, false, 1, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      break;
+    case 2:
+      A.yin = (const S *)mb.ya;
+      A.yout = (S *)mb.yb;
+      A.cy = E.dt / 2.0;
+      stage_tile<S, H, false, 2, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      break;
+    case 3:
+      A.yin = (const S *)mb.yb;
+      A.yout = (S *)mb.ya;
+      A.cy = E.dt;
+      stage_tile<S, H, false, 3, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      break;
+    default:
+      A.yin = (const S *)mb.ya;
+      A.yout = nullptr;
+      stage_tile<S, H, false, 4, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      break;
+  }
+}
+
+// Grid-wide barrier with a bounded spin.  Returns false (and sets *err) if the
+// other CTAs did not arrive within the limit; all CTAs are co-resident under a
+// cooperative launch, so this only trips if that guarantee is violated.
+__device__ __forceinline__ bool grid_barrier(const EnsArgs &E) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    ok = 1;
+    volatile unsigned *gen = E.bar_gen;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(E.bar_count, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      *E.bar_count = 0u;
+      __threadfence();
+      atomicAdd((unsigned *)E.bar_gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*gen == g) {
+        if (*(volatile int *)E.err) {
+          ok = 0;
+          break;
+        }
+        if (++spins > (1LL << 24)) {  // ~ seconds with the sleep below
+          atomicExch(E.err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(128);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+template <typename S, int H, int SHAPE>
+__global__ void __launch_bounds__(256) k_ens_persistent(const EnsArgs E) {
+  constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
+  __shared__ S sm[TileSmem<S, H, TXv, TYv>::count];
+  const long long step0 = *E.step_counter;
+  for (int j = 0; j < E.nsteps; ++j) {
+    for (int stage = 1; stage <= 4; ++stage) {
+      for (int i = blockIdx.x; i < E.n_items; i += gridDim.x)
+        ens_item_stage<S, H, SHAPE>(E, E.items[i], stage, step0 + j, sm);
+      if (!grid_barrier(E)) return;
+    }
+  }
+}
+
+template <typename S, int H, int SHAPE>
+__global__ void __launch_bounds__(256) k_ens_stage(const EnsArgs E, int stage, long long step) {
+  constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
+  __shared__ S sm[TileSmem<S, H, TXv, TYv>::count];
+  ens_item_stage<S, H, SHAPE>(E, E.items[blockIdx.x], stage, step, sm);
+}
+
+__global__ void k_counter_add(long long *c, long long v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *c += v;
+}
+
+// Batched energy density of the members of one size class (blockIdx.y = member in class).
+template <typename S>
+__global__ void k_ens_energy(const EnsMember *members, const int *class_members, double *rho, int N, double a2) {
+  const EnsMember mb = members[class_members[blockIdx.y]];
+  const long long N3 = mb.N3, NN = (long long)N * N;
+  const S *x = (const S *)mb.x;
+  const S *xlo = (sizeof(S) == 4) ? x + 2 * N3 : nullptr;
+  double *out = rho + (long long)blockIdx.y * N3;
+  const double inv = mb.inv_scale / a2;
+  auto phi = [&](long long i) -> double { return (double)x[i] + (xlo ? (double)xlo[i] : 0.0); };
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N3; i += stride) {
+    const int c = (int)(i % N), b = (int)((i / N) % N), a = (int)(i / NN);
+    const double dx = phi(NN * ((a + 1) % N) + (long long)N * b + c) - phi(NN * ((a + N - 1) % N) + (long long)N * b + c);
+    const double dy = phi(NN * a + (long long)N * ((b + 1) % N) + c) - phi(NN * a + (long long)N * ((b + N - 1) % N) + c);
+    const double dz = phi(NN * a + (long long)N * b + (c + 1) % N) - phi(NN * a + (long long)N * b + (c + N - 1) % N);
+    const double f = phi(i);
+    const double p = (double)x[N3 + i] + (xlo ? (double)xlo[N3 + i] : 0.0);
+    out[i] = 0.5 * (p * p + mb.m2 * f * f + 0.25 * inv * (dx * dx + dy * dy + dz * dz));
+  }
+}
+
+// batched binning (blockIdx.y = batch entry), same fixed-point scheme as cf_spectrum.cu
+int bin_batched(const double *hc, int N, int batch, unsigned long long *maxbits, unsigned long long *bins,
+                double *out, long long nb, cudaStream_t st, cf_ctx *ctx);
+
+}  // namespace cfb
+
+struct cf_ensemble {
+  cf_params base{};
+  int count = 0;
+  int precision = CF_FP64;
+  int stencil = 7;
+  size_t word = 8;
+  std::vector<cf_params> p;
+  std::vector<cfb::EnsMember> hm;
+  cfb::EnsMember *dm = nullptr;
+  std::vector<void *> allocs;
+  // work list (per schedule; rebuilt by the autotuner)
+  std::vector<cfb::EnsItem> items;
+  cfb::EnsItem *d_items = nullptr;
+  std::map<int, std::pair<int, int>> tune;  // N -> (shape, a_chunk)
+  int shape = 0;                            // shape used by the persistent kernel
+  // time table
+  cfb::EnsCoef *d_coef = nullptr;
+  long long coef_cap = 0;
+  double coef_t0 = 0, coef_dt = 0;
+  long long *d_step = nullptr;
+  unsigned *d_bar = nullptr;  // count, gen
+  int *d_err = nullptr;
+  // spectra per size class
+  struct Cls {
+    int N;
+    std::vector<int> members;
+    int *d_members = nullptr;
+    double *rho = nullptr, *hc = nullptr;
+    cufftHandle plan = 0;
+    bool have_plan = false;
+  };
+  std::vector<Cls> classes;
+  unsigned long long *d_max = nullptr, *d_bins = nullptr;
+  long long max_bins = 0;
+  std::vector<long long> out_offset;  // per member offset into the concatenated spectra
+  long long out_total = 0;
+  // graph
+  cudaGraphExec_t gexec = nullptr;
+  long long g_steps = 0;
+  double g_t0 = 0, g_dt = 0;
+  double *g_out = nullptr;
+  bool graph_failed = false;  // capture of the cooperative launch unavailable on this driver
+  int64_t launches = 0;
+  int coop_blocks = 0;
+};
+
+namespace cfb {
+
+static int ens_fail(const char *msg) {
+  set_error("%s", msg);
+  return CF_ERR_INVALID;
+}
+
+static void build_items(cf_ensemble *E) {
+  E->items.clear();
+  for (int i = 0; i < E->count; ++i) {
+    const int N = E->hm[i].N;
+    auto tn = E->tune.count(N) ? E->tune[N] : std::make_pair(E->shape, 16);
+    const int shape = E->shape;  // one kernel instantiation per launch
+    const int TX = shape == 0 ? EnsShape<0>::TX : EnsShape<1>::TX;
+    const int TY = shape == 0 ? EnsShape<0>::TY : EnsShape<1>::TY;
+    const int TW = TX * (int)(16 / E->word);
+    const int ach = tn.second;
+    for (int a = 0; a < N; a += ach)
+      for (int b = 0; b < N; b += TY)
+        for (int c = 0; c < N; c += TW) E->items.push_back({i, c, b, a, std::min(a + ach, N), shape});
+  }
+  // largest lattices first: better balance of the round-robin
+  std::stable_sort(E->items.begin(), E->items.end(),
+                   [&](const EnsItem &x, const EnsItem &y) { return E->hm[x.member].N > E->hm[y.member].N; });
+}
+
+static int upload_items(cf_ensemble *E) {
+  cudaFree(E->d_items);
+  E->d_items = nullptr;
+  CF_TRY_CUDA(cudaMalloc(&E->d_items, sizeof(EnsItem) * E->items.size()));
+  CF_TRY_CUDA(cudaMemcpy(E->d_items, E->items.data(), sizeof(EnsItem) * E->items.size(), cudaMemcpyHostToDevice));
+  return CF_OK;
+}
+
+static int ensure_coef(cf_ensemble *E, double t0, double dt, long long nsteps_total, cudaStream_t st) {
+  if (E->d_coef && E->coef_cap >= nsteps_total && E->coef_t0 == t0 && E->coef_dt == dt) return CF_OK;
+  std::vector<EnsCoef> h((size_t)(4 * nsteps_total));
+  cf_params q = E->base;
+  for (long long n = 0; n < nsteps_total; ++n) {
+    const double t = t0 + (double)n * dt, dh = dt / 2.0;
+    const double ts[4] = {t, t + dh, t + dh, t + dt};
+    for (int s = 0; s < 4; ++s) {
+      if (q.equation == CF_EQ_KG) {
+        h[4 * n + s].a2 = 1.0;
+        h[4 * n + s].hub3 = 0.0;
+      } else {
+        const double a = cosmo_a(q, ts[s]);
+        h[4 * n + s].a2 = a * a;
+        h[4 * n + s].hub3 = 3.0 * cosmo_H(q, ts[s]);
+      }
+    }
+  }
+  cudaFree(E->d_coef);
+  E->d_coef = nullptr;
+  CF_TRY_CUDA(cudaMalloc(&E->d_coef, sizeof(EnsCoef) * h.size()));
+  CF_TRY_CUDA(cudaMemcpyAsync(E->d_coef, h.data(), sizeof(EnsCoef) * h.size(), cudaMemcpyHostToDevice, st));
+  CF_TRY_CUDA(cudaStreamSynchronize(st));
+  E->coef_cap = nsteps_total;
+  E->coef_t0 = t0;
+  E->coef_dt = dt;
+  return CF_OK;
+}
+
+template <typename S, int H, int SHAPE>
+static int launch_persistent(cf_ensemble *E, int nsteps, double dt, cudaStream_t st) {
+  auto kern = k_ens_persistent<S, H, SHAPE>;
+  if (!E->coop_blocks) {
+    int per_sm = 0, dev = 0, sms = 0;
+    CF_TRY_CUDA(cudaGetDevice(&dev));
+    CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+    if (per_sm < 1) return ens_fail("ensemble: persistent kernel does not fit on an SM");
+    E->coop_blocks = per_sm * sms;
+  }
+  EnsArgs A{};
+  A.members = E->dm;
+  A.items = E->d_items;
+  A.n_items = (int)E->items.size();
+  A.coef = E->d_coef;
+  A.step_counter = E->d_step;
+  A.nsteps = nsteps;
+  A.dt = dt;
+  A.bar_count = E->d_bar;
+  A.bar_gen = E->d_bar + 1;
+  A.err = E->d_err;
+  void *args[] = {(void *)&A};
+  const int blocks = std::min(E->coop_blocks, A.n_items);
+  const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
+  CF_TRY_CUDA(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), block, args, 0, st));
+  E->launches++;
+  return CF_OK;
+}
+
+template <typename S, int H, int SHAPE>
+static int launch_batched_stage(cf_ensemble *E, int stage, long long step, double dt, cudaStream_t st) {
+  EnsArgs A{};
+  A.members = E->dm;
+  A.items = E->d_items;
+  A.n_items = (int)E->items.size();
+  A.coef = E->d_coef;
+  A.dt = dt;
+  const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
+  k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, stage, step);
+  CF_TRY_CUDA(cudaGetLastError());
+  E->launches++;
+  return CF_OK;
+}
+
+template <typename S, int H, int SHAPE>
+static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, double dt, cudaStream_t st) {
+  if (mode == CF_ENS_PERSISTENT) {
+    CF_TRY_CUDA(cudaMemcpyAsync(E->d_step, &step0, sizeof(long long), cudaMemcpyHostToDevice, st));
+    CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 2 * sizeof(unsigned), st));
+    CF_TRY(launch_persistent<S, H, SHAPE>(E, (int)nsteps, dt, st));
+    int err = 0;
+    CF_TRY_CUDA(cudaMemcpyAsync(&err, E->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CF_TRY_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+      set_error("ensemble: grid barrier timed out");
+      return CF_ERR_TIMEOUT;
+    }
+    return CF_OK;
+  }
+  if (mode == CF_ENS_BATCHED) {
+    for (long long j = 0; j < nsteps; ++j)
+      for (int s = 1; s <= 4; ++s) CF_TRY((launch_batched_stage<S, H, SHAPE>(E, s, step0 + j, dt, st)));
+    return CF_OK;
+  }
+  // CF_ENS_LOOP: the single-instance path, member by member
+  std::vector<EnsItem> all = E->items;
+  for (long long j = 0; j < nsteps; ++j)
+    for (int s = 1; s <= 4; ++s) {
+      size_t i0 = 0;
+      while (i0 < all.size()) {
+        size_t i1 = i0;
+        while (i1 < all.size() && all[i1].member == all[i0].member) ++i1;
+        EnsArgs A{};
+        A.members = E->dm;
+        A.items = E->d_items + i0;
+        A.n_items = (int)(i1 - i0);
+        A.coef = E->d_coef;
+        A.dt = dt;
+        const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
+        k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, s, step0 + j);
+        CF_TRY_CUDA(cudaGetLastError());
+        E->launches++;
+        i0 = i1;
+      }
+    }
+  return CF_OK;
+}
+
+template <typename S, int H>
+static int run_shape(cf_ensemble *E, int mode, long long step0, long long nsteps, double dt, cudaStream_t st) {
+  if (E->shape == 1) return run_t<S, H, 1>(E, mode, step0, nsteps, dt, st);
+  return run_t<S, H, 0>(E, mode, step0, nsteps, dt, st);
+}
+
+static int run(cf_ensemble *E, int mode, long long step0, long long nsteps, double dt, cudaStream_t st) {
+  if (E->word == 4) {
+    if (E->stencil == 13) return run_shape<float, 2>(E, mode, step0, nsteps, dt, st);
+    return run_shape<float, 1>(E, mode, step0, nsteps, dt, st);
+  }
+  if (E->stencil == 13) return run_shape<double, 2>(E, mode, step0, nsteps, dt, st);
+  return run_shape<double, 1>(E, mode, step0, nsteps, dt, st);
+}
+
+// One observer segment: barrier reset, persistent kernel over `steps` steps from
+// the device step counter, counter advance (graph-capturable).
+static int persistent_segment(cf_ensemble *E, long long steps, double dt, cudaStream_t st) {
+  CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 2 * sizeof(unsigned), st));
+  int s;
+  if (E->word == 4) {
+    if (E->stencil == 13)
+      s = E->shape ? launch_persistent<float, 2, 1>(E, (int)steps, dt, st)
+                   : launch_persistent<float, 2, 0>(E, (int)steps, dt, st);
+    else
+      s = E->shape ? launch_persistent<float, 1, 1>(E, (int)steps, dt, st)
+                   : launch_persistent<float, 1, 0>(E, (int)steps, dt, st);
+  } else {
+    if (E->stencil == 13)
+      s = E->shape ? launch_persistent<double, 2, 1>(E, (int)steps, dt, st)
+                   : launch_persistent<double, 2, 0>(E, (int)steps, dt, st);
+    else
+      s = E->shape ? launch_persistent<double, 1, 1>(E, (int)steps, dt, st)
+                   : launch_persistent<double, 1, 0>(E, (int)steps, dt, st);
+  }
+  if (s != CF_OK) return s;
+  k_counter_add<<<1, 32, 0, st>>>(E->d_step, steps);
+  CF_TRY_CUDA(cudaGetLastError());
+  return CF_OK;
+}
+
+static int ensure_spectra(cf_ensemble *E) {
+  if (!E->classes.empty()) return CF_OK;
+  std::map<int, std::vector<int>> byN;
+  for (int i = 0; i < E->count; ++i) byN[E->hm[i].N].push_back(i);
+  E->out_offset.assign(E->count, 0);
+  long long off = 0;
+  for (int i = 0; i < E->count; ++i) {
+    E->out_offset[i] = off;
+    const long long N = E->hm[i].N;
+    off += 3 * (N / 2) * (N / 2) + 1;
+  }
+  E->out_total = off;
+  for (auto &kv : byN) {
+    cf_ensemble::Cls c;
+    c.N = kv.first;
+    c.members = kv.second;
+    const long long N = c.N, n = (long long)c.members.size();
+    const long long N3 = N * N * N, hc = 2 * N * N * (N / 2 + 1);
+    CF_TRY_CUDA(cudaMalloc(&c.d_members, sizeof(int) * n));
+    CF_TRY_CUDA(cudaMemcpy(c.d_members, c.members.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CF_TRY_CUDA(cudaMalloc(&c.rho, sizeof(double) * N3 * n));
+    CF_TRY_CUDA(cudaMalloc(&c.hc, sizeof(double) * hc * n));
+    long long nn[3] = {N, N, N}, ie[3] = {N, N, N}, oe[3] = {N, N, N / 2 + 1};
+    size_t work = 0;
+    CF_TRY_CUFFT(cufftCreate(&c.plan));
+    CF_TRY_CUFFT(cufftMakePlanMany64(c.plan, 3, nn, ie, 1, N3, oe, 1, hc / 2, CUFFT_D2Z, n, &work));
+    c.have_plan = true;
+    E->max_bins = std::max<long long>(E->max_bins, (3 * (N / 2) * (N / 2) + 1) * n);
+    E->classes.push_back(c);
+  }
+  CF_TRY_CUDA(cudaMalloc(&E->d_max, sizeof(unsigned long long) * E->count));
+  CF_TRY_CUDA(cudaMalloc(&E->d_bins, sizeof(unsigned long long) * 2 * E->max_bins));
+  return CF_OK;
+}
+
+static int spectra(cf_ensemble *E, double t, double *d_out, cudaStream_t st) {
+  CF_TRY(ensure_spectra(E));
+  cf_params q = E->base;
+  double a2 = 1.0;
+  if (q.equation != CF_EQ_KG) {
+    const double a = cosmo_a(q, t);
+    a2 = a * a;
+  }
+  for (auto &c : E->classes) {
+    const int n = (int)c.members.size();
+    const long long N3 = (long long)c.N * c.N * c.N;
+    dim3 grid((unsigned)std::min<long long>((N3 + 255) / 256, 148LL * 4), n);
+    if (E->word == 4)
+      k_ens_energy<float><<<grid, 256, 0, st>>>(E->dm, c.d_members, c.rho, c.N, a2);
+    else
+      k_ens_energy<double><<<grid, 256, 0, st>>>(E->dm, c.d_members, c.rho, c.N, a2);
+    CF_TRY_CUDA(cudaGetLastError());
+    E->launches++;
+    CF_TRY_CUFFT(cufftSetStream(c.plan, st));
+    CF_TRY_CUFFT(cufftExecD2Z(c.plan, c.rho, (cufftDoubleComplex *)c.hc));
+    // members of a class are consecutive in the output only if their indices are; bin into
+    // a class-contiguous buffer, then copy each member's spectrum to its slot
+    const long long nb = 3 * (c.N / 2) * (c.N / 2) + 1;
+    double *tmp = c.rho;  // reuse: the density is no longer needed once transformed
+    CF_TRY(bin_batched(c.hc, c.N, n, E->d_max, E->d_bins, tmp, nb, st, nullptr));
+    E->launches += 3;
+    for (int k = 0; k < n; ++k)
+      CF_TRY_CUDA(cudaMemcpyAsync(d_out + E->out_offset[c.members[k]], tmp + nb * k, sizeof(double) * nb,
+                                  cudaMemcpyDeviceToDevice, st));
+  }
+  return CF_OK;
+}
+
+}  // namespace cfb
+
+using namespace cfb;
+
+extern "C" {
+
+int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out) {
+  if (!members || count < 1 || !out) return ens_fail("cf_ensemble_create: need members, count >= 1, out");
+  *out = nullptr;
+  const cf_params &b = members[0];
+  for (int i = 0; i < count; ++i) {
+    const cf_params &p = members[i];
+    if (p.N < 8 || p.N > 1024 || p.N % 8) return ens_fail("ensemble member N must be a multiple of 8 in [8, 1024]");
+    if (p.equation != b.equation || p.precision != b.precision || p.stencil != b.stencil || p.a1 != b.a1 ||
+        p.H1 != b.H1 || p.t1 != b.t1 || p.p != b.p)
+      return ens_fail("ensemble members must share equation, precision, stencil and cosmology");
+    if (p.equation == CF_EQ_COMOVING_FRW) return ens_fail("ensembles cover the flat and FRW Klein-Gordon equations");
+    if (!(p.L > 0)) return ens_fail("member L must be positive");
+  }
+  if (b.stencil != 7 && b.stencil != 13) return ens_fail("stencil must be 7 or 13");
+  cf_ensemble *E = new cf_ensemble();
+  E->base = b;
+  E->count = count;
+  E->precision = b.precision;
+  E->stencil = b.stencil;
+  E->word = b.precision == CF_FP32_COMP ? 4 : 8;
+  E->p.assign(members, members + count);
+  E->hm.resize(count);
+  for (int i = 0; i < count; ++i) {
+    const cf_params &p = members[i];
+    const long long N3 = p.N * p.N * p.N;
+    void *mem = nullptr;
+    const size_t sb = 16 * (size_t)N3;  // one state (either precision)
+    if (cudaMalloc(&mem, 4 * sb) != cudaSuccess) {
+      cudaGetLastError();
+      for (void *a : E->allocs) cudaFree(a);
+      delete E;
+      set_error("ensemble: device allocation failed for member %d", i);
+      return CF_ERR_NOMEM;
+    }
+    E->allocs.push_back(mem);
+    EnsMember &m = E->hm[i];
+    m.x = mem;
+    m.acc = (char *)mem + sb;
+    m.ya = (char *)mem + 2 * sb;
+    m.yb = (char *)mem + 3 * sb;
+    m.N = (int)p.N;
+    m.N3 = N3;
+    m.m2 = p.m * p.m;
+    const double h = p.L / (double)p.N;
+    m.inv_scale = 1.0 / (h * h);
+  }
+  bool ok = cudaMalloc(&E->dm, sizeof(EnsMember) * count) == cudaSuccess &&
+            cudaMalloc(&E->d_step, sizeof(long long)) == cudaSuccess &&
+            cudaMalloc(&E->d_bar, 2 * sizeof(unsigned)) == cudaSuccess &&
+            cudaMalloc(&E->d_err, sizeof(int)) == cudaSuccess;
+  if (!ok) {
+    set_error("ensemble: device allocation failed");
+    *out = E;
+    cf_ensemble_destroy(E);
+    *out = nullptr;
+    return CF_ERR_NOMEM;
+  }
+  cudaMemcpy(E->dm, E->hm.data(), sizeof(EnsMember) * count, cudaMemcpyHostToDevice);
+  cudaMemset(E->d_bar, 0, 2 * sizeof(unsigned));
+  cudaMemset(E->d_err, 0, sizeof(int));
+  cudaMemset(E->d_step, 0, sizeof(long long));
+  build_items(E);
+  int s = upload_items(E);
+  if (s != CF_OK) {
+    cf_ensemble_destroy(E);
+    return s;
+  }
+  *out = E;
+  return CF_OK;
+}
+
+int cf_ensemble_destroy(cf_ensemble *E) {
+  if (!E) return CF_OK;
+  cudaDeviceSynchronize();
+  if (E->gexec) cudaGraphExecDestroy(E->gexec);
+  for (void *a : E->allocs) cudaFree(a);
+  cudaFree(E->dm);
+  cudaFree(E->d_items);
+  cudaFree(E->d_coef);
+  cudaFree(E->d_step);
+  cudaFree(E->d_bar);
+  cudaFree(E->d_err);
+  for (auto &c : E->classes) {
+    cudaFree(c.d_members);
+    cudaFree(c.rho);
+    cudaFree(c.hc);
+    if (c.have_plan) cufftDestroy(c.plan);
+  }
+  cudaFree(E->d_max);
+  cudaFree(E->d_bins);
+  delete E;
+  return CF_OK;
+}
+
+int cf_ensemble_info(const cf_ensemble *E, int64_t *spectra_total, int64_t *work_items) {
+  if (!E) return ens_fail("NULL ensemble");
+  if (spectra_total) {
+    long long off = 0;
+    for (int i = 0; i < E->count; ++i) off += 3 * (E->hm[i].N / 2) * (E->hm[i].N / 2) + 1;
+    *spectra_total = off;
+  }
+  if (work_items) *work_items = (int64_t)E->items.size();
+  return CF_OK;
+}
+
+int64_t cf_ensemble_launch_count(const cf_ensemble *E) { return E ? E->launches : -1; }
+
+int cf_ensemble_state_upload(cf_ensemble *E, int member, const double *h_xy, void *stream) {
+  if (!E || member < 0 || member >= E->count || !h_xy) return ens_fail("bad ensemble, member or pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const EnsMember &m = E->hm[member];
+  const size_t n2 = 2 * (size_t)m.N3;
+  if (E->word == 8) {
+    CF_TRY_CUDA(cudaMemcpyAsync(m.x, h_xy, n2 * 8, cudaMemcpyHostToDevice, st));
+    return CF_OK;
+  }
+  std::vector<float> hs(2 * n2);
+  for (size_t i = 0; i < n2; ++i) {
+    const float h = (float)h_xy[i];
+    hs[i] = h;
+    hs[n2 + i] = (float)(h_xy[i] - (double)h);
+  }
+  CF_TRY_CUDA(cudaMemcpyAsync(m.x, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, st));
+  CF_TRY_CUDA(cudaStreamSynchronize(st));
+  return CF_OK;
+}
+
+int cf_ensemble_state_download(cf_ensemble *E, int member, double *h_xy, void *stream) {
+  if (!E || member < 0 || member >= E->count || !h_xy) return ens_fail("bad ensemble, member or pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const EnsMember &m = E->hm[member];
+  const size_t n2 = 2 * (size_t)m.N3;
+  if (E->word == 8) {
+    CF_TRY_CUDA(cudaMemcpyAsync(h_xy, m.x, n2 * 8, cudaMemcpyDeviceToHost, st));
+    CF_TRY_CUDA(cudaStreamSynchronize(st));
+    return CF_OK;
+  }
+  std::vector<float> hs(2 * n2);
+  CF_TRY_CUDA(cudaMemcpyAsync(hs.data(), m.x, hs.size() * 4, cudaMemcpyDeviceToHost, st));
+  CF_TRY_CUDA(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < n2; ++i) h_xy[i] = (double)hs[i] + (double)hs[n2 + i];
+  return CF_OK;
+}
+
+int cf_ensemble_rk4_steps(cf_ensemble *E, double t0, double dt, int64_t step0, int64_t nsteps, int mode,
+                          void *stream) {
+  if (!E || nsteps < 0 || step0 < 0) return ens_fail("bad ensemble or step range");
+  if (mode != CF_ENS_PERSISTENT && mode != CF_ENS_BATCHED && mode != CF_ENS_LOOP) return ens_fail("unknown mode");
+  cudaStream_t st = (cudaStream_t)stream;
+  CF_TRY(ensure_coef(E, t0, dt, step0 + nsteps, st));
+  return run(E, mode, step0, nsteps, dt, st);
+}
+
+int cf_ensemble_density_spectra_s2(cf_ensemble *E, double t, double *d_out, void *stream) {
+  if (!E || !d_out) return ens_fail("bad ensemble or output");
+  return spectra(E, t, d_out, (cudaStream_t)stream);
+}
+
+int cf_ensemble_run_graph(cf_ensemble *E, double t0, double dt, int64_t steps_per_segment, int64_t nsegments,
+                          double *d_spectra, void *stream) {
+  if (!E || steps_per_segment < 1 || nsegments < 0) return ens_fail("bad ensemble or segment sizes");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!st) return ens_fail("cf_ensemble_run_graph needs a non-default stream (graph capture)");
+  CF_TRY(ensure_coef(E, t0, dt, steps_per_segment * std::max<int64_t>(nsegments, 1), st));
+  CF_TRY(ensure_spectra(E));
+  long long zero = 0;
+  CF_TRY_CUDA(cudaMemcpyAsync(E->d_step, &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+  // The graph holds one segment: barrier reset, the persistent kernel (its first
+  // step read from the device step counter) and the counter advance, so replaying
+  // the same graph walks the run forward.  Each segment's spectra are enqueued on
+  // the same stream after its replay (their a(t) differs per segment).
+  for (int64_t sgi = 0; sgi < nsegments; ++sgi) {
+    if (!E->graph_failed &&
+        (!E->gexec || E->g_steps != steps_per_segment || E->g_t0 != t0 || E->g_dt != dt || E->g_out != d_spectra)) {
+      if (E->gexec) cudaGraphExecDestroy(E->gexec);
+      E->gexec = nullptr;
+      cudaGraph_t g = nullptr;
+      bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      int s = ok ? persistent_segment(E, steps_per_segment, dt, st) : CF_ERR_CUDA;
+      if (ok) ok = cudaStreamEndCapture(st, &g) == cudaSuccess && s == CF_OK;
+      if (ok) ok = cudaGraphInstantiate(&E->gexec, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      if (!ok) {
+        // capture of the cooperative launch unavailable: run the same segment
+        // launches directly (same kernels, same results)
+        cudaGetLastError();
+        if (E->gexec) cudaGraphExecDestroy(E->gexec);
+        E->gexec = nullptr;
+        E->graph_failed = true;
+      } else {
+        E->g_steps = steps_per_segment;
+        E->g_t0 = t0;
+        E->g_dt = dt;
+        E->g_out = d_spectra;
+      }
+    }
+    if (E->gexec) {
+      CF_TRY_CUDA(cudaGraphLaunch(E->gexec, st));
+      E->launches++;
+    } else {
+      CF_TRY(persistent_segment(E, steps_per_segment, dt, st));
+    }
+    if (d_spectra) {
+      const double t_end = t0 + (double)((sgi + 1) * steps_per_segment) * dt;
+      CF_TRY(spectra(E, t_end, d_spectra + sgi * E->out_total, st));
+    }
+  }
+  int err = 0;
+  CF_TRY_CUDA(cudaMemcpyAsync(&err, E->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CF_TRY_CUDA(cudaStreamSynchronize(st));
+  if (err) {
+    set_error("ensemble: grid barrier timed out");
+    return CF_ERR_TIMEOUT;
+  }
+  return CF_OK;
+}
+
+int cf_ensemble_autotune(cf_ensemble *E, double t0, double dt, int64_t steps, void *stream, int *h_shape,
+                         int *h_a_chunk) {
+  if (!E || steps < 1) return ens_fail("bad ensemble or steps");
+  cudaStream_t st = (cudaStream_t)stream;
+  CF_TRY(ensure_coef(E, t0, dt, steps, st));
+  // the state is not preserved across candidate timings: tune before uploading initial data
+  cudaEvent_t a, b;
+  CF_TRY_CUDA(cudaEventCreate(&a));
+  CF_TRY_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_shape = 0, best_chunk = 16;
+  const int chunks[3] = {8, 16, 32};
+  for (int shape = 0; shape < ENS_SHAPES; ++shape)
+    for (int ch : chunks) {
+      E->shape = shape;
+      E->tune.clear();
+      for (int i = 0; i < E->count; ++i) E->tune[E->hm[i].N] = {shape, ch};
+      build_items(E);
+      CF_TRY(upload_items(E));
+      E->coop_blocks = 0;
+      CF_TRY(run(E, CF_ENS_BATCHED, 0, 1, dt, st));  // warm
+      CF_TRY_CUDA(cudaEventRecord(a, st));
+      CF_TRY(run(E, CF_ENS_BATCHED, 0, steps, dt, st));
+      CF_TRY_CUDA(cudaEventRecord(b, st));
+      CF_TRY_CUDA(cudaEventSynchronize(b));
+      float ms = 0;
+      CF_TRY_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (ms < best) {
+        best = ms;
+        best_shape = shape;
+        best_chunk = ch;
+      }
+    }
+  E->shape = best_shape;
+  E->tune.clear();
+  for (int i = 0; i < E->count; ++i) E->tune[E->hm[i].N] = {best_shape, best_chunk};
+  build_items(E);
+  CF_TRY(upload_items(E));
+  E->coop_blocks = 0;
+  if (E->gexec) {
+    cudaGraphExecDestroy(E->gexec);
+    E->gexec = nullptr;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (h_shape) *h_shape = best_shape;
+  if (h_a_chunk) *h_a_chunk = best_chunk;
+  return CF_OK;
+}
+
+}  // extern "C"

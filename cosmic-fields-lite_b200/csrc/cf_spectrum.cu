@@ -210,6 +210,73 @@ __global__ void k_s2_counts(int N, long long pairs, unsigned long long *counts) 
   }
 }
 
+// ---- batched binning (blockIdx.y = batch entry; used by ensembles) ----------
+__global__ void k_specb_max(const double *hc, long long hc_count, int N, long long pairs, unsigned long long *maxbits) {
+  SpecIn A{};
+  A.f = hc + (long long)blockIdx.y * hc_count;
+  A.N = N;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+    int c;
+    long long s2;
+    decode_mode(N, i, c, s2);
+    m = fmax(m, mode_value(A, i, c, s2));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits + blockIdx.y, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void k_specb_bin(const double *hc, long long hc_count, int N, long long pairs,
+                            const unsigned long long *maxbits, unsigned long long *bins, long long nb) {
+  SpecIn A{};
+  A.f = hc + (long long)blockIdx.y * hc_count;
+  A.N = N;
+  unsigned long long *bb = bins + 2 * nb * blockIdx.y;
+  const int e = fixed_exponent(maxbits[blockIdx.y], pairs);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+    int c;
+    long long s2;
+    decode_mode(N, i, c, s2);
+    const double y = ldexp(mode_value(A, i, c, s2), e);
+    const unsigned long long hi = __double2ull_rz(ldexp(y, -64));
+    const unsigned long long lo = __double2ull_rz(y - ldexp((double)hi, 64));
+    unsigned long long carry = 0;
+    if (lo) {
+      const unsigned long long old = atomicAdd(&bb[2 * s2], lo);
+      carry = (old + lo < old) ? 1ull : 0ull;
+    }
+    if (hi + carry) atomicAdd(&bb[2 * s2 + 1], hi + carry);
+  }
+}
+
+__global__ void k_specb_final(const unsigned long long *bins, const unsigned long long *maxbits, long long pairs,
+                              double *out, long long nb) {
+  const int e = fixed_exponent(maxbits[blockIdx.y], pairs);
+  const unsigned long long *bb = bins + 2 * nb * blockIdx.y;
+  double *o = out + nb * blockIdx.y;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += stride)
+    o[s] = fixed_to_double(bb[2 * s], bb[2 * s + 1], e);
+}
+
+int bin_batched(const double *hc, int N, int batch, unsigned long long *maxbits, unsigned long long *bins, double *out,
+                long long nb, cudaStream_t st, cf_ctx *) {
+  const long long hc_count = 2LL * N * N * (N / 2 + 1), pairs = hc_count / 2;
+  CF_TRY_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long) * batch, st));
+  CF_TRY_CUDA(cudaMemsetAsync(bins, 0, sizeof(unsigned long long) * 2 * nb * batch, st));
+  const unsigned gx = (unsigned)std::min<long long>((pairs + 255) / 256, 148LL * 8);
+  k_specb_max<<<dim3(gx, batch), 256, 0, st>>>(hc, hc_count, N, pairs, maxbits);
+  CF_TRY_CUDA(cudaGetLastError());
+  k_specb_bin<<<dim3(gx, batch), 256, 0, st>>>(hc, hc_count, N, pairs, maxbits, bins, nb);
+  CF_TRY_CUDA(cudaGetLastError());
+  const unsigned gf = (unsigned)std::min<long long>((nb + 255) / 256, 148LL * 8);
+  k_specb_final<<<dim3(gf, batch), 256, 0, st>>>(bins, maxbits, pairs, out, nb);
+  CF_TRY_CUDA(cudaGetLastError());
+  return CF_OK;
+}
+
 static unsigned grid_for(long long n, int per = 256) {
   long long b = (n + per - 1) / per;
   if (b > 148LL * 32) b = 148LL * 32;

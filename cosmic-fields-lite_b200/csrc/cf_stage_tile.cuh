@@ -1,0 +1,300 @@
+// cf_stage_tile.cuh -- one fused RK4 stage over one (b, c) tile of one lattice,
+// marching along a (shared by the single-lattice stage kernels and the
+// ensemble kernels).
+//
+// Stage semantics (stepper/runge_kutta4_classic.hpp:88-138, with the odeint
+// scale_sum combinations of src/odeint_thrust/thrust_operations.cu:238-313 fused in):
+//   STAGE 0: dxdt = f(y)                       (plain right-hand side, cf_rhs)
+//   STAGE 1: k = f(x)  acc  = k     y' = x + cy k
+//   STAGE 2: k = f(y)  acc += 2k    y' = x + cy k
+//   STAGE 3: k = f(y)  acc += 2k    y' = x + cy k
+//   STAGE 4: k = f(y)  x   += dt/6 (acc + k)   (FP32: hi/lo compensated)
+// with f(phi, pi) = (pi, (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} inv lap phi)
+// (src/equations_cuda.cu:15-36, :263-287; Psi = dPsi = 0 when !COMOV).
+//
+// Tile: TXv x TYv threads; thread (tx, ty) owns V consecutive sites along c
+// (16-byte vectors) in row b0 + ty.  phi of planes a-H..a+H of the thread's own
+// sites live in a register queue; the current plane plus an H-wide periodic
+// halo in b and c is staged in shared memory (sm: (TYv + 2H) x (TXv V + 2H)).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace cfb {
+
+template <typename S>
+struct VecT;
+template <>
+struct VecT<double> {
+  using T = double2;
+  static constexpr int n = 2;
+};
+template <>
+struct VecT<float> {
+  using T = float4;
+  static constexpr int n = 4;
+};
+
+template <typename S>
+struct Pack {
+  S v[VecT<S>::n];
+};
+
+template <typename S>
+__device__ __forceinline__ Pack<S> unpack(const typename VecT<S>::T &t) {
+  Pack<S> r;
+  if constexpr (VecT<S>::n == 2) {
+    r.v[0] = t.x;
+    r.v[1] = t.y;
+  } else {
+    r.v[0] = t.x;
+    r.v[1] = t.y;
+    r.v[2] = t.z;
+    r.v[3] = t.w;
+  }
+  return r;
+}
+
+// read-only path (buffers the kernel does not write)
+template <typename S>
+__device__ __forceinline__ Pack<S> ldv(const S *p) {
+  return unpack<S>(__ldg(reinterpret_cast<const typename VecT<S>::T *>(p)));
+}
+
+// plain load for buffers the same kernel also writes (acc, x)
+template <typename S>
+__device__ __forceinline__ Pack<S> ldv_rw(const S *p) {
+  return unpack<S>(*reinterpret_cast<const typename VecT<S>::T *>(p));
+}
+
+template <typename S>
+__device__ __forceinline__ void stv(S *p, const Pack<S> &r) {
+  typename VecT<S>::T t;
+  if constexpr (VecT<S>::n == 2) {
+    t.x = r.v[0];
+    t.y = r.v[1];
+  } else {
+    t.x = r.v[0];
+    t.y = r.v[1];
+    t.z = r.v[2];
+    t.w = r.v[3];
+  }
+  *reinterpret_cast<typename VecT<S>::T *>(p) = t;
+}
+
+template <typename S>
+struct StageArgs {
+  const S *yin;  // stage input [phi | pi]; for stages 0 and 1 the state x (hi part)
+  S *yout;       // stage output [phi | pi] (stages 1-3); dxdt for stage 0
+  S *acc;        // k accumulator [phi | pi]
+  S *x;          // base state [phi | pi] (hi part in FP32_COMP)
+  S *xlo;        // FP32_COMP compensation [phi | pi] (stage 4 only)
+  const S *psi;  // comoving: Psi(t_stage), N^3
+  const S *dpsi; // comoving: dPsi/dt(t_stage), N^3
+  int N;
+  int a_chunk;
+  long long N3;
+  double m2;    // m^2
+  double inv;   // h^-2 a^-2
+  double hub3;  // 3 H
+  double cy;    // y' = x + cy * k
+  double dt6;   // dt / 6
+};
+
+// exp(2 Psi) and exp(4 Psi).  FP64: the reference's exp of the doubled argument.
+// FP32: Psi is an FP32 field of magnitude ~1e-2; 1 + expm1f keeps the absolute
+// error of e^{2Psi} near 1e-9 (FP32 relative accuracy on the small part).
+__device__ __forceinline__ void psi_factors(double psi, double &e2, double &e4) {
+  e2 = exp(2 * psi);
+  e4 = exp(4 * psi);
+}
+__device__ __forceinline__ void psi_factors(float psi, double &e2, double &e4) {
+  e2 = 1.0 + (double)expm1f(2.0f * psi);
+  e4 = 1.0 + (double)expm1f(4.0f * psi);
+}
+
+// Two plane buffers: plane a is staged in buffer (a - a_begin) & 1, so one
+// barrier per plane suffices -- a thread that writes buffer k for plane a + 2 has
+// passed the barrier of plane a + 1, which every thread reaches only after it has
+// finished reading plane a.
+template <typename S, int H, int TXv, int TYv>
+struct TileSmem {
+  static constexpr int V = VecT<S>::n;
+  static constexpr int TW = TXv * V;
+  static constexpr int SP = TW + 2 * H;
+  static constexpr int SR = TYv + 2 * H;
+  static constexpr int plane = SR * SP;
+  static constexpr int count = 2 * plane;
+};
+
+template <typename S, int H, bool COMOV, int STAGE, int TXv, int TYv>
+__device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0, int a_begin, int a_end, S *sm2) {
+  using TS = TileSmem<S, H, TXv, TYv>;
+  constexpr int V = TS::V;
+  constexpr int TW = TS::TW;
+  constexpr int SP = TS::SP;
+  const int N = A.N;
+  const long long N3 = A.N3;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TXv + tx;
+  const int twe = min(TW, N - c0);   // active tile width (a multiple of V: N % 8 == 0)
+  const int tye = min(TYv, N - b0);  // active tile height
+  const int sre = tye + 2 * H;       // shared-memory rows in use
+  const int c = c0 + tx * V;
+  const int b = b0 + ty;
+  const bool act = (tx * V) < twe && ty < tye;
+  const long long rowoff = (long long)N * b + c;  // offset within a plane
+  const long long NN = (long long)N * N;
+  const S *phi_in = A.yin;
+  const S *pi_in = A.yin + N3;
+
+  Pack<S> q[2 * H + 1];
+  if (act) {
+#pragma unroll
+    for (int j = 0; j < 2 * H; ++j) q[j + 1] = ldv(phi_in + NN * ((a_begin - H + j + N) % N) + rowoff);
+  }
+
+  for (int a = a_begin; a < a_end; ++a) {
+    const long long site = NN * a + rowoff;
+#pragma unroll
+    for (int j = 0; j < 2 * H; ++j) q[j] = q[j + 1];
+    Pack<S> pi0, xp, xq, cp, cq, lp, lq, ps, dps;
+    if (act) {
+      q[2 * H] = ldv(phi_in + NN * ((a + H) % N) + rowoff);
+      pi0 = ldv(pi_in + site);
+      if constexpr (STAGE == 2 || STAGE == 3 || STAGE == 4) {
+        xp = ldv_rw(A.x + site);
+        xq = ldv_rw(A.x + N3 + site);
+        cp = ldv_rw(A.acc + site);
+        cq = ldv_rw(A.acc + N3 + site);
+      }
+      if constexpr (STAGE == 4 && sizeof(S) == 4) {
+        lp = ldv_rw(A.xlo + site);
+        lq = ldv_rw(A.xlo + N3 + site);
+      }
+      if constexpr (COMOV) {
+        ps = ldv(A.psi + site);
+        dps = ldv(A.dpsi + site);
+      }
+    }
+    S *sm = sm2 + ((a - a_begin) & 1) * TS::plane;
+    if (act) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) sm[(ty + H) * SP + H + tx * V + v] = q[H].v[v];
+      // halo rows: H above the tile and H below its active height, interior columns
+      if (ty < H || ty >= tye - H) {
+        const int r = (ty < H) ? ty : ty + 2 * H;
+        const int gb = (b0 - H + r + N) % N;
+        const Pack<S> h = ldv(phi_in + NN * a + (long long)N * gb + c);
+#pragma unroll
+        for (int v = 0; v < V; ++v) sm[r * SP + H + tx * V + v] = h.v[v];
+      }
+      // (a thread that is both in the top and the bottom band, tye < 2H, writes its bottom row below)
+      if (ty < H && ty >= tye - H) {
+        const int r = ty + 2 * H;
+        const int gb = (b0 - H + r + N) % N;
+        const Pack<S> h = ldv(phi_in + NN * a + (long long)N * gb + c);
+#pragma unroll
+        for (int v = 0; v < V; ++v) sm[r * SP + H + tx * V + v] = h.v[v];
+      }
+    }
+    // halo columns: H left and H right of the active width, all rows in use
+    for (int i = tid; i < sre * 2 * H; i += TXv * TYv) {
+      const int r = i / (2 * H);
+      const int j = i % (2 * H);
+      const int gb = (b0 - H + r + N) % N;
+      int col, gc;
+      if (j < H) {
+        col = j;
+        gc = (c0 - H + j + N) % N;
+      } else {
+        col = twe + H + (j - H);
+        gc = (c0 + twe + (j - H)) % N;
+      }
+      sm[r * SP + col] = phi_in[NN * a + (long long)N * gb + gc];
+    }
+    __syncthreads();
+    if (!act) continue;
+
+    Pack<S> o_phi, o_pi;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int col = H + tx * V + v;
+      const int row = ty + H;
+      const double f0 = (double)q[H].v[v];
+      double lap;
+      if constexpr (H == 1) {
+        const double s = -6.0 * f0 + (double)q[2].v[v] + (double)q[0].v[v] + (double)sm[(row + 1) * SP + col] +
+                         (double)sm[(row - 1) * SP + col];
+        lap = s + ((double)sm[row * SP + col + 1] + (double)sm[row * SP + col - 1]);
+      } else {
+        const double s1 = (double)q[3].v[v] + (double)q[1].v[v] + (double)sm[(row + 1) * SP + col] +
+                          (double)sm[(row - 1) * SP + col] + (double)sm[row * SP + col + 1] +
+                          (double)sm[row * SP + col - 1];
+        const double s2 = (double)q[4].v[v] + (double)q[0].v[v] + (double)sm[(row + 2) * SP + col] +
+                          (double)sm[(row - 2) * SP + col] + (double)sm[row * SP + col + 2] +
+                          (double)sm[row * SP + col - 2];
+        lap = (16.0 * s1 - s2 - 90.0 * f0) / 12.0;
+      }
+      const double p0 = (double)pi0.v[v];
+      const double kphi = p0;
+      double kpi;
+      if constexpr (COMOV) {
+        double e2, e4;
+        psi_factors(ps.v[v], e2, e4);
+        kpi = (-A.hub3 + 4.0 * (double)dps.v[v]) * p0 - e2 * A.m2 * f0 + e4 * A.inv * lap;
+      } else {
+        kpi = -A.hub3 * p0 - A.m2 * f0 + A.inv * lap;
+      }
+      if constexpr (STAGE == 0) {
+        o_phi.v[v] = (S)kphi;
+        o_pi.v[v] = (S)kpi;
+      } else if constexpr (STAGE == 1) {
+        cp.v[v] = (S)kphi;
+        cq.v[v] = (S)kpi;
+        o_phi.v[v] = (S)(f0 + A.cy * kphi);
+        o_pi.v[v] = (S)(p0 + A.cy * kpi);
+      } else if constexpr (STAGE == 2 || STAGE == 3) {
+        cp.v[v] = (S)((double)cp.v[v] + 2.0 * kphi);
+        cq.v[v] = (S)((double)cq.v[v] + 2.0 * kpi);
+        o_phi.v[v] = (S)((double)xp.v[v] + A.cy * kphi);
+        o_pi.v[v] = (S)((double)xq.v[v] + A.cy * kpi);
+      } else {  // STAGE 4
+        const double ip = A.dt6 * ((double)cp.v[v] + kphi);
+        const double iq = A.dt6 * ((double)cq.v[v] + kpi);
+        if constexpr (sizeof(S) == 8) {
+          xp.v[v] = (S)((double)xp.v[v] + ip);
+          xq.v[v] = (S)((double)xq.v[v] + iq);
+        } else {
+          const double np = ((double)xp.v[v] + (double)lp.v[v]) + ip;
+          const double nq = ((double)xq.v[v] + (double)lq.v[v]) + iq;
+          const float hp = (float)np, hq = (float)nq;
+          xp.v[v] = hp;
+          xq.v[v] = hq;
+          lp.v[v] = (float)(np - (double)hp);
+          lq.v[v] = (float)(nq - (double)hq);
+        }
+      }
+    }
+    if constexpr (STAGE == 0) {
+      stv(A.yout + site, o_phi);
+      stv(A.yout + N3 + site, o_pi);
+    } else if constexpr (STAGE <= 3) {
+      stv(A.acc + site, cp);
+      stv(A.acc + N3 + site, cq);
+      stv(A.yout + site, o_phi);
+      stv(A.yout + N3 + site, o_pi);
+    } else {
+      stv(A.x + site, xp);
+      stv(A.x + N3 + site, xq);
+      if constexpr (sizeof(S) == 4) {
+        stv(A.xlo + site, lp);
+        stv(A.xlo + N3 + site, lq);
+      }
+    }
+  }
+  // the caller may stage another tile into the same buffers next (ensemble work lists)
+  __syncthreads();
+}
+
+}  // namespace cfb

@@ -168,8 +168,10 @@ int cf_check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, void *stre
  *   cf_adjoint_create: checkpoints every `checkpoint_every` of `nsteps` steps.
  *   cf_adjoint_forward: runs the nsteps from d_state (in: x0, out: x_T), t_j = t0 + j dt,
  *     storing checkpoints.
- *   cf_adjoint_shell_log_loss: L = sum_s (log P_s - log T_s)^2 over unit shells s with
- *     P_s, T_s > 0, where P_s is the shell density spectrum of x_T at t_T (as
+ *   cf_adjoint_shell_log_loss: L = sum_s (log P_s - log T_s)^2 over the unit shells s with
+ *     P_s > 0 and T_s > rel_floor * max_s T_s (shells at the rounding floor of the
+ *     spectrum carry no smooth information; 0 keeps every shell with T_s > 0), where
+ *     P_s is the shell density spectrum of x_T at t_T (as
  *     cf_density_spectrum_s2 + cf_s2_to_shells); sets dL/dx_T as the adjoint seed.
  *   cf_adjoint_set_lambda: sets the seed dL/dx_T (FP64 2N^3, device) directly, with the
  *     part of dL/dm not carried by the state.
@@ -184,7 +186,7 @@ int cf_adjoint_create(cf_ctx *ctx, int64_t nsteps, int64_t checkpoint_every, cf_
 int cf_adjoint_destroy(cf_adjoint *adj);
 int cf_adjoint_forward(cf_adjoint *adj, void *d_state, double t0, double dt, void *stream);
 int cf_adjoint_shell_log_loss(cf_adjoint *adj, const void *d_state, const double *h_target_shells,
-                              double *h_loss, void *stream);
+                              double rel_floor, double *h_loss, void *stream);
 int cf_adjoint_set_lambda(cf_adjoint *adj, const double *d_lambda, double dL_dm_direct, void *stream);
 int cf_adjoint_backward(cf_adjoint *adj, double *d_lambda0, double *h_dL_dm, void *stream);
 int cf_field_from_shell_amplitudes(cf_ctx *ctx, const double *d_xi_hc, const double *d_sqrtP_s2,
@@ -193,6 +195,39 @@ int cf_field_from_shell_amplitudes(cf_ctx *ctx, const double *d_xi_hc, const dou
 int cf_shell_amplitude_gradient(cf_ctx *ctx, const double *d_lambda_phi, const double *d_xi_hc,
                                 const double *d_sqrtP_s2, const double *h_theta, int ngroups,
                                 int shells_per_group, double *h_grad, void *stream);
+
+/* ---- ensembles ------------------------------------------------------------------
+ * Independent CF_EQ_KG / CF_EQ_KG_FRW lattices of uneven N (each N % 8 == 0,
+ * N <= 1024) sharing equation, precision, stencil, cosmology and time grid,
+ * advanced together.  No reference counterpart: the reference runs one lattice
+ * per process (src/main.cpp:82-196).
+ *   CF_ENS_PERSISTENT: one cooperative kernel for all nsteps (grid barriers between
+ *     stages; a barrier that waits too long returns CF_ERR_TIMEOUT, never hangs).
+ *   CF_ENS_BATCHED: one launch per stage over all members.
+ *   CF_ENS_LOOP: one launch per stage per member (single-instance path).
+ * cf_ensemble_run_graph: nsegments observer intervals of steps_per_segment steps from
+ *   t0 (absolute steps 0..): a CUDA graph of the persistent kernel is captured once
+ *   and replayed per segment; when d_spectra is non-NULL the members' density
+ *   spectra (S2 bins, concatenated member by member, cf_ensemble_info gives the
+ *   per-segment length) at each segment end follow each replay.  Needs a
+ *   non-default stream.
+ * cf_ensemble_autotune: times tile shapes and a-chunk lengths on the members
+ *   (overwrites their states: tune before uploading initial data). */
+typedef enum cf_ens_mode { CF_ENS_PERSISTENT = 0, CF_ENS_BATCHED = 1, CF_ENS_LOOP = 2 } cf_ens_mode;
+typedef struct cf_ensemble cf_ensemble;
+int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out);
+int cf_ensemble_destroy(cf_ensemble *ens);
+int cf_ensemble_info(const cf_ensemble *ens, int64_t *spectra_total, int64_t *work_items);
+int64_t cf_ensemble_launch_count(const cf_ensemble *ens);
+int cf_ensemble_state_upload(cf_ensemble *ens, int member, const double *h_xy, void *stream);
+int cf_ensemble_state_download(cf_ensemble *ens, int member, double *h_xy, void *stream);
+int cf_ensemble_rk4_steps(cf_ensemble *ens, double t0, double dt, int64_t step0, int64_t nsteps, int mode,
+                          void *stream);
+int cf_ensemble_density_spectra_s2(cf_ensemble *ens, double t, double *d_out, void *stream);
+int cf_ensemble_run_graph(cf_ensemble *ens, double t0, double dt, int64_t steps_per_segment, int64_t nsegments,
+                          double *d_spectra, void *stream);
+int cf_ensemble_autotune(cf_ensemble *ens, double t0, double dt, int64_t steps, void *stream, int *h_shape,
+                         int *h_a_chunk);
 
 /* ---- profiling ----------------------------------------------------------------
  * When enabled, every kernel (or cuFFT call) the context launches is bracketed by
