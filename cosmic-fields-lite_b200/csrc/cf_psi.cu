@@ -48,26 +48,44 @@ __global__ void k_transfer_table(double *__restrict__ table, long long nb, int N
 }
 
 // Psi_k = R_k T_Psi(s^2), dPsi_k = R_k T_dPsi(s^2); output: two HC arrays of the
-// storage complex type, consecutive.
+// storage complex type, consecutive.  Grid: y/z = the (a, b) row, threads along c
+// (no index division; each complex entry is one 8- or 16-byte access).
 template <typename S>
-__global__ void k_transfer(const S *__restrict__ R, S *__restrict__ out, const double *__restrict__ table, int N,
-                           long long hc_pairs) {
+struct Cplx;
+template <>
+struct Cplx<float> {
+  using T = float2;
+};
+template <>
+struct Cplx<double> {
+  using T = double2;
+};
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_transfer(const S *__restrict__ R, S *__restrict__ out,
+                                                  const double *__restrict__ table, int N, long long hc_pairs) {
+  using C = typename Cplx<S>::T;
   const int nh = N / 2 + 1;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < hc_pairs; i += stride) {
-    const int c = (int)(i % nh);
-    const long long ab = i / nh;
-    const int b = (int)(ab % N);
-    const int a = (int)(ab / N);
-    const int as = (a <= N / 2) ? a : N - a;
-    const int bs = (b <= N / 2) ? b : N - b;
-    const long long s2 = (long long)as * as + (long long)bs * bs + (long long)c * c;
+  const int a = blockIdx.z, b = blockIdx.y;
+  const int as = (a <= N / 2) ? a : N - a;
+  const int bs = (b <= N / 2) ? b : N - b;
+  const int ab2 = as * as + bs * bs;
+  const long long row = ((long long)a * N + b) * nh;
+  const C *Rr = reinterpret_cast<const C *>(R) + row;
+  C *op = reinterpret_cast<C *>(out) + row;
+  C *od = reinterpret_cast<C *>(out) + hc_pairs + row;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nh; c += gridDim.x * blockDim.x) {
+    const int s2 = ab2 + c * c;
     const double tp = table[2 * s2], td = table[2 * s2 + 1];
-    const double rr = (double)R[2 * i], ri = (double)R[2 * i + 1];
-    out[2 * i] = (S)(rr * tp);
-    out[2 * i + 1] = (S)(ri * tp);
-    out[2 * hc_pairs + 2 * i] = (S)(rr * td);
-    out[2 * hc_pairs + 2 * i + 1] = (S)(ri * td);
+    const C r = Rr[c];
+    const double rr = (double)r.x, ri = (double)r.y;
+    C p, d;
+    p.x = (S)(rr * tp);
+    p.y = (S)(ri * tp);
+    d.x = (S)(rr * td);
+    d.y = (S)(ri * td);
+    op[c] = p;
+    od[c] = d;
   }
 }
 
@@ -136,19 +154,20 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void 
   const double H_t = cosmo_H(ctx->p, t);
   const double factor = (2 * 3.14159265358979323846 / ctx->p.L) * eta_t / sqrt(3);
   const long long pairs = ctx->hc_count / 2;
-  unsigned blocks = (unsigned)std::min<long long>((pairs + 255) / 256, 148LL * 32);
   CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
   {
     ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
     unsigned tb = (unsigned)std::min<long long>((ctx->s2_bins + 255) / 256, 148LL * 8);
     k_transfer_table<<<tb, 256, 0, st>>>(ctx->psi_table, ctx->s2_bins, (int)ctx->N, factor, H_t);
     CF_LAUNCHED(ctx);
+    const int nh = (int)ctx->N / 2 + 1;
+    const dim3 tg((unsigned)((nh + 255) / 256), (unsigned)ctx->N, (unsigned)ctx->N);
     if (ctx->word == 8)
-      k_transfer<double><<<blocks, 256, 0, st>>>((const double *)ctx->R_fft, (double *)ctx->psi_hc,
-                                                 ctx->psi_table, (int)ctx->N, pairs);
+      k_transfer<double><<<tg, 256, 0, st>>>((const double *)ctx->R_fft, (double *)ctx->psi_hc, ctx->psi_table,
+                                             (int)ctx->N, pairs);
     else
-      k_transfer<float><<<blocks, 256, 0, st>>>((const float *)ctx->R_fft, (float *)ctx->psi_hc, ctx->psi_table,
-                                                (int)ctx->N, pairs);
+      k_transfer<float><<<tg, 256, 0, st>>>((const float *)ctx->R_fft, (float *)ctx->psi_hc, ctx->psi_table,
+                                            (int)ctx->N, pairs);
     CF_LAUNCHED(ctx);
   }
   {

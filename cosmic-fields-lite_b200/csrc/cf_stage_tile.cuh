@@ -113,10 +113,17 @@ __device__ __forceinline__ void psi_factors(float psi, double &e2, double &e4) {
   e4 = 1.0 + (double)expm1f(4.0f * psi);
 }
 
-// Two plane buffers: plane a is staged in buffer (a - a_begin) & 1, so one
-// barrier per plane suffices -- a thread that writes buffer k for plane a + 2 has
-// passed the barrier of plane a + 1, which every thread reaches only after it has
-// finished reading plane a.
+// Plane staging.  Double-buffered (DB): plane a goes to buffer (a - a_begin) & 1
+// and one barrier per plane suffices -- a thread that writes buffer k for plane
+// a + 2 has passed the barrier of plane a + 1, which every thread reaches only
+// after it has finished reading plane a.  Single-buffered: a second barrier
+// before the buffer is overwritten, and fewer live registers (measured faster
+// for FP64, where registers limit the resident CTAs; DB is faster for FP32).
+template <typename S>
+struct DoubleBuffered {
+  static constexpr bool value = sizeof(S) == 4;
+};
+
 template <typename S, int H, int TXv, int TYv>
 struct TileSmem {
   static constexpr int V = VecT<S>::n;
@@ -124,12 +131,15 @@ struct TileSmem {
   static constexpr int SP = TW + 2 * H;
   static constexpr int SR = TYv + 2 * H;
   static constexpr int plane = SR * SP;
-  static constexpr int count = 2 * plane;
+  static constexpr int count = (DoubleBuffered<S>::value ? 2 : 1) * plane;
 };
 
-template <typename S, int H, bool COMOV, int STAGE, int TXv, int TYv>
+// FULL: the caller guarantees the tile lies inside the lattice (N % TW == 0 and
+// N % TYv == 0), so the active width and height are compile-time constants.
+template <typename S, int H, bool COMOV, int STAGE, int TXv, int TYv, bool FULL = false>
 __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0, int a_begin, int a_end, S *sm2) {
   using TS = TileSmem<S, H, TXv, TYv>;
+  constexpr bool DB = DoubleBuffered<S>::value;
   constexpr int V = TS::V;
   constexpr int TW = TS::TW;
   constexpr int SP = TS::SP;
@@ -137,8 +147,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
   const long long N3 = A.N3;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * TXv + tx;
-  const int twe = min(TW, N - c0);   // active tile width (a multiple of V: N % 8 == 0)
-  const int tye = min(TYv, N - b0);  // active tile height
+  const int twe = FULL ? TW : min(TW, N - c0);    // active tile width (a multiple of V: N % 8 == 0)
+  const int tye = FULL ? TYv : min(TYv, N - b0);  // active tile height
   const int sre = tye + 2 * H;       // shared-memory rows in use
   const int c = c0 + tx * V;
   const int b = b0 + ty;
@@ -177,7 +187,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
         dps = ldv(A.dpsi + site);
       }
     }
-    S *sm = sm2 + ((a - a_begin) & 1) * TS::plane;
+    S *sm = sm2;
+    if constexpr (DB) {
+      sm = sm2 + ((a - a_begin) & 1) * TS::plane;
+    } else {
+      __syncthreads();  // the previous plane's shared-memory reads are complete
+    }
     if (act) {
 #pragma unroll
       for (int v = 0; v < V; ++v) sm[(ty + H) * SP + H + tx * V + v] = q[H].v[v];

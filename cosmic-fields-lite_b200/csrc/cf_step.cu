@@ -31,18 +31,22 @@ namespace cfb {
 constexpr int TX = 32;  // threads along c (each owns V consecutive sites)
 constexpr int TY = 8;   // threads along b
 
-// Resident CTAs per SM the register allocation must allow (occupancy floor).
-#ifndef CF_STAGE_MIN_BLOCKS
-#define CF_STAGE_MIN_BLOCKS 3
-#endif
+// Resident CTAs per SM the register allocation must allow (occupancy floor),
+// from measurements at N = 512: 4 for FP32 (double-buffered planes) and for the
+// uncoupled FP64 stages; the compiler's choice for the FP64 comoving stages,
+// whose Psi terms would spill at 64 registers.
+template <typename S, bool COMOV>
+struct StageMinBlocks {
+  static constexpr int value = (sizeof(S) == 4 || !COMOV) ? 4 : 1;
+};
 
-template <typename S, int H, bool COMOV, int STAGE>
-__global__ void __launch_bounds__(TX *TY, CF_STAGE_MIN_BLOCKS) k_stage(const StageArgs<S> A) {
+template <typename S, int H, bool COMOV, int STAGE, bool FULL>
+__global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_stage(const StageArgs<S> A) {
   using TS = TileSmem<S, H, TX, TY>;
   __shared__ S sm[TS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
-  stage_tile<S, H, COMOV, STAGE, TX, TY>(A, blockIdx.x * TS::TW, blockIdx.y * TY, a_begin,
-                                         min(a_begin + A.a_chunk, A.N), sm);
+  stage_tile<S, H, COMOV, STAGE, TX, TY, FULL>(A, blockIdx.x * TS::TW, blockIdx.y * TY, a_begin,
+                                               min(a_begin + A.a_chunk, A.N), sm);
 }
 
 // Planes per CTA along a: enough CTAs to fill the GPU several times over.
@@ -61,7 +65,10 @@ static int launch_stage_t(cf_ctx *ctx, const StageArgs<S> &A0, cudaStream_t st) 
   A.a_chunk = pick_a_chunk(A.N, (int)(gx * gy));
   dim3 grid(gx, gy, ceil_div(A.N, A.a_chunk));
   ProfScope ps(ctx, STAGE == 0 ? CF_PROF_OTHER : STAGE - 1, st);
-  k_stage<S, H, COMOV, STAGE><<<grid, block, 0, st>>>(A);
+  if (A.N % TW == 0 && A.N % TY == 0)
+    k_stage<S, H, COMOV, STAGE, true><<<grid, block, 0, st>>>(A);
+  else
+    k_stage<S, H, COMOV, STAGE, false><<<grid, block, 0, st>>>(A);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
