@@ -26,6 +26,7 @@ STATUS = {0: "CF_OK", -1: "CF_ERR_INVALID", -2: "CF_ERR_CUDA", -3: "CF_ERR_CUFFT
           -5: "CF_ERR_NONFINITE", -6: "CF_ERR_TIMEOUT", -7: "CF_ERR_UNSUPPORTED"}
 EQ_KG, EQ_KG_FRW, EQ_COMOVING_FRW = 0, 1, 2
 FP64, FP32_COMP = 0, 1
+FLAG_FULL_PSI_FFT = 1
 
 
 class CfError(RuntimeError):
@@ -161,9 +162,9 @@ class Context:
     """One cf_ctx: a lattice, an equation, a precision and a stencil."""
 
     def __init__(self, N, L, m=1.0, equation=EQ_KG_FRW, precision=FP64, stencil=7, a1=1.0, H1=0.0,
-                 t1=0.0, p=1.0):
+                 t1=0.0, p=1.0, flags=0):
         self.params = cf_params(int(N), float(L), float(m), float(a1), float(H1), float(t1), float(p),
-                                int(equation), int(precision), int(stencil), 0)
+                                int(equation), int(precision), int(stencil), int(flags))
         h = ctypes.c_void_p()
         check(lib().cf_create(ctypes.byref(self.params), ctypes.byref(h)))
         self.h = h

@@ -110,10 +110,16 @@ def curvature_R_fft(N, L, eta_start, psi_rms, k_max, seed, use_torch=False):
     T = transfer_psi(k * eta_start / np.sqrt(3.0))
     var1 = float((shape * T ** 2 * _mult_half(N)).sum()) / N ** 3
     A = psi_rms ** 2 / var1 if var1 > 0 else 0.0
-    R = _grf_from_sqrtP(N, np.sqrt(A * shape), np.random.default_rng(seed), use_torch)
+    # The reference's R_fft = r2c(c2r(sqrtP r2c(w / N^3))) equals sqrtP r2c(w) up to
+    # rounding; building it directly keeps the modes beyond k_max exactly zero.
+    sqrtP = np.sqrt(A * shape)
+    rng = np.random.default_rng(seed)
     if use_torch:
         import torch
-        hc = torch.fft.rfftn(R.reshape(N, N, N))
+        g = torch.Generator(device="cuda")
+        g.manual_seed(int(rng.integers(1 << 62)))
+        w = torch.randn((N, N, N), generator=g, device="cuda", dtype=torch.float64)
+        hc = torch.fft.rfftn(w) * torch.from_numpy(sqrtP).to("cuda")
         return torch.view_as_real(hc).reshape(-1).contiguous()
-    hc = np.fft.rfftn(R.reshape(N, N, N))
+    hc = np.fft.rfftn(rng.standard_normal((N, N, N))) * sqrtP
     return np.ascontiguousarray(hc).view(np.float64).ravel()

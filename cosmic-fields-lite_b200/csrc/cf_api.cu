@@ -240,6 +240,7 @@ int cf_destroy(cf_ctx *ctx) {
   cudaFree(ctx->psi_table);
   for (auto &s : ctx->slot) cudaFree(s.psi);
   if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
+  psi_release(ctx);
   if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);
   if (ctx->have_d2z2) cufftDestroy(ctx->plan_d2z2);
   cudaFree(ctx->spec_hc);

@@ -82,6 +82,14 @@ struct cf_ctx {
   uint64_t slot_clock = 0;
   cufftHandle plan_psi = 0;  // batched (2) C2R/Z2D into dense N^3
   bool have_plan_psi = false;
+  // Pruned synthesis when R_fft is exactly zero outside |i|, |j| <= Ka, Kb and
+  // k <= Kc (cf_psi.cu): three 1-D passes over the support only.
+  bool pruned = false;
+  int Ka = -1, Kb = -1, Kc = -1;
+  int pr_Ka = -1, pr_Kb = -1, pr_Kc = -1;  // box the pruned plans / buffers were built for
+  void *pz_a = nullptr, *pz_b = nullptr;
+  cufftHandle plan_pa = 0, plan_pb = 0, plan_pc = 0;
+  bool have_pruned = false;
 
   // Spectra: FP64 R2C plans and scratch.
   cufftHandle plan_d2z1 = 0, plan_d2z2 = 0;
@@ -114,6 +122,8 @@ int ensure_psi(cf_ctx *ctx);
 // Returns the cached Psi / dPsi/dt slot for stage time t, refreshing one slot
 // (transfer kernel + batched C2R on `stream`) if t is not cached.
 int psi_at(cf_ctx *ctx, double t, cudaStream_t stream, const void **psi, const void **dpsi);
+// Frees the pruned-synthesis buffers and plans (context teardown).
+void psi_release(cf_ctx *ctx);
 
 // Host-side StaticEOSCosmology (reference src/physics.hpp:34-55), bit-identical
 // to the reference's host code: same expressions, same libm.

@@ -89,6 +89,116 @@ __global__ void __launch_bounds__(256) k_transfer(const S *__restrict__ R, S *__
   }
 }
 
+// ---- pruned synthesis for a band-limited R_fft ------------------------------
+// When R_fft is exactly zero outside |i| <= Ka, |j| <= Kb, k <= Kc (a "box" of
+// the half-complex grid), the inverse 3-D DFT factorises into three 1-D passes
+// that only need the lines crossing the box:
+//   A: along a, for the (Kc+1)(2Kb+1) lines (k, j) of the box     (C2C, length N)
+//   B: along b, for the (Kc+1) N lines (k, a)                        (C2C, length N)
+//   C: along c, for all N^2 rows (a, b), input zero beyond Kc        (C2R, length N)
+// (unnormalised inverse transforms, like the full C2R; the transfer factors are
+// applied in A's input).  Both fields (Psi, dPsi) go through each pass as one batch.
+
+// Support box of the non-zero entries of an HC array (grid: z = a, y = b, threads c).
+template <typename S>
+__global__ void k_support(const S *__restrict__ R, int N, int *__restrict__ box) {
+  using C = typename Cplx<S>::T;
+  const int nh = N / 2 + 1;
+  const int a = blockIdx.z, b = blockIdx.y;
+  const C *row = reinterpret_cast<const C *>(R) + ((long long)a * N + b) * nh;
+  int ma = -1, mb = -1, mc = -1;
+  for (int c = threadIdx.x; c < nh; c += blockDim.x) {
+    const C v = row[c];
+    if (v.x != (S)0 || v.y != (S)0) {
+      ma = (a <= N / 2) ? a : N - a;
+      mb = (b <= N / 2) ? b : N - b;
+      mc = max(mc, c);
+    }
+  }
+  ma = __reduce_max_sync(0xffffffffu, ma);
+  mb = __reduce_max_sync(0xffffffffu, mb);
+  mc = __reduce_max_sync(0xffffffffu, mc);
+  if ((threadIdx.x & 31) == 0 && mc >= 0) {
+    atomicMax(box + 0, ma);
+    atomicMax(box + 1, mb);
+    atomicMax(box + 2, mc);
+  }
+}
+
+// Pass-A input: pz_a[f][k][jj][a] (f = Psi / dPsi, k <= Kc, jj indexes j in
+// -Kb..Kb as 0..Kb, then N-Kb..N-1), zero where |i| > Ka.
+template <typename S>
+__global__ void k_prune_a(const S *__restrict__ R, const double *__restrict__ table, S *__restrict__ pz, int N, int Ka,
+                          int Kb, int Kc) {
+  using C = typename Cplx<S>::T;
+  const int nh = N / 2 + 1, nj = 2 * Kb + 1;
+  const int jj = blockIdx.y, k = blockIdx.z;
+  const int b = (jj <= Kb) ? jj : jj - nj + N;
+  const int bs = (b <= N / 2) ? b : N - b;
+  const long long fstride = (long long)(Kc + 1) * nj * N;
+  C *o0 = reinterpret_cast<C *>(pz) + ((long long)k * nj + jj) * N;
+  C *o1 = o0 + fstride;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < N; a += gridDim.x * blockDim.x) {
+    const int as = (a <= N / 2) ? a : N - a;
+    C p, d;
+    p.x = p.y = d.x = d.y = (S)0;
+    if (as <= Ka) {
+      const int s2 = as * as + bs * bs + k * k;
+      const double tp = table[2 * s2], td = table[2 * s2 + 1];
+      const C r = reinterpret_cast<const C *>(R)[((long long)a * N + b) * nh + k];
+      p.x = (S)((double)r.x * tp);
+      p.y = (S)((double)r.y * tp);
+      d.x = (S)((double)r.x * td);
+      d.y = (S)((double)r.y * td);
+    }
+    o0[a] = p;
+    o1[a] = d;
+  }
+}
+
+// Pass-B input: pz_b[f][k][a][b] = pz_a[f][k][jj(b)][a] for b in the box, else 0.
+template <typename S>
+__global__ void k_prune_b(const S *__restrict__ pa, S *__restrict__ pb, int N, int Kb, int Kc) {
+  using C = typename Cplx<S>::T;
+  const int nj = 2 * Kb + 1;
+  const int a = blockIdx.y, fk = blockIdx.z;  // fk = f * (Kc + 1) + k
+  const C *in = reinterpret_cast<const C *>(pa) + (long long)fk * nj * N;
+  C *out = reinterpret_cast<C *>(pb) + ((long long)fk * N + a) * N;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < N; b += gridDim.x * blockDim.x) {
+    C v;
+    v.x = v.y = (S)0;
+    const int jj = (b <= Kb) ? b : (b >= N - Kb ? b - N + nj : -1);
+    if (jj >= 0) v = in[(long long)jj * N + a];
+    out[b] = v;
+  }
+}
+
+// Pass-C input (the HC rows of the 1-D C2R): pc[f][a][b][k] = pz_b[f][k][a][b] for
+// k <= Kc, 0 up to N/2.  Block: one (f, a) and 32 consecutive b; the (Kc+1) x 32
+// tile goes through shared memory so both sides are coalesced.
+template <typename S>
+__global__ void __launch_bounds__(256) k_prune_c(const S *__restrict__ pb, S *__restrict__ pc, int N, int Kc) {
+  using C = typename Cplx<S>::T;
+  extern __shared__ unsigned char smraw[];
+  C *tile = reinterpret_cast<C *>(smraw);  // [Kc+1][33]
+  const int nh = N / 2 + 1;
+  const int b0 = blockIdx.x * 32, a = blockIdx.y, f = blockIdx.z;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int k = ty; k <= Kc; k += 8)
+    tile[k * 33 + tx] = reinterpret_cast<const C *>(pb)[(((long long)f * (Kc + 1) + k) * N + a) * N + b0 + tx];
+  __syncthreads();
+  C *outbase = reinterpret_cast<C *>(pc) + (((long long)f * N + a) * N + b0) * nh;
+  for (int bb = ty; bb < 32; bb += 8) {
+    C *row = outbase + (long long)bb * nh;
+    for (int k = tx; k < nh; k += 32) {
+      C v;
+      v.x = v.y = (S)0;
+      if (k <= Kc) v = tile[k * 33 + bb];
+      row[k] = v;
+    }
+  }
+}
+
 template <typename S>
 __global__ void k_copy_convert(const double *__restrict__ in, S *__restrict__ out, long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -136,6 +246,102 @@ int ensure_psi(cf_ctx *ctx) {
   return CF_OK;
 }
 
+static void free_pruned(cf_ctx *ctx) {
+  if (!ctx->have_pruned) return;
+  cudaFree(ctx->pz_a);
+  cudaFree(ctx->pz_b);
+  cufftDestroy(ctx->plan_pa);
+  cufftDestroy(ctx->plan_pb);
+  cufftDestroy(ctx->plan_pc);
+  ctx->pz_a = ctx->pz_b = nullptr;
+  ctx->have_pruned = false;
+}
+
+void psi_release(cf_ctx *ctx) { free_pruned(ctx); }
+
+static int ensure_pruned(cf_ctx *ctx) {
+  if (ctx->have_pruned && ctx->pr_Ka == ctx->Ka && ctx->pr_Kb == ctx->Kb && ctx->pr_Kc == ctx->Kc) return CF_OK;
+  free_pruned(ctx);
+  const long long N = ctx->N, nh = N / 2 + 1;
+  const long long nj = 2 * ctx->Kb + 1, nk = ctx->Kc + 1;
+  const size_t cb = 2 * ctx->word;  // bytes per complex
+  if (cudaMalloc(&ctx->pz_a, 2 * nk * nj * N * cb) != cudaSuccess ||
+      cudaMalloc(&ctx->pz_b, 2 * nk * N * N * cb) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMalloc of the pruned Psi buffers failed");
+    return CF_ERR_NOMEM;
+  }
+  const bool dp = ctx->word == 8;
+  long long n1[1] = {N};
+  size_t work = 0;
+  CF_TRY_CUFFT(cufftCreate(&ctx->plan_pa));
+  CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pa, 1, n1, nullptr, 1, N, nullptr, 1, N, dp ? CUFFT_Z2Z : CUFFT_C2C,
+                                   2 * nk * nj, &work));
+  CF_TRY_CUFFT(cufftCreate(&ctx->plan_pb));
+  CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pb, 1, n1, nullptr, 1, N, nullptr, 1, N, dp ? CUFFT_Z2Z : CUFFT_C2C,
+                                   2 * nk * N, &work));
+  long long ie[1] = {nh}, oe[1] = {N};
+  CF_TRY_CUFFT(cufftCreate(&ctx->plan_pc));
+  CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pc, 1, n1, ie, 1, nh, oe, 1, N, dp ? CUFFT_Z2D : CUFFT_C2R, 2 * N * N,
+                                   &work));
+  ctx->have_pruned = true;
+  ctx->pr_Ka = ctx->Ka;
+  ctx->pr_Kb = ctx->Kb;
+  ctx->pr_Kc = ctx->Kc;
+  return CF_OK;
+}
+
+template <typename S>
+static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
+  const int N = (int)ctx->N, Ka = ctx->Ka, Kb = ctx->Kb, Kc = ctx->Kc;
+  const int nj = 2 * Kb + 1;
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+    k_prune_a<S><<<dim3((N + 255) / 256, nj, Kc + 1), 256, 0, st>>>((const S *)ctx->R_fft, ctx->psi_table,
+                                                                    (S *)ctx->pz_a, N, Ka, Kb, Kc);
+    CF_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    CF_TRY_CUFFT(cufftSetStream(ctx->plan_pa, st));
+    if (ctx->word == 8)
+      CF_TRY_CUFFT(cufftExecZ2Z(ctx->plan_pa, (cufftDoubleComplex *)ctx->pz_a, (cufftDoubleComplex *)ctx->pz_a,
+                                CUFFT_INVERSE));
+    else
+      CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pa, (cufftComplex *)ctx->pz_a, (cufftComplex *)ctx->pz_a, CUFFT_INVERSE));
+  }
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+    k_prune_b<S><<<dim3((N + 255) / 256, N, 2 * (Kc + 1)), 256, 0, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b, N, Kb,
+                                                                         Kc);
+    CF_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    CF_TRY_CUFFT(cufftSetStream(ctx->plan_pb, st));
+    if (ctx->word == 8)
+      CF_TRY_CUFFT(cufftExecZ2Z(ctx->plan_pb, (cufftDoubleComplex *)ctx->pz_b, (cufftDoubleComplex *)ctx->pz_b,
+                                CUFFT_INVERSE));
+    else
+      CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pb, (cufftComplex *)ctx->pz_b, (cufftComplex *)ctx->pz_b, CUFFT_INVERSE));
+  }
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+    const size_t smem = (size_t)(Kc + 1) * 33 * 2 * sizeof(S);
+    k_prune_c<S><<<dim3(N / 32, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)ctx->psi_hc, N, Kc);
+    CF_LAUNCHED(ctx);
+  }
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    CF_TRY_CUFFT(cufftSetStream(ctx->plan_pc, st));
+    if (ctx->word == 8)
+      CF_TRY_CUFFT(cufftExecZ2D(ctx->plan_pc, (cufftDoubleComplex *)ctx->psi_hc, (cufftDoubleReal *)out));
+    else
+      CF_TRY_CUFFT(cufftExecC2R(ctx->plan_pc, (cufftComplex *)ctx->psi_hc, (cufftReal *)out));
+  }
+  return CF_OK;
+}
+
 int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void **dpsi) {
   CF_TRY(ensure_psi(ctx));
   for (auto &s : ctx->slot) {
@@ -154,12 +360,28 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void 
   const double H_t = cosmo_H(ctx->p, t);
   const double factor = (2 * 3.14159265358979323846 / ctx->p.L) * eta_t / sqrt(3);
   const long long pairs = ctx->hc_count / 2;
-  CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
   {
     ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
     unsigned tb = (unsigned)std::min<long long>((ctx->s2_bins + 255) / 256, 148LL * 8);
     k_transfer_table<<<tb, 256, 0, st>>>(ctx->psi_table, ctx->s2_bins, (int)ctx->N, factor, H_t);
     CF_LAUNCHED(ctx);
+  }
+  if (ctx->pruned) {
+    CF_TRY(ensure_pruned(ctx));
+    if (ctx->word == 8)
+      CF_TRY(refresh_pruned<double>(ctx, v->psi, st));
+    else
+      CF_TRY(refresh_pruned<float>(ctx, v->psi, st));
+    v->t = t;
+    v->valid = true;
+    v->stamp = ++ctx->slot_clock;
+    *psi = v->psi;
+    *dpsi = v->dpsi;
+    return CF_OK;
+  }
+  CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
+  {
+    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
     const int nh = (int)ctx->N / 2 + 1;
     const dim3 tg((unsigned)((nh + 255) / 256), (unsigned)ctx->N, (unsigned)ctx->N);
     if (ctx->word == 8)
@@ -220,6 +442,28 @@ int set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, cudaStream_t st) 
   }
   if (tmp) CF_TRY_CUDA(cudaFreeAsync(tmp, st));
   for (auto &s : ctx->slot) s.valid = false;
+  // support of the new R_fft: decides between the pruned and the full synthesis
+  int *d_box = nullptr;
+  CF_TRY_CUDA(cudaMallocAsync((void **)&d_box, 3 * sizeof(int), st));
+  CF_TRY_CUDA(cudaMemsetAsync(d_box, 0xff, 3 * sizeof(int), st));  // -1
+  const dim3 sg(1, (unsigned)ctx->N, (unsigned)ctx->N);
+  if (w == 8)
+    k_support<double><<<sg, 128, 0, st>>>((const double *)ctx->R_fft, (int)ctx->N, d_box);
+  else
+    k_support<float><<<sg, 128, 0, st>>>((const float *)ctx->R_fft, (int)ctx->N, d_box);
+  CF_LAUNCHED(ctx);
+  int box[3];
+  CF_TRY_CUDA(cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, st));
+  CF_TRY_CUDA(cudaFreeAsync(d_box, st));
+  CF_TRY_CUDA(cudaStreamSynchronize(st));
+  ctx->Ka = std::max(box[0], 0);
+  ctx->Kb = std::max(box[1], 0);
+  ctx->Kc = std::max(box[2], 0);
+  const int N = (int)ctx->N;
+  // pruned when the box is small against the lattice: passes A and B then touch a
+  // small fraction of the lines, and pass C's transpose tile fits shared memory
+  ctx->pruned = !(ctx->p.flags & CF_FLAG_FULL_PSI_FFT) && N % 32 == 0 && 2 * ctx->Ka + 1 <= N / 2 &&
+                2 * ctx->Kb + 1 <= N / 2 && ctx->Kc + 1 <= 64 && ctx->Kc + 1 <= N / 4;
   return CF_OK;
 }
 

@@ -74,8 +74,13 @@ typedef struct cf_params {
   int32_t equation;  /* cf_equation */
   int32_t precision; /* cf_precision */
   int32_t stencil;   /* 7 (reference) or 13 (fourth-order Laplacian) */
-  int32_t flags;     /* reserved, 0 */
+  int32_t flags;     /* CF_FLAG_* bits, 0 = defaults */
 } cf_params;
+
+/* Always synthesise Psi / dPsi/dt with the full 3-D C2R, even when R_fft is
+ * band-limited (the pruned synthesis is used by default when R_fft is exactly
+ * zero outside a small box of modes; both give the same fields to rounding). */
+#define CF_FLAG_FULL_PSI_FFT 1
 
 typedef struct cf_ctx cf_ctx;
 

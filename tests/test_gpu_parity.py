@@ -78,6 +78,33 @@ def test_rk4_fp64_matches_oracle(eq, stencil):
     assert rel(got[N ** 3:], want[N ** 3:]) <= 1e-12
 
 
+@pytest.mark.parametrize("prec,tol", [(cfb200.FP64, 1e-13), (cfb200.FP32_COMP, 1e-6)])
+@pytest.mark.parametrize("k_max", [1.0, 2.5])
+def test_pruned_psi_synthesis_equals_full(prec, tol, k_max):
+    """A band-limited R_fft (exact zeros beyond k_max) takes the pruned three-pass
+    synthesis when its support box is small (k_max = 1: |i| <= 10 at N = 64) and
+    the full 3-D C2R otherwise (k_max = 2.5); the flag CF_FLAG_FULL_PSI_FFT forces
+    the full C2R.  Both give the same fields and the same trajectory."""
+    N, L = 64, 64.0
+    x, _ = make_inputs(N, L, 1, 5)
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=8)
+    out = []
+    for flags in (0, cfb200.FLAG_FULL_PSI_FFT):
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=prec, flags=flags, **FRW)
+        c.set_R_fft(Rf, on_device=False)
+        st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+        c.upload(st, x)
+        c.rk4_steps(st, 1.0, 0.05, 6)
+        rho = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
+        c.energy_density(st, 1.3, rho)
+        got = np.empty_like(x)
+        c.download(got, st)
+        torch.cuda.synchronize()
+        out.append((got, rho.cpu().numpy()))
+    assert rel(out[0][0], out[1][0]) <= tol
+    assert rel(out[0][1], out[1][1]) <= tol
+
+
 @pytest.mark.parametrize("eq", [0, 1, 2])
 def test_rk4_split_calls_equal_one_call(eq):
     """step0 offsets reproduce integrate_const's direct time t0 + step*dt."""
