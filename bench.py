@@ -238,6 +238,66 @@ def make_case(N, L, precision, stencil, comoving, use_torch_inputs=True):
     return ctx, st
 
 
+def ensemble_bench(steps=100, per_segment=50):
+    """Config 3: 96 FRW Klein-Gordon lattices (32 x 64^3, 32 x 96^3, 32 x 128^3),
+    L = N, m ~ U[0.5, 2] (seed 12345), GRF initial fields (k* = 0.5, <phi^2> = 1,
+    dphi = 0, seeds 1000 + i), FP32-comp, 7-point, dt = 0.1 from t = 1, density
+    spectra every 50 steps.  The same `steps` are timed as (a) CUDA-graph replays
+    of the persistent kernel (+ the spectra) and (b) one launch per stage per
+    member (the single-instance path)."""
+    import numpy as np
+    import torch
+
+    import cfb200
+    from cfb200 import fields
+    rng = np.random.default_rng(12345)
+    sizes = [64] * 32 + [96] * 32 + [128] * 32
+    spec = [dict(N=n, L=float(n), m=float(rng.uniform(0.5, 2.0)), equation=cfb200.EQ_KG_FRW,
+                 precision=cfb200.FP32_COMP, stencil=7, **FRW) for n in sizes]
+    ens = cfb200.Ensemble(spec)
+    tune = ens.autotune(1.0, 0.1, steps=2)
+    x0 = [fields.initial_state(d["N"], d["L"], 0.5, 1000 + i, use_torch=True).cpu().numpy()
+          for i, d in enumerate(spec)]
+    sites = sum(n ** 3 for n in sizes)
+    out = torch.empty((steps // per_segment) * ens.spectra_total, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    res = {"members": len(sizes), "sites": sites, "steps": steps, "autotune": {"shape": tune[0], "a_chunk": tune[1]},
+           "work_items": ens.work_items}
+    for name in ("graph_persistent", "loop_single_launches", "batched_launches"):
+        for i, x in enumerate(x0):
+            ens.upload(i, x)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = ens.launches
+        with torch.cuda.stream(stream):
+            if name == "graph_persistent":
+                ens.run_graph(1.0, 0.1, per_segment, 1, None, stream=stream)  # capture + warm
+                for i, x in enumerate(x0):
+                    ens.upload(i, x, stream=stream)
+                e0.record(stream)
+                ens.run_graph(1.0, 0.1, per_segment, steps // per_segment, out, stream=stream)
+                e1.record(stream)
+            else:
+                mode = cfb200.ENS_LOOP if name == "loop_single_launches" else cfb200.ENS_BATCHED
+                ens.rk4_steps(1.0, 0.1, 2, mode=mode, stream=stream)  # warm
+                for i, x in enumerate(x0):
+                    ens.upload(i, x, stream=stream)
+                e0.record(stream)
+                for s in range(steps // per_segment):
+                    ens.rk4_steps(1.0, 0.1, per_segment, step0=s * per_segment, mode=mode, stream=stream)
+                    ens.density_spectra_s2(1.0 + (s + 1) * per_segment * 0.1,
+                                           out[s * ens.spectra_total:], stream=stream)
+                e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name] = {"site_updates_per_s": sites * steps / (ms * 1e-3), "ms": ms, "launches": ens.launches - l0}
+    res["graph_vs_loop"] = res["graph_persistent"]["site_updates_per_s"] / res["loop_single_launches"]["site_updates_per_s"]
+    ens.close()
+    torch.cuda.empty_cache()
+    return res
+
+
 def time_steps(ctx, st, steps, warmup, profile=False):
     import torch
     W = WORKLOAD
@@ -336,6 +396,12 @@ def run_product(args):
                            "stage_kernels_gbs": bb * N ** 3 * ks / (sm * 1e-3) / 1e9}
         del c2, s2_
         torch.cuda.empty_cache()
+
+    # ---- config 3: ensemble of uneven N in one captured persistent launch per interval
+    try:
+        secondary["ensemble_config3"] = ensemble_bench()
+    except Exception as e:  # reported, not hidden
+        secondary["ensemble_config3"] = {"error": str(e)}
 
     # ---- end to end through the C ABI with host buffers: one observer interval
     # (dt_save = 5 -> 100 RK4 steps) per e2e step: upload the state from pinned
