@@ -179,6 +179,49 @@ int launch_forward_stage(cf_ctx *ctx, int stage, const void *yin, void *yout, vo
   return forward_stage_t<double>(ctx, stage, yin, yout, x, xlo, t, cy, dt6, st);
 }
 
+// One RK4 step of the uncoupled equations with caller-provided accumulator and
+// stage buffers (acc, ya, yb: 2N^3 words each of the storage type); allocates
+// nothing.  Same kernels and coefficients as rk4_steps.
+template <typename S>
+static int rk4_step_buffers_t(cf_ctx *ctx, void *d_state, void *acc, void *ya, void *yb, double t, double dt,
+                              cudaStream_t st) {
+  const long long N3 = ctx->N3;
+  S *x = (S *)d_state;
+  StageArgs<S> A{};
+  A.N = (int)ctx->N;
+  A.N3 = N3;
+  A.m2 = ctx->p.m * ctx->p.m;
+  A.x = x;
+  A.xlo = (sizeof(S) == 4) ? x + 2 * N3 : nullptr;
+  A.acc = (S *)acc;
+  const double dh = dt / 2.0;
+  A.dt6 = dt / 6.0;
+  CF_TRY(fill_stage_coeffs(ctx, A, t, st));
+  A.yin = x;
+  A.yout = (S *)ya;
+  A.cy = dh;
+  CF_TRY(launch_stage<S, 1>(ctx, A, st));
+  CF_TRY(fill_stage_coeffs(ctx, A, t + dh, st));
+  A.yin = (const S *)ya;
+  A.yout = (S *)yb;
+  A.cy = dh;
+  CF_TRY(launch_stage<S, 2>(ctx, A, st));
+  A.yin = (const S *)yb;
+  A.yout = (S *)ya;
+  A.cy = dt;
+  CF_TRY(launch_stage<S, 3>(ctx, A, st));
+  CF_TRY(fill_stage_coeffs(ctx, A, t + dt, st));
+  A.yin = (const S *)ya;
+  A.yout = nullptr;
+  return launch_stage<S, 4>(ctx, A, st);
+}
+
+int rk4_step_buffers(cf_ctx *ctx, void *d_state, void *acc, void *ya, void *yb, double t, double dt,
+                     cudaStream_t st) {
+  if (ctx->p.precision == CF_FP32_COMP) return rk4_step_buffers_t<float>(ctx, d_state, acc, ya, yb, t, dt, st);
+  return rk4_step_buffers_t<double>(ctx, d_state, acc, ya, yb, t, dt, st);
+}
+
 int rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, cudaStream_t st) {
   if (ctx->p.precision == CF_FP32_COMP) return rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st);
   return rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);

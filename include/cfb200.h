@@ -130,6 +130,22 @@ int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream);
 int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
                  void *stream);
 
+/* The same stepping as cf_rk4_steps for callers that must not allocate device
+ * memory -- applications that hand all device memory to their own pool and
+ * forbid library allocations, or loops that cannot take cudaMalloc's
+ * synchronisation or its failure mid-run.  No counterpart in the reference.
+ * The three RK4 work buffers come from a fixed 24 MiB array compiled into the
+ * library (held by every GPU that loads it until exit) instead of the context:
+ * N <= 80 in CF_FP64, N <= 96 in CF_FP32_COMP, CF_EQ_KG / CF_EQ_KG_FRW only;
+ * anything else is rejected (CF_ERR_INVALID / CF_ERR_UNSUPPORTED).  All calls on
+ * a device share the array, which keeps the last call's contents (nothing needs
+ * clearing: each step writes every entry before reading it); calls whose GPU work
+ * overlaps race and must be serialised by the caller.  The first call on a device
+ * looks up the array's device address with that device current: make it before
+ * any stream capture.  Calls no cudaMalloc, cudaFree or allocating library routine. */
+int cf_rk4_steps_noalloc(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
+                         void *stream);
+
 /* ---- odeint building blocks (FP64 device arrays of 2N^3) --------------------
  * cf_rhs: dxdt = Equation(x, t)  (Equation::operator(), src/equations_cuda.cu:522-534,
  * :678-731).  cf_scale_sum: out = sum_i alpha_i * in_i over len doubles
@@ -233,7 +249,6 @@ int cf_ensemble_run_graph(cf_ensemble *ens, double t0, double dt, int64_t steps_
                           double *d_spectra, void *stream);
 int cf_ensemble_autotune(cf_ensemble *ens, double t0, double dt, int64_t steps, void *stream, int *h_shape,
                          int *h_a_chunk);
-
 /* ---- profiling ----------------------------------------------------------------
  * When enabled, every kernel (or cuFFT call) the context launches is bracketed by
  * a pair of CUDA events on its stream and its device time is accumulated per
