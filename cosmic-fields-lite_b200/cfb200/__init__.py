@@ -27,6 +27,7 @@ STATUS = {0: "CF_OK", -1: "CF_ERR_INVALID", -2: "CF_ERR_CUDA", -3: "CF_ERR_CUFFT
 EQ_KG, EQ_KG_FRW, EQ_COMOVING_FRW = 0, 1, 2
 FP64, FP32_COMP = 0, 1
 FLAG_FULL_PSI_FFT = 1
+PSI_NONE, PSI_FULL, PSI_PRUNED, PSI_PRUNED_FUSED = 0, 1, 2, 3
 
 
 class CfError(RuntimeError):
@@ -44,7 +45,8 @@ class cf_params(ctypes.Structure):
 
 class cf_info(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int64), ("state_bytes", ctypes.c_int64), ("field_count", ctypes.c_int64),
-                ("hc_count", ctypes.c_int64), ("s2_bins", ctypes.c_int64), ("shells", ctypes.c_int64)]
+                ("hc_count", ctypes.c_int64), ("s2_bins", ctypes.c_int64), ("shells", ctypes.c_int64),
+                ("psi_route", ctypes.c_int64)]
 
 
 _vp = ctypes.c_void_p
@@ -63,6 +65,7 @@ _SIGS = {
     "cf_state_import": ([_vp, _vp, _vp, _vp], _i),
     "cf_state_export": ([_vp, _vp, _vp, _vp], _i),
     "cf_set_R_fft": ([_vp, _vp, _i, _vp], _i),
+    "cf_psi_fields": ([_vp, _d, _vp, _vp], _i),
     "cf_rk4_steps": ([_vp, _vp, _d, _d, _i64, _i64, _vp], _i),
     "cf_rhs": ([_vp, _vp, _vp, _d, _vp], _i),
     "cf_scale_sum": ([_vp, _vp, _i, _vp, _vp, _i64, _vp], _i),
@@ -89,8 +92,9 @@ _SIGS = {
     "cf_ensemble_state_download": ([_vp, _i, _vp, _vp], _i),
     "cf_ensemble_rk4_steps": ([_vp, _d, _d, _i64, _i64, _i, _vp], _i),
     "cf_ensemble_density_spectra_s2": ([_vp, _d, _vp, _vp], _i),
-    "cf_ensemble_run_graph": ([_vp, _d, _d, _i64, _i64, _vp, _vp], _i),
+    "cf_ensemble_run_graph": ([_vp, _d, _d, _i64, _i64, _i, _vp, _vp], _i),
     "cf_ensemble_autotune": ([_vp, _d, _d, _i64, _vp, ctypes.POINTER(_i), ctypes.POINTER(_i)], _i),
+    "cf_ensemble_set_barrier_test": ([_vp, _i, _i64], _i),
     "cf_profile_enable": ([_vp, _i], _i),
     "cf_profile_read": ([_vp, _vp], _i),
     "cf_profile_reset": ([_vp], _i),
@@ -168,10 +172,14 @@ class Context:
         h = ctypes.c_void_p()
         check(lib().cf_create(ctypes.byref(self.params), ctypes.byref(h)))
         self.h = h
+        self.N = int(N)
+
+    @property
+    def info(self):
+        """cf_get_info, read afresh (psi_route follows cf_set_R_fft)."""
         info = cf_info()
         check(lib().cf_get_info(self.h, ctypes.byref(info)))
-        self.info = info
-        self.N = int(N)
+        return info
 
     def close(self):
         if getattr(self, "h", None):
@@ -209,6 +217,10 @@ class Context:
 
     def set_R_fft(self, R_fft, on_device, stream=None):
         check(lib().cf_set_R_fft(self.h, _ptr(R_fft), int(on_device), _stream(stream)))
+
+    def psi_fields(self, t, d_out, stream=None):
+        """Psi and dPsi/dt at time t into d_out (2 N^3 doubles on the device)."""
+        check(lib().cf_psi_fields(self.h, float(t), _ptr(d_out), _stream(stream)))
 
     # ---- hot path
     def rk4_steps(self, d_state, t0, dt, nsteps, step0=0, stream=None):
@@ -359,9 +371,12 @@ class Ensemble:
     def density_spectra_s2(self, t, d_out, stream=None):
         check(lib().cf_ensemble_density_spectra_s2(self.h, float(t), _ptr(d_out), _stream(stream)))
 
-    def run_graph(self, t0, dt, steps_per_segment, nsegments, d_spectra=None, stream=None):
+    def run_graph(self, t0, dt, steps_per_segment, nsegments, d_spectra=None, stream=None, mode=ENS_BATCHED):
         check(lib().cf_ensemble_run_graph(self.h, float(t0), float(dt), int(steps_per_segment), int(nsegments),
-                                          _ptr(d_spectra), _stream(stream)))
+                                          int(mode), _ptr(d_spectra), _stream(stream)))
+
+    def set_barrier_test(self, extra_arrivals, spin_limit=1 << 24):
+        check(lib().cf_ensemble_set_barrier_test(self.h, int(extra_arrivals), int(spin_limit)))
 
     def autotune(self, t0, dt, steps=2, stream=None):
         shape, chunk = _i(0), _i(0)

@@ -264,6 +264,7 @@ int cf_get_info(const cf_ctx *ctx, cf_info *info) {
   info->hc_count = ctx->hc_count;
   info->s2_bins = ctx->s2_bins;
   info->shells = ctx->shells;
+  info->psi_route = psi_route(ctx);
   return CF_OK;
 }
 
@@ -334,6 +335,17 @@ int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream) 
   CF_TRY(check_ptr(R_fft, "R_fft", 8));
   CF_TRY(use_device(ctx));
   return set_R_fft(ctx, R_fft, on_device, (cudaStream_t)stream);
+}
+
+int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_out, "d_out", 8));
+  if (ctx->p.equation != CF_EQ_COMOVING_FRW || !ctx->R_fft) {
+    set_error("cf_psi_fields: comoving-curvature equation with R_fft set required");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  return psi_fields(ctx, t, d_out, (cudaStream_t)stream);
 }
 
 int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, void *stream) {

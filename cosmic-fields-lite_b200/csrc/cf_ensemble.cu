@@ -62,7 +62,10 @@ struct EnsArgs {
   double dt;
   unsigned *bar_count;
   unsigned *bar_gen;
+  unsigned *work;  // next work item of the current stage (persistent kernel)
   int *err;
+  unsigned bar_extra;    // arrivals the barrier waits for beyond the grid (0; > 0 only in failure tests)
+  long long spin_limit;  // bounded wait of the barrier, in sleep iterations
 };
 
 // Tile shapes compiled for the ensemble kernels (threads along c x along b).
@@ -135,8 +138,9 @@ __device__ __forceinline__ bool grid_barrier(const EnsArgs &E) {
     const unsigned g = *gen;
     __threadfence();
     const unsigned arrived = atomicAdd(E.bar_count, 1u) + 1u;
-    if (arrived == gridDim.x) {
+    if (arrived == gridDim.x + E.bar_extra) {
       *E.bar_count = 0u;
+      *E.work = 0u;  // every CTA has left the stage's fetch loop
       __threadfence();
       atomicAdd((unsigned *)E.bar_gen, 1u);
     } else {
@@ -146,7 +150,7 @@ __device__ __forceinline__ bool grid_barrier(const EnsArgs &E) {
           ok = 0;
           break;
         }
-        if (++spins > (1LL << 24)) {  // ~ seconds with the sleep below
+        if (++spins > E.spin_limit) {  // default 2^24: seconds with the sleep below
           atomicExch(E.err, 1);
           ok = 0;
           break;
@@ -160,25 +164,55 @@ __device__ __forceinline__ bool grid_barrier(const EnsArgs &E) {
   return ok != 0;
 }
 
+// Resident CTAs per SM that the ensemble kernels' register allocation must
+// allow (per-stage kernel, persistent kernel).  Uncapped, the persistent kernel,
+// which inlines all four stages, takes ~180 registers in FP32: one CTA per SM.
+// Measured on B200, 96 FRW lattices 32 x {64,96,128}^3, FP32-comp 7-point
+// (G site-updates/s, per-stage batched / persistent graph):
+//   caps 1/1: 17.6 / 17.2;  2/2: 28.9 / 26.3;  3/3: 33.9 / 24.8 (persistent spills).
+#ifndef CF_ENS_MIN_BLOCKS
+#define CF_ENS_MIN_BLOCKS 3
+#endif
+#ifndef CF_ENS_PERSIST_MIN_BLOCKS
+#define CF_ENS_PERSIST_MIN_BLOCKS 2
+#endif
+
+// One stage of the persistent kernel: CTAs take work items from a shared
+// counter (the items differ in cost: edge tiles, a-chunk remainders), then meet
+// at the grid barrier, whose last arrival resets the counter.
 template <typename S, int H, int SHAPE>
-__global__ void __launch_bounds__(256) k_ens_persistent(const EnsArgs E) {
+__device__ __forceinline__ bool ens_stage_pass(const EnsArgs &E, int stage, long long step, S *sm) {
+  __shared__ int next;
+  for (;;) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) next = (int)atomicAdd(E.work, 1u);
+    __syncthreads();
+    const int i = next;
+    if (i >= E.n_items) break;
+    // stage_tile synchronises the CTA before it returns, so `next` is read by
+    // all threads before thread 0 overwrites it
+    ens_item_stage<S, H, SHAPE>(E, E.items[i], stage, step, sm);
+  }
+  return grid_barrier(E);
+}
+
+template <typename S, int H, int SHAPE>
+__global__ void __launch_bounds__(256, CF_ENS_PERSIST_MIN_BLOCKS) k_ens_persistent(const EnsArgs E) {
   constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
   __shared__ S sm[TileSmem<S, H, TXv, TYv>::count];
   const long long step0 = *E.step_counter;
   for (int j = 0; j < E.nsteps; ++j) {
-    for (int stage = 1; stage <= 4; ++stage) {
-      for (int i = blockIdx.x; i < E.n_items; i += gridDim.x)
-        ens_item_stage<S, H, SHAPE>(E, E.items[i], stage, step0 + j, sm);
-      if (!grid_barrier(E)) return;
-    }
+    for (int stage = 1; stage <= 4; ++stage)
+      if (!ens_stage_pass<S, H, SHAPE>(E, stage, step0 + j, sm)) return;
   }
 }
 
 template <typename S, int H, int SHAPE>
-__global__ void __launch_bounds__(256) k_ens_stage(const EnsArgs E, int stage, long long step) {
+// One stage over the work list, one CTA per item; the step is the device step
+// counter plus `step_off`, so a captured graph of these launches walks forward.
+__global__ void __launch_bounds__(256, CF_ENS_MIN_BLOCKS) k_ens_stage(const EnsArgs E, int stage, int step_off) {
   constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
   __shared__ S sm[TileSmem<S, H, TXv, TYv>::count];
-  ens_item_stage<S, H, SHAPE>(E, E.items[blockIdx.x], stage, step, sm);
+  ens_item_stage<S, H, SHAPE>(E, E.items[blockIdx.x], stage, *E.step_counter + step_off, sm);
 }
 
 __global__ void k_counter_add(long long *c, long long v) {
@@ -233,7 +267,7 @@ struct cf_ensemble {
   long long coef_cap = 0;
   double coef_t0 = 0, coef_dt = 0;
   long long *d_step = nullptr;
-  unsigned *d_bar = nullptr;  // count, gen
+  unsigned *d_bar = nullptr;  // count, gen, work
   int *d_err = nullptr;
   // spectra per size class
   struct Cls {
@@ -254,7 +288,11 @@ struct cf_ensemble {
   long long g_steps = 0;
   double g_t0 = 0, g_dt = 0;
   double *g_out = nullptr;
+  int g_mode = -1;
+  int64_t g_kernels = 0;  // kernels in one replay of the graph
   bool graph_failed = false;  // capture of the cooperative launch unavailable on this driver
+  unsigned bar_extra = 0;
+  long long spin_limit = 1LL << 24;
   int64_t launches = 0;
   int coop_blocks = 0;
 };
@@ -343,7 +381,10 @@ static int launch_persistent(cf_ensemble *E, int nsteps, double dt, cudaStream_t
   A.dt = dt;
   A.bar_count = E->d_bar;
   A.bar_gen = E->d_bar + 1;
+  A.work = E->d_bar + 2;
   A.err = E->d_err;
+  A.bar_extra = E->bar_extra;
+  A.spin_limit = E->spin_limit;
   void *args[] = {(void *)&A};
   const int blocks = std::min(E->coop_blocks, A.n_items);
   const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
@@ -353,15 +394,16 @@ static int launch_persistent(cf_ensemble *E, int nsteps, double dt, cudaStream_t
 }
 
 template <typename S, int H, int SHAPE>
-static int launch_batched_stage(cf_ensemble *E, int stage, long long step, double dt, cudaStream_t st) {
+static int launch_batched_stage(cf_ensemble *E, int stage, int step_off, double dt, cudaStream_t st) {
   EnsArgs A{};
   A.members = E->dm;
   A.items = E->d_items;
   A.n_items = (int)E->items.size();
   A.coef = E->d_coef;
+  A.step_counter = E->d_step;
   A.dt = dt;
   const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
-  k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, stage, step);
+  k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, stage, step_off);
   CF_TRY_CUDA(cudaGetLastError());
   E->launches++;
   return CF_OK;
@@ -369,9 +411,10 @@ static int launch_batched_stage(cf_ensemble *E, int stage, long long step, doubl
 
 template <typename S, int H, int SHAPE>
 static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, double dt, cudaStream_t st) {
+  CF_TRY_CUDA(cudaMemcpyAsync(E->d_step, &step0, sizeof(long long), cudaMemcpyHostToDevice, st));
   if (mode == CF_ENS_PERSISTENT) {
-    CF_TRY_CUDA(cudaMemcpyAsync(E->d_step, &step0, sizeof(long long), cudaMemcpyHostToDevice, st));
-    CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 2 * sizeof(unsigned), st));
+    CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 3 * sizeof(unsigned), st));
+    CF_TRY_CUDA(cudaMemsetAsync(E->d_err, 0, sizeof(int), st));
     CF_TRY(launch_persistent<S, H, SHAPE>(E, (int)nsteps, dt, st));
     int err = 0;
     CF_TRY_CUDA(cudaMemcpyAsync(&err, E->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -384,7 +427,7 @@ static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, do
   }
   if (mode == CF_ENS_BATCHED) {
     for (long long j = 0; j < nsteps; ++j)
-      for (int s = 1; s <= 4; ++s) CF_TRY((launch_batched_stage<S, H, SHAPE>(E, s, step0 + j, dt, st)));
+      for (int s = 1; s <= 4; ++s) CF_TRY((launch_batched_stage<S, H, SHAPE>(E, s, (int)j, dt, st)));
     return CF_OK;
   }
   // CF_ENS_LOOP: the single-instance path, member by member
@@ -400,9 +443,10 @@ static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, do
         A.items = E->d_items + i0;
         A.n_items = (int)(i1 - i0);
         A.coef = E->d_coef;
+        A.step_counter = E->d_step;
         A.dt = dt;
         const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
-        k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, s, step0 + j);
+        k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, s, (int)j);
         CF_TRY_CUDA(cudaGetLastError());
         E->launches++;
         i0 = i1;
@@ -426,11 +470,36 @@ static int run(cf_ensemble *E, int mode, long long step0, long long nsteps, doub
   return run_shape<double, 1>(E, mode, step0, nsteps, dt, st);
 }
 
-// One observer segment: barrier reset, persistent kernel over `steps` steps from
-// the device step counter, counter advance (graph-capturable).
-static int persistent_segment(cf_ensemble *E, long long steps, double dt, cudaStream_t st) {
-  CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 2 * sizeof(unsigned), st));
+template <typename S, int H>
+static int batched_launches(cf_ensemble *E, long long steps, double dt, cudaStream_t st) {
+  for (long long j = 0; j < steps; ++j)
+    for (int s = 1; s <= 4; ++s) {
+      if (E->shape == 1)
+        CF_TRY((launch_batched_stage<S, H, 1>(E, s, (int)j, dt, st)));
+      else
+        CF_TRY((launch_batched_stage<S, H, 0>(E, s, (int)j, dt, st)));
+    }
+  return CF_OK;
+}
+
+// One observer segment from the device step counter, then the counter advance
+// (graph-capturable: nothing is read from host memory).  CF_ENS_PERSISTENT: barrier
+// reset + the persistent kernel; CF_ENS_BATCHED: 4 launches per step.
+static int segment(cf_ensemble *E, int mode, long long steps, double dt, cudaStream_t st) {
   int s;
+  if (mode == CF_ENS_BATCHED) {
+    if (E->word == 4)
+      s = E->stencil == 13 ? batched_launches<float, 2>(E, steps, dt, st) : batched_launches<float, 1>(E, steps, dt, st);
+    else
+      s = E->stencil == 13 ? batched_launches<double, 2>(E, steps, dt, st)
+                           : batched_launches<double, 1>(E, steps, dt, st);
+    if (s != CF_OK) return s;
+    k_counter_add<<<1, 32, 0, st>>>(E->d_step, steps);
+    CF_TRY_CUDA(cudaGetLastError());
+    E->launches++;
+    return CF_OK;
+  }
+  CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 3 * sizeof(unsigned), st));
   if (E->word == 4) {
     if (E->stencil == 13)
       s = E->shape ? launch_persistent<float, 2, 1>(E, (int)steps, dt, st)
@@ -449,6 +518,7 @@ static int persistent_segment(cf_ensemble *E, long long steps, double dt, cudaSt
   if (s != CF_OK) return s;
   k_counter_add<<<1, 32, 0, st>>>(E->d_step, steps);
   CF_TRY_CUDA(cudaGetLastError());
+  E->launches++;
   return CF_OK;
 }
 
@@ -574,7 +644,7 @@ int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out) {
   }
   bool ok = cudaMalloc(&E->dm, sizeof(EnsMember) * count) == cudaSuccess &&
             cudaMalloc(&E->d_step, sizeof(long long)) == cudaSuccess &&
-            cudaMalloc(&E->d_bar, 2 * sizeof(unsigned)) == cudaSuccess &&
+            cudaMalloc(&E->d_bar, 3 * sizeof(unsigned)) == cudaSuccess &&
             cudaMalloc(&E->d_err, sizeof(int)) == cudaSuccess;
   if (!ok) {
     set_error("ensemble: device allocation failed");
@@ -584,7 +654,7 @@ int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out) {
     return CF_ERR_NOMEM;
   }
   cudaMemcpy(E->dm, E->hm.data(), sizeof(EnsMember) * count, cudaMemcpyHostToDevice);
-  cudaMemset(E->d_bar, 0, 2 * sizeof(unsigned));
+  cudaMemset(E->d_bar, 0, 3 * sizeof(unsigned));
   cudaMemset(E->d_err, 0, sizeof(int));
   cudaMemset(E->d_step, 0, sizeof(long long));
   build_items(E);
@@ -685,26 +755,33 @@ int cf_ensemble_density_spectra_s2(cf_ensemble *E, double t, double *d_out, void
 }
 
 int cf_ensemble_run_graph(cf_ensemble *E, double t0, double dt, int64_t steps_per_segment, int64_t nsegments,
-                          double *d_spectra, void *stream) {
+                          int mode, double *d_spectra, void *stream) {
   if (!E || steps_per_segment < 1 || nsegments < 0) return ens_fail("bad ensemble or segment sizes");
+  if (mode != CF_ENS_PERSISTENT && mode != CF_ENS_BATCHED) return ens_fail("run_graph: mode must be PERSISTENT or BATCHED");
+  if (mode == CF_ENS_BATCHED && steps_per_segment > (1 << 20)) return ens_fail("run_graph: too many steps per segment");
   cudaStream_t st = (cudaStream_t)stream;
   if (!st) return ens_fail("cf_ensemble_run_graph needs a non-default stream (graph capture)");
   CF_TRY(ensure_coef(E, t0, dt, steps_per_segment * std::max<int64_t>(nsegments, 1), st));
   CF_TRY(ensure_spectra(E));
   long long zero = 0;
   CF_TRY_CUDA(cudaMemcpyAsync(E->d_step, &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
-  // The graph holds one segment: barrier reset, the persistent kernel (its first
-  // step read from the device step counter) and the counter advance, so replaying
-  // the same graph walks the run forward.  Each segment's spectra are enqueued on
-  // the same stream after its replay (their a(t) differs per segment).
+  CF_TRY_CUDA(cudaMemsetAsync(E->d_err, 0, sizeof(int), st));
+  // The graph holds one segment (its first step read from the device step
+  // counter, which the segment advances), so replaying the same graph walks the
+  // run forward.  Each segment's spectra are enqueued on the same stream after its
+  // replay (their a(t) differs per segment).
   for (int64_t sgi = 0; sgi < nsegments; ++sgi) {
-    if (!E->graph_failed &&
-        (!E->gexec || E->g_steps != steps_per_segment || E->g_t0 != t0 || E->g_dt != dt || E->g_out != d_spectra)) {
+    const bool fallback = mode == CF_ENS_PERSISTENT && E->graph_failed;
+    if (!fallback && (!E->gexec || E->g_mode != mode || E->g_steps != steps_per_segment || E->g_t0 != t0 ||
+                      E->g_dt != dt || E->g_out != d_spectra)) {
       if (E->gexec) cudaGraphExecDestroy(E->gexec);
       E->gexec = nullptr;
       cudaGraph_t g = nullptr;
+      const int64_t l0 = E->launches;
       bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-      int s = ok ? persistent_segment(E, steps_per_segment, dt, st) : CF_ERR_CUDA;
+      int s = ok ? segment(E, mode, steps_per_segment, dt, st) : CF_ERR_CUDA;
+      E->g_kernels = E->launches - l0;
+      E->launches = l0;
       if (ok) ok = cudaStreamEndCapture(st, &g) == cudaSuccess && s == CF_OK;
       if (ok) ok = cudaGraphInstantiate(&E->gexec, g, 0) == cudaSuccess;
       if (g) cudaGraphDestroy(g);
@@ -714,8 +791,10 @@ int cf_ensemble_run_graph(cf_ensemble *E, double t0, double dt, int64_t steps_pe
         cudaGetLastError();
         if (E->gexec) cudaGraphExecDestroy(E->gexec);
         E->gexec = nullptr;
+        if (mode == CF_ENS_BATCHED) return ens_fail("run_graph: capture of the batched launches failed");
         E->graph_failed = true;
       } else {
+        E->g_mode = mode;
         E->g_steps = steps_per_segment;
         E->g_t0 = t0;
         E->g_dt = dt;
@@ -724,9 +803,9 @@ int cf_ensemble_run_graph(cf_ensemble *E, double t0, double dt, int64_t steps_pe
     }
     if (E->gexec) {
       CF_TRY_CUDA(cudaGraphLaunch(E->gexec, st));
-      E->launches++;
+      E->launches += E->g_kernels;
     } else {
-      CF_TRY(persistent_segment(E, steps_per_segment, dt, st));
+      CF_TRY(segment(E, mode, steps_per_segment, dt, st));
     }
     if (d_spectra) {
       const double t_end = t0 + (double)((sgi + 1) * steps_per_segment) * dt;
@@ -739,6 +818,17 @@ int cf_ensemble_run_graph(cf_ensemble *E, double t0, double dt, int64_t steps_pe
   if (err) {
     set_error("ensemble: grid barrier timed out");
     return CF_ERR_TIMEOUT;
+  }
+  return CF_OK;
+}
+
+int cf_ensemble_set_barrier_test(cf_ensemble *E, int extra_arrivals, int64_t spin_limit) {
+  if (!E || extra_arrivals < 0 || spin_limit < 1) return ens_fail("bad ensemble, extra_arrivals or spin_limit");
+  E->bar_extra = (unsigned)extra_arrivals;
+  E->spin_limit = spin_limit;
+  if (E->gexec) {  // a captured graph holds the old kernel arguments
+    cudaGraphExecDestroy(E->gexec);
+    E->gexec = nullptr;
   }
   return CF_OK;
 }

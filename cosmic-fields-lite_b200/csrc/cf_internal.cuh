@@ -90,6 +90,10 @@ struct cf_ctx {
   void *pz_a = nullptr, *pz_b = nullptr;
   cufftHandle plan_pa = 0, plan_pb = 0, plan_pc = 0;
   bool have_pruned = false;
+  // Pass C as one kernel (power-of-two N, 32..2048): twiddles e^{2 pi i j / N},
+  // j < N, in the storage complex type; no padded HC rows, no C2R plan.
+  bool pc_fused = false;
+  void *pr_wN = nullptr;
 
   // Spectra: FP64 R2C plans and scratch.
   cufftHandle plan_d2z1 = 0, plan_d2z2 = 0;
@@ -122,6 +126,10 @@ int ensure_psi(cf_ctx *ctx);
 // Returns the cached Psi / dPsi/dt slot for stage time t, refreshing one slot
 // (transfer kernel + batched C2R on `stream`) if t is not cached.
 int psi_at(cf_ctx *ctx, double t, cudaStream_t stream, const void **psi, const void **dpsi);
+// Psi and dPsi at t, widened to FP64, into d_out (2 N^3 doubles).
+int psi_fields(cf_ctx *ctx, double t, double *d_out, cudaStream_t stream);
+// CF_PSI_* route the next Psi refresh takes.
+int psi_route(const cf_ctx *ctx);
 // Frees the pruned-synthesis buffers and plans (context teardown).
 void psi_release(cf_ctx *ctx);
 

@@ -16,6 +16,7 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <vector>
 
 #include "cf_internal.cuh"
 
@@ -199,6 +200,217 @@ __global__ void __launch_bounds__(256) k_prune_c(const S *__restrict__ pb, S *__
   }
 }
 
+// ---- pass C as one kernel: pruned half-complex rows -> real rows ------------
+// For power-of-two N the C2R of pass C runs in one kernel that reads only the
+// Kc+1 non-zero entries of each row and writes the real row once (the cuFFT
+// route pads every row to N/2+1 entries in HBM and reads it back).
+//
+// A length-N C2R of a Hermitian row X[0..N/2] is an M = N/2 point complex
+// inverse DFT: with z[m] = x[2m] + i x[2m+1] and w = e^{2 pi i / N},
+//   Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) w^k,
+//   z[m] = sum_k Z[k] e^{2 pi i k m / M}          (unnormalised, like cuFFT).
+// With X zero beyond Kc < M/2 (the pruned box) this is
+//   Z[k]   = X[k] + i X[k] w^k                    for 0 <= k <= Kc,
+//   Z[M-j] = conj(X[j] - i X[j] w^j)              for 1 <= j <= Kc,
+// and zero in between; X[0] enters by its real part (the Hermitian projection
+// every C2R applies).  The M-point DFT is split M = R1 x R2 ("four-step"):
+//   pass 1: for each k2 < R2, an R1-point DFT over k1 of Z[k2 + R2 k1], times
+//           e^{2 pi i k2 m1 / M};
+//   pass 2: for each m1 < R1, an R2-point DFT over k2, giving z[m1 + R1 m2].
+// Each R-point DFT (R <= 32) runs in registers (radix-2, unrolled, twiddles
+// e^{2 pi i e / 32} from the kernel's parameter bank).  A CTA takes ROWS rows
+// (consecutive b of one (f, a)); between the passes the rows sit in shared
+// memory as T[m1][k2][r] with the row index fastest, padded to an odd m1
+// stride, so pass 1 stores and pass 2 loads are free of bank conflicts, and
+// pass 2's global stores run along m1, i.e. along the output row.
+
+template <typename S>
+struct Tw32 {
+  typename Cplx<S>::T w[16];  // e^{2 pi i e / 32}, e < 16
+};
+
+template <typename C>
+__device__ __forceinline__ C c_add(C a, C b) {
+  return C{a.x + b.x, a.y + b.y};
+}
+template <typename C>
+__device__ __forceinline__ C c_sub(C a, C b) {
+  return C{a.x - b.x, a.y - b.y};
+}
+template <typename C>
+__device__ __forceinline__ C c_mul(C a, C b) {
+  return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename C>
+__device__ __forceinline__ C c_mul_i(C a) {
+  return C{-a.y, a.x};
+}
+
+__host__ __device__ constexpr int bit_reverse(int i, int R) {
+  int r = 0;
+  for (int b = 1; b < R; b <<= 1) {
+    r = (r << 1) | (i & 1);
+    i >>= 1;
+  }
+  return r;
+}
+
+// In-register R-point inverse DFT (e^{+2 pi i k m / R}), natural order in and out.
+template <typename S, int R>
+__device__ __forceinline__ void dft_inv(typename Cplx<S>::T (&v)[R], const Tw32<S> &tw) {
+  static_assert(R >= 2 && R <= 32 && (R & (R - 1)) == 0, "radix");
+  using C = typename Cplx<S>::T;
+  C a[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) a[i] = v[bit_reverse(i, R)];
+#pragma unroll
+  for (int len = 2; len <= R; len *= 2) {
+#pragma unroll
+    for (int i = 0; i < R; i += len) {
+#pragma unroll
+      for (int j = 0; j < len / 2; ++j) {
+        const int e = j * (32 / len);  // e^{2 pi i j / len} = e^{2 pi i e / 32}
+        C t = a[i + j + len / 2];
+        if (e == 8)
+          t = c_mul_i(t);
+        else if (e != 0)
+          t = c_mul(t, tw.w[e]);
+        const C u = a[i + j];
+        a[i + j] = c_add(u, t);
+        a[i + j + len / 2] = c_sub(u, t);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = a[i];
+}
+
+template <typename S, int R1, int R2, int ROWS>
+__global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S *__restrict__ out,
+                                                     const typename Cplx<S>::T *__restrict__ wN, int N, int Kc,
+                                                     const __grid_constant__ Tw32<S> tw) {
+  using C = typename Cplx<S>::T;
+  constexpr int M = R1 * R2;  // N == 2 M
+  constexpr int TS = R2 * ROWS + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *T = reinterpret_cast<C *>(smraw);  // [R1][TS]
+  C *Xs = T + R1 * TS;                  // [Kc+1][ROWS]
+  const int b0 = blockIdx.x * ROWS, a = blockIdx.y, f = blockIdx.z;
+  const C *src = reinterpret_cast<const C *>(pb) + ((long long)f * (Kc + 1) * N + a) * N + b0;
+  for (int i = threadIdx.x; i < (Kc + 1) * ROWS; i += blockDim.x) {
+    const int k = i / ROWS, r = i - k * ROWS;
+    Xs[i] = src[(long long)k * N * N + r];
+  }
+  __syncthreads();
+  for (int task = threadIdx.x; task < R2 * ROWS; task += blockDim.x) {
+    const int k2 = task / ROWS, r = task - k2 * ROWS;
+    C v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      const int k = k2 + R2 * k1;
+      C z{(S)0, (S)0};
+      if (k <= Kc) {
+        C x = Xs[k * ROWS + r];
+        if (k == 0) x.y = (S)0;
+        z = c_add(x, c_mul_i(c_mul(x, wN[k])));
+      } else if (k >= M - Kc) {
+        const int j = M - k;
+        const C x = Xs[j * ROWS + r];
+        const C d = c_sub(x, c_mul_i(c_mul(x, wN[j])));
+        z = C{d.x, -d.y};
+      }
+      v[k1] = z;
+    }
+    dft_inv<S, R1>(v, tw);
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+      C y = v[m1];
+      if (m1 > 0) y = c_mul(y, wN[(2 * k2 * m1) & (N - 1)]);  // e^{2 pi i k2 m1 / M}
+      T[m1 * TS + k2 * ROWS + r] = y;
+    }
+  }
+  __syncthreads();
+  for (int task = threadIdx.x; task < R1 * ROWS; task += blockDim.x) {
+    const int r = task / R1, m1 = task - r * R1;
+    C u[R2];
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[m1 * TS + k2 * ROWS + r];
+    dft_inv<S, R2>(u, tw);
+    C *row = reinterpret_cast<C *>(out) + ((long long)(f * N + a) * N + b0 + r) * M;
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
+  }
+}
+
+// Pass-C shapes (M = N/2 = R1 x R2) and rows per CTA: staging tile <= ~64 KB.
+struct PcShape {
+  int R1, R2, rows;
+};
+static bool pc_shape(long long N, size_t word, PcShape *sh) {
+  if (N < 32 || N > 2048 || (N & (N - 1))) return false;
+  const int M = (int)(N / 2);
+  int R1 = 4, R2 = 4;
+  switch (M) {
+    case 16: R1 = 4, R2 = 4; break;
+    case 32: R1 = 8, R2 = 4; break;
+    case 64: R1 = 8, R2 = 8; break;
+    case 128: R1 = 16, R2 = 8; break;
+    case 256: R1 = 16, R2 = 16; break;
+    case 512: R1 = 32, R2 = 16; break;
+    default: R1 = 32, R2 = 32; break;
+  }
+  int rows = 16;
+  while (rows > 4 && (size_t)M * rows * 2 * word > 64 * 1024) rows /= 2;
+  *sh = PcShape{R1, R2, rows};
+  return true;
+}
+static size_t pc_fused_smem(const cf_ctx *ctx, const PcShape &sh) {
+  return ((size_t)sh.R1 * (sh.R2 * sh.rows + 1) + (size_t)(ctx->Kc + 1) * sh.rows) * 2 * ctx->word;
+}
+
+template <typename S, int R1, int R2, int ROWS>
+static int launch_pc_fused_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+  using C = typename Cplx<S>::T;
+  auto kern = k_prune_c_fft<S, R1, R2, ROWS>;
+  if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Tw32<S> tw;
+  for (int e = 0; e < 16; ++e) {
+    const double ang = 2.0 * 3.14159265358979323846 * e / 32.0;
+    tw.w[e] = C{(S)std::cos(ang), (S)std::sin(ang)};
+  }
+  const int N = (int)ctx->N;
+  kern<<<dim3(N / ROWS, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)out, (const C *)ctx->pr_wN, N, ctx->Kc,
+                                                 tw);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+template <typename S>
+static int launch_pc_fused(cf_ctx *ctx, void *out, cudaStream_t st) {
+  PcShape sh;
+  if (!pc_shape(ctx->N, sizeof(S), &sh)) return set_error("fused pass C: unsupported N"), CF_ERR_INVALID;
+  const size_t smem = pc_fused_smem(ctx, sh);
+#define CF_PC(r1, r2, rw) \
+  if (sh.R1 == r1 && sh.R2 == r2 && sh.rows == rw) return launch_pc_fused_t<S, r1, r2, rw>(ctx, out, smem, st);
+  CF_PC(4, 4, 16)
+  CF_PC(8, 4, 16)
+  CF_PC(8, 8, 16)
+  CF_PC(16, 8, 16)
+  CF_PC(16, 16, 16)
+  CF_PC(32, 16, 16)
+  CF_PC(32, 16, 8)
+  CF_PC(32, 32, 8)
+  CF_PC(32, 32, 4)
+#undef CF_PC
+  set_error("fused pass C: no kernel for R1=%d R2=%d rows=%d", sh.R1, sh.R2, sh.rows);
+  return CF_ERR_INVALID;
+}
+
+// Shared memory of k_prune_c's (Kc+1) x 33 complex tile, and the most it may take.
+static size_t prune_c_smem(const cf_ctx *ctx) { return (size_t)(ctx->Kc + 1) * 33 * 2 * ctx->word; }
+static constexpr size_t kPruneCSmemMax = 200 * 1024;
+static constexpr size_t kPcFusedSmemMax = 200 * 1024;
+
 template <typename S>
 __global__ void k_copy_convert(const double *__restrict__ in, S *__restrict__ out, long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -206,8 +418,7 @@ __global__ void k_copy_convert(const double *__restrict__ in, S *__restrict__ ou
 }
 
 int ensure_psi(cf_ctx *ctx) {
-  if (ctx->have_plan_psi) return CF_OK;
-  const int N = (int)ctx->N;
+  if (ctx->psi_table) return CF_OK;  // buffers in place
   const size_t w = ctx->word;
   const size_t hc_bytes = (size_t)ctx->hc_count * w;
   if (!ctx->R_fft) {
@@ -221,10 +432,6 @@ int ensure_psi(cf_ctx *ctx) {
     set_error("cudaMalloc transfer table failed");
     return CF_ERR_NOMEM;
   }
-  if (cudaMalloc(&ctx->psi_hc, 2 * hc_bytes) != cudaSuccess) {
-    set_error("cudaMalloc Psi transfer buffers (%zu bytes) failed", 2 * hc_bytes);
-    return CF_ERR_NOMEM;
-  }
   for (auto &s : ctx->slot) {
     if (cudaMalloc(&s.psi, 2 * (size_t)ctx->N3 * w) != cudaSuccess) {
       set_error("cudaMalloc Psi slot failed");
@@ -233,6 +440,28 @@ int ensure_psi(cf_ctx *ctx) {
     s.dpsi = (char *)s.psi + (size_t)ctx->N3 * w;
     s.valid = false;
   }
+  return CF_OK;
+}
+
+// The two padded HC arrays (Psi_k, dPsi_k) that the cuFFT C2R routes read:
+// allocated when a refresh first takes one of them.
+static int ensure_psi_hc(cf_ctx *ctx) {
+  if (ctx->psi_hc) return CF_OK;
+  const size_t bytes = 2 * (size_t)ctx->hc_count * ctx->word;
+  if (cudaMalloc(&ctx->psi_hc, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMalloc Psi transfer buffers (%zu bytes) failed", bytes);
+    return CF_ERR_NOMEM;
+  }
+  return CF_OK;
+}
+
+// The batched 3-D C2R of the full synthesis (created when a refresh first takes
+// the full path, so the pruned path does not hold its work area).
+static int ensure_full_plan(cf_ctx *ctx) {
+  if (ctx->have_plan_psi) return CF_OK;
+  const int N = (int)ctx->N;
+  const size_t w = ctx->word;
   long long n[3] = {N, N, N};
   long long inembed[3] = {N, N, N / 2 + 1};
   long long onembed[3] = {N, N, N};
@@ -250,10 +479,11 @@ static void free_pruned(cf_ctx *ctx) {
   if (!ctx->have_pruned) return;
   cudaFree(ctx->pz_a);
   cudaFree(ctx->pz_b);
+  cudaFree(ctx->pr_wN);
   cufftDestroy(ctx->plan_pa);
   cufftDestroy(ctx->plan_pb);
-  cufftDestroy(ctx->plan_pc);
-  ctx->pz_a = ctx->pz_b = nullptr;
+  if (!ctx->pc_fused) cufftDestroy(ctx->plan_pc);
+  ctx->pz_a = ctx->pz_b = ctx->pr_wN = nullptr;
   ctx->have_pruned = false;
 }
 
@@ -280,10 +510,34 @@ static int ensure_pruned(cf_ctx *ctx) {
   CF_TRY_CUFFT(cufftCreate(&ctx->plan_pb));
   CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pb, 1, n1, nullptr, 1, N, nullptr, 1, N, dp ? CUFFT_Z2Z : CUFFT_C2C,
                                    2 * nk * N, &work));
-  long long ie[1] = {nh}, oe[1] = {N};
-  CF_TRY_CUFFT(cufftCreate(&ctx->plan_pc));
-  CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pc, 1, n1, ie, 1, nh, oe, 1, N, dp ? CUFFT_Z2D : CUFFT_C2R, 2 * N * N,
-                                   &work));
+  PcShape sh;
+  ctx->pc_fused = pc_shape(N, ctx->word, &sh) && pc_fused_smem(ctx, sh) <= kPcFusedSmemMax;
+  if (ctx->pc_fused) {
+    // e^{2 pi i j / N}, j < N, from the host's double-precision cos / sin
+    std::vector<double> w(2 * N);
+    for (long long j = 0; j < N; ++j) {
+      const double ang = 2.0 * 3.14159265358979323846 * (double)j / (double)N;
+      w[2 * j] = std::cos(ang);
+      w[2 * j + 1] = std::sin(ang);
+    }
+    if (cudaMalloc(&ctx->pr_wN, (size_t)N * cb) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMalloc of the pass-C twiddles failed");
+      return CF_ERR_NOMEM;
+    }
+    if (dp) {
+      CF_TRY_CUDA(cudaMemcpy(ctx->pr_wN, w.data(), (size_t)N * cb, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> wf(w.begin(), w.end());
+      CF_TRY_CUDA(cudaMemcpy(ctx->pr_wN, wf.data(), (size_t)N * cb, cudaMemcpyHostToDevice));
+    }
+  } else {
+    CF_TRY(ensure_psi_hc(ctx));
+    long long ie[1] = {nh}, oe[1] = {N};
+    CF_TRY_CUFFT(cufftCreate(&ctx->plan_pc));
+    CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pc, 1, n1, ie, 1, nh, oe, 1, N, dp ? CUFFT_Z2D : CUFFT_C2R,
+                                     2 * N * N, &work));
+  }
   ctx->have_pruned = true;
   ctx->pr_Ka = ctx->Ka;
   ctx->pr_Kb = ctx->Kb;
@@ -325,9 +579,15 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
     else
       CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pb, (cufftComplex *)ctx->pz_b, (cufftComplex *)ctx->pz_b, CUFFT_INVERSE));
   }
+  if (ctx->pc_fused) {
+    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    return launch_pc_fused<S>(ctx, out, st);
+  }
   {
     ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
-    const size_t smem = (size_t)(Kc + 1) * 33 * 2 * sizeof(S);
+    const size_t smem = prune_c_smem(ctx);
+    if (smem > 48 * 1024)
+      CF_TRY_CUDA(cudaFuncSetAttribute(k_prune_c<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_prune_c<S><<<dim3(N / 32, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)ctx->psi_hc, N, Kc);
     CF_LAUNCHED(ctx);
   }
@@ -379,6 +639,8 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void 
     *dpsi = v->dpsi;
     return CF_OK;
   }
+  CF_TRY(ensure_psi_hc(ctx));
+  CF_TRY(ensure_full_plan(ctx));
   CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
   {
     ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
@@ -404,6 +666,37 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void 
   v->stamp = ++ctx->slot_clock;
   *psi = v->psi;
   *dpsi = v->dpsi;
+  return CF_OK;
+}
+
+int psi_route(const cf_ctx *ctx) {
+  if (ctx->p.equation != CF_EQ_COMOVING_FRW || !ctx->R_fft) return CF_PSI_NONE;
+  if (!ctx->pruned) return CF_PSI_FULL;
+  PcShape sh;
+  return (pc_shape(ctx->N, ctx->word, &sh) && pc_fused_smem(ctx, sh) <= kPcFusedSmemMax) ? CF_PSI_PRUNED_FUSED
+                                                                                         : CF_PSI_PRUNED;
+}
+
+template <typename S>
+__global__ void k_widen(const S *__restrict__ in, double *__restrict__ out, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (double)in[i];
+}
+
+int psi_fields(cf_ctx *ctx, double t, double *d_out, cudaStream_t st) {
+  const void *psi = nullptr, *dpsi = nullptr;
+  CF_TRY(psi_at(ctx, t, st, &psi, &dpsi));
+  const long long n = ctx->N3;
+  if (ctx->word == 8) {
+    CF_TRY_CUDA(cudaMemcpyAsync(d_out, psi, n * 8, cudaMemcpyDeviceToDevice, st));
+    CF_TRY_CUDA(cudaMemcpyAsync(d_out + n, dpsi, n * 8, cudaMemcpyDeviceToDevice, st));
+  } else {
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_widen<float><<<blocks, 256, 0, st>>>((const float *)psi, d_out, n);
+    CF_LAUNCHED(ctx);
+    k_widen<float><<<blocks, 256, 0, st>>>((const float *)dpsi, d_out + n, n);
+    CF_LAUNCHED(ctx);
+  }
   return CF_OK;
 }
 
@@ -462,8 +755,11 @@ int set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, cudaStream_t st) 
   const int N = (int)ctx->N;
   // pruned when the box is small against the lattice: passes A and B then touch a
   // small fraction of the lines, and pass C's transpose tile fits shared memory
+  PcShape sh;
+  const bool pc_ok = (pc_shape(N, ctx->word, &sh) && pc_fused_smem(ctx, sh) <= kPcFusedSmemMax) ||
+                     prune_c_smem(ctx) <= kPruneCSmemMax;
   ctx->pruned = !(ctx->p.flags & CF_FLAG_FULL_PSI_FFT) && N % 32 == 0 && 2 * ctx->Ka + 1 <= N / 2 &&
-                2 * ctx->Kb + 1 <= N / 2 && ctx->Kc + 1 <= 64 && ctx->Kc + 1 <= N / 4;
+                2 * ctx->Kb + 1 <= N / 2 && ctx->Kc + 1 <= N / 4 && pc_ok;
   return CF_OK;
 }
 

@@ -92,7 +92,16 @@ typedef struct cf_info {
   int64_t hc_count;     /* doubles in one HC array: 2*N*N*(N/2+1) */
   int64_t s2_bins;      /* 3*(N/2)^2+1 */
   int64_t shells;       /* isqrt(3*(N/2)^2)+1 */
+  int64_t psi_route;    /* comoving equation: how Psi is synthesised (CF_PSI_*) */
 } cf_info;
+
+/* cf_info.psi_route: 0 = no R_fft set (or not the comoving equation);
+ * full 3-D C2R; pruned passes A, B with a padded cuFFT C2R as pass C (N not a
+ * power of two); pruned passes A, B with pass C as one kernel. */
+#define CF_PSI_NONE 0
+#define CF_PSI_FULL 1
+#define CF_PSI_PRUNED 2
+#define CF_PSI_PRUNED_FUSED 3
 
 /* ---- context --------------------------------------------------------------
  * Replaces WorkspaceGeneric's tools (FFT wrapper, Psi buffers) and the odeint
@@ -119,6 +128,12 @@ int cf_state_export(cf_ctx *ctx, double *d_xy, const void *d_state, void *stream
 /* R_fft: HC array of the comoving curvature perturbation (the reference's
  * workspace.R_fft, src/initializer.hpp:200-205), host or device pointer. */
 int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream);
+
+/* Psi(x, t) and dPsi/dt(x, t) of the comoving-curvature equation into d_out
+ * (2 N^3 doubles: Psi, then dPsi), the fields the right-hand side uses at time t
+ * (the reference computes them inside Equation::operator(),
+ * src/equations_cuda.cu:678-731, and exposes no call of its own). */
+int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream);
 
 /* ---- the hot path -----------------------------------------------------------
  * nsteps classic RK4 steps in place; step j runs at t = t0 + (step0 + j) * dt
@@ -227,8 +242,10 @@ int cf_shell_amplitude_gradient(cf_ctx *ctx, const double *d_lambda_phi, const d
  *   CF_ENS_BATCHED: one launch per stage over all members.
  *   CF_ENS_LOOP: one launch per stage per member (single-instance path).
  * cf_ensemble_run_graph: nsegments observer intervals of steps_per_segment steps from
- *   t0 (absolute steps 0..): a CUDA graph of the persistent kernel is captured once
- *   and replayed per segment; when d_spectra is non-NULL the members' density
+ *   t0 (absolute steps 0..): a CUDA graph of one interval -- the persistent kernel
+ *   (mode CF_ENS_PERSISTENT) or the 4 * steps_per_segment batched launches (mode
+ *   CF_ENS_BATCHED), each reading its step from a device counter that the graph
+ *   advances -- is captured once and replayed per segment; when d_spectra is non-NULL the members' density
  *   spectra (S2 bins, concatenated member by member, cf_ensemble_info gives the
  *   per-segment length) at each segment end follow each replay.  Needs a
  *   non-default stream.
@@ -246,9 +263,16 @@ int cf_ensemble_rk4_steps(cf_ensemble *ens, double t0, double dt, int64_t step0,
                           void *stream);
 int cf_ensemble_density_spectra_s2(cf_ensemble *ens, double t, double *d_out, void *stream);
 int cf_ensemble_run_graph(cf_ensemble *ens, double t0, double dt, int64_t steps_per_segment, int64_t nsegments,
-                          double *d_spectra, void *stream);
+                          int mode, double *d_spectra, void *stream);
 int cf_ensemble_autotune(cf_ensemble *ens, double t0, double dt, int64_t steps, void *stream, int *h_shape,
                          int *h_a_chunk);
+/* Failure-detection test hook: the persistent kernel's grid barrier waits for
+ * `extra_arrivals` CTAs that never come, giving up after `spin_limit` sleep
+ * iterations (default 2^24).  The run then returns CF_ERR_TIMEOUT with the
+ * state untouched (stage 1 writes only work buffers) and the ensemble stays
+ * usable; (0, 2^24) restores normal operation. */
+int cf_ensemble_set_barrier_test(cf_ensemble *ens, int extra_arrivals, int64_t spin_limit);
+
 /* ---- profiling ----------------------------------------------------------------
  * When enabled, every kernel (or cuFFT call) the context launches is bracketed by
  * a pair of CUDA events on its stream and its device time is accumulated per

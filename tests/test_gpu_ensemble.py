@@ -82,8 +82,9 @@ def test_ensemble_fp64_member_matches_oracle():
         assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)
 
 
+@pytest.mark.parametrize("mode", [cfb200.ENS_PERSISTENT, cfb200.ENS_BATCHED])
 @pytest.mark.parametrize("stencil", [7, 13])
-def test_ensemble_graph_run_and_spectra(stencil):
+def test_ensemble_graph_run_and_spectra(stencil, mode):
     spec = members_spec(cfb200.FP32_COMP, stencil=stencil)
     ens = cfb200.Ensemble(spec)
     xs = [initial(d, i) for i, d in enumerate(spec)]
@@ -93,7 +94,7 @@ def test_ensemble_graph_run_and_spectra(stencil):
     out = torch.zeros(nseg * ens.spectra_total, dtype=torch.float64, device="cuda")
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
-        ens.run_graph(t0, dt, S, nseg, out, stream=stream)
+        ens.run_graph(t0, dt, S, nseg, out, stream=stream, mode=mode)
     stream.synchronize()
     out = out.cpu().numpy()
     for i, d in enumerate(spec):
@@ -123,6 +124,52 @@ def test_ensemble_autotune_keeps_results():
         ens.download(i, got)
         want, _, _ = single_run(d, xs[i], 1.0, 0.1, 4)
         assert np.array_equal(got, want)
+
+
+def test_persistent_barrier_timeout_is_reported_and_recoverable():
+    """Failure detection without a GPU fault: the grid barrier is made to wait for
+    one CTA that never arrives, with a short spin limit.  The bounded wait gives
+    up, the call returns CF_ERR_TIMEOUT, the state is untouched, and the same
+    ensemble then runs normally."""
+    spec = members_spec(cfb200.FP64, Ns=(16, 24))
+    ens = cfb200.Ensemble(spec)
+    xs = [initial(d, i) for i, d in enumerate(spec)]
+    for i, x in enumerate(xs):
+        ens.upload(i, x)
+    ens.set_barrier_test(1, spin_limit=1 << 16)
+    with pytest.raises(cfb200.CfError) as e:
+        ens.rk4_steps(1.0, 0.1, 2, mode=cfb200.ENS_PERSISTENT)
+    assert e.value.code == -6
+    for i, x in enumerate(xs):
+        got = np.empty_like(x)
+        ens.download(i, got)
+        assert np.array_equal(got, x)
+    ens.set_barrier_test(0)
+    ens.rk4_steps(1.0, 0.1, 3, mode=cfb200.ENS_PERSISTENT)
+    for i, d in enumerate(spec):
+        got = np.empty_like(xs[i])
+        ens.download(i, got)
+        want, _, _ = single_run(d, xs[i], 1.0, 0.1, 3)
+        assert np.array_equal(got, want)
+
+
+def test_checkpoint_resume_matches_uninterrupted_run():
+    """Checkpoint/resume: stepping 6, downloading the state to the host, loading
+    it into a fresh context and stepping 6 more equals 12 uninterrupted steps
+    (bit for bit unless a value sits on an FP32 rounding tie when the FP64
+    checkpoint is split back into hi + lo; 1e-13 relative covers that)."""
+    d = members_spec(cfb200.FP32_COMP, Ns=(32,))[0]
+    x = initial(d, 0)
+    full, _, _ = single_run(d, x, 1.0, 0.1, 12)
+    half, _, _ = single_run(d, x, 1.0, 0.1, 6)
+    c = cfb200.Context(d["N"], d["L"], m=d["m"], equation=cfb200.EQ_KG_FRW, precision=d["precision"], **FRW)
+    st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    c.upload(st, half)
+    c.rk4_steps(st, 1.0, 0.1, 6, step0=6)
+    got = np.empty_like(x)
+    c.download(got, st)
+    torch.cuda.synchronize()
+    assert np.linalg.norm(got - full) <= 1e-13 * np.linalg.norm(full)
 
 
 def test_ensemble_rejects_mixed_settings():

@@ -105,6 +105,37 @@ def test_pruned_psi_synthesis_equals_full(prec, tol, k_max):
     assert rel(out[0][1], out[1][1]) <= tol
 
 
+@pytest.mark.parametrize("prec,tol_pf,tol_or", [(cfb200.FP64, 1e-13, 1e-12), (cfb200.FP32_COMP, 2e-6, 2e-6)])
+@pytest.mark.parametrize("N,k_max,route", [(64, 1.0, cfb200.PSI_PRUNED_FUSED),
+                                           (64, 1.5, cfb200.PSI_PRUNED_FUSED),   # Kc = N/4 - 1
+                                           (128, 0.6, cfb200.PSI_PRUNED_FUSED),
+                                           (96, 1.0, cfb200.PSI_PRUNED),        # not a power of two
+                                           (64, 2.5, cfb200.PSI_FULL)])         # box too wide to prune
+def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or, N, k_max, route):
+    """Psi and dPsi/dt at a stage time, read back through cf_psi_fields: the
+    route the box selects (pass C as one kernel for power-of-two N, the padded
+    cuFFT pass C otherwise, or the full 3-D C2R) equals the forced full C2R and
+    the oracle's FFTW-based synthesis (FP64: 1e-13 / 1e-12; FP32 storage: 2e-6)."""
+    L = float(N)
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=31)
+    got = {}
+    for flags in (0, cfb200.FLAG_FULL_PSI_FFT):
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=prec, flags=flags, **FRW)
+        c.set_R_fft(Rf, on_device=False)
+        assert c.info.psi_route == (route if flags == 0 else cfb200.PSI_FULL)
+        out = torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
+        c.psi_fields(1.3, out)
+        torch.cuda.synchronize()
+        got[flags] = out.cpu().numpy()
+    P = O.make_params(N, L, 1.0, eq=2, **FRW)
+    psi, dpsi = O.psi_fields(P, Rf, 1.3)
+    a, b = got[0], got[cfb200.FLAG_FULL_PSI_FFT]
+    for sl, want in ((slice(0, N ** 3), psi), (slice(N ** 3, None), dpsi)):
+        assert rel(a[sl], b[sl]) <= tol_pf
+        assert rel(a[sl], want) <= tol_or
+        assert rel(b[sl], want) <= tol_or
+
+
 @pytest.mark.parametrize("eq", [0, 1, 2])
 def test_rk4_split_calls_equal_one_call(eq):
     """step0 offsets reproduce integrate_const's direct time t0 + step*dt."""
