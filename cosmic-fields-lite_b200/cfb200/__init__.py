@@ -27,6 +27,7 @@ STATUS = {0: "CF_OK", -1: "CF_ERR_INVALID", -2: "CF_ERR_CUDA", -3: "CF_ERR_CUFFT
 EQ_KG, EQ_KG_FRW, EQ_COMOVING_FRW = 0, 1, 2
 FP64, FP32_COMP = 0, 1
 FLAG_FULL_PSI_FFT = 1
+FLAG_STAGE_KERNELS = 2
 PSI_NONE, PSI_FULL, PSI_PRUNED, PSI_PRUNED_FUSED = 0, 1, 2, 3
 
 
@@ -100,11 +101,13 @@ _SIGS = {
     "cf_profile_reset": ([_vp], _i),
 }
 
-PROF_KINDS = ["stage1", "stage2", "stage3", "stage4", "psi_transfer", "psi_fft", "spectrum", "other"]
+PROF_KINDS = ["stage1", "stage2", "stage3", "stage4", "psi_transfer", "psi_fft", "spectrum", "other", "pair_a",
+              "pair_b"]
+STEP_KINDS = ("stage1", "stage2", "stage3", "stage4", "pair_a", "pair_b")
 
 
 class cf_profile(ctypes.Structure):
-    _fields_ = [("launches", ctypes.c_int64 * 8), ("ms", ctypes.c_double * 8)]
+    _fields_ = [("launches", ctypes.c_int64 * len(PROF_KINDS)), ("ms", ctypes.c_double * len(PROF_KINDS))]
 
 _lib = None
 

@@ -194,6 +194,10 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     set_error("stencil must be 7 or 13, got %d", p.stencil);
     return CF_ERR_INVALID;
   }
+  if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS)) {
+    set_error("unknown flags 0x%x", (unsigned)p.flags);
+    return CF_ERR_INVALID;
+  }
   if (p.equation != CF_EQ_KG && (!(p.p > 0) || !std::isfinite(p.a1) || !std::isfinite(p.H1) || !std::isfinite(p.t1))) {
     set_error("FRW parameters must be finite with p > 0");
     return CF_ERR_INVALID;

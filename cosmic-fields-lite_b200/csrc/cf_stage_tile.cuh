@@ -101,16 +101,92 @@ struct StageArgs {
   double dt6;   // dt / 6
 };
 
+// Arithmetic type of the stage evaluations: FP64 for FP64 storage; FP32 for
+// FP32_COMP, whose stage inputs and accumulator are FP32 words anyway.  In FP32
+// every rounding must be unbiased, or it acts like a changed time step or mass
+// and the error grows with time: coefficients (dt/2, dt/6, h^-2 a^-2, 3H, m^2)
+// enter as hi + lo pairs, e^{2 Psi} as 1 + expm1f (never rounded as 1 + eps),
+// and the state update x += dt/6 (acc + k4) is formed in FP64 and kept as the
+// hi + lo pair.
+template <typename S>
+struct Arith {
+  using T = S;
+};
+
+// A coefficient in the arithmetic type: FP64 as is, FP32 as hi + lo.
+template <typename T>
+struct Coef;
+template <>
+struct Coef<double> {
+  double hi;
+  __host__ __device__ Coef(double c) : hi(c) {}
+  __device__ __forceinline__ double mul(double v) const { return hi * v; }
+  __device__ __forceinline__ double fma(double v, double add) const { return add + hi * v; }
+};
+template <>
+struct Coef<float> {
+  float hi, lo;
+  __host__ __device__ Coef(double c) : hi((float)c), lo((float)(c - (double)(float)c)) {}
+  // c v with the product's error random (hi v + lo v)
+  __device__ __forceinline__ float mul(float v) const { return fmaf(hi, v, lo * v); }
+  // add + c v
+  __device__ __forceinline__ float fma(float v, float add) const { return add + fmaf(hi, v, lo * v); }
+};
+
 // exp(2 Psi) and exp(4 Psi).  FP64: the reference's exp of the doubled argument.
-// FP32: Psi is an FP32 field of magnitude ~1e-2; 1 + expm1f keeps the absolute
-// error of e^{2Psi} near 1e-9 (FP32 relative accuracy on the small part).
 __device__ __forceinline__ void psi_factors(double psi, double &e2, double &e4) {
   e2 = exp(2 * psi);
   e4 = exp(4 * psi);
 }
-__device__ __forceinline__ void psi_factors(float psi, double &e2, double &e4) {
-  e2 = 1.0 + (double)expm1f(2.0f * psi);
-  e4 = 1.0 + (double)expm1f(4.0f * psi);
+
+// Laplacian sum (times h^2) at (row, col) of a staged plane whose a-neighbours
+// are q[0..2H] (q[H] the plane itself): 7-point for H = 1, 13-point 4th order for
+// H = 2 (src/fdm3d_cuda.cu:20-83).  The single-stage and the paired-stage tiles
+// both form it here, so their sums round identically.
+template <typename S, int H, int SP, typename T = typename Arith<S>::T>
+__device__ __forceinline__ T lap_at(const Pack<S> (&q)[2 * H + 1], const S *sm, int row, int col, int v) {
+  const T f0 = (T)q[H].v[v];
+  if constexpr (H == 1) {
+    const T s = (T)-6 * f0 + (T)q[2].v[v] + (T)q[0].v[v] + (T)sm[(row + 1) * SP + col] + (T)sm[(row - 1) * SP + col];
+    return s + ((T)sm[row * SP + col + 1] + (T)sm[row * SP + col - 1]);
+  } else {
+    const T s1 = (T)q[3].v[v] + (T)q[1].v[v] + (T)sm[(row + 1) * SP + col] + (T)sm[(row - 1) * SP + col] +
+                 (T)sm[row * SP + col + 1] + (T)sm[row * SP + col - 1];
+    const T s2 = (T)q[4].v[v] + (T)q[0].v[v] + (T)sm[(row + 2) * SP + col] + (T)sm[(row - 2) * SP + col] +
+                 (T)sm[row * SP + col + 2] + (T)sm[row * SP + col - 2];
+    return ((T)16 * s1 - s2 - (T)90 * f0) / (T)12;
+  }
+}
+
+// Stage coefficients in the arithmetic type.
+template <typename T>
+struct StageCoef {
+  Coef<T> m2, inv, hub3;
+};
+
+// pi component of the right-hand side (src/equations_cuda.cu:15-36, :263-287):
+//   (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} h^-2 a^-2 lap phi.
+template <bool COMOV, typename S, typename T = typename Arith<S>::T>
+__device__ __forceinline__ T kpi_of(T p0, T f0, T lap, S ps, S dps, const StageCoef<T> &k) {
+  if constexpr (sizeof(T) == 8) {
+    if constexpr (COMOV) {
+      T e2, e4;
+      psi_factors(ps, e2, e4);
+      return (-k.hub3.hi + (T)4 * (T)dps) * p0 - e2 * k.m2.hi * f0 + e4 * k.inv.hi * lap;
+    } else {
+      return -k.hub3.hi * p0 - k.m2.hi * f0 + k.inv.hi * lap;
+    }
+  } else {
+    const float mf = k.m2.mul(f0);
+    const float g = k.inv.mul(lap);
+    if constexpr (COMOV) {
+      const float e2m1 = expm1f(2.0f * (float)ps), e4m1 = expm1f(4.0f * (float)ps);
+      const float fr = 4.0f * (float)dps * p0 - k.hub3.mul(p0);
+      return fr - fmaf(e2m1, mf, mf) + fmaf(e4m1, g, g);
+    } else {
+      return -k.hub3.mul(p0) - mf + g;
+    }
+  }
 }
 
 // Plane staging.  Double-buffered (DB): plane a goes to buffer (a - a_begin) & 1
@@ -157,6 +233,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
   const long long NN = (long long)N * N;
   const S *phi_in = A.yin;
   const S *pi_in = A.yin + N3;
+  using T = typename Arith<S>::T;
+  const StageCoef<T> kc{Coef<T>(A.m2), Coef<T>(A.inv), Coef<T>(A.hub3)};
+  const Coef<T> cy(A.cy);
 
   Pack<S> q[2 * H + 1];
   if (act) {
@@ -236,47 +315,27 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
     for (int v = 0; v < V; ++v) {
       const int col = H + tx * V + v;
       const int row = ty + H;
-      const double f0 = (double)q[H].v[v];
-      double lap;
-      if constexpr (H == 1) {
-        const double s = -6.0 * f0 + (double)q[2].v[v] + (double)q[0].v[v] + (double)sm[(row + 1) * SP + col] +
-                         (double)sm[(row - 1) * SP + col];
-        lap = s + ((double)sm[row * SP + col + 1] + (double)sm[row * SP + col - 1]);
-      } else {
-        const double s1 = (double)q[3].v[v] + (double)q[1].v[v] + (double)sm[(row + 1) * SP + col] +
-                          (double)sm[(row - 1) * SP + col] + (double)sm[row * SP + col + 1] +
-                          (double)sm[row * SP + col - 1];
-        const double s2 = (double)q[4].v[v] + (double)q[0].v[v] + (double)sm[(row + 2) * SP + col] +
-                          (double)sm[(row - 2) * SP + col] + (double)sm[row * SP + col + 2] +
-                          (double)sm[row * SP + col - 2];
-        lap = (16.0 * s1 - s2 - 90.0 * f0) / 12.0;
-      }
-      const double p0 = (double)pi0.v[v];
-      const double kphi = p0;
-      double kpi;
-      if constexpr (COMOV) {
-        double e2, e4;
-        psi_factors(ps.v[v], e2, e4);
-        kpi = (-A.hub3 + 4.0 * (double)dps.v[v]) * p0 - e2 * A.m2 * f0 + e4 * A.inv * lap;
-      } else {
-        kpi = -A.hub3 * p0 - A.m2 * f0 + A.inv * lap;
-      }
+      const T f0 = (T)q[H].v[v];
+      const T lap = lap_at<S, H, SP>(q, sm, row, col, v);
+      const T p0 = (T)pi0.v[v];
+      const T kphi = p0;
+      const T kpi = kpi_of<COMOV, S>(p0, f0, lap, COMOV ? ps.v[v] : (S)0, COMOV ? dps.v[v] : (S)0, kc);
       if constexpr (STAGE == 0) {
         o_phi.v[v] = (S)kphi;
         o_pi.v[v] = (S)kpi;
       } else if constexpr (STAGE == 1) {
         cp.v[v] = (S)kphi;
         cq.v[v] = (S)kpi;
-        o_phi.v[v] = (S)(f0 + A.cy * kphi);
-        o_pi.v[v] = (S)(p0 + A.cy * kpi);
+        o_phi.v[v] = (S)cy.fma(kphi, f0);
+        o_pi.v[v] = (S)cy.fma(kpi, p0);
       } else if constexpr (STAGE == 2 || STAGE == 3) {
-        cp.v[v] = (S)((double)cp.v[v] + 2.0 * kphi);
-        cq.v[v] = (S)((double)cq.v[v] + 2.0 * kpi);
-        o_phi.v[v] = (S)((double)xp.v[v] + A.cy * kphi);
-        o_pi.v[v] = (S)((double)xq.v[v] + A.cy * kpi);
+        cp.v[v] = (S)((T)cp.v[v] + (T)2 * kphi);
+        cq.v[v] = (S)((T)cq.v[v] + (T)2 * kpi);
+        o_phi.v[v] = (S)cy.fma(kphi, (T)xp.v[v]);
+        o_pi.v[v] = (S)cy.fma(kpi, (T)xq.v[v]);
       } else {  // STAGE 4
-        const double ip = A.dt6 * ((double)cp.v[v] + kphi);
-        const double iq = A.dt6 * ((double)cq.v[v] + kpi);
+        const double ip = A.dt6 * (double)((T)cp.v[v] + kphi);
+        const double iq = A.dt6 * (double)((T)cq.v[v] + kpi);
         if constexpr (sizeof(S) == 8) {
           xp.v[v] = (S)((double)xp.v[v] + ip);
           xq.v[v] = (S)((double)xq.v[v] + iq);

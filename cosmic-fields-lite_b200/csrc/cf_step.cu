@@ -1,9 +1,13 @@
 // cf_step.cu -- fused RK4 stage kernels (the hot path), cf_rhs, cf_scale_sum.
 //
-// One RK4 step (stepper/runge_kutta4_classic.hpp:88-138) is four stage kernels.
-// Each makes ONE pass over HBM: it streams its stage input y through a
-// 2.5-D blocked stencil and fuses the odeint linear combinations
-// (thrust_operations::scale_sum2 / scale_sum5) into the same pass:
+// One RK4 step (stepper/runge_kutta4_classic.hpp:88-138) is four stages.  By
+// default cf_rk4_steps runs them as two paired-stage passes (stages 1+2, 3+4;
+// cf_pair_tile.cuh), which keep the intermediate stage inputs out of HBM; the
+// four single-stage kernels remain for CF_FLAG_STAGE_KERNELS, the adjoint's
+// recompute and the ensembles.  A single-stage kernel makes ONE pass over HBM:
+// it streams its stage input y through a 2.5-D blocked stencil and fuses the
+// odeint linear combinations (thrust_operations::scale_sum2 / scale_sum5) into
+// the same pass:
 //
 //   stage 1 (t)       k1 = f(x)      acc  = k1        y' = x + dt/2 k1
 //   stage 2 (t+dt/2)  k2 = f(y)      acc += 2 k2      y' = x + dt/2 k2
@@ -24,6 +28,7 @@
 #include <cmath>
 
 #include "cf_internal.cuh"
+#include "cf_pair_tile.cuh"
 #include "cf_stage_tile.cuh"
 
 namespace cfb {
@@ -47,6 +52,38 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
   const int a_begin = blockIdx.z * A.a_chunk;
   stage_tile<S, H, COMOV, STAGE, TX, TY, FULL>(A, blockIdx.x * TS::TW, blockIdx.y * TY, a_begin,
                                                min(a_begin + A.a_chunk, A.N), sm);
+}
+
+// Paired-stage kernels: the same tile, two stages per pass.  Occupancy floors
+// per storage type (FP32 7-point, FP32 13-point; FP64 uncoupled; FP64 comoving),
+// measured at N = 512 (ms per step: FP32 comoving 7-point, floors 2 / 3 / 4 ->
+// 4.80 / 4.29 / 4.52; 13-point 5.16 / 5.76 / 6.89; FP64 FRW 7-point 4.60 / 3.64 /
+// 3.23; FP64 comoving 7-point, floors 1 / 2 -> 9.49 / 5.97).
+#ifndef CF_PAIR_MB_F32
+#define CF_PAIR_MB_F32 3
+#endif
+#ifndef CF_PAIR_MB_F32_H2
+#define CF_PAIR_MB_F32_H2 2
+#endif
+#ifndef CF_PAIR_MB_F64
+#define CF_PAIR_MB_F64 4
+#endif
+#ifndef CF_PAIR_MB_F64_COMOV
+#define CF_PAIR_MB_F64_COMOV 2
+#endif
+template <typename S, int H, bool COMOV>
+struct PairMinBlocks {
+  static constexpr int value = sizeof(S) == 4 ? (H == 1 ? CF_PAIR_MB_F32 : CF_PAIR_MB_F32_H2)
+                                              : (COMOV ? CF_PAIR_MB_F64_COMOV : CF_PAIR_MB_F64);
+};
+
+template <typename S, int H, bool COMOV, int PASS, bool FULL>
+__global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, COMOV>::value)) k_pair(const PairArgs<S> A) {
+  using PS = PairSmem<S, H, TX, TY>;
+  __shared__ S sm[PS::count];
+  const int a_begin = blockIdx.z * A.a_chunk;
+  pair_tile<S, H, COMOV, PASS, TX, TY, FULL>(A, blockIdx.x * PS::TS::TW, blockIdx.y * TY, a_begin,
+                                             min(a_begin + A.a_chunk, A.N), sm);
 }
 
 // Planes per CTA along a: enough CTAs to fill the GPU several times over.
@@ -83,6 +120,97 @@ template <typename S, int STAGE>
 static int launch_stage(cf_ctx *ctx, const StageArgs<S> &A, cudaStream_t st) {
   if (ctx->p.equation == CF_EQ_COMOVING_FRW) return launch_stage_h<S, true, STAGE>(ctx, ctx->p.stencil, A, st);
   return launch_stage_h<S, false, STAGE>(ctx, ctx->p.stencil, A, st);
+}
+
+template <typename S, int H, bool COMOV, int PASS>
+static int launch_pair_t(cf_ctx *ctx, const PairArgs<S> &A0, cudaStream_t st) {
+  constexpr int TW = TX * VecT<S>::n;
+  PairArgs<S> A = A0;
+  dim3 block(TX, TY);
+  unsigned gx = ceil_div(A.N, TW), gy = ceil_div(A.N, TY);
+  A.a_chunk = pick_a_chunk(A.N, (int)(gx * gy));
+  dim3 grid(gx, gy, ceil_div(A.N, A.a_chunk));
+  ProfScope ps(ctx, PASS == 1 ? CF_PROF_PAIR_A : CF_PROF_PAIR_B, st);
+  if (A.N % TW == 0 && A.N % TY == 0)
+    k_pair<S, H, COMOV, PASS, true><<<grid, block, 0, st>>>(A);
+  else
+    k_pair<S, H, COMOV, PASS, false><<<grid, block, 0, st>>>(A);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+template <typename S, int PASS>
+static int launch_pair(cf_ctx *ctx, const PairArgs<S> &A, cudaStream_t st) {
+  const bool com = ctx->p.equation == CF_EQ_COMOVING_FRW;
+  if (ctx->p.stencil == 13)
+    return com ? launch_pair_t<S, 2, true, PASS>(ctx, A, st) : launch_pair_t<S, 2, false, PASS>(ctx, A, st);
+  return com ? launch_pair_t<S, 1, true, PASS>(ctx, A, st) : launch_pair_t<S, 1, false, PASS>(ctx, A, st);
+}
+
+// Stage-time coefficients (and, comoving, the Psi slot) of a paired pass.
+template <typename S>
+static int pair_coeffs(cf_ctx *ctx, double t, double *inv, double *hub3, const S **psi, const S **dpsi,
+                       cudaStream_t st) {
+  double H;
+  stage_coeffs(ctx->p, t, inv, &H);
+  *hub3 = 3.0 * H;
+  *psi = *dpsi = nullptr;
+  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
+    const void *ps, *dps;
+    CF_TRY(psi_at(ctx, t, st, &ps, &dps));
+    *psi = (const S *)ps;
+    *dpsi = (const S *)dps;
+  }
+  return CF_OK;
+}
+
+// nsteps RK4 steps as paired-stage passes.  The new phi of pass B alternates
+// between the state's phi plane and the first half of the ya scratch; after an
+// odd number of steps it is copied back.
+template <typename S>
+static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
+                             cudaStream_t st) {
+  CF_TRY(ensure_rk4_scratch(ctx));
+  const long long N3 = ctx->N3;
+  S *x = (S *)d_state;
+  S *phi[2] = {x, (S *)ctx->ya};
+  int cur = 0;
+  PairArgs<S> A{};
+  A.N = (int)ctx->N;
+  A.N3 = N3;
+  A.m2 = ctx->p.m * ctx->p.m;
+  A.xpi = x + N3;
+  A.xlo = (sizeof(S) == 4) ? x + 2 * N3 : nullptr;
+  A.acc = (S *)ctx->acc;
+  A.yb = (S *)ctx->yb;
+  const double dh = dt / 2.0;
+  A.dt6 = dt / 6.0;
+  for (int64_t j = 0; j < nsteps; ++j) {
+    const double t = t0 + (double)(step0 + j) * dt;
+    const double th = t + dh;
+    // pass A: stages 1 (t) and 2 (t + dt/2)
+    CF_TRY(pair_coeffs<S>(ctx, t, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st));
+    CF_TRY(pair_coeffs<S>(ctx, th, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st));
+    A.uphi = phi[cur];
+    A.upi = x + N3;
+    A.xphi = phi[cur];
+    A.xphi_out = nullptr;
+    A.cw = dh;
+    A.cy = dh;
+    CF_TRY(launch_pair<S, 1>(ctx, A, st));
+    // pass B: stages 3 (t + dt/2) and 4 (t + dt)
+    CF_TRY(pair_coeffs<S>(ctx, th, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st));
+    CF_TRY(pair_coeffs<S>(ctx, t + dt, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st));
+    A.uphi = A.yb;
+    A.upi = A.yb + N3;
+    A.xphi = phi[cur];
+    A.xphi_out = phi[cur ^ 1];
+    A.cw = dt;
+    CF_TRY(launch_pair<S, 2>(ctx, A, st));
+    cur ^= 1;
+  }
+  if (cur) CF_TRY_CUDA(cudaMemcpyAsync(x, phi[1], N3 * sizeof(S), cudaMemcpyDeviceToDevice, st));
+  return CF_OK;
 }
 
 template <typename S>
@@ -223,8 +351,12 @@ int rk4_step_buffers(cf_ctx *ctx, void *d_state, void *acc, void *ya, void *yb, 
 }
 
 int rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, cudaStream_t st) {
-  if (ctx->p.precision == CF_FP32_COMP) return rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st);
-  return rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
+  const bool single = (ctx->p.flags & CF_FLAG_STAGE_KERNELS) != 0;
+  if (ctx->p.precision == CF_FP32_COMP)
+    return single ? rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
+                  : rk4_steps_pairs_t<float>(ctx, d_state, t0, dt, step0, nsteps, st);
+  return single ? rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st)
+                : rk4_steps_pairs_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
 }
 
 int rhs(cf_ctx *ctx, const double *d_x, double *d_dxdt, double t, cudaStream_t st) {

@@ -81,6 +81,9 @@ typedef struct cf_params {
  * band-limited (the pruned synthesis is used by default when R_fft is exactly
  * zero outside a small box of modes; both give the same fields to rounding). */
 #define CF_FLAG_FULL_PSI_FFT 1
+/* cf_rk4_steps runs each step as four single-stage passes instead of two
+ * paired-stage passes (stages 1+2, 3+4); both give bit-identical states. */
+#define CF_FLAG_STAGE_KERNELS 2
 
 typedef struct cf_ctx cf_ctx;
 
@@ -286,7 +289,9 @@ typedef enum cf_prof_kind {
   CF_PROF_PSI_FFT = 5,      /* batched C2R of Psi / dPsi (cuFFT) */
   CF_PROF_SPECTRUM = 6,     /* energy density, R2C, binning */
   CF_PROF_OTHER = 7,
-  CF_PROF_KINDS = 8
+  CF_PROF_PAIR_A = 8,       /* paired-stage passes: stages 1+2, stages 3+4 */
+  CF_PROF_PAIR_B = 9,
+  CF_PROF_KINDS = 10
 } cf_prof_kind;
 
 typedef struct cf_profile {
