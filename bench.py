@@ -387,7 +387,9 @@ def run_product(args):
     stage_launches = sum(prof[k][0] for k in cfb200.STEP_KINDS)
     bps = stage_bytes_per_site("fp32comp", True)
     achieved = bps * N ** 3 * args.steps / (stage_ms * 1e-3) / 1e9
-    traffic = traffic_from_profiles("pair_kernels_n512.md")
+    # DRAM bytes per site-update of the two passes from an ncu capture at N = 256
+    # (inputs 10x L2), scaled by the sites a launch processes
+    traffic = traffic_from_profiles("pair_kernels_n256.md")
     roofline = {"bound": "hbm", "kernel": "k_pair (paired RK4 stages 1+2 and 3+4, FP32-comp, comoving)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
