@@ -198,7 +198,7 @@ __device__ __forceinline__ bool ens_stage_pass(const EnsArgs &E, int stage, long
 template <typename S, int H, int SHAPE>
 __global__ void __launch_bounds__(256, CF_ENS_PERSIST_MIN_BLOCKS) k_ens_persistent(const EnsArgs E) {
   constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
-  __shared__ S sm[TileSmem<S, H, TXv, TYv>::count];
+  __shared__ __align__(16) S sm[TileSmem<S, H, TXv, TYv>::count];
   const long long step0 = *E.step_counter;
   for (int j = 0; j < E.nsteps; ++j) {
     for (int stage = 1; stage <= 4; ++stage)
@@ -211,7 +211,7 @@ template <typename S, int H, int SHAPE>
 // counter plus `step_off`, so a captured graph of these launches walks forward.
 __global__ void __launch_bounds__(256, CF_ENS_MIN_BLOCKS) k_ens_stage(const EnsArgs E, int stage, int step_off) {
   constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
-  __shared__ S sm[TileSmem<S, H, TXv, TYv>::count];
+  __shared__ __align__(16) S sm[TileSmem<S, H, TXv, TYv>::count];
   ens_item_stage<S, H, SHAPE>(E, E.items[blockIdx.x], stage, *E.step_counter + step_off, sm);
 }
 

@@ -43,7 +43,7 @@ struct PairArgs {
   S *xlo;           // FP32_COMP compensation [phi | pi] (pass B, in place)
   S *acc;           // [phi | pi]: pass A writes k1 + 2 k2; pass B reads it
   S *yb;            // [phi | pi]: pass A output x + dt/2 k2
-  const S *psi1;    // comoving: Psi, dPsi/dt at the first stage's time
+  const S *psi1;    // comoving: e^{2 Psi} - 1, dPsi/dt at the first stage's time
   const S *dpsi1;
   const S *psi2;    // ... at the second stage's time
   const S *dpsi2;

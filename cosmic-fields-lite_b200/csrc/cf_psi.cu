@@ -11,6 +11,12 @@
 //
 // Storage follows the context precision: FP64 (Z2D) or FP32 (C2R); the
 // transfer function is always evaluated in FP64.
+//
+// A slot holds (e^{2 Psi} - 1, dPsi/dt), not Psi: the right-hand side uses Psi
+// only through e^{2 Psi} and e^{4 Psi} = (e^{2 Psi})^2, so the exponential is
+// taken once per refresh here (at pass C's store, or in place after a cuFFT
+// C2R) instead of twice per stage evaluation in the steppers.  expm1 keeps the
+// small part of e^{2 Psi} (|Psi| ~ 1e-2) at full relative precision.
 
 #include <cuda_runtime.h>
 #include <cufft.h>
@@ -224,6 +230,16 @@ __global__ void __launch_bounds__(256) k_prune_c(const S *__restrict__ pb, S *__
 // stride, so pass 1 stores and pass 2 loads are free of bank conflicts, and
 // pass 2's global stores run along m1, i.e. along the output row.
 
+// e^{2 Psi} - 1 in the storage type.
+__device__ __forceinline__ double e2m1_of(double psi) { return expm1(2.0 * psi); }
+__device__ __forceinline__ float e2m1_of(float psi) { return expm1f(2.0f * psi); }
+
+template <typename S>
+__global__ void k_psi_to_e2m1(S *__restrict__ f, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) f[i] = e2m1_of(f[i]);
+}
+
 template <typename S>
 struct Tw32 {
   typename Cplx<S>::T w[16];  // e^{2 pi i e / 32}, e < 16
@@ -338,8 +354,25 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
     dft_inv<S, R2>(u, tw);
     C *row = reinterpret_cast<C *>(out) + ((long long)(f * N + a) * N + b0 + r) * M;
 #pragma unroll
-    for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
+    for (int m2 = 0; m2 < R2; ++m2) {
+      C o = u[m2];
+      if (f == 0) o = C{e2m1_of(o.x), e2m1_of(o.y)};  // the slot holds e^{2 Psi} - 1
+      row[m1 + R1 * m2] = o;
+    }
   }
+}
+
+// Psi -> e^{2 Psi} - 1 in place after a cuFFT C2R (the slot's first field).
+static int psi_to_e2m1(cf_ctx *ctx, void *f, cudaStream_t st) {
+  ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+  const long long n = ctx->N3;
+  const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (ctx->word == 8)
+    k_psi_to_e2m1<double><<<blocks, 256, 0, st>>>((double *)f, n);
+  else
+    k_psi_to_e2m1<float><<<blocks, 256, 0, st>>>((float *)f, n);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
 }
 
 // Pass-C shapes (M = N/2 = R1 x R2) and rows per CTA: staging tile <= ~64 KB.
@@ -599,7 +632,7 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
     else
       CF_TRY_CUFFT(cufftExecC2R(ctx->plan_pc, (cufftComplex *)ctx->psi_hc, (cufftReal *)out));
   }
-  return CF_OK;
+  return psi_to_e2m1(ctx, out, st);
 }
 
 int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void **dpsi) {
@@ -661,6 +694,7 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void 
     else
       CF_TRY_CUFFT(cufftExecC2R(ctx->plan_psi, (cufftComplex *)ctx->psi_hc, (cufftReal *)v->psi));
   }
+  CF_TRY(psi_to_e2m1(ctx, v->psi, st));
   v->t = t;
   v->valid = true;
   v->stamp = ++ctx->slot_clock;
@@ -677,26 +711,27 @@ int psi_route(const cf_ctx *ctx) {
                                                                                          : CF_PSI_PRUNED;
 }
 
+// Slot -> (Psi, dPsi/dt) in FP64: Psi = log1p(e^{2 Psi} - 1) / 2.
 template <typename S>
-__global__ void k_widen(const S *__restrict__ in, double *__restrict__ out, long long n) {
+__global__ void k_slot_to_fields(const S *__restrict__ e2m1, const S *__restrict__ dpsi, double *__restrict__ out,
+                                 long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (double)in[i];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    out[i] = 0.5 * log1p((double)e2m1[i]);
+    out[n + i] = (double)dpsi[i];
+  }
 }
 
 int psi_fields(cf_ctx *ctx, double t, double *d_out, cudaStream_t st) {
   const void *psi = nullptr, *dpsi = nullptr;
   CF_TRY(psi_at(ctx, t, st, &psi, &dpsi));
   const long long n = ctx->N3;
-  if (ctx->word == 8) {
-    CF_TRY_CUDA(cudaMemcpyAsync(d_out, psi, n * 8, cudaMemcpyDeviceToDevice, st));
-    CF_TRY_CUDA(cudaMemcpyAsync(d_out + n, dpsi, n * 8, cudaMemcpyDeviceToDevice, st));
-  } else {
-    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
-    k_widen<float><<<blocks, 256, 0, st>>>((const float *)psi, d_out, n);
-    CF_LAUNCHED(ctx);
-    k_widen<float><<<blocks, 256, 0, st>>>((const float *)dpsi, d_out + n, n);
-    CF_LAUNCHED(ctx);
-  }
+  const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (ctx->word == 8)
+    k_slot_to_fields<double><<<blocks, 256, 0, st>>>((const double *)psi, (const double *)dpsi, d_out, n);
+  else
+    k_slot_to_fields<float><<<blocks, 256, 0, st>>>((const float *)psi, (const float *)dpsi, d_out, n);
+  CF_LAUNCHED(ctx);
   return CF_OK;
 }
 

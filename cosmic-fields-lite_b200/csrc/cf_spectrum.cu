@@ -22,7 +22,7 @@ namespace cfb {
 // ---- energy density -----------------------------------------------------
 // rho = 1/2 (e^{-2Psi} pi^2 + m^2 phi^2 + e^{2Psi} 1/4 h^-2 a^-2 sum_axes (phi_{+1} - phi_{-1})^2)
 // with Psi = 0 for the uncoupled equations (src/equations_cuda.cu:332-369, :451-473;
-// src/equations.cpp:38-69, :106-138, :265-322).
+// src/equations.cpp:38-69, :106-138, :265-322); `psi` holds e^{2 Psi} - 1.
 template <typename S, bool COMOV>
 __global__ void k_energy(const S *__restrict__ x, const S *__restrict__ xlo, const S *__restrict__ psi,
                          double *__restrict__ rho, int N, double m2, double inv) {
@@ -47,8 +47,8 @@ __global__ void k_energy(const S *__restrict__ x, const S *__restrict__ xlo, con
     double p = (double)x[N3 + i];
     if (xlo) p += (double)xlo[N3 + i];
     if constexpr (COMOV) {
-      const double ps = (double)psi[i];
-      rho[i] = 0.5 * (exp(-2 * ps) * p * p + m2 * f * f + exp(2 * ps) * 0.25 * inv * grad);
+      const double e2 = 1.0 + (double)psi[i];
+      rho[i] = 0.5 * (p * p / e2 + m2 * f * f + e2 * 0.25 * inv * grad);
     } else {
       rho[i] = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad);
     }

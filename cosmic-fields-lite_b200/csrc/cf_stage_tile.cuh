@@ -89,7 +89,7 @@ struct StageArgs {
   S *acc;        // k accumulator [phi | pi]
   S *x;          // base state [phi | pi] (hi part in FP32_COMP)
   S *xlo;        // FP32_COMP compensation [phi | pi] (stage 4 only)
-  const S *psi;  // comoving: Psi(t_stage), N^3
+  const S *psi;  // comoving: e^{2 Psi(t_stage)} - 1, N^3
   const S *dpsi; // comoving: dPsi/dt(t_stage), N^3
   int N;
   int a_chunk;
@@ -133,10 +133,10 @@ struct Coef<float> {
   __device__ __forceinline__ float fma(float v, float add) const { return add + fmaf(hi, v, lo * v); }
 };
 
-// exp(2 Psi) and exp(4 Psi).  FP64: the reference's exp of the doubled argument.
-__device__ __forceinline__ void psi_factors(double psi, double &e2, double &e4) {
-  e2 = exp(2 * psi);
-  e4 = exp(4 * psi);
+// e^{2 Psi} and e^{4 Psi} from the Psi slot's e^{2 Psi} - 1 (FP64).
+__device__ __forceinline__ void psi_factors(double e2m1, double &e2, double &e4) {
+  e2 = 1.0 + e2m1;
+  e4 = e2 * e2;
 }
 
 // Laplacian sum (times h^2) at (row, col) of a staged plane whose a-neighbours
@@ -165,7 +165,8 @@ struct StageCoef {
 };
 
 // pi component of the right-hand side (src/equations_cuda.cu:15-36, :263-287):
-//   (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} h^-2 a^-2 lap phi.
+//   (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} h^-2 a^-2 lap phi,
+// with ps = e^{2 Psi} - 1 (the Psi slot's first field).
 template <bool COMOV, typename S, typename T = typename Arith<S>::T>
 __device__ __forceinline__ T kpi_of(T p0, T f0, T lap, S ps, S dps, const StageCoef<T> &k) {
   if constexpr (sizeof(T) == 8) {
@@ -180,7 +181,7 @@ __device__ __forceinline__ T kpi_of(T p0, T f0, T lap, S ps, S dps, const StageC
     const float mf = k.m2.mul(f0);
     const float g = k.inv.mul(lap);
     if constexpr (COMOV) {
-      const float e2m1 = expm1f(2.0f * (float)ps), e4m1 = expm1f(4.0f * (float)ps);
+      const float e2m1 = (float)ps, e4m1 = e2m1 * (e2m1 + 2.0f);  // e^{4Psi} - 1 = (e^{2Psi} - 1)(e^{2Psi} + 1)
       const float fr = 4.0f * (float)dps * p0 - k.hub3.mul(p0);
       return fr - fmaf(e2m1, mf, mf) + fmaf(e4m1, g, g);
     } else {

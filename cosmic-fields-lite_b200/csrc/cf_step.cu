@@ -48,7 +48,7 @@ struct StageMinBlocks {
 template <typename S, int H, bool COMOV, int STAGE, bool FULL>
 __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_stage(const StageArgs<S> A) {
   using TS = TileSmem<S, H, TX, TY>;
-  __shared__ S sm[TS::count];
+  __shared__ __align__(16) S sm[TS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
   stage_tile<S, H, COMOV, STAGE, TX, TY, FULL>(A, blockIdx.x * TS::TW, blockIdx.y * TY, a_begin,
                                                min(a_begin + A.a_chunk, A.N), sm);
@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
 // per storage type (FP32 7-point, FP32 13-point; FP64 uncoupled; FP64 comoving),
 // measured at N = 512 (ms per step: FP32 comoving 7-point, floors 2 / 3 / 4 ->
 // 4.80 / 4.29 / 4.52; 13-point 5.16 / 5.76 / 6.89; FP64 FRW 7-point 4.60 / 3.64 /
-// 3.23; FP64 comoving 7-point, floors 1 / 2 -> 9.49 / 5.97).
+// 3.23, 13-point 5.27 / 4.83 / 5.60; FP64 comoving 7-point, floors 1 / 2 -> 9.49
+// / 5.97).
 #ifndef CF_PAIR_MB_F32
 #define CF_PAIR_MB_F32 3
 #endif
@@ -68,19 +69,22 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
 #ifndef CF_PAIR_MB_F64
 #define CF_PAIR_MB_F64 4
 #endif
+#ifndef CF_PAIR_MB_F64_H2
+#define CF_PAIR_MB_F64_H2 3
+#endif
 #ifndef CF_PAIR_MB_F64_COMOV
 #define CF_PAIR_MB_F64_COMOV 2
 #endif
 template <typename S, int H, bool COMOV>
 struct PairMinBlocks {
   static constexpr int value = sizeof(S) == 4 ? (H == 1 ? CF_PAIR_MB_F32 : CF_PAIR_MB_F32_H2)
-                                              : (COMOV ? CF_PAIR_MB_F64_COMOV : CF_PAIR_MB_F64);
+                                              : (COMOV ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
 };
 
 template <typename S, int H, bool COMOV, int PASS, bool FULL>
 __global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, COMOV>::value)) k_pair(const PairArgs<S> A) {
   using PS = PairSmem<S, H, TX, TY>;
-  __shared__ S sm[PS::count];
+  __shared__ __align__(16) S sm[PS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
   pair_tile<S, H, COMOV, PASS, TX, TY, FULL>(A, blockIdx.x * PS::TS::TW, blockIdx.y * TY, a_begin,
                                              min(a_begin + A.a_chunk, A.N), sm);
