@@ -11,8 +11,9 @@
 //                      gives up with CF_ERR_TIMEOUT instead of hanging) before the
 //                      next stage.  Stage coefficients come from a per-step table
 //                      in device memory, so a captured graph replays it.
-//   CF_ENS_BATCHED     one launch per stage over the whole work list.
-//   CF_ENS_LOOP        one launch per stage per member (the single-instance path).
+//   CF_ENS_BATCHED     two launches per step over the whole work list: the paired
+//                      passes of cf_rk4_steps (stages 1+2, 3+4; cf_pair_tile.cuh).
+//   CF_ENS_LOOP        the same passes, one launch per member (the single-instance path).
 //
 // cf_ensemble_run_graph captures one observer interval -- barrier reset, the
 // persistent kernel for S steps and the advance of a device step counter -- in a
@@ -31,6 +32,7 @@
 #include <vector>
 
 #include "cf_internal.cuh"
+#include "cf_pair_tile.cuh"
 #include "cf_stage_tile.cuh"
 
 namespace cfb {
@@ -165,16 +167,16 @@ __device__ __forceinline__ bool grid_barrier(const EnsArgs &E) {
 }
 
 // Resident CTAs per SM that the ensemble kernels' register allocation must
-// allow (per-stage kernel, persistent kernel).  Uncapped, the persistent kernel,
-// which inlines all four stages, takes ~180 registers in FP32: one CTA per SM.
-// Measured on B200, 96 FRW lattices 32 x {64,96,128}^3, FP32-comp 7-point
-// (G site-updates/s, per-stage batched / persistent graph):
+// allow (persistent kernel, paired-stage kernels).  Uncapped, the persistent
+// kernel, which inlines all four stages, takes ~180 registers in FP32: one CTA
+// per SM.  Measured on B200, 96 FRW lattices 32 x {64,96,128}^3, FP32-comp
+// 7-point, single-stage tiles (G site-updates/s, batched / persistent graph):
 //   caps 1/1: 17.6 / 17.2;  2/2: 28.9 / 26.3;  3/3: 33.9 / 24.8 (persistent spills).
-#ifndef CF_ENS_MIN_BLOCKS
-#define CF_ENS_MIN_BLOCKS 3
-#endif
 #ifndef CF_ENS_PERSIST_MIN_BLOCKS
 #define CF_ENS_PERSIST_MIN_BLOCKS 2
+#endif
+#ifndef CF_ENS_PAIR_MIN_BLOCKS
+#define CF_ENS_PAIR_MIN_BLOCKS 3
 #endif
 
 // One stage of the persistent kernel: CTAs take work items from a shared
@@ -206,13 +208,72 @@ __global__ void __launch_bounds__(256, CF_ENS_PERSIST_MIN_BLOCKS) k_ens_persiste
   }
 }
 
-template <typename S, int H, int SHAPE>
-// One stage over the work list, one CTA per item; the step is the device step
-// counter plus `step_off`, so a captured graph of these launches walks forward.
-__global__ void __launch_bounds__(256, CF_ENS_MIN_BLOCKS) k_ens_stage(const EnsArgs E, int stage, int step_off) {
+// Paired-stage pass PASS (1: stages 1+2, 2: stages 3+4) of one work item, as
+// rk4_steps' paired route with the same coefficients.  Within a run, step j keeps
+// phi in x for even j and in the first half of ya for odd j (pass B writes the
+// other one); a run of odd length ends with k_ens_phi_back.
+template <typename S, int H, int SHAPE, int PASS>
+__device__ __forceinline__ void ens_item_pair(const EnsArgs &E, const EnsItem &it, long long step, bool odd, S *sm) {
   constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
-  __shared__ __align__(16) S sm[TileSmem<S, H, TXv, TYv>::count];
-  ens_item_stage<S, H, SHAPE>(E, E.items[blockIdx.x], stage, *E.step_counter + step_off, sm);
+  const EnsMember mb = E.members[it.member];
+  S *x = (S *)mb.x, *ya = (S *)mb.ya, *yb = (S *)mb.yb;
+  S *phi_cur = odd ? ya : x, *phi_nxt = odd ? x : ya;
+  PairArgs<S> A;
+  A.N = mb.N;
+  A.N3 = mb.N3;
+  A.m2 = mb.m2;
+  A.a_chunk = 0;
+  A.xphi = phi_cur;
+  A.xpi = x + mb.N3;
+  A.xlo = (sizeof(S) == 4) ? x + 2 * mb.N3 : nullptr;
+  A.acc = (S *)mb.acc;
+  A.yb = yb;
+  A.psi1 = A.dpsi1 = A.psi2 = A.dpsi2 = nullptr;
+  const EnsCoef c1 = E.coef[4 * step + (PASS == 1 ? 0 : 2)];
+  const EnsCoef c2 = E.coef[4 * step + (PASS == 1 ? 1 : 3)];
+  A.inv1 = mb.inv_scale / c1.a2;
+  A.hub3_1 = c1.hub3;
+  A.inv2 = mb.inv_scale / c2.a2;
+  A.hub3_2 = c2.hub3;
+  A.dt6 = E.dt / 6.0;
+  if constexpr (PASS == 1) {
+    A.uphi = phi_cur;
+    A.upi = x + mb.N3;
+    A.xphi_out = nullptr;
+    A.cw = E.dt / 2.0;
+    A.cy = E.dt / 2.0;
+  } else {
+    A.uphi = yb;
+    A.upi = yb + mb.N3;
+    A.xphi_out = phi_nxt;
+    A.cw = E.dt;
+    A.cy = 0.0;
+  }
+  pair_tile<S, H, false, PASS, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+}
+
+template <typename S, int H, int SHAPE, int PASS>
+__global__ void __launch_bounds__(256, CF_ENS_PAIR_MIN_BLOCKS) k_ens_pair(const EnsArgs E, int step_off) {
+  constexpr int TXv = EnsShape<SHAPE>::TX, TYv = EnsShape<SHAPE>::TY;
+  __shared__ __align__(16) S sm[PairSmem<S, H, TXv, TYv>::count];
+  ens_item_pair<S, H, SHAPE, PASS>(E, E.items[blockIdx.x], *E.step_counter + step_off, (step_off & 1) != 0, sm);
+}
+
+// phi back from ya to x over one work item's sites (after a run of odd length).
+template <typename S, int SHAPE>
+__global__ void __launch_bounds__(256) k_ens_phi_back(const EnsArgs E) {
+  constexpr int TXv = EnsShape<SHAPE>::TX;
+  constexpr int V = VecT<S>::n, TW = TXv * V;
+  const EnsItem it = E.items[blockIdx.x];
+  const EnsMember mb = E.members[it.member];
+  const int N = mb.N;
+  const int c = it.c0 + threadIdx.x * V, b = it.b0 + threadIdx.y;
+  if (threadIdx.x * V >= min(TW, N - it.c0) || b >= N) return;
+  const long long NN = (long long)N * N;
+  for (int a = it.a_begin; a < it.a_end; ++a) {
+    const long long site = NN * a + (long long)N * b + c;
+    stv((S *)mb.x + site, ldv((const S *)mb.ya + site));
+  }
 }
 
 __global__ void k_counter_add(long long *c, long long v) {
@@ -393,19 +454,36 @@ static int launch_persistent(cf_ensemble *E, int nsteps, double dt, cudaStream_t
   return CF_OK;
 }
 
-template <typename S, int H, int SHAPE>
-static int launch_batched_stage(cf_ensemble *E, int stage, int step_off, double dt, cudaStream_t st) {
+// One launch over work items [i0, i1): paired pass PASS (1, 2), or (PASS 0) phi
+// back from ya to x.
+template <typename S, int H, int SHAPE, int PASS>
+static int launch_items_pair(cf_ensemble *E, size_t i0, size_t i1, int step_off, double dt, cudaStream_t st) {
   EnsArgs A{};
   A.members = E->dm;
-  A.items = E->d_items;
-  A.n_items = (int)E->items.size();
+  A.items = E->d_items + i0;
+  A.n_items = (int)(i1 - i0);
   A.coef = E->d_coef;
   A.step_counter = E->d_step;
   A.dt = dt;
   const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
-  k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, stage, step_off);
+  if constexpr (PASS == 0)
+    k_ens_phi_back<S, SHAPE><<<A.n_items, block, 0, st>>>(A);
+  else
+    k_ens_pair<S, H, SHAPE, PASS><<<A.n_items, block, 0, st>>>(A, step_off);
   CF_TRY_CUDA(cudaGetLastError());
   E->launches++;
+  return CF_OK;
+}
+
+// nsteps RK4 steps over work items [i0, i1) as paired passes, steps from the
+// device step counter; phi back to x after an odd count.
+template <typename S, int H, int SHAPE>
+static int pair_steps(cf_ensemble *E, size_t i0, size_t i1, long long nsteps, double dt, cudaStream_t st) {
+  for (long long j = 0; j < nsteps; ++j) {
+    CF_TRY((launch_items_pair<S, H, SHAPE, 1>(E, i0, i1, (int)j, dt, st)));
+    CF_TRY((launch_items_pair<S, H, SHAPE, 2>(E, i0, i1, (int)j, dt, st)));
+  }
+  if (nsteps & 1) CF_TRY((launch_items_pair<S, H, SHAPE, 0>(E, i0, i1, 0, dt, st)));
   return CF_OK;
 }
 
@@ -425,33 +503,22 @@ static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, do
     }
     return CF_OK;
   }
-  if (mode == CF_ENS_BATCHED) {
-    for (long long j = 0; j < nsteps; ++j)
-      for (int s = 1; s <= 4; ++s) CF_TRY((launch_batched_stage<S, H, SHAPE>(E, s, (int)j, dt, st)));
-    return CF_OK;
+  if (mode == CF_ENS_BATCHED) return pair_steps<S, H, SHAPE>(E, 0, E->items.size(), nsteps, dt, st);
+  // CF_ENS_LOOP: the single-instance path, member by member (each member's
+  // items are contiguous in the work list)
+  std::vector<std::pair<size_t, size_t>> ranges;
+  for (size_t i0 = 0; i0 < E->items.size();) {
+    size_t i1 = i0;
+    while (i1 < E->items.size() && E->items[i1].member == E->items[i0].member) ++i1;
+    ranges.push_back({i0, i1});
+    i0 = i1;
   }
-  // CF_ENS_LOOP: the single-instance path, member by member
-  std::vector<EnsItem> all = E->items;
-  for (long long j = 0; j < nsteps; ++j)
-    for (int s = 1; s <= 4; ++s) {
-      size_t i0 = 0;
-      while (i0 < all.size()) {
-        size_t i1 = i0;
-        while (i1 < all.size() && all[i1].member == all[i0].member) ++i1;
-        EnsArgs A{};
-        A.members = E->dm;
-        A.items = E->d_items + i0;
-        A.n_items = (int)(i1 - i0);
-        A.coef = E->d_coef;
-        A.step_counter = E->d_step;
-        A.dt = dt;
-        const dim3 block(EnsShape<SHAPE>::TX, EnsShape<SHAPE>::TY);
-        k_ens_stage<S, H, SHAPE><<<A.n_items, block, 0, st>>>(A, s, (int)j);
-        CF_TRY_CUDA(cudaGetLastError());
-        E->launches++;
-        i0 = i1;
-      }
-    }
+  for (long long j = 0; j < nsteps; ++j) {
+    for (auto &r : ranges) CF_TRY((launch_items_pair<S, H, SHAPE, 1>(E, r.first, r.second, (int)j, dt, st)));
+    for (auto &r : ranges) CF_TRY((launch_items_pair<S, H, SHAPE, 2>(E, r.first, r.second, (int)j, dt, st)));
+  }
+  if (nsteps & 1)
+    for (auto &r : ranges) CF_TRY((launch_items_pair<S, H, SHAPE, 0>(E, r.first, r.second, 0, dt, st)));
   return CF_OK;
 }
 
@@ -472,19 +539,13 @@ static int run(cf_ensemble *E, int mode, long long step0, long long nsteps, doub
 
 template <typename S, int H>
 static int batched_launches(cf_ensemble *E, long long steps, double dt, cudaStream_t st) {
-  for (long long j = 0; j < steps; ++j)
-    for (int s = 1; s <= 4; ++s) {
-      if (E->shape == 1)
-        CF_TRY((launch_batched_stage<S, H, 1>(E, s, (int)j, dt, st)));
-      else
-        CF_TRY((launch_batched_stage<S, H, 0>(E, s, (int)j, dt, st)));
-    }
-  return CF_OK;
+  if (E->shape == 1) return pair_steps<S, H, 1>(E, 0, E->items.size(), steps, dt, st);
+  return pair_steps<S, H, 0>(E, 0, E->items.size(), steps, dt, st);
 }
 
 // One observer segment from the device step counter, then the counter advance
 // (graph-capturable: nothing is read from host memory).  CF_ENS_PERSISTENT: barrier
-// reset + the persistent kernel; CF_ENS_BATCHED: 4 launches per step.
+// reset + the persistent kernel; CF_ENS_BATCHED: 2 paired-stage launches per step.
 static int segment(cf_ensemble *E, int mode, long long steps, double dt, cudaStream_t st) {
   int s;
   if (mode == CF_ENS_BATCHED) {

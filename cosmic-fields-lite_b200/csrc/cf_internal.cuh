@@ -94,6 +94,7 @@ struct cf_ctx {
   // j < N, in the storage complex type; no padded HC rows, no C2R plan.
   bool pc_fused = false;
   void *pr_wN = nullptr;
+  void *pr_twM = nullptr;  // pass-1 twiddles e^{2 pi i k2 m1 / (N/2)}, [m1][k2]
 
   // Spectra: FP64 R2C plans and scratch.
   cufftHandle plan_d2z1 = 0, plan_d2z2 = 0;

@@ -228,11 +228,42 @@ __global__ void __launch_bounds__(256) k_prune_c(const S *__restrict__ pb, S *__
 // (consecutive b of one (f, a)); between the passes the rows sit in shared
 // memory as T[m1][k2][r] with the row index fastest, padded to an odd m1
 // stride, so pass 1 stores and pass 2 loads are free of bank conflicts, and
-// pass 2's global stores run along m1, i.e. along the output row.
+// pass 2's global stores run along m1, i.e. along the output row.  The input
+// tile holds X[k] and i X[k] w^k (formed once per input at load), and the
+// pass-1 twiddles e^{2 pi i k2 m1 / M} are staged in shared memory as TW[m1][k2].
 
-// e^{2 Psi} - 1 in the storage type.
-__device__ __forceinline__ double e2m1_of(double psi) { return expm1(2.0 * psi); }
-__device__ __forceinline__ float e2m1_of(float psi) { return expm1f(2.0f * psi); }
+// e^{2 Psi} - 1 in the storage type.  For |2 Psi| <= 1/4 (the fields' range:
+// rms 1e-2) the Taylor series of e^x - 1 truncated after x^7 in FP32 (relative
+// truncation error < 2^-29) and after x^13 in FP64 (< 2^-62), by Horner's rule;
+// outside that range the library expm1.
+__device__ __forceinline__ float e2m1_of(float psi) {
+  const float x = 2.0f * psi;
+  if (fabsf(x) > 0.25f) return expm1f(x);
+  float q = 1.0f / 5040.0f;
+  q = fmaf(q, x, 1.0f / 720.0f);
+  q = fmaf(q, x, 1.0f / 120.0f);
+  q = fmaf(q, x, 1.0f / 24.0f);
+  q = fmaf(q, x, 1.0f / 6.0f);
+  q = fmaf(q, x, 0.5f);
+  return fmaf(q, x * x, x);
+}
+__device__ __forceinline__ double e2m1_of(double psi) {
+  const double x = 2.0 * psi;
+  if (fabs(x) > 0.25) return expm1(x);
+  double q = 1.0 / 6227020800.0;  // 1/13!
+  q = fma(q, x, 1.0 / 479001600.0);
+  q = fma(q, x, 1.0 / 39916800.0);
+  q = fma(q, x, 1.0 / 3628800.0);
+  q = fma(q, x, 1.0 / 362880.0);
+  q = fma(q, x, 1.0 / 40320.0);
+  q = fma(q, x, 1.0 / 5040.0);
+  q = fma(q, x, 1.0 / 720.0);
+  q = fma(q, x, 1.0 / 120.0);
+  q = fma(q, x, 1.0 / 24.0);
+  q = fma(q, x, 1.0 / 6.0);
+  q = fma(q, x, 0.5);
+  return fma(q, x * x, x);
+}
 
 template <typename S>
 __global__ void k_psi_to_e2m1(S *__restrict__ f, long long n) {
@@ -303,19 +334,26 @@ __device__ __forceinline__ void dft_inv(typename Cplx<S>::T (&v)[R], const Tw32<
 
 template <typename S, int R1, int R2, int ROWS>
 __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S *__restrict__ out,
-                                                     const typename Cplx<S>::T *__restrict__ wN, int N, int Kc,
+                                                     const typename Cplx<S>::T *__restrict__ wN,
+                                                     const typename Cplx<S>::T *__restrict__ twM, int N, int Kc,
                                                      const __grid_constant__ Tw32<S> tw) {
   using C = typename Cplx<S>::T;
   constexpr int M = R1 * R2;  // N == 2 M
   constexpr int TS = R2 * ROWS + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   C *T = reinterpret_cast<C *>(smraw);  // [R1][TS]
-  C *Xs = T + R1 * TS;                  // [Kc+1][ROWS]
+  C *TW = T + R1 * TS;                  // [R1][R2]: e^{2 pi i k2 m1 / M}
+  C *Xs = TW + M;                       // [Kc+1][ROWS]: X[k] (X[0] by its real part)
+  C *XPs = Xs + (Kc + 1) * ROWS;        // [Kc+1][ROWS]: i X[k] w^k
   const int b0 = blockIdx.x * ROWS, a = blockIdx.y, f = blockIdx.z;
   const C *src = reinterpret_cast<const C *>(pb) + ((long long)f * (Kc + 1) * N + a) * N + b0;
+  for (int i = threadIdx.x; i < M; i += blockDim.x) TW[i] = twM[i];
   for (int i = threadIdx.x; i < (Kc + 1) * ROWS; i += blockDim.x) {
     const int k = i / ROWS, r = i - k * ROWS;
-    Xs[i] = src[(long long)k * N * N + r];
+    C x = src[(long long)k * N * N + r];
+    if (k == 0) x.y = (S)0;
+    Xs[i] = x;
+    XPs[i] = c_mul_i(c_mul(x, wN[k]));
   }
   __syncthreads();
   for (int task = threadIdx.x; task < R2 * ROWS; task += blockDim.x) {
@@ -326,13 +364,10 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
       const int k = k2 + R2 * k1;
       C z{(S)0, (S)0};
       if (k <= Kc) {
-        C x = Xs[k * ROWS + r];
-        if (k == 0) x.y = (S)0;
-        z = c_add(x, c_mul_i(c_mul(x, wN[k])));
+        z = c_add(Xs[k * ROWS + r], XPs[k * ROWS + r]);  // X + i X w^k
       } else if (k >= M - Kc) {
         const int j = M - k;
-        const C x = Xs[j * ROWS + r];
-        const C d = c_sub(x, c_mul_i(c_mul(x, wN[j])));
+        const C d = c_sub(Xs[j * ROWS + r], XPs[j * ROWS + r]);  // conj(X - i X w^j)
         z = C{d.x, -d.y};
       }
       v[k1] = z;
@@ -341,7 +376,7 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
       C y = v[m1];
-      if (m1 > 0) y = c_mul(y, wN[(2 * k2 * m1) & (N - 1)]);  // e^{2 pi i k2 m1 / M}
+      if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);  // e^{2 pi i k2 m1 / M}
       T[m1 * TS + k2 * ROWS + r] = y;
     }
   }
@@ -398,7 +433,8 @@ static bool pc_shape(long long N, size_t word, PcShape *sh) {
   return true;
 }
 static size_t pc_fused_smem(const cf_ctx *ctx, const PcShape &sh) {
-  return ((size_t)sh.R1 * (sh.R2 * sh.rows + 1) + (size_t)(ctx->Kc + 1) * sh.rows) * 2 * ctx->word;
+  return ((size_t)sh.R1 * (sh.R2 * sh.rows + 1) + (size_t)sh.R1 * sh.R2 + 2 * (size_t)(ctx->Kc + 1) * sh.rows) * 2 *
+         ctx->word;
 }
 
 template <typename S, int R1, int R2, int ROWS>
@@ -412,8 +448,8 @@ static int launch_pc_fused_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t s
     tw.w[e] = C{(S)std::cos(ang), (S)std::sin(ang)};
   }
   const int N = (int)ctx->N;
-  kern<<<dim3(N / ROWS, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)out, (const C *)ctx->pr_wN, N, ctx->Kc,
-                                                 tw);
+  kern<<<dim3(N / ROWS, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)out, (const C *)ctx->pr_wN,
+                                                 (const C *)ctx->pr_twM, N, ctx->Kc, tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
@@ -513,10 +549,11 @@ static void free_pruned(cf_ctx *ctx) {
   cudaFree(ctx->pz_a);
   cudaFree(ctx->pz_b);
   cudaFree(ctx->pr_wN);
+  cudaFree(ctx->pr_twM);
   cufftDestroy(ctx->plan_pa);
   cufftDestroy(ctx->plan_pb);
   if (!ctx->pc_fused) cufftDestroy(ctx->plan_pc);
-  ctx->pz_a = ctx->pz_b = ctx->pr_wN = nullptr;
+  ctx->pz_a = ctx->pz_b = ctx->pr_wN = ctx->pr_twM = nullptr;
   ctx->have_pruned = false;
 }
 
@@ -553,16 +590,28 @@ static int ensure_pruned(cf_ctx *ctx) {
       w[2 * j] = std::cos(ang);
       w[2 * j + 1] = std::sin(ang);
     }
-    if (cudaMalloc(&ctx->pr_wN, (size_t)N * cb) != cudaSuccess) {
+    // pass-1 twiddles e^{2 pi i k2 m1 / M} = w^{2 k2 m1}, laid out [m1][k2]
+    const long long M = N / 2;
+    std::vector<double> t(2 * M);
+    for (int m1 = 0; m1 < sh.R1; ++m1)
+      for (int k2 = 0; k2 < sh.R2; ++k2) {
+        const long long e = (2LL * k2 * m1) % N;
+        t[2 * (m1 * sh.R2 + k2)] = w[2 * e];
+        t[2 * (m1 * sh.R2 + k2) + 1] = w[2 * e + 1];
+      }
+    if (cudaMalloc(&ctx->pr_wN, (size_t)N * cb) != cudaSuccess ||
+        cudaMalloc(&ctx->pr_twM, (size_t)M * cb) != cudaSuccess) {
       cudaGetLastError();
       set_error("cudaMalloc of the pass-C twiddles failed");
       return CF_ERR_NOMEM;
     }
     if (dp) {
       CF_TRY_CUDA(cudaMemcpy(ctx->pr_wN, w.data(), (size_t)N * cb, cudaMemcpyHostToDevice));
+      CF_TRY_CUDA(cudaMemcpy(ctx->pr_twM, t.data(), (size_t)M * cb, cudaMemcpyHostToDevice));
     } else {
-      std::vector<float> wf(w.begin(), w.end());
+      std::vector<float> wf(w.begin(), w.end()), tf(t.begin(), t.end());
       CF_TRY_CUDA(cudaMemcpy(ctx->pr_wN, wf.data(), (size_t)N * cb, cudaMemcpyHostToDevice));
+      CF_TRY_CUDA(cudaMemcpy(ctx->pr_twM, tf.data(), (size_t)M * cb, cudaMemcpyHostToDevice));
     }
   } else {
     CF_TRY(ensure_psi_hc(ctx));

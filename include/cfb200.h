@@ -242,8 +242,9 @@ int cf_shell_amplitude_gradient(cf_ctx *ctx, const double *d_lambda_phi, const d
  * per process (src/main.cpp:82-196).
  *   CF_ENS_PERSISTENT: one cooperative kernel for all nsteps (grid barriers between
  *     stages; a barrier that waits too long returns CF_ERR_TIMEOUT, never hangs).
- *   CF_ENS_BATCHED: one launch per stage over all members.
- *   CF_ENS_LOOP: one launch per stage per member (single-instance path).
+ *   CF_ENS_BATCHED: two launches per step over all members (the paired-stage
+ *     passes of cf_rk4_steps: stages 1+2, 3+4).
+ *   CF_ENS_LOOP: the same passes, one launch per member (single-instance path).
  * cf_ensemble_run_graph: nsegments observer intervals of steps_per_segment steps from
  *   t0 (absolute steps 0..): a CUDA graph of one interval -- the persistent kernel
  *   (mode CF_ENS_PERSISTENT) or the 4 * steps_per_segment batched launches (mode
