@@ -276,6 +276,76 @@ def accuracy_run(N, L, nsteps, every):
             "max_bin_rel_ge_1e-6_max": worst_bin}
 
 
+def adjoint_bench(N=256, nsteps=200, every=20, ngroups=32, floor=1e-12):
+    """Config 4: plain FRW KG at N=256, L=256, 200 RK4 steps (dt = 0.05 from t = 1)
+    with checkpoints every 20 steps; phi0 = c2r(sqrt(theta_g) sqrtP(k) xi_k) with 32
+    shell-group amplitudes theta (GRF baseline k* = 0.25), dphi0 = 0; loss = sum over
+    the shells within 12 decades of the peak of (log P_rho - log P_target)^2, the
+    target from the m = 1.1 run.  Times one gradient (checkpointed forward, loss,
+    reverse sweep, theta gradient) in FP64 and FP32-comp, and checks dL/dm and
+    dL/dtheta_0 of the FP64 adjoint against central differences (h = 1e-4)."""
+    import numpy as np
+    import torch
+
+    import cfb200
+    from cfb200 import fields
+    L, dt, t0 = float(N), 0.05, 1.0
+    xi = torch.from_numpy(fields.white_noise_hc(N, 11)).cuda()
+    sqrtP = torch.from_numpy(fields.gaussian_sqrtP_by_s2(N, L, 0.25)).cuda()
+
+    def run(theta, m, precision, target=None, grad=False):
+        ctx = cfb200.Context(N, L, m=m, equation=cfb200.EQ_KG_FRW, precision=precision, stencil=7, **FRW)
+        nsh = ctx.info.shells
+        spg = -(-nsh // ngroups)
+        phi = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
+        cfb200.field_from_shell_amplitudes(ctx, xi, sqrtP, theta, spg, phi)
+        st = torch.empty(ctx.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+        ctx.import_f64(st, torch.cat([phi, torch.zeros_like(phi)]))
+        adj = cfb200.Adjoint(ctx, nsteps, every)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        adj.forward(st, t0, dt)
+        if target is None:
+            sh = torch.empty(nsh, dtype=torch.float64, device="cuda")
+            s2 = torch.empty(ctx.info.s2_bins, dtype=torch.float64, device="cuda")
+            ctx.density_spectrum_s2(st, t0 + nsteps * dt, s2)
+            ctx.s2_to_shells(sh)
+            out = sh.cpu().numpy()
+            adj.close()
+            return out
+        loss = adj.shell_log_loss(st, target, floor)
+        if not grad:
+            adj.close()
+            return loss
+        lam0 = torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
+        dm = adj.backward(lam0)
+        gth = cfb200.shell_amplitude_gradient(ctx, lam0[: N ** 3], xi, sqrtP, theta, spg)
+        e1.record()
+        torch.cuda.synchronize()
+        adj.close()
+        return loss, gth, dm, e0.elapsed_time(e1)
+
+    theta = np.ones(ngroups)
+    target = run(theta, 1.1, cfb200.FP64)
+    res = {"N": N, "steps": nsteps, "checkpoint_every": every, "parameters": ngroups + 1}
+    for name, prec in (("fp64", cfb200.FP64), ("fp32comp", cfb200.FP32_COMP)):
+        run(theta, 1.0, prec, target, grad=True)  # warm
+        loss, gth, dm, ms = run(theta, 1.0, prec, target, grad=True)
+        res[name] = {"ms_per_gradient": ms, "loss": loss, "dL_dm": dm}
+        if name == "fp64":
+            h = 1e-4
+            fd_m = (run(theta, 1.0 + h, prec, target) - run(theta, 1.0 - h, prec, target)) / (2 * h)
+            tp, tm = theta.copy(), theta.copy()
+            tp[0] += h
+            tm[0] -= h
+            fd_t = (run(tp, 1.0, prec, target) - run(tm, 1.0, prec, target)) / (2 * h)
+            res["fd_check_fp64"] = {"dL_dm_rel_err": abs(dm - fd_m) / abs(fd_m),
+                                    "dL_dtheta0_err_rel_to_max_grad": abs(gth[0] - fd_t) / np.abs(gth).max()}
+    torch.cuda.empty_cache()
+    return res
+
+
 def ensemble_bench(steps=100, per_segment=50):
     """Config 3: 96 FRW Klein-Gordon lattices (32 x 64^3, 32 x 96^3, 32 x 128^3),
     L = N, m ~ U[0.5, 2] (seed 12345), GRF initial fields (k* = 0.5, <phi^2> = 1,
@@ -433,11 +503,16 @@ def run_product(args):
         del c2, s2_
         torch.cuda.empty_cache()
 
-    # ---- config 3: ensemble of uneven N in one captured persistent launch per interval
+    # ---- config 3: ensemble of uneven N, one captured graph per observer interval
     try:
         secondary["ensemble_config3"] = ensemble_bench()
     except Exception as e:  # reported, not hidden
         secondary["ensemble_config3"] = {"error": str(e)}
+    # ---- config 4: adjoint gradient of the shell-spectrum loss
+    try:
+        secondary["adjoint_config4"] = adjoint_bench()
+    except Exception as e:  # reported, not hidden
+        secondary["adjoint_config4"] = {"error": str(e)}
 
     # ---- end to end through the C ABI with host buffers: one observer interval
     # (dt_save = 5 -> 100 RK4 steps) per e2e step: upload the state from pinned
@@ -484,6 +559,19 @@ def run_product(args):
                              f"on the same workload at N={nb}, 2 RK4 steps ({el:.1f} s), single thread as "
                              f"shipped; FFTs through the FFTW3 restatement"}
 
+    # ---- config 2 at N = 1024 (the headline workload, 8x the sites)
+    try:
+        del ctx, st
+        torch.cuda.empty_cache()
+        c2, s2_ = make_case(1024, 1024.0, "fp32comp", 7, True)
+        t2, _, p2 = time_steps(c2, s2_, 10, 3, profile=True)
+        secondary["fp32comp_comoving_7pt_n1024"] = {
+            "value": world * 1024 ** 3 * 10 / (max_over_ranks(t2, pg) * 1e-3), "ms_per_step": t2 / 10,
+            "psi_route": int(c2.info.psi_route)}
+        del c2, s2_
+        torch.cuda.empty_cache()
+    except Exception as e:  # reported, not hidden
+        secondary["fp32comp_comoving_7pt_n1024"] = {"error": str(e)}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
