@@ -63,6 +63,12 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
 #ifndef CF_PAIR_MB_F32
 #define CF_PAIR_MB_F32 3
 #endif
+// pass A of the uncoupled equations fits 64 registers without spills: 4 CTAs/SM
+// (FP32 KG-FRW 7-point pass A: floors 3 / 4 -> 0.93 / 0.80 ms; comoving pass A 1.06 /
+// 1.12 ms, pass B 1.71 / 2.05 ms)
+#ifndef CF_PAIR_MB_F32_A
+#define CF_PAIR_MB_F32_A 4
+#endif
 #ifndef CF_PAIR_MB_F32_H2
 #define CF_PAIR_MB_F32_H2 2
 #endif
@@ -75,14 +81,15 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
 #ifndef CF_PAIR_MB_F64_COMOV
 #define CF_PAIR_MB_F64_COMOV 2
 #endif
-template <typename S, int H, bool COMOV>
+template <typename S, int H, bool COMOV, int PASS>
 struct PairMinBlocks {
-  static constexpr int value = sizeof(S) == 4 ? (H == 1 ? CF_PAIR_MB_F32 : CF_PAIR_MB_F32_H2)
-                                              : (COMOV ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
+  static constexpr int value =
+      sizeof(S) == 4 ? (H == 1 ? ((PASS == 1 && !COMOV) ? CF_PAIR_MB_F32_A : CF_PAIR_MB_F32) : CF_PAIR_MB_F32_H2)
+                     : (COMOV ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
 };
 
 template <typename S, int H, bool COMOV, int PASS, bool FULL>
-__global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, COMOV>::value)) k_pair(const PairArgs<S> A) {
+__global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, COMOV, PASS>::value)) k_pair(const PairArgs<S> A) {
   using PS = PairSmem<S, H, TX, TY>;
   __shared__ __align__(16) S sm[PS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
