@@ -3,11 +3,12 @@
 //
 // Every member is an independent lattice (its own N, L, m; a shared
 // cosmology, time grid, precision and stencil).  A step of the whole ensemble is
-// the same four fused RK4 stages as cf_rk4_steps (cf_stage_tile.cuh), applied to
-// a work list of (member, b-tile, c-tile, a-chunk) items.  Three schedules:
+// the same fused RK4 passes as cf_rk4_steps, applied to a work list of (member,
+// b-tile, c-tile, a-chunk) items.  Three schedules:
 //
-//   CF_ENS_PERSISTENT  one cooperative kernel for all steps: each CTA walks the
-//                      work list of a stage, then a grid barrier (bounded spin:
+//   CF_ENS_PERSISTENT  one cooperative kernel for all steps over the four
+//                      single-stage tiles (cf_stage_tile.cuh): each CTA takes work
+//                      items of a stage, then a grid barrier (bounded spin:
 //                      gives up with CF_ERR_TIMEOUT instead of hanging) before the
 //                      next stage.  Stage coefficients come from a per-step table
 //                      in device memory, so a captured graph replays it.
@@ -15,10 +16,11 @@
 //                      passes of cf_rk4_steps (stages 1+2, 3+4; cf_pair_tile.cuh).
 //   CF_ENS_LOOP        the same passes, one launch per member (the single-instance path).
 //
-// cf_ensemble_run_graph captures one observer interval -- barrier reset, the
-// persistent kernel for S steps and the advance of a device step counter -- in a
-// CUDA graph and replays it once per interval; the members' density spectra at
-// each interval end are enqueued on the same stream after the replay.
+// cf_ensemble_run_graph captures one observer interval -- the batched launches
+// (or barrier reset + the persistent kernel) for S steps and the advance of a
+// device step counter -- in a CUDA graph and replays it once per interval; the
+// members' density spectra at each interval end are enqueued on the same stream
+// after the replay.
 //
 // Tile shapes and a-chunk lengths are chosen per size class by cf_ensemble_autotune
 // (timing of the candidates on the members themselves).
@@ -373,7 +375,7 @@ static void build_items(cf_ensemble *E) {
     const int shape = E->shape;  // one kernel instantiation per launch
     const int TX = shape == 0 ? EnsShape<0>::TX : EnsShape<1>::TX;
     const int TY = shape == 0 ? EnsShape<0>::TY : EnsShape<1>::TY;
-    const int TW = TX * (int)(16 / E->word);
+    const int TW = TX * (E->word == 4 ? VecT<float>::n : VecT<double>::n);
     const int ach = tn.second;
     for (int a = 0; a < N; a += ach)
       for (int b = 0; b < N; b += TY)

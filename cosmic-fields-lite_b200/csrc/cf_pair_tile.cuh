@@ -58,9 +58,9 @@ struct PairArgs {
   double dt6;           // pass B: dt / 6
 };
 
-template <typename S, int H, int TXv, int TYv>
+template <typename S, int H, int TXv, int TYv, int VW = VecT<S>::n>
 struct PairSmem {
-  using TS = TileSmem<S, H, TXv, TYv>;
+  using TS = TileSmem<S, H, TXv, TYv, VW>;
   static constexpr int plane = TS::plane;
   static constexpr int bufs = DoubleBuffered<S>::value ? 2 : 1;
   static constexpr int count = 2 * bufs * plane;  // u and w planes
@@ -71,10 +71,10 @@ __device__ __forceinline__ S w_of(S xphi, S upi, const Coef<T> &cw) {
   return (S)cw.fma((T)upi, (T)xphi);
 }
 
-template <typename S, int H, bool COMOV, int PASS, int TXv, int TYv, bool FULL = false>
+template <typename S, int H, bool COMOV, int PASS, int TXv, int TYv, bool FULL = false, int VW = VecT<S>::n>
 __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, int a_begin, int a_end, S *smem) {
-  using TS = TileSmem<S, H, TXv, TYv>;
-  using PS = PairSmem<S, H, TXv, TYv>;
+  using TS = TileSmem<S, H, TXv, TYv, VW>;
+  using PS = PairSmem<S, H, TXv, TYv, VW>;
   constexpr bool DB = DoubleBuffered<S>::value;
   constexpr int V = TS::V;
   constexpr int TW = TS::TW;
@@ -99,21 +99,21 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
   const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(A.inv2), Coef<T>(A.hub3_2)};
   const Coef<T> cw(A.cw), cy(A.cy);
 
-  auto load_w = [&](long long off) -> Pack<S> {
-    const Pack<S> p = ldv(upi + off);
-    const Pack<S> f = (PASS == 1) ? ldv(uphi + off) : ldv(xphi + off);
-    Pack<S> w;
+  auto load_w = [&](long long off) -> Pack<S, V> {
+    const Pack<S, V> p = ldv<S, V>(upi + off);
+    const Pack<S, V> f = (PASS == 1) ? ldv<S, V>(uphi + off) : ldv<S, V>(xphi + off);
+    Pack<S, V> w;
 #pragma unroll
     for (int v = 0; v < V; ++v) w.v[v] = w_of(f.v[v], p.v[v], cw);
     return w;
   };
 
-  Pack<S> qu[2 * H + 1], qw[2 * H + 1];
+  Pack<S, V> qu[2 * H + 1], qw[2 * H + 1];
   if (act) {
 #pragma unroll
     for (int j = 0; j < 2 * H; ++j) {
       const long long off = NN * ((a_begin - H + j + N) % N) + rowoff;
-      qu[j + 1] = ldv(uphi + off);
+      qu[j + 1] = ldv<S, V>(uphi + off);
       qw[j + 1] = load_w(off);
     }
   }
@@ -125,27 +125,27 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
       qu[j] = qu[j + 1];
       qw[j] = qw[j + 1];
     }
-    Pack<S> p0v, xp, xq, cp, cq, lp, lq, ps1, dps1, ps2, dps2;
+    Pack<S, V> p0v, xp, xq, cp, cq, lp, lq, ps1, dps1, ps2, dps2;
     if (act) {
       const long long head = NN * ((a + H) % N) + rowoff;
-      qu[2 * H] = ldv(uphi + head);
+      qu[2 * H] = ldv<S, V>(uphi + head);
       qw[2 * H] = load_w(head);
-      p0v = ldv(upi + site);
+      p0v = ldv<S, V>(upi + site);
       if constexpr (PASS == 2) {
-        xp = ldv(xphi + site);
-        xq = ldv_rw(A.xpi + site);
-        cp = ldv(A.acc + site);
-        cq = ldv(A.acc + N3 + site);
+        xp = ldv<S, V>(xphi + site);
+        xq = ldv_rw<S, V>(A.xpi + site);
+        cp = ldv<S, V>(A.acc + site);
+        cq = ldv<S, V>(A.acc + N3 + site);
         if constexpr (sizeof(S) == 4) {
-          lp = ldv_rw(A.xlo + site);
-          lq = ldv_rw(A.xlo + N3 + site);
+          lp = ldv_rw<S, V>(A.xlo + site);
+          lq = ldv_rw<S, V>(A.xlo + N3 + site);
         }
       }
       if constexpr (COMOV) {
-        ps1 = ldv(A.psi1 + site);
-        dps1 = ldv(A.dpsi1 + site);
-        ps2 = ldv(A.psi2 + site);
-        dps2 = ldv(A.dpsi2 + site);
+        ps1 = ldv<S, V>(A.psi1 + site);
+        dps1 = ldv<S, V>(A.dpsi1 + site);
+        ps2 = ldv<S, V>(A.psi2 + site);
+        dps2 = ldv<S, V>(A.dpsi2 + site);
       }
     }
     S *smu = smem;
@@ -172,8 +172,8 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
         if (r >= 0) {
           const int gb = (b0 - H + r + N) % N;
           const long long off = NN * a + (long long)N * gb + c;
-          const Pack<S> hu = ldv(uphi + off);
-          const Pack<S> hw = load_w(off);
+          const Pack<S, V> hu = ldv<S, V>(uphi + off);
+          const Pack<S, V> hw = load_w(off);
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             smu[r * SP + H + tx * V + v] = hu.v[v];
@@ -202,7 +202,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
     __syncthreads();
     if (!act) continue;
 
-    Pack<S> o1, o2, o3, o4;
+    Pack<S, V> o1, o2, o3, o4;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const int col = H + tx * V + v;

@@ -22,28 +22,38 @@
 
 namespace cfb {
 
-template <typename S>
-struct VecT;
+// A thread's consecutive sites along c, moved as one vector: V = 4 floats or 2
+// doubles (16 bytes) by default; some kernels take V = 2 floats (8 bytes), which
+// halves the registers a thread's sites occupy.
+template <typename S, int V>
+struct VecOf;
 template <>
-struct VecT<double> {
+struct VecOf<double, 2> {
   using T = double2;
-  static constexpr int n = 2;
 };
 template <>
-struct VecT<float> {
+struct VecOf<float, 4> {
   using T = float4;
-  static constexpr int n = 4;
+};
+template <>
+struct VecOf<float, 2> {
+  using T = float2;
+};
+template <typename S>
+struct VecT {
+  static constexpr int n = 16 / sizeof(S);
+  using T = typename VecOf<S, n>::T;
 };
 
-template <typename S>
+template <typename S, int V = VecT<S>::n>
 struct Pack {
-  S v[VecT<S>::n];
+  S v[V];
 };
 
-template <typename S>
-__device__ __forceinline__ Pack<S> unpack(const typename VecT<S>::T &t) {
-  Pack<S> r;
-  if constexpr (VecT<S>::n == 2) {
+template <typename S, int V>
+__device__ __forceinline__ Pack<S, V> unpack(const typename VecOf<S, V>::T &t) {
+  Pack<S, V> r;
+  if constexpr (V == 2) {
     r.v[0] = t.x;
     r.v[1] = t.y;
   } else {
@@ -56,21 +66,21 @@ __device__ __forceinline__ Pack<S> unpack(const typename VecT<S>::T &t) {
 }
 
 // read-only path (buffers the kernel does not write)
-template <typename S>
-__device__ __forceinline__ Pack<S> ldv(const S *p) {
-  return unpack<S>(__ldg(reinterpret_cast<const typename VecT<S>::T *>(p)));
+template <typename S, int V = VecT<S>::n>
+__device__ __forceinline__ Pack<S, V> ldv(const S *p) {
+  return unpack<S, V>(__ldg(reinterpret_cast<const typename VecOf<S, V>::T *>(p)));
 }
 
 // plain load for buffers the same kernel also writes (acc, x)
-template <typename S>
-__device__ __forceinline__ Pack<S> ldv_rw(const S *p) {
-  return unpack<S>(*reinterpret_cast<const typename VecT<S>::T *>(p));
+template <typename S, int V = VecT<S>::n>
+__device__ __forceinline__ Pack<S, V> ldv_rw(const S *p) {
+  return unpack<S, V>(*reinterpret_cast<const typename VecOf<S, V>::T *>(p));
 }
 
-template <typename S>
-__device__ __forceinline__ void stv(S *p, const Pack<S> &r) {
-  typename VecT<S>::T t;
-  if constexpr (VecT<S>::n == 2) {
+template <typename S, int V>
+__device__ __forceinline__ void stv(S *p, const Pack<S, V> &r) {
+  typename VecOf<S, V>::T t;
+  if constexpr (V == 2) {
     t.x = r.v[0];
     t.y = r.v[1];
   } else {
@@ -79,7 +89,7 @@ __device__ __forceinline__ void stv(S *p, const Pack<S> &r) {
     t.z = r.v[2];
     t.w = r.v[3];
   }
-  *reinterpret_cast<typename VecT<S>::T *>(p) = t;
+  *reinterpret_cast<typename VecOf<S, V>::T *>(p) = t;
 }
 
 template <typename S>
@@ -143,8 +153,8 @@ __device__ __forceinline__ void psi_factors(double e2m1, double &e2, double &e4)
 // are q[0..2H] (q[H] the plane itself): 7-point for H = 1, 13-point 4th order for
 // H = 2 (src/fdm3d_cuda.cu:20-83).  The single-stage and the paired-stage tiles
 // both form it here, so their sums round identically.
-template <typename S, int H, int SP, typename T = typename Arith<S>::T>
-__device__ __forceinline__ T lap_at(const Pack<S> (&q)[2 * H + 1], const S *sm, int row, int col, int v) {
+template <typename S, int H, int SP, int V, typename T = typename Arith<S>::T>
+__device__ __forceinline__ T lap_at(const Pack<S, V> (&q)[2 * H + 1], const S *sm, int row, int col, int v) {
   const T f0 = (T)q[H].v[v];
   if constexpr (H == 1) {
     const T s = (T)-6 * f0 + (T)q[2].v[v] + (T)q[0].v[v] + (T)sm[(row + 1) * SP + col] + (T)sm[(row - 1) * SP + col];
@@ -201,9 +211,9 @@ struct DoubleBuffered {
   static constexpr bool value = sizeof(S) == 4;
 };
 
-template <typename S, int H, int TXv, int TYv>
+template <typename S, int H, int TXv, int TYv, int VW = VecT<S>::n>
 struct TileSmem {
-  static constexpr int V = VecT<S>::n;
+  static constexpr int V = VW;
   static constexpr int TW = TXv * V;
   static constexpr int SP = TW + 2 * H;
   static constexpr int SR = TYv + 2 * H;

@@ -81,19 +81,36 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
 #ifndef CF_PAIR_MB_F64_COMOV
 #define CF_PAIR_MB_F64_COMOV 2
 #endif
+// Sites per thread of a paired pass: 16-byte vectors, except the FP32 comoving
+// 7-point pass B, the pass with the most live values, which takes 2 floats per
+// thread and 4 CTAs/SM without spills (N = 512: 1.71 -> 1.52 ms per step; the
+// other FP32 passes measured slower with 2 floats per thread).
+template <typename S, int H, bool COMOV, int PASS>
+struct PairVec {
+  static constexpr int value = (sizeof(S) == 4 && COMOV && H == 1 && PASS == 2) ? 2 : VecT<S>::n;
+};
+#ifndef CF_PAIR_MB_F32_V2
+#define CF_PAIR_MB_F32_V2 4
+#endif
+
 template <typename S, int H, bool COMOV, int PASS>
 struct PairMinBlocks {
   static constexpr int value =
-      sizeof(S) == 4 ? (H == 1 ? ((PASS == 1 && !COMOV) ? CF_PAIR_MB_F32_A : CF_PAIR_MB_F32) : CF_PAIR_MB_F32_H2)
-                     : (COMOV ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
+      sizeof(S) == 4
+          ? (H == 1 ? (PairVec<S, H, COMOV, PASS>::value == 2
+                           ? CF_PAIR_MB_F32_V2
+                           : ((PASS == 1 && !COMOV) ? CF_PAIR_MB_F32_A : CF_PAIR_MB_F32))
+                    : CF_PAIR_MB_F32_H2)
+          : (COMOV ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
 };
 
 template <typename S, int H, bool COMOV, int PASS, bool FULL>
 __global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, COMOV, PASS>::value)) k_pair(const PairArgs<S> A) {
-  using PS = PairSmem<S, H, TX, TY>;
+  constexpr int VW = PairVec<S, H, COMOV, PASS>::value;
+  using PS = PairSmem<S, H, TX, TY, VW>;
   __shared__ __align__(16) S sm[PS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
-  pair_tile<S, H, COMOV, PASS, TX, TY, FULL>(A, blockIdx.x * PS::TS::TW, blockIdx.y * TY, a_begin,
+  pair_tile<S, H, COMOV, PASS, TX, TY, FULL, VW>(A, blockIdx.x * PS::TS::TW, blockIdx.y * TY, a_begin,
                                              min(a_begin + A.a_chunk, A.N), sm);
 }
 
@@ -135,7 +152,7 @@ static int launch_stage(cf_ctx *ctx, const StageArgs<S> &A, cudaStream_t st) {
 
 template <typename S, int H, bool COMOV, int PASS>
 static int launch_pair_t(cf_ctx *ctx, const PairArgs<S> &A0, cudaStream_t st) {
-  constexpr int TW = TX * VecT<S>::n;
+  constexpr int TW = TX * PairVec<S, H, COMOV, PASS>::value;
   PairArgs<S> A = A0;
   dim3 block(TX, TY);
   unsigned gx = ceil_div(A.N, TW), gy = ceil_div(A.N, TY);
