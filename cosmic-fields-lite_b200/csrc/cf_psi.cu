@@ -332,7 +332,10 @@ __device__ __forceinline__ void dft_inv(typename Cplx<S>::T (&v)[R], const Tw32<
   for (int i = 0; i < R; ++i) v[i] = a[i];
 }
 
-template <typename S, int R1, int R2, int ROWS>
+// B: Z is zero outside the k1 rows [0, B) and [R1 - B, R1) (the band |k| <= Kc
+// with B = ceil((Kc+1)/R2)); as a template argument those zeros are constants
+// and the pass-1 DFT drops the work on them.  B = R1/2 keeps every row.
+template <typename S, int R1, int R2, int ROWS, int B>
 __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S *__restrict__ out,
                                                      const typename Cplx<S>::T *__restrict__ wN,
                                                      const typename Cplx<S>::T *__restrict__ twM, int N, int Kc,
@@ -363,7 +366,9 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
     for (int k1 = 0; k1 < R1; ++k1) {
       const int k = k2 + R2 * k1;
       C z{(S)0, (S)0};
-      if (k <= Kc) {
+      if (k1 >= B && k1 < R1 - B) {
+        // outside the band's rows: zero
+      } else if (k <= Kc) {
         z = c_add(Xs[k * ROWS + r], XPs[k * ROWS + r]);  // X + i X w^k
       } else if (k >= M - Kc) {
         const int j = M - k;
@@ -437,10 +442,10 @@ static size_t pc_fused_smem(const cf_ctx *ctx, const PcShape &sh) {
          ctx->word;
 }
 
-template <typename S, int R1, int R2, int ROWS>
-static int launch_pc_fused_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+template <typename S, int R1, int R2, int ROWS, int B>
+static int launch_pc_fused_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
   using C = typename Cplx<S>::T;
-  auto kern = k_prune_c_fft<S, R1, R2, ROWS>;
+  auto kern = k_prune_c_fft<S, R1, R2, ROWS, B>;
   if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Tw32<S> tw;
   for (int e = 0; e < 16; ++e) {
@@ -452,6 +457,19 @@ static int launch_pc_fused_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t s
                                                  (const C *)ctx->pr_twM, N, ctx->Kc, tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
+}
+
+// The smallest compiled band B >= ceil((Kc+1)/R2) (2, 3, 4, 6 or all rows).
+template <typename S, int R1, int R2, int ROWS>
+static int launch_pc_fused_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+  const int need = (ctx->Kc + 1 + R2 - 1) / R2;
+  if constexpr (R1 >= 16) {
+    if (need <= 2) return launch_pc_fused_b<S, R1, R2, ROWS, 2>(ctx, out, smem, st);
+    if (need <= 3) return launch_pc_fused_b<S, R1, R2, ROWS, 3>(ctx, out, smem, st);
+    if (need <= 4) return launch_pc_fused_b<S, R1, R2, ROWS, 4>(ctx, out, smem, st);
+    if (need <= 6) return launch_pc_fused_b<S, R1, R2, ROWS, 6>(ctx, out, smem, st);
+  }
+  return launch_pc_fused_b<S, R1, R2, ROWS, R1 / 2>(ctx, out, smem, st);
 }
 
 template <typename S>

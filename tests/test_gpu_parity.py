@@ -105,17 +105,24 @@ def test_pruned_psi_synthesis_equals_full(prec, tol, k_max):
     assert rel(out[0][1], out[1][1]) <= tol
 
 
-@pytest.mark.parametrize("prec,tol_pf,tol_or", [(cfb200.FP64, 1e-13, 1e-12), (cfb200.FP32_COMP, 2e-6, 2e-6)])
+@pytest.mark.parametrize("prec,tol_pf,tol_or", [(cfb200.FP64, 1e-13, (1e-12, 1e-9)), (cfb200.FP32_COMP, 2e-6, (2e-6, 2e-6))])
 @pytest.mark.parametrize("N,k_max,route", [(64, 1.0, cfb200.PSI_PRUNED_FUSED),
                                            (64, 1.5, cfb200.PSI_PRUNED_FUSED),   # Kc = N/4 - 1
                                            (128, 0.6, cfb200.PSI_PRUNED_FUSED),
+                                           (256, 0.3, cfb200.PSI_PRUNED_FUSED),  # pass-1 band of 2 rows
+                                           (256, 0.6, cfb200.PSI_PRUNED_FUSED),  # 4 rows
                                            (96, 1.0, cfb200.PSI_PRUNED),        # not a power of two
                                            (64, 2.5, cfb200.PSI_FULL)])         # box too wide to prune
 def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or, N, k_max, route):
     """Psi and dPsi/dt at a stage time, read back through cf_psi_fields: the
     route the box selects (pass C as one kernel for power-of-two N, the padded
-    cuFFT pass C otherwise, or the full 3-D C2R) equals the forced full C2R and
-    the oracle's FFTW-based synthesis (FP64: 1e-13 / 1e-12; FP32 storage: 2e-6)."""
+    cuFFT pass C otherwise, or the full 3-D C2R) equals the forced full C2R
+    (FP64 1e-13) and the oracle's FFTW-based synthesis (FP64: Psi 1e-12, dPsi/dt
+    1e-9; FP32 storage 2e-6).  The dPsi/dt bound is the conditioning of the
+    reference's transfer function: 3x cos x + (x^2 - 3) sin x ~ -x^5/15 at small
+    x = k eta / sqrt(3), so a one-ulp difference between two libraries' sincos
+    grows by ~5e-15 / x^4 -- about 5e-9 at the fundamental mode of N = 256
+    (x ~ 0.03); both GPU routes, which share one sincos, agree to 1e-13."""
     L = float(N)
     Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=31)
     got = {}
@@ -130,10 +137,10 @@ def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or,
     P = O.make_params(N, L, 1.0, eq=2, **FRW)
     psi, dpsi = O.psi_fields(P, Rf, 1.3)
     a, b = got[0], got[cfb200.FLAG_FULL_PSI_FFT]
-    for sl, want in ((slice(0, N ** 3), psi), (slice(N ** 3, None), dpsi)):
+    for sl, want, tol in ((slice(0, N ** 3), psi, tol_or[0]), (slice(N ** 3, None), dpsi, tol_or[1])):
         assert rel(a[sl], b[sl]) <= tol_pf
-        assert rel(a[sl], want) <= tol_or
-        assert rel(b[sl], want) <= tol_or
+        assert rel(a[sl], want) <= tol
+        assert rel(b[sl], want) <= tol
 
 
 @pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
