@@ -77,6 +77,12 @@ _SIGS = {
     "cf_s2_to_shells": ([_vp, _vp, _vp, _vp], _i),
     "cf_s2_counts": ([_vp, _vp, _vp], _i),
     "cf_check_finite": ([_vp, _vp, ctypes.POINTER(_i64), _vp], _i),
+    "cf_fft_create": ([_i64, _vp], _i),
+    "cf_fft_destroy": ([_vp], _i),
+    "cf_fft_d2z": ([_vp, _vp, _vp, _vp], _i),
+    "cf_fft_batched_d2z": ([_vp, _vp, _vp, _vp], _i),
+    "cf_fft_z2d": ([_vp, _vp, _vp, _vp], _i),
+    "cf_fft_inplace_z2d": ([_vp, _vp, _vp], _i),
     "cf_adjoint_create": ([_vp, _i64, _i64, ctypes.POINTER(_vp)], _i),
     "cf_adjoint_destroy": ([_vp], _i),
     "cf_adjoint_forward": ([_vp, _vp, _d, _d, _vp], _i),
@@ -315,6 +321,39 @@ class Adjoint:
         dm = _d(0.0)
         check(lib().cf_adjoint_backward(self.h, _ptr(d_lambda0), ctypes.byref(dm), _stream(stream)))
         return float(dm.value)
+
+
+class FFT:
+    """cf_fft: the reference's fft_wrapper (3-D FP64 D2Z / Z2D of an N^3 lattice)."""
+
+    def __init__(self, N):
+        h = ctypes.c_void_p()
+        check(lib().cf_fft_create(int(N), ctypes.byref(h)))
+        self.h = h
+        self.N = int(N)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cf_fft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def d2z(self, d_in, d_out, stream=None):
+        check(lib().cf_fft_d2z(self.h, _ptr(d_in), _ptr(d_out), _stream(stream)))
+
+    def batched_d2z(self, d_in, d_out, stream=None):
+        check(lib().cf_fft_batched_d2z(self.h, _ptr(d_in), _ptr(d_out), _stream(stream)))
+
+    def z2d(self, d_in, d_out, stream=None):
+        check(lib().cf_fft_z2d(self.h, _ptr(d_in), _ptr(d_out), _stream(stream)))
+
+    def inplace_z2d(self, d_inout, stream=None):
+        check(lib().cf_fft_inplace_z2d(self.h, _ptr(d_inout), _stream(stream)))
 
 
 ENS_PERSISTENT, ENS_BATCHED, ENS_LOOP = 0, 1, 2

@@ -196,6 +196,27 @@ int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stre
 /* Mode multiplicity per S2 bin (exact, the rule of plot_util.py:53-58). */
 int cf_s2_counts(cf_ctx *ctx, int64_t *d_counts, void *stream);
 
+/* ---- FFT wrapper ---------------------------------------------------------------
+ * The reference's cufftWrapperNoBatching (src/cuda_wrapper.cuh:113-130,
+ * src/cuda_wrapper.cu:202-255), used through workspace.fft_wrapper by initializers,
+ * observers and WKB code: 3-D FP64 transforms of an N^3 lattice (N even, 8..2048),
+ * unnormalised, forward sign e^{-2 pi i k.x/N}, HC layout N x N x (N/2+1) complex.
+ * The handle belongs to the device current at cf_fft_create; its cuFFT plans are
+ * made on first use.
+ *   cf_fft_d2z:          N^3 real -> HC                       (execute_d2z)
+ *   cf_fft_batched_d2z:  2 N^3 real [phi | dphi] -> 2 HC      (execute_batched_d2z)
+ *   cf_fft_z2d:          HC -> N^3 real; overwrites d_in      (execute_z2d)
+ *   cf_fft_inplace_z2d:  HC -> real in place, rows padded to 2(N/2+1) doubles
+ *                        (PADDED_IDX_OF, src/fdm3d.hpp:24)     (execute_inplace_z2d)
+ * Device pointers 16-byte aligned; sizes are the caller's to provide. */
+typedef struct cf_fft cf_fft;
+int cf_fft_create(int64_t N, cf_fft **out);
+int cf_fft_destroy(cf_fft *fft);
+int cf_fft_d2z(cf_fft *fft, const double *d_in, double *d_out, void *stream);
+int cf_fft_batched_d2z(cf_fft *fft, const double *d_in, double *d_out, void *stream);
+int cf_fft_z2d(cf_fft *fft, double *d_in, double *d_out, void *stream);
+int cf_fft_inplace_z2d(cf_fft *fft, double *d_inout, void *stream);
+
 /* Scans a state for NaN/Inf; synchronises `stream` and sets *h_bad to the number
  * of non-finite entries found (0 if clean).  Returns CF_ERR_NONFINITE if any. */
 int cf_check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, void *stream);

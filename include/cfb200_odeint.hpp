@@ -168,6 +168,48 @@ inline void copy_vector(std::vector<double> &out, const DeviceState &in) {
   }
 }
 
+/* ---- FFT wrapper (cufftWrapperNoBatching, src/cuda_wrapper.cuh:113-130, and its
+ * dispatcher, src/dispatcher.hpp:24-46): what workspace.fft_wrapper gives the
+ * reference's initializers, observers and WKB code.  FP64 vectors in the
+ * reference's layouts; unnormalised transforms on the default stream, like the
+ * reference's.  execute_z2d overwrites its input, as cuFFT's does there. */
+class FFTWrapper {
+ public:
+  int N;
+  explicit FFTWrapper(int N_) : N(N_) { check(cf_fft_create(N_, &h_)); }
+  ~FFTWrapper() { cf_fft_destroy(h_); }
+  FFTWrapper(const FFTWrapper &) = delete;
+  FFTWrapper &operator=(const FFTWrapper &) = delete;
+
+  DeviceState execute_d2z(DeviceState &in) {
+    DeviceState out(hc());
+    check(cf_fft_d2z(h_, in.f64(), out.f64(), nullptr));
+    return out;
+  }
+  DeviceState execute_batched_d2z(DeviceState &in) {
+    DeviceState out(2 * hc());
+    check(cf_fft_batched_d2z(h_, in.f64(), out.f64(), nullptr));
+    return out;
+  }
+  DeviceState execute_z2d(DeviceState &in) {
+    DeviceState out((size_t)N * N * N);
+    check(cf_fft_z2d(h_, in.f64(), out.f64(), nullptr));
+    return out;
+  }
+  void execute_inplace_z2d(DeviceState &inout) { check(cf_fft_inplace_z2d(h_, inout.f64(), nullptr)); }
+
+ private:
+  size_t hc() const { return 2 * (size_t)N * N * (N / 2 + 1); }
+  cf_fft *h_ = nullptr;
+};
+
+template <typename Vector>
+struct fftWrapperDispatcher;
+template <>
+struct fftWrapperDispatcher<DeviceState> {
+  typedef FFTWrapper Generic;
+};
+
 /* odeint operations for DeviceState (replaces thrust_operations::scale_sumN). */
 struct device_operations {
   template <size_t K>
@@ -276,9 +318,11 @@ struct WorkspaceGeneric {
   int stencil = 7;
   std::shared_ptr<Context> ctx; /* created when an Equation binds the workspace */
   int equation = -1;
+  typename fftWrapperDispatcher<Vector>::Generic fft_wrapper; /* src/workspace.hpp:79 */
 
   template <HasLatticeParams Param, typename Init>
-  WorkspaceGeneric(const Param &param, Init &initializer) : N(param.N), L(param.L) {
+  WorkspaceGeneric(const Param &param, Init &initializer)
+      : N(param.N), L(param.L), fft_wrapper((int)param.N) {
     if constexpr (HasFRWParameters<Param>) cosmology = StaticEOSCosmology(param);
     if constexpr (HasMass<Param>) m = param.m;
     if constexpr (HasPrecision<Param>) precision = (int)param.precision;

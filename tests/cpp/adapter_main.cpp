@@ -11,7 +11,9 @@
 //   mode 3: ComovingCurvatureEquationInFRW with cfb200::fused_rk4 (FP64), R_fft from file
 //   mode 4: KleinGordonEquation (flat) with the stock runge_kutta4_classic
 // Writes out_dir/state.dat (final FP64 state), the observer's spectra files and
-// out_dir/t_list.dat.
+// out_dir/t_list.dat.  The initializer also uses workspace.fft_wrapper the way
+// the reference's initializers do (src/initializer.hpp:204): out_dir/fft_phi0.dat
+// is execute_d2z(phi0), out_dir/fft_roundtrip.dat is execute_z2d of it.
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -59,9 +61,19 @@ static std::vector<double> read_file(const std::string &name) {
 template <typename Equation, typename Stepper, typename Param>
 static int run(const Param &param, const std::vector<double> &x0, const std::vector<double> &R_fft, double dt,
                const std::string &dir) {
-  auto init = [&](const auto &, auto &ws) {
+  auto init = [&](const auto &p, auto &ws) {
     ws.state.copy_from_host(x0.data(), x0.size());
     ws.R_fft = R_fft;
+    const size_t N3 = (size_t)p.N * p.N * p.N;
+    cfb200::DeviceState phi;
+    phi.copy_from_host(x0.data(), N3);
+    cfb200::DeviceState fk = ws.fft_wrapper.execute_d2z(phi);
+    std::vector<double> h;
+    cfb200::copy_vector(h, fk);
+    cfb200::write_vector_to_file(h, dir + "fft_phi0.dat");
+    cfb200::DeviceState back = ws.fft_wrapper.execute_z2d(fk);
+    cfb200::copy_vector(h, back);
+    cfb200::write_vector_to_file(h, dir + "fft_roundtrip.dat");
   };
   typename Equation::Workspace workspace(param, init);
   Equation eqn(workspace);

@@ -38,6 +38,14 @@ def test_create_rejects_bad_parameters_on_host(kw, msg):
     assert e.value.code == -1 and msg in str(e.value)
 
 
+def test_fft_wrapper_rejects_bad_sizes_on_host():
+    import ctypes
+    h = ctypes.c_void_p()
+    for n in (7, 4, 4096):
+        assert cfb200.lib().cf_fft_create(n, ctypes.byref(h)) == -1
+        assert b"cf_fft_create" in cfb200.lib().cf_last_error()
+
+
 def test_calls_reject_null_context():
     L = cfb200.lib()
     assert L.cf_rk4_steps(None, None, 0.0, 0.1, 0, 1, None) == -1

@@ -58,6 +58,11 @@ def test_adapter_integrate_const_matches_reference(mode):
         spectra = [(np.fromfile(os.path.join(d, f"varphi_plus_spectrum_{i}.dat")),
                     np.fromfile(os.path.join(d, f"rho_spectrum_{i}.dat")),
                     np.fromfile(os.path.join(d, f"rho_slice_{i}.dat"))) for i in range(len(t_list))]
+        fk = np.fromfile(os.path.join(d, "fft_phi0.dat")).view(complex)
+        back = np.fromfile(os.path.join(d, "fft_roundtrip.dat"))
+    # workspace.fft_wrapper as the reference's initializers use it (FP64, unnormalised)
+    assert rel(fk, np.fft.rfftn(x[: N ** 3].reshape(N, N, N)).ravel()) <= 1e-13
+    assert rel(back, x[: N ** 3] * N ** 3) <= 1e-13
     if O.ref_available():
         want, obs = O.ref_integrate(eq, N, L, 1.0, x, t0, t_end, dt, R_fft=Rf, t_interval=ti, observe=True, **cos)
         assert np.allclose(t_list, obs["t_list"], rtol=0, atol=1e-12)
