@@ -25,6 +25,7 @@ CF_OK = 0
 STATUS = {0: "CF_OK", -1: "CF_ERR_INVALID", -2: "CF_ERR_CUDA", -3: "CF_ERR_CUFFT", -4: "CF_ERR_NOMEM",
           -5: "CF_ERR_NONFINITE", -6: "CF_ERR_TIMEOUT", -7: "CF_ERR_UNSUPPORTED"}
 EQ_KG, EQ_KG_FRW, EQ_COMOVING_FRW = 0, 1, 2
+EQ_LAMBDA_FRW, EQ_SQRT_FRW, EQ_FIXED_CURVATURE_FRW, EQ_APPROX_COMOVING_FRW = 3, 4, 5, 6
 FP64, FP32_COMP = 0, 1
 FLAG_FULL_PSI_FFT = 1
 FLAG_STAGE_KERNELS = 2
@@ -41,7 +42,8 @@ class cf_params(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int64), ("L", ctypes.c_double), ("m", ctypes.c_double),
                 ("a1", ctypes.c_double), ("H1", ctypes.c_double), ("t1", ctypes.c_double),
                 ("p", ctypes.c_double), ("equation", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("stencil", ctypes.c_int32), ("flags", ctypes.c_int32)]
+                ("stencil", ctypes.c_int32), ("flags", ctypes.c_int32), ("lam", ctypes.c_double),
+                ("f_a", ctypes.c_double), ("M", ctypes.c_int64)]
 
 
 class cf_info(ctypes.Structure):
@@ -66,11 +68,13 @@ _SIGS = {
     "cf_state_import": ([_vp, _vp, _vp, _vp], _i),
     "cf_state_export": ([_vp, _vp, _vp, _vp], _i),
     "cf_set_R_fft": ([_vp, _vp, _i, _vp], _i),
+    "cf_set_psi": ([_vp, _vp, _i, _vp], _i),
     "cf_psi_fields": ([_vp, _d, _vp, _vp], _i),
     "cf_rk4_steps": ([_vp, _vp, _d, _d, _i64, _i64, _vp], _i),
     "cf_rhs": ([_vp, _vp, _vp, _d, _vp], _i),
     "cf_scale_sum": ([_vp, _vp, _i, _vp, _vp, _i64, _vp], _i),
     "cf_energy_density": ([_vp, _vp, _d, _vp, _vp], _i),
+    "cf_dot_energy_density": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_power_spectrum_s2": ([_vp, _vp, _vp, _vp], _i),
     "cf_mode_power_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_density_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
@@ -175,9 +179,12 @@ class Context:
     """One cf_ctx: a lattice, an equation, a precision and a stencil."""
 
     def __init__(self, N, L, m=1.0, equation=EQ_KG_FRW, precision=FP64, stencil=7, a1=1.0, H1=0.0,
-                 t1=0.0, p=1.0, flags=0):
+                 t1=0.0, p=1.0, flags=0, lam=0.0, f_a=1.0, M=0):
+        """lam, f_a, M: the workspace's lambda (EQ_LAMBDA_FRW), f_a (EQ_SQRT_FRW; the
+        reference's default 1) and M (EQ_APPROX_COMOVING_FRW)."""
         self.params = cf_params(int(N), float(L), float(m), float(a1), float(H1), float(t1), float(p),
-                                int(equation), int(precision), int(stencil), int(flags))
+                                int(equation), int(precision), int(stencil), int(flags), float(lam),
+                                float(f_a), int(M))
         h = ctypes.c_void_p()
         check(lib().cf_create(ctypes.byref(self.params), ctypes.byref(h)))
         self.h = h
@@ -227,6 +234,10 @@ class Context:
     def set_R_fft(self, R_fft, on_device, stream=None):
         check(lib().cf_set_R_fft(self.h, _ptr(R_fft), int(on_device), _stream(stream)))
 
+    def set_psi(self, Psi, on_device, stream=None):
+        """The fixed Psi(x) of EQ_FIXED_CURVATURE_FRW (N^3 doubles, host or device)."""
+        check(lib().cf_set_psi(self.h, _ptr(Psi), int(on_device), _stream(stream)))
+
     def psi_fields(self, t, d_out, stream=None):
         """Psi and dPsi/dt at time t into d_out (2 N^3 doubles on the device)."""
         check(lib().cf_psi_fields(self.h, float(t), _ptr(d_out), _stream(stream)))
@@ -249,6 +260,9 @@ class Context:
     # ---- observers
     def energy_density(self, d_state, t, d_rho, stream=None):
         check(lib().cf_energy_density(self.h, _ptr(d_state), float(t), _ptr(d_rho), _stream(stream)))
+
+    def dot_energy_density(self, d_state, t, d_out, stream=None):
+        check(lib().cf_dot_energy_density(self.h, _ptr(d_state), float(t), _ptr(d_out), _stream(stream)))
 
     def power_spectrum_s2(self, d_f, d_out, stream=None):
         check(lib().cf_power_spectrum_s2(self.h, _ptr(d_f), _ptr(d_out), _stream(stream)))
@@ -370,7 +384,7 @@ class Ensemble:
             arr[i] = cf_params(int(d["N"]), float(d["L"]), float(d.get("m", 1.0)), float(d.get("a1", 1.0)),
                                float(d.get("H1", 0.0)), float(d.get("t1", 0.0)), float(d.get("p", 1.0)),
                                int(d.get("equation", EQ_KG_FRW)), int(d.get("precision", FP64)),
-                               int(d.get("stencil", 7)), 0)
+                               int(d.get("stencil", 7)), 0, 0.0, 1.0, 0)
         self.members = members
         h = ctypes.c_void_p()
         check(lib().cf_ensemble_create(ctypes.cast(arr, ctypes.c_void_p), len(members), ctypes.byref(h)))

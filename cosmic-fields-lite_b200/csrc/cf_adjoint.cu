@@ -364,7 +364,7 @@ static long long adj_cta_count(const cf_ctx *ctx) {
 }
 
 int adjoint_create(cf_ctx *ctx, int64_t nsteps, int64_t every, cf_adjoint **out) {
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
+  if (ctx->p.equation != CF_EQ_KG && ctx->p.equation != CF_EQ_KG_FRW) {
     set_error("the adjoint covers the flat and FRW Klein-Gordon equations");
     return CF_ERR_UNSUPPORTED;
   }

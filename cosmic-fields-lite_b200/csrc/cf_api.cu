@@ -65,6 +65,7 @@ int rhs(cf_ctx *, const double *, double *, double, cudaStream_t);
 int scale_sum(cf_ctx *, double *, int, const double *const *, const double *, int64_t, cudaStream_t);
 int set_R_fft(cf_ctx *, const double *, int, cudaStream_t);
 int energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
+int dot_energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
 int power_spectrum_s2(cf_ctx *, const double *, double *, cudaStream_t);
 int mode_power_spectrum_s2(cf_ctx *, const void *, double, double *, cudaStream_t);
 int density_spectrum_s2(cf_ctx *, const void *, double, double *, cudaStream_t);
@@ -159,6 +160,21 @@ static int use_device(const cf_ctx *ctx) {
   return CF_OK;
 }
 
+// The curvature input the context's equation needs before it can be evaluated:
+// R_fft for the comoving equations, Psi for the fixed-curvature one.
+static int check_curvature(const cf_ctx *ctx) {
+  const int eq = ctx->p.equation;
+  if ((eq == CF_EQ_COMOVING_FRW || eq == CF_EQ_APPROX_COMOVING_FRW) && !ctx->R_fft) {
+    set_error("comoving-curvature equation: call cf_set_R_fft first");
+    return CF_ERR_INVALID;
+  }
+  if (eq == CF_EQ_FIXED_CURVATURE_FRW && !ctx->fixed_e2m1) {
+    set_error("fixed-curvature equation: call cf_set_psi first");
+    return CF_ERR_INVALID;
+  }
+  return CF_OK;
+}
+
 }  // namespace cfb
 
 using namespace cfb;
@@ -182,7 +198,7 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     set_error("L must be positive and finite, m finite");
     return CF_ERR_INVALID;
   }
-  if (p.equation < CF_EQ_KG || p.equation > CF_EQ_COMOVING_FRW) {
+  if (p.equation < CF_EQ_KG || p.equation > CF_EQ_APPROX_COMOVING_FRW) {
     set_error("unknown equation %d", p.equation);
     return CF_ERR_INVALID;
   }
@@ -202,8 +218,22 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     set_error("FRW parameters must be finite with p > 0");
     return CF_ERR_INVALID;
   }
-  if (p.equation == CF_EQ_COMOVING_FRW && (p.H1 == 0.0 || p.a1 == 0.0)) {
+  if ((p.equation == CF_EQ_COMOVING_FRW || p.equation == CF_EQ_APPROX_COMOVING_FRW) &&
+      (p.H1 == 0.0 || p.a1 == 0.0)) {
     set_error("the comoving-curvature equation needs a1 != 0 and H1 != 0 (conformal time)");
+    return CF_ERR_INVALID;
+  }
+  if (p.equation == CF_EQ_LAMBDA_FRW && !std::isfinite(p.lambda)) {
+    set_error("lambda must be finite");
+    return CF_ERR_INVALID;
+  }
+  if (p.equation == CF_EQ_SQRT_FRW && !(p.f_a > 0 && std::isfinite(p.f_a))) {
+    set_error("the sqrt potential needs a finite f_a > 0");
+    return CF_ERR_INVALID;
+  }
+  if (p.equation == CF_EQ_APPROX_COMOVING_FRW && (p.M < 8 || p.M % 8 != 0 || p.M > p.N || p.N % p.M != 0)) {
+    set_error("the approximate comoving equation needs M %% 8 == 0, 8 <= M <= N and N %% M == 0 (M = %lld)",
+              (long long)p.M);
     return CF_ERR_INVALID;
   }
   int dev = 0;
@@ -245,6 +275,7 @@ int cf_destroy(cf_ctx *ctx) {
   for (auto &s : ctx->slot) cudaFree(s.psi);
   if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
   psi_release(ctx);
+  approx_release(ctx);
   if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);
   if (ctx->have_d2z2) cufftDestroy(ctx->plan_d2z2);
   cudaFree(ctx->spec_hc);
@@ -341,6 +372,17 @@ int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream) 
   return set_R_fft(ctx, R_fft, on_device, (cudaStream_t)stream);
 }
 
+int cf_set_psi(cf_ctx *ctx, const double *Psi, int on_device, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(Psi, "Psi", 8));
+  if (ctx->p.equation != CF_EQ_FIXED_CURVATURE_FRW) {
+    set_error("cf_set_psi: the context's equation is not CF_EQ_FIXED_CURVATURE_FRW");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  return set_fixed_psi(ctx, Psi, on_device, (cudaStream_t)stream);
+}
+
 int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream) {
   CF_TRY(check_ctx(ctx));
   CF_TRY(check_ptr(d_out, "d_out", 8));
@@ -359,10 +401,7 @@ int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0
     set_error("nsteps must be >= 0 and t0, dt finite");
     return CF_ERR_INVALID;
   }
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW && !ctx->R_fft) {
-    set_error("comoving-curvature equation: call cf_set_R_fft first");
-    return CF_ERR_INVALID;
-  }
+  CF_TRY(check_curvature(ctx));
   CF_TRY(use_device(ctx));
   return rk4_steps(ctx, d_state, t0, dt, step0, nsteps, (cudaStream_t)stream);
 }
@@ -371,16 +410,13 @@ int cf_rhs(cf_ctx *ctx, const double *d_x, double *d_dxdt, double t, void *strea
   CF_TRY(check_ctx(ctx));
   CF_TRY(check_ptr(d_x, "d_x"));
   CF_TRY(check_ptr(d_dxdt, "d_dxdt"));
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
-    if (ctx->p.precision != CF_FP64) {
-      set_error("cf_rhs of the comoving-curvature equation needs a CF_FP64 context");
-      return CF_ERR_UNSUPPORTED;
-    }
-    if (!ctx->R_fft) {
-      set_error("comoving-curvature equation: call cf_set_R_fft first");
-      return CF_ERR_INVALID;
-    }
+  const int eq = ctx->p.equation;
+  if ((eq == CF_EQ_COMOVING_FRW || eq == CF_EQ_FIXED_CURVATURE_FRW || eq == CF_EQ_APPROX_COMOVING_FRW) &&
+      ctx->p.precision != CF_FP64) {
+    set_error("cf_rhs of a curvature-coupled equation needs a CF_FP64 context");
+    return CF_ERR_UNSUPPORTED;
   }
+  CF_TRY(check_curvature(ctx));
   CF_TRY(use_device(ctx));
   return rhs(ctx, d_x, d_dxdt, t, (cudaStream_t)stream);
 }
@@ -402,12 +438,21 @@ int cf_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho,
   CF_TRY(check_ctx(ctx));
   CF_TRY(check_ptr(d_state, "d_state"));
   CF_TRY(check_ptr(d_rho, "d_rho", 8));
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW && !ctx->R_fft) {
-    set_error("comoving-curvature equation: call cf_set_R_fft first");
-    return CF_ERR_INVALID;
-  }
+  CF_TRY(check_curvature(ctx));
   CF_TRY(use_device(ctx));
   return energy_density(ctx, d_state, t, d_rho, (cudaStream_t)stream);
+}
+
+int cf_dot_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  CF_TRY(check_ptr(d_out, "d_out", 8));
+  if (ctx->p.equation != CF_EQ_KG_FRW) {
+    set_error("cf_dot_energy_density: CF_EQ_KG_FRW only (CudaKleinGordonEquationInFRW)");
+    return CF_ERR_UNSUPPORTED;
+  }
+  CF_TRY(use_device(ctx));
+  return dot_energy_density(ctx, d_state, t, d_out, (cudaStream_t)stream);
 }
 
 int cf_power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, void *stream) {
@@ -434,10 +479,7 @@ int cf_density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d
   CF_TRY(check_ctx(ctx));
   CF_TRY(check_ptr(d_state, "d_state"));
   CF_TRY(check_ptr(d_out, "d_out", 8));
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW && !ctx->R_fft) {
-    set_error("comoving-curvature equation: call cf_set_R_fft first");
-    return CF_ERR_INVALID;
-  }
+  CF_TRY(check_curvature(ctx));
   CF_TRY(use_device(ctx));
   return density_spectrum_s2(ctx, d_state, t, d_out, (cudaStream_t)stream);
 }

@@ -98,6 +98,9 @@ __device__ __forceinline__ void ens_item_stage(const EnsArgs &E, const EnsItem &
   A.xlo = (sizeof(S) == 4) ? (S *)mb.x + 2 * mb.N3 : nullptr;
   A.acc = (S *)mb.acc;
   A.psi = A.dpsi = nullptr;
+  A.cmap = nullptr;
+  A.M = 0;
+  A.q1 = A.q2 = 0.0;
   A.a_chunk = 0;
   const EnsCoef cf = E.coef[4 * step + stage - 1];
   A.inv = mb.inv_scale / cf.a2;
@@ -108,24 +111,24 @@ __device__ __forceinline__ void ens_item_stage(const EnsArgs &E, const EnsItem &
       A.yin = (const S *)mb.x;
       A.yout = (S *)mb.ya;
       A.cy = E.dt / 2.0;
-      stage_tile<S, H, false, 1, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      stage_tile<S, H, EQ_FRW, 1, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
       break;
     case 2:
       A.yin = (const S *)mb.ya;
       A.yout = (S *)mb.yb;
       A.cy = E.dt / 2.0;
-      stage_tile<S, H, false, 2, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      stage_tile<S, H, EQ_FRW, 2, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
       break;
     case 3:
       A.yin = (const S *)mb.yb;
       A.yout = (S *)mb.ya;
       A.cy = E.dt;
-      stage_tile<S, H, false, 3, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      stage_tile<S, H, EQ_FRW, 3, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
       break;
     default:
       A.yin = (const S *)mb.ya;
       A.yout = nullptr;
-      stage_tile<S, H, false, 4, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+      stage_tile<S, H, EQ_FRW, 4, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
       break;
   }
 }
@@ -231,6 +234,9 @@ __device__ __forceinline__ void ens_item_pair(const EnsArgs &E, const EnsItem &i
   A.acc = (S *)mb.acc;
   A.yb = yb;
   A.psi1 = A.dpsi1 = A.psi2 = A.dpsi2 = nullptr;
+  A.cmap = nullptr;
+  A.M = 0;
+  A.q1 = A.q2 = 0.0;
   const EnsCoef c1 = E.coef[4 * step + (PASS == 1 ? 0 : 2)];
   const EnsCoef c2 = E.coef[4 * step + (PASS == 1 ? 1 : 3)];
   A.inv1 = mb.inv_scale / c1.a2;
@@ -251,7 +257,7 @@ __device__ __forceinline__ void ens_item_pair(const EnsArgs &E, const EnsItem &i
     A.cw = E.dt;
     A.cy = 0.0;
   }
-  pair_tile<S, H, false, PASS, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+  pair_tile<S, H, EQ_FRW, PASS, TXv, TYv>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
 }
 
 template <typename S, int H, int SHAPE, int PASS>
@@ -669,7 +675,8 @@ int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out) {
     if (p.equation != b.equation || p.precision != b.precision || p.stencil != b.stencil || p.a1 != b.a1 ||
         p.H1 != b.H1 || p.t1 != b.t1 || p.p != b.p)
       return ens_fail("ensemble members must share equation, precision, stencil and cosmology");
-    if (p.equation == CF_EQ_COMOVING_FRW) return ens_fail("ensembles cover the flat and FRW Klein-Gordon equations");
+    if (p.equation != CF_EQ_KG && p.equation != CF_EQ_KG_FRW)
+      return ens_fail("ensembles cover the flat and FRW Klein-Gordon equations");
     if (!(p.L > 0)) return ens_fail("member L must be positive");
   }
   if (b.stencil != 7 && b.stencil != 13) return ens_fail("stencil must be 7 or 13");

@@ -61,6 +61,15 @@ struct PsiSlot {
   uint64_t stamp = 0;
 };
 
+// One cached coarse curvature table at a stage time (approximate comoving
+// equation): M^3 x 4 words of the storage type.
+struct ApproxSlot {
+  double t = 0;
+  bool valid = false;
+  void *tab = nullptr;
+  uint64_t stamp = 0;
+};
+
 }  // namespace cfb
 
 struct cf_ctx {
@@ -95,6 +104,21 @@ struct cf_ctx {
   bool pc_fused = false;
   void *pr_wN = nullptr;
   void *pr_twM = nullptr;  // pass-1 twiddles e^{2 pi i k2 m1 / (N/2)}, [m1][k2]
+
+  // Fixed curvature: e^{2 Psi(x)} - 1 of cf_set_psi, N^3 of the storage type.
+  void *fixed_e2m1 = nullptr;
+
+  // Approximate comoving curvature (cf_approx.cu): the M-grid modes of R_fft,
+  // the transfer outputs, the synthesised fields, the lattice-to-coarse index
+  // map and three cached coarse tables.
+  double *ap_R = nullptr;   // M-grid HC, FP64
+  double *ap_hc = nullptr;  // 2 M-grid HC arrays (Psi_k, dPsi_k), FP64
+  double *ap_f = nullptr;   // 2 M^3 fields (Psi, dPsi/dt), FP64
+  int *ap_cmap = nullptr;   // N ints: ((i + (N/M)/2) % N) / (N/M)
+  cfb::ApproxSlot ap_slot[3];
+  uint64_t ap_clock = 0;
+  cufftHandle plan_ap = 0;  // batched (2) Z2D on M^3
+  bool have_plan_ap = false;
 
   // Spectra: FP64 R2C plans and scratch.
   cufftHandle plan_d2z1 = 0, plan_d2z2 = 0;
@@ -131,6 +155,14 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t stream, const void **psi, const v
 int psi_fields(cf_ctx *ctx, double t, double *d_out, cudaStream_t stream);
 // CF_PSI_* route the next Psi refresh takes.
 int psi_route(const cf_ctx *ctx);
+// Approximate comoving equation: takes the M-grid modes of a new R_fft (FP64,
+// device), and returns the coarse table for stage time t (refreshing one slot).
+int approx_set_R(cf_ctx *ctx, const double *d_R_fft, cudaStream_t stream);
+int approx_at(cf_ctx *ctx, double t, cudaStream_t stream, const void **tab);
+// Frees the fixed and the approximate curvature buffers (context teardown).
+void approx_release(cf_ctx *ctx);
+// Fixed curvature: Psi (FP64, N^3, host or device) -> e^{2 Psi} - 1 in the storage type.
+int set_fixed_psi(cf_ctx *ctx, const double *Psi, int on_device, cudaStream_t stream);
 // Frees the pruned-synthesis buffers and plans (context teardown).
 void psi_release(cf_ctx *ctx);
 

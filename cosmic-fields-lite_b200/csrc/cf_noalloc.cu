@@ -88,9 +88,9 @@ extern "C" int cf_rk4_steps_noalloc(cf_ctx *ctx, void *d_state, double t0, doubl
     set_error("nsteps must be >= 0 and t0, dt finite");
     return CF_ERR_INVALID;
   }
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
-    set_error("cf_rk4_steps_noalloc covers the flat and FRW Klein-Gordon equations (the comoving-curvature "
-              "equation needs allocated Psi buffers and cuFFT plans)");
+  if (ctx->p.equation != CF_EQ_KG && ctx->p.equation != CF_EQ_KG_FRW) {
+    set_error("cf_rk4_steps_noalloc covers the flat and FRW Klein-Gordon equations (the other equations "
+              "need their own coefficients, curvature buffers or cuFFT plans)");
     return CF_ERR_UNSUPPORTED;
   }
   const size_t buf = 2 * (size_t)ctx->N3 * ctx->word;  // one RK4 work buffer

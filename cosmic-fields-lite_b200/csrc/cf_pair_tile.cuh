@@ -43,13 +43,16 @@ struct PairArgs {
   S *xlo;           // FP32_COMP compensation [phi | pi] (pass B, in place)
   S *acc;           // [phi | pi]: pass A writes k1 + 2 k2; pass B reads it
   S *yb;            // [phi | pi]: pass A output x + dt/2 k2
-  const S *psi1;    // comoving: e^{2 Psi} - 1, dPsi/dt at the first stage's time
+  const S *psi1;    // curvature (StageArgs::psi / dpsi) at the first stage's time
   const S *dpsi1;
   const S *psi2;    // ... at the second stage's time
   const S *dpsi2;
+  const int *cmap;  // EQ_APPROX: coarse index of each lattice index (N entries)
+  int M;            // EQ_APPROX: coarse grid size
   int N;
   int a_chunk;
   long long N3;
+  double q1, q2;    // EQ_LAMBDA: lambda; EQ_SQRT: f_a^2, 1/f_a^2
   double m2;
   double inv1, hub3_1;  // first stage: h^-2 a^-2, 3H
   double inv2, hub3_2;  // second stage
@@ -71,7 +74,7 @@ __device__ __forceinline__ S w_of(S xphi, S upi, const Coef<T> &cw) {
   return (S)cw.fma((T)upi, (T)xphi);
 }
 
-template <typename S, int H, bool COMOV, int PASS, int TXv, int TYv, bool FULL = false, int VW = VecT<S>::n>
+template <typename S, int H, int EQ, int PASS, int TXv, int TYv, bool FULL = false, int VW = VecT<S>::n>
 __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, int a_begin, int a_end, S *smem) {
   using TS = TileSmem<S, H, TXv, TYv, VW>;
   using PS = PairSmem<S, H, TXv, TYv, VW>;
@@ -95,9 +98,10 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
   const S *upi = A.upi;
   const S *xphi = A.xphi;  // w's base phi (pass A: the same array as uphi)
   using T = typename Arith<S>::T;
-  const StageCoef<T> k1c{Coef<T>(A.m2), Coef<T>(A.inv1), Coef<T>(A.hub3_1)};
-  const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(A.inv2), Coef<T>(A.hub3_2)};
+  const StageCoef<T> k1c{Coef<T>(A.m2), Coef<T>(A.inv1), Coef<T>(A.hub3_1), Coef<T>(A.q1), Coef<T>(A.q2)};
+  const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(A.inv2), Coef<T>(A.hub3_2), Coef<T>(A.q1), Coef<T>(A.q2)};
   const Coef<T> cw(A.cw), cy(A.cy);
+  const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
 
   auto load_w = [&](long long off) -> Pack<S, V> {
     const Pack<S, V> p = ldv<S, V>(upi + off);
@@ -125,7 +129,8 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
       qu[j] = qu[j + 1];
       qw[j] = qw[j + 1];
     }
-    Pack<S, V> p0v, xp, xq, cp, cq, lp, lq, ps1, dps1, ps2, dps2;
+    Pack<S, V> p0v, xp, xq, cp, cq, lp, lq;
+    Coupling<S, V> cpl1, cpl2;
     if (act) {
       const long long head = NN * ((a + H) % N) + rowoff;
       qu[2 * H] = ldv<S, V>(uphi + head);
@@ -141,11 +146,13 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
           lq = ldv_rw<S, V>(A.xlo + N3 + site);
         }
       }
-      if constexpr (COMOV) {
-        ps1 = ldv<S, V>(A.psi1 + site);
-        dps1 = ldv<S, V>(A.dpsi1 + site);
-        ps2 = ldv<S, V>(A.psi2 + site);
-        dps2 = ldv<S, V>(A.dpsi2 + site);
+      if constexpr (EqOf<EQ>::coupled) {
+        const int ca = EqOf<EQ>::coarse ? __ldg(A.cmap + a) : 0;
+        load_coupling<EQ, S, V>(cpl1, A.psi1, A.dpsi1, site, A.M, ca, cc);
+        if constexpr (EQ == EQ_FIXED)
+          cpl2 = cpl1;  // a time-independent Psi: both stages read the same plane
+        else
+          load_coupling<EQ, S, V>(cpl2, A.psi2, A.dpsi2, site, A.M, ca, cc);
       }
     }
     S *smu = smem;
@@ -211,7 +218,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
       const T f0 = (T)qu[H].v[v];
       const T p0 = (T)p0v.v[v];
       const T lap1 = lap_at<S, H, SP>(qu, smu, row, col, v);
-      const T k1pi = kpi_of<COMOV, S>(p0, f0, lap1, COMOV ? ps1.v[v] : (S)0, COMOV ? dps1.v[v] : (S)0, k1c);
+      const T k1pi = kpi_of<EQ, S, V>(p0, f0, lap1, cpl1, v, k1c);
       // the second stage's input: w (phi, already formed) and its pi
       const S wphi = qw[H].v[v];
       S c1phi, c1pi, wpi;
@@ -228,7 +235,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
       const T f1 = (T)wphi;
       const T p1 = (T)wpi;
       const T lap2 = lap_at<S, H, SP>(qw, smw, row, col, v);
-      const T k2pi = kpi_of<COMOV, S>(p1, f1, lap2, COMOV ? ps2.v[v] : (S)0, COMOV ? dps2.v[v] : (S)0, k2c);
+      const T k2pi = kpi_of<EQ, S, V>(p1, f1, lap2, cpl2, v, k2c);
       if constexpr (PASS == 1) {
         o1.v[v] = (S)((T)c1phi + (T)2 * p1);  // acc += 2 k2
         o2.v[v] = (S)((T)c1pi + (T)2 * k2pi);

@@ -835,6 +835,14 @@ int set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, cudaStream_t st) 
       CF_LAUNCHED(ctx);
     }
   }
+  if (ctx->p.equation == CF_EQ_APPROX_COMOVING_FRW) {
+    // the coarse grid takes its modes from the FP64 input
+    const int s = approx_set_R(ctx, w == 8 ? (const double *)ctx->R_fft : src, st);
+    if (s != CF_OK) {
+      if (tmp) cudaFreeAsync(tmp, st);
+      return s;
+    }
+  }
   if (tmp) CF_TRY_CUDA(cudaFreeAsync(tmp, st));
   for (auto &s : ctx->slot) s.valid = false;
   // support of the new R_fft: decides between the pruned and the full synthesis

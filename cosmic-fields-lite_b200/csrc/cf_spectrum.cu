@@ -20,12 +20,20 @@
 namespace cfb {
 
 // ---- energy density -----------------------------------------------------
-// rho = 1/2 (e^{-2Psi} pi^2 + m^2 phi^2 + e^{2Psi} 1/4 h^-2 a^-2 sum_axes (phi_{+1} - phi_{-1})^2)
-// with Psi = 0 for the uncoupled equations (src/equations_cuda.cu:332-369, :451-473;
-// src/equations.cpp:38-69, :106-138, :265-322); `psi` holds e^{2 Psi} - 1.
-template <typename S, bool COMOV>
+// Potential term of the energy density by equation (ED_*):
+//   ED_QUAD    1/2 m^2 phi^2                                (src/equations_cuda.cu:332-369, lambda = 0)
+//   ED_LAMBDA  1/2 m^2 phi^2 + 1/4 lambda phi^4              (:332-369)
+//   ED_SQRT    m^2 f_a^2 (sqrt(1 + phi^2/f_a^2) - 1)         (:431-449)
+//   ED_CURV    1/2 m^2 phi^2 with e^{-2Psi} kinetic and e^{2Psi} gradient weights (:451-473)
+// and rho = 1/2 pi^2 w_k + 1/8 inv w_g sum_axes (phi_{+1} - phi_{-1})^2 + V
+// (src/equations.cpp:38-69, :106-138, :265-322 for the CPU twins).  `psi` holds
+// e^{2 Psi} - 1.  The sqrt potential is formed as m^2 phi^2 / (sqrt(1 + phi^2/f_a^2) + 1),
+// the same value without the cancellation of sqrt(1 + u) - 1 at small u.
+enum EdKind : int { ED_QUAD = 0, ED_LAMBDA = 1, ED_SQRT = 2, ED_CURV = 3 };
+
+template <typename S, int ED>
 __global__ void k_energy(const S *__restrict__ x, const S *__restrict__ xlo, const S *__restrict__ psi,
-                         double *__restrict__ rho, int N, double m2, double inv) {
+                         double *__restrict__ rho, int N, double m2, double inv, double q) {
   const long long N3 = (long long)N * N * N;
   const long long NN = (long long)N * N;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -46,12 +54,56 @@ __global__ void k_energy(const S *__restrict__ x, const S *__restrict__ xlo, con
     const double f = phi(i);
     double p = (double)x[N3 + i];
     if (xlo) p += (double)xlo[N3 + i];
-    if constexpr (COMOV) {
+    if constexpr (ED == ED_CURV) {
       const double e2 = 1.0 + (double)psi[i];
       rho[i] = 0.5 * (p * p / e2 + m2 * f * f + e2 * 0.25 * inv * grad);
+    } else if constexpr (ED == ED_LAMBDA) {
+      rho[i] = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad) + 0.25 * q * f * f * f * f;
+    } else if constexpr (ED == ED_SQRT) {  // q = 1 / f_a^2
+      rho[i] = 0.5 * (p * p + 0.25 * inv * grad) + m2 * f * f / (sqrt(1.0 + f * f * q) + 1.0);
     } else {
       rho[i] = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad);
     }
+  }
+}
+
+// d rho / dt of the FRW Klein-Gordon equation (src/equations_cuda.cu:372-424):
+//   pi lap_inv + 1/4 inv sum_axes (dpi_e)(dphi_e) - 3H (rho + p),
+//   rho = 1/2 pi^2 + 1/8 inv G + 1/2 m^2 phi^2,  p = 1/2 pi^2 - 1/2 m^2 phi^2 - 1/24 inv G,
+// with dphi_e, dpi_e the central differences (phi_{+e} - phi_{-e}) along each axis,
+// G = sum_e dphi_e^2 and lap_inv = inv times the 7-point Laplacian sum.
+template <typename S>
+__global__ void k_dot_energy(const S *__restrict__ x, const S *__restrict__ xlo, double *__restrict__ out, int N,
+                             double m2, double inv, double H_t) {
+  const long long N3 = (long long)N * N * N;
+  const long long NN = (long long)N * N;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  auto val = [&](long long i) -> double {
+    double v = (double)x[i];
+    if (xlo) v += (double)xlo[i];
+    return v;
+  };
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N3; i += stride) {
+    const int c = (int)(i % N);
+    const int b = (int)((i / N) % N);
+    const int a = (int)(i / NN);
+    const long long nb[6] = {NN * ((a + 1) % N) + (long long)N * b + c, NN * ((a + N - 1) % N) + (long long)N * b + c,
+                             NN * a + (long long)N * ((b + 1) % N) + c, NN * a + (long long)N * ((b + N - 1) % N) + c,
+                             NN * a + (long long)N * b + (c + 1) % N, NN * a + (long long)N * b + (c + N - 1) % N};
+    const double f = val(i), p = val(N3 + i);
+    double G = 0.0, cross = 0.0, lap = -6.0 * f;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const double fp = val(nb[2 * e]), fm = val(nb[2 * e + 1]);
+      const double df = fp - fm;
+      const double dp = val(N3 + nb[2 * e]) - val(N3 + nb[2 * e + 1]);
+      G += df * df;
+      cross += dp * df;
+      lap += fp + fm;
+    }
+    const double rho = 0.5 * p * p + (0.5 / 4.0) * inv * G + 0.5 * m2 * f * f;
+    const double pr = 0.5 * p * p - 0.5 * m2 * f * f - (1.0 / 4.0 / 6.0) * inv * G;
+    out[i] = p * (inv * lap) + 0.25 * inv * cross - 3.0 * H_t * (rho + pr);
   }
 }
 
@@ -387,30 +439,59 @@ int mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double 
   return bin_spectrum(ctx, true, a_t, d_out, st);
 }
 
+template <typename S, int ED>
+static void launch_energy(cf_ctx *ctx, const void *d_state, const void *psi, double *d_rho, double m2, double inv,
+                          double q, cudaStream_t st) {
+  const long long N3 = ctx->N3;
+  const S *x = (const S *)d_state;
+  k_energy<S, ED><<<grid_for(N3), 256, 0, st>>>(x, sizeof(S) == 4 ? x + 2 * N3 : nullptr, (const S *)psi, d_rho,
+                                                (int)ctx->N, m2, inv, q);
+}
+
+template <int ED>
+static void launch_energy_p(cf_ctx *ctx, const void *d_state, const void *psi, double *d_rho, double m2, double inv,
+                            double q, cudaStream_t st) {
+  if (ctx->p.precision == CF_FP32_COMP)
+    launch_energy<float, ED>(ctx, d_state, psi, d_rho, m2, inv, q, st);
+  else
+    launch_energy<double, ED>(ctx, d_state, psi, d_rho, m2, inv, q, st);
+}
+
 int energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, cudaStream_t st) {
   double inv, H;
   stage_coeffs(ctx->p, t, &inv, &H);
-  const int N = (int)ctx->N;
+  const double m2 = ctx->p.m * ctx->p.m;
+  const int eq = ctx->p.equation;
+  const void *ps = nullptr, *dps = nullptr;
+  // the approximate comoving equation reports the full comoving energy density
+  // (src/equations_cuda.cu:812-815)
+  if (eq == CF_EQ_COMOVING_FRW || eq == CF_EQ_APPROX_COMOVING_FRW) CF_TRY(psi_at(ctx, t, st, &ps, &dps));
+  if (eq == CF_EQ_FIXED_CURVATURE_FRW) ps = ctx->fixed_e2m1;
+  ProfScope prof(ctx, CF_PROF_SPECTRUM, st);
+  if (ps)
+    launch_energy_p<ED_CURV>(ctx, d_state, ps, d_rho, m2, inv, 0.0, st);
+  else if (eq == CF_EQ_LAMBDA_FRW)
+    launch_energy_p<ED_LAMBDA>(ctx, d_state, nullptr, d_rho, m2, inv, ctx->p.lambda, st);
+  else if (eq == CF_EQ_SQRT_FRW)
+    launch_energy_p<ED_SQRT>(ctx, d_state, nullptr, d_rho, m2, inv, 1.0 / (ctx->p.f_a * ctx->p.f_a), st);
+  else
+    launch_energy_p<ED_QUAD>(ctx, d_state, nullptr, d_rho, m2, inv, 0.0, st);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+int dot_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_out, cudaStream_t st) {
+  double inv, H;
+  stage_coeffs(ctx->p, t, &inv, &H);
   const double m2 = ctx->p.m * ctx->p.m;
   const long long N3 = ctx->N3;
-  const bool f32 = ctx->p.precision == CF_FP32_COMP;
-  unsigned g = grid_for(N3);
-  const void *ps = nullptr, *dps = nullptr;
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) CF_TRY(psi_at(ctx, t, st, &ps, &dps));
   ProfScope prof(ctx, CF_PROF_SPECTRUM, st);
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
-    if (f32)
-      k_energy<float, true><<<g, 256, 0, st>>>((const float *)d_state, (const float *)d_state + 2 * N3,
-                                               (const float *)ps, d_rho, N, m2, inv);
-    else
-      k_energy<double, true><<<g, 256, 0, st>>>((const double *)d_state, nullptr, (const double *)ps, d_rho, N,
-                                                m2, inv);
+  if (ctx->p.precision == CF_FP32_COMP) {
+    const float *x = (const float *)d_state;
+    k_dot_energy<float><<<grid_for(N3), 256, 0, st>>>(x, x + 2 * N3, d_out, (int)ctx->N, m2, inv, H);
   } else {
-    if (f32)
-      k_energy<float, false><<<g, 256, 0, st>>>((const float *)d_state, (const float *)d_state + 2 * N3, nullptr,
-                                                d_rho, N, m2, inv);
-    else
-      k_energy<double, false><<<g, 256, 0, st>>>((const double *)d_state, nullptr, nullptr, d_rho, N, m2, inv);
+    k_dot_energy<double><<<grid_for(N3), 256, 0, st>>>((const double *)d_state, nullptr, d_out, (int)ctx->N, m2,
+                                                       inv, H);
   }
   CF_LAUNCHED(ctx);
   return CF_OK;

@@ -10,7 +10,8 @@
 //   STAGE 3: k = f(y)  acc += 2k    y' = x + cy k
 //   STAGE 4: k = f(y)  x   += dt/6 (acc + k)   (FP32: hi/lo compensated)
 // with f(phi, pi) = (pi, (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} inv lap phi)
-// (src/equations_cuda.cu:15-36, :263-287; Psi = dPsi = 0 when !COMOV).
+// (src/equations_cuda.cu:15-36, :263-287; Psi = dPsi = 0 for EQ_FRW) and the
+// other equation shapes of EqShape below.
 //
 // Tile: TXv x TYv threads; thread (tx, ty) owns V consecutive sites along c
 // (16-byte vectors) in row b0 + ty.  phi of planes a-H..a+H of the thread's own
@@ -99,11 +100,14 @@ struct StageArgs {
   S *acc;        // k accumulator [phi | pi]
   S *x;          // base state [phi | pi] (hi part in FP32_COMP)
   S *xlo;        // FP32_COMP compensation [phi | pi] (stage 4 only)
-  const S *psi;  // comoving: e^{2 Psi(t_stage)} - 1, N^3
-  const S *dpsi; // comoving: dPsi/dt(t_stage), N^3
+  const S *psi;  // EQ_COMOV, EQ_FIXED: e^{2 Psi(t_stage)} - 1, N^3; EQ_APPROX: the coarse table
+  const S *dpsi; // EQ_COMOV: dPsi/dt(t_stage), N^3
+  const int *cmap;  // EQ_APPROX: coarse index of each lattice index (N entries)
+  int M;            // EQ_APPROX: coarse grid size
   int N;
   int a_chunk;
   long long N3;
+  double q1, q2;  // EQ_LAMBDA: lambda; EQ_SQRT: f_a^2, 1/f_a^2
   double m2;    // m^2
   double inv;   // h^-2 a^-2
   double hub3;  // 3 H
@@ -168,32 +172,130 @@ __device__ __forceinline__ T lap_at(const Pack<S, V> (&q)[2 * H + 1], const S *s
   }
 }
 
-// Stage coefficients in the arithmetic type.
-template <typename T>
-struct StageCoef {
-  Coef<T> m2, inv, hub3;
+// Equation shapes of the tile kernels: the pointwise terms of the pi component
+// of the right-hand side (the phi component is always pi).
+enum EqShape : int {
+  EQ_FRW = 0,     // -3H pi - m^2 phi + inv lap (flat KG: H = 0, inv = h^-2)
+  EQ_COMOV = 1,   // (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} inv lap, Psi(t) planes
+  EQ_LAMBDA = 2,  // -3H pi - m^2 phi - lambda phi^3 + inv lap
+  EQ_SQRT = 3,    // -3H pi - m^2 phi / sqrt(1 + phi^2 / f_a^2) + inv lap
+  EQ_FIXED = 4,   // -3H pi - e^{2Psi} m^2 phi + e^{4Psi} inv lap, one fixed Psi plane
+  EQ_APPROX = 5,  // as EQ_COMOV with Psi, dPsi from a coarse table, quadratic exponentials
 };
 
-// pi component of the right-hand side (src/equations_cuda.cu:15-36, :263-287):
-//   (-3H + 4 dPsi) pi - e^{2Psi} m^2 phi + e^{4Psi} h^-2 a^-2 lap phi,
-// with ps = e^{2 Psi} - 1 (the Psi slot's first field).
-template <bool COMOV, typename S, typename T = typename Arith<S>::T>
-__device__ __forceinline__ T kpi_of(T p0, T f0, T lap, S ps, S dps, const StageCoef<T> &k) {
+template <int EQ>
+struct EqOf {
+  static constexpr bool psi_plane = EQ == EQ_COMOV || EQ == EQ_FIXED;  // reads e^{2Psi} - 1 per site
+  static constexpr bool dpsi_plane = EQ == EQ_COMOV;                   // reads dPsi/dt per site
+  static constexpr bool coarse = EQ == EQ_APPROX;                      // gathers the coarse table
+  static constexpr bool coupled = psi_plane || coarse;
+};
+
+// Stage coefficients in the arithmetic type (q1, q2: the equation's own
+// constants, StageArgs::q1 / q2).
+template <typename T>
+struct StageCoef {
+  Coef<T> m2, inv, hub3, q1, q2;
+};
+
+// The per-site curvature values of one stage at a thread's V sites: ps = e^{2Psi}
+// - 1 (EQ_APPROX: 2 Psi + 2 Psi^2), dps = dPsi/dt, ps4 = 4 Psi + 8 Psi^2 (EQ_APPROX).
+template <typename S, int V>
+struct Coupling {
+  Pack<S, V> ps, dps, ps4;
+};
+
+// The coarse columns of a thread's V sites c..c+V-1 and the coarse row of its b
+// (EQ_APPROX; constant along a, so formed once per tile).
+template <int V>
+struct CoarseCols {
+  int col[V];
+  int row_b;  // coarse index of b
+};
+
+template <int EQ, int V>
+__device__ __forceinline__ CoarseCols<V> coarse_cols(const int *cmap, bool act, int b, int c) {
+  CoarseCols<V> cc{};
+  if constexpr (EqOf<EQ>::coarse) {
+    if (act) {  // b < N and c + V <= N only for active threads
+      cc.row_b = __ldg(cmap + b);
+#pragma unroll
+      for (int v = 0; v < V; ++v) cc.col[v] = __ldg(cmap + c + v);
+    }
+  }
+  return cc;
+}
+
+// Loads the curvature values of sites (a, b, c..c+V-1): `site` their offset in an
+// N^3 plane set; ca the coarse index of a (EQ_APPROX).  The coarse table holds 4
+// words per coarse site: (2Psi + 2Psi^2, 4Psi + 8Psi^2, dPsi/dt, 0).
+template <int EQ, typename S, int V>
+__device__ __forceinline__ void load_coupling(Coupling<S, V> &cp, const S *psi, const S *dpsi, long long site,
+                                              int M, int ca, const CoarseCols<V> &cc) {
+  if constexpr (EqOf<EQ>::psi_plane) cp.ps = ldv<S, V>(psi + site);
+  if constexpr (EqOf<EQ>::dpsi_plane) cp.dps = ldv<S, V>(dpsi + site);
+  if constexpr (EqOf<EQ>::coarse) {
+    const int row = (ca * M + cc.row_b) * M;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int idx = row + cc.col[v];
+      if constexpr (sizeof(S) == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(psi) + idx);
+        cp.ps.v[v] = t.x;
+        cp.ps4.v[v] = t.y;
+        cp.dps.v[v] = t.z;
+      } else {
+        const double2 t0 = __ldg(reinterpret_cast<const double2 *>(psi) + 2 * idx);
+        const double2 t1 = __ldg(reinterpret_cast<const double2 *>(psi) + 2 * idx + 1);
+        cp.ps.v[v] = t0.x;
+        cp.ps4.v[v] = t0.y;
+        cp.dps.v[v] = t1.x;
+      }
+    }
+  }
+}
+
+// pi component of the right-hand side at site v of a thread's sites
+// (src/equations_cuda.cu:15-36 FRW, :38-76 lambda, :84-104 sqrt potential,
+// :112-136 fixed Psi, :263-287 comoving, :299-329 approximate comoving).
+template <int EQ, typename S, int V, typename T = typename Arith<S>::T>
+__device__ __forceinline__ T kpi_of(T p0, T f0, T lap, const Coupling<S, V> &cp, int v, const StageCoef<T> &k) {
   if constexpr (sizeof(T) == 8) {
-    if constexpr (COMOV) {
+    if constexpr (EQ == EQ_COMOV || EQ == EQ_FIXED) {
       T e2, e4;
-      psi_factors(ps, e2, e4);
-      return (-k.hub3.hi + (T)4 * (T)dps) * p0 - e2 * k.m2.hi * f0 + e4 * k.inv.hi * lap;
+      psi_factors(cp.ps.v[v], e2, e4);
+      if constexpr (EQ == EQ_COMOV)
+        return (-k.hub3.hi + (T)4 * (T)cp.dps.v[v]) * p0 - e2 * k.m2.hi * f0 + e4 * k.inv.hi * lap;
+      else
+        return -k.hub3.hi * p0 - e2 * k.m2.hi * f0 + e4 * k.inv.hi * lap;
+    } else if constexpr (EQ == EQ_APPROX) {
+      const T e2 = (T)1 + (T)cp.ps.v[v], e4 = (T)1 + (T)cp.ps4.v[v];
+      return (-k.hub3.hi + (T)4 * (T)cp.dps.v[v]) * p0 - e2 * k.m2.hi * f0 + e4 * k.inv.hi * lap;
+    } else if constexpr (EQ == EQ_LAMBDA) {
+      return -k.hub3.hi * p0 - k.m2.hi * f0 - k.q1.hi * f0 * f0 * f0 + k.inv.hi * lap;
+    } else if constexpr (EQ == EQ_SQRT) {
+      return -k.hub3.hi * p0 - k.m2.hi * f0 / sqrt(1.0 + f0 * f0 / k.q1.hi) + k.inv.hi * lap;
     } else {
       return -k.hub3.hi * p0 - k.m2.hi * f0 + k.inv.hi * lap;
     }
   } else {
     const float mf = k.m2.mul(f0);
     const float g = k.inv.mul(lap);
-    if constexpr (COMOV) {
-      const float e2m1 = (float)ps, e4m1 = e2m1 * (e2m1 + 2.0f);  // e^{4Psi} - 1 = (e^{2Psi} - 1)(e^{2Psi} + 1)
-      const float fr = 4.0f * (float)dps * p0 - k.hub3.mul(p0);
+    if constexpr (EQ == EQ_COMOV || EQ == EQ_FIXED || EQ == EQ_APPROX) {
+      const float e2m1 = (float)cp.ps.v[v];
+      // e^{4Psi} - 1 = (e^{2Psi} - 1)(e^{2Psi} + 1); the approximate equation's own quadratic
+      const float e4m1 = (EQ == EQ_APPROX) ? (float)cp.ps4.v[v] : e2m1 * (e2m1 + 2.0f);
+      const float fr = (EQ == EQ_FIXED) ? -k.hub3.mul(p0) : 4.0f * (float)cp.dps.v[v] * p0 - k.hub3.mul(p0);
       return fr - fmaf(e2m1, mf, mf) + fmaf(e4m1, g, g);
+    } else if constexpr (EQ == EQ_LAMBDA) {
+      return -k.hub3.mul(p0) - mf - k.q1.mul(f0 * f0 * f0) + g;
+    } else if constexpr (EQ == EQ_SQRT) {
+      // m^2 phi / sqrt(1 + u) = m^2 phi (1 - w), w = u / (s (1 + s)), s = sqrt(1 + u):
+      // the correction is formed relative to m^2 phi, never as a rounded 1 + eps
+      const float u = k.q2.mul(f0 * f0);
+      const float sq = sqrtf(1.0f + u);
+      const float w = u / (sq * (1.0f + sq));
+      return -k.hub3.mul(p0) - fmaf(-w, mf, mf) + g;
     } else {
       return -k.hub3.mul(p0) - mf + g;
     }
@@ -223,7 +325,7 @@ struct TileSmem {
 
 // FULL: the caller guarantees the tile lies inside the lattice (N % TW == 0 and
 // N % TYv == 0), so the active width and height are compile-time constants.
-template <typename S, int H, bool COMOV, int STAGE, int TXv, int TYv, bool FULL = false>
+template <typename S, int H, int EQ, int STAGE, int TXv, int TYv, bool FULL = false>
 __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0, int a_begin, int a_end, S *sm2) {
   using TS = TileSmem<S, H, TXv, TYv>;
   constexpr bool DB = DoubleBuffered<S>::value;
@@ -245,8 +347,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
   const S *phi_in = A.yin;
   const S *pi_in = A.yin + N3;
   using T = typename Arith<S>::T;
-  const StageCoef<T> kc{Coef<T>(A.m2), Coef<T>(A.inv), Coef<T>(A.hub3)};
+  const StageCoef<T> kc{Coef<T>(A.m2), Coef<T>(A.inv), Coef<T>(A.hub3), Coef<T>(A.q1), Coef<T>(A.q2)};
   const Coef<T> cy(A.cy);
+  const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
 
   Pack<S> q[2 * H + 1];
   if (act) {
@@ -258,7 +361,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
     const long long site = NN * a + rowoff;
 #pragma unroll
     for (int j = 0; j < 2 * H; ++j) q[j] = q[j + 1];
-    Pack<S> pi0, xp, xq, cp, cq, lp, lq, ps, dps;
+    Pack<S> pi0, xp, xq, cp, cq, lp, lq;
+    Coupling<S, V> cpl;
     if (act) {
       q[2 * H] = ldv(phi_in + NN * ((a + H) % N) + rowoff);
       pi0 = ldv(pi_in + site);
@@ -272,10 +376,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
         lp = ldv_rw(A.xlo + site);
         lq = ldv_rw(A.xlo + N3 + site);
       }
-      if constexpr (COMOV) {
-        ps = ldv(A.psi + site);
-        dps = ldv(A.dpsi + site);
-      }
+      if constexpr (EqOf<EQ>::coupled)
+        load_coupling<EQ, S, V>(cpl, A.psi, A.dpsi, site, A.M, EqOf<EQ>::coarse ? __ldg(A.cmap + a) : 0, cc);
     }
     S *sm = sm2;
     if constexpr (DB) {
@@ -330,7 +432,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
       const T lap = lap_at<S, H, SP>(q, sm, row, col, v);
       const T p0 = (T)pi0.v[v];
       const T kphi = p0;
-      const T kpi = kpi_of<COMOV, S>(p0, f0, lap, COMOV ? ps.v[v] : (S)0, COMOV ? dps.v[v] : (S)0, kc);
+      const T kpi = kpi_of<EQ, S, V>(p0, f0, lap, cpl, v, kc);
       if constexpr (STAGE == 0) {
         o_phi.v[v] = (S)kphi;
         o_pi.v[v] = (S)kpi;

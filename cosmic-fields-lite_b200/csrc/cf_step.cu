@@ -14,8 +14,10 @@
 //   stage 3 (t+dt/2)  k3 = f(y)      acc += 2 k3      y' = x + dt   k3
 //   stage 4 (t+dt)    k4 = f(y)      x   += dt/6 (acc + k4)
 //
-// with f the Klein-Gordon right-hand side (src/equations_cuda.cu:15-36 for flat
-// and FRW, :263-287 for the comoving-curvature coupling).  The tile code is in
+// with f the Klein-Gordon right-hand side of the context's equation
+// (src/equations_cuda.cu:15-36 flat and FRW, :38-76 lambda phi^4, :84-104 sqrt
+// potential, :112-136 fixed curvature, :263-287 comoving curvature, :299-329
+// approximate comoving curvature; the EqShape of cf_stage_tile.cuh).  The tile code is in
 // cf_stage_tile.cuh: a CTA of 32 x 8 threads owns a (b, c) tile of 8 rows x 64
 // (FP64) or 128 (FP32) columns and marches along a over a chunk of planes.
 //
@@ -40,18 +42,18 @@ constexpr int TY = 8;   // threads along b
 // from measurements at N = 512: 4 for FP32 (double-buffered planes) and for the
 // uncoupled FP64 stages; the compiler's choice for the FP64 comoving stages,
 // whose Psi terms would spill at 64 registers.
-template <typename S, bool COMOV>
+template <typename S, int EQ>
 struct StageMinBlocks {
-  static constexpr int value = (sizeof(S) == 4 || !COMOV) ? 4 : 1;
+  static constexpr int value = EQ == EQ_SQRT ? 3 : ((sizeof(S) == 4 || !EqOf<EQ>::coupled) ? 4 : 1);
 };
 
-template <typename S, int H, bool COMOV, int STAGE, bool FULL>
-__global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_stage(const StageArgs<S> A) {
+template <typename S, int H, int EQ, int STAGE, bool FULL>
+__global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, EQ>::value)) k_stage(const StageArgs<S> A) {
   using TS = TileSmem<S, H, TX, TY>;
   __shared__ __align__(16) S sm[TS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
-  stage_tile<S, H, COMOV, STAGE, TX, TY, FULL>(A, blockIdx.x * TS::TW, blockIdx.y * TY, a_begin,
-                                               min(a_begin + A.a_chunk, A.N), sm);
+  stage_tile<S, H, EQ, STAGE, TX, TY, FULL>(A, blockIdx.x * TS::TW, blockIdx.y * TY, a_begin,
+                                            min(a_begin + A.a_chunk, A.N), sm);
 }
 
 // Paired-stage kernels: the same tile, two stages per pass.  Occupancy floors
@@ -85,33 +87,39 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, COMOV>::value)) k_s
 // 7-point pass B, the pass with the most live values, which takes 2 floats per
 // thread and 4 CTAs/SM without spills (N = 512: 1.71 -> 1.52 ms per step; the
 // other FP32 passes measured slower with 2 floats per thread).
-template <typename S, int H, bool COMOV, int PASS>
+template <typename S, int H, int EQ, int PASS>
 struct PairVec {
-  static constexpr int value = (sizeof(S) == 4 && COMOV && H == 1 && PASS == 2) ? 2 : VecT<S>::n;
+  static constexpr int value = (sizeof(S) == 4 && EqOf<EQ>::coupled && H == 1 && PASS == 2) ? 2 : VecT<S>::n;
 };
 #ifndef CF_PAIR_MB_F32_V2
 #define CF_PAIR_MB_F32_V2 4
 #endif
 
-template <typename S, int H, bool COMOV, int PASS>
+// The sqrt potential's IEEE square root and division need registers of their
+// own: 7-point floors 3 (pass A) and 2 (pass B) in both storage types, where the
+// uncoupled floors spill (ptxas -v).
+template <typename S, int H, int EQ, int PASS>
 struct PairMinBlocks {
+  static constexpr bool cpl = EqOf<EQ>::coupled;
+  static constexpr int sqrt_h1 = PASS == 1 ? 3 : 2;
   static constexpr int value =
+      (EQ == EQ_SQRT && H == 1) ? sqrt_h1 :
       sizeof(S) == 4
-          ? (H == 1 ? (PairVec<S, H, COMOV, PASS>::value == 2
+          ? (H == 1 ? (PairVec<S, H, EQ, PASS>::value == 2
                            ? CF_PAIR_MB_F32_V2
-                           : ((PASS == 1 && !COMOV) ? CF_PAIR_MB_F32_A : CF_PAIR_MB_F32))
+                           : ((PASS == 1 && !cpl) ? CF_PAIR_MB_F32_A : CF_PAIR_MB_F32))
                     : CF_PAIR_MB_F32_H2)
-          : (COMOV ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
+          : (cpl ? CF_PAIR_MB_F64_COMOV : (H == 1 ? CF_PAIR_MB_F64 : CF_PAIR_MB_F64_H2));
 };
 
-template <typename S, int H, bool COMOV, int PASS, bool FULL>
-__global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, COMOV, PASS>::value)) k_pair(const PairArgs<S> A) {
-  constexpr int VW = PairVec<S, H, COMOV, PASS>::value;
+template <typename S, int H, int EQ, int PASS, bool FULL>
+__global__ void __launch_bounds__(TX *TY, (PairMinBlocks<S, H, EQ, PASS>::value)) k_pair(const PairArgs<S> A) {
+  constexpr int VW = PairVec<S, H, EQ, PASS>::value;
   using PS = PairSmem<S, H, TX, TY, VW>;
   __shared__ __align__(16) S sm[PS::count];
   const int a_begin = blockIdx.z * A.a_chunk;
-  pair_tile<S, H, COMOV, PASS, TX, TY, FULL, VW>(A, blockIdx.x * PS::TS::TW, blockIdx.y * TY, a_begin,
-                                             min(a_begin + A.a_chunk, A.N), sm);
+  pair_tile<S, H, EQ, PASS, TX, TY, FULL, VW>(A, blockIdx.x * PS::TS::TW, blockIdx.y * TY, a_begin,
+                                          min(a_begin + A.a_chunk, A.N), sm);
 }
 
 // Planes per CTA along a: enough CTAs to fill the GPU several times over.
@@ -121,7 +129,7 @@ static int pick_a_chunk(int N, int tiles_xy) {
   return chunk;
 }
 
-template <typename S, int H, bool COMOV, int STAGE>
+template <typename S, int H, int EQ, int STAGE>
 static int launch_stage_t(cf_ctx *ctx, const StageArgs<S> &A0, cudaStream_t st) {
   constexpr int TW = TX * VecT<S>::n;
   StageArgs<S> A = A0;
@@ -131,28 +139,47 @@ static int launch_stage_t(cf_ctx *ctx, const StageArgs<S> &A0, cudaStream_t st) 
   dim3 grid(gx, gy, ceil_div(A.N, A.a_chunk));
   ProfScope ps(ctx, STAGE == 0 ? CF_PROF_OTHER : STAGE - 1, st);
   if (A.N % TW == 0 && A.N % TY == 0)
-    k_stage<S, H, COMOV, STAGE, true><<<grid, block, 0, st>>>(A);
+    k_stage<S, H, EQ, STAGE, true><<<grid, block, 0, st>>>(A);
   else
-    k_stage<S, H, COMOV, STAGE, false><<<grid, block, 0, st>>>(A);
+    k_stage<S, H, EQ, STAGE, false><<<grid, block, 0, st>>>(A);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
 
-template <typename S, bool COMOV, int STAGE>
+template <typename S, int EQ, int STAGE>
 static int launch_stage_h(cf_ctx *ctx, int stencil, const StageArgs<S> &A, cudaStream_t st) {
-  if (stencil == 13) return launch_stage_t<S, 2, COMOV, STAGE>(ctx, A, st);
-  return launch_stage_t<S, 1, COMOV, STAGE>(ctx, A, st);
+  if (stencil == 13) return launch_stage_t<S, 2, EQ, STAGE>(ctx, A, st);
+  return launch_stage_t<S, 1, EQ, STAGE>(ctx, A, st);
+}
+
+// The tile kernels' equation shape of a cf_equation.
+static int shape_of(int equation) {
+  switch (equation) {
+    case CF_EQ_COMOVING_FRW: return EQ_COMOV;
+    case CF_EQ_LAMBDA_FRW: return EQ_LAMBDA;
+    case CF_EQ_SQRT_FRW: return EQ_SQRT;
+    case CF_EQ_FIXED_CURVATURE_FRW: return EQ_FIXED;
+    case CF_EQ_APPROX_COMOVING_FRW: return EQ_APPROX;
+    default: return EQ_FRW;  // CF_EQ_KG (H = 0), CF_EQ_KG_FRW
+  }
 }
 
 template <typename S, int STAGE>
 static int launch_stage(cf_ctx *ctx, const StageArgs<S> &A, cudaStream_t st) {
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) return launch_stage_h<S, true, STAGE>(ctx, ctx->p.stencil, A, st);
-  return launch_stage_h<S, false, STAGE>(ctx, ctx->p.stencil, A, st);
+  const int sten = ctx->p.stencil;
+  switch (shape_of(ctx->p.equation)) {
+    case EQ_COMOV: return launch_stage_h<S, EQ_COMOV, STAGE>(ctx, sten, A, st);
+    case EQ_LAMBDA: return launch_stage_h<S, EQ_LAMBDA, STAGE>(ctx, sten, A, st);
+    case EQ_SQRT: return launch_stage_h<S, EQ_SQRT, STAGE>(ctx, sten, A, st);
+    case EQ_FIXED: return launch_stage_h<S, EQ_FIXED, STAGE>(ctx, sten, A, st);
+    case EQ_APPROX: return launch_stage_h<S, EQ_APPROX, STAGE>(ctx, sten, A, st);
+    default: return launch_stage_h<S, EQ_FRW, STAGE>(ctx, sten, A, st);
+  }
 }
 
-template <typename S, int H, bool COMOV, int PASS>
+template <typename S, int H, int EQ, int PASS>
 static int launch_pair_t(cf_ctx *ctx, const PairArgs<S> &A0, cudaStream_t st) {
-  constexpr int TW = TX * PairVec<S, H, COMOV, PASS>::value;
+  constexpr int TW = TX * PairVec<S, H, EQ, PASS>::value;
   PairArgs<S> A = A0;
   dim3 block(TX, TY);
   unsigned gx = ceil_div(A.N, TW), gy = ceil_div(A.N, TY);
@@ -160,36 +187,69 @@ static int launch_pair_t(cf_ctx *ctx, const PairArgs<S> &A0, cudaStream_t st) {
   dim3 grid(gx, gy, ceil_div(A.N, A.a_chunk));
   ProfScope ps(ctx, PASS == 1 ? CF_PROF_PAIR_A : CF_PROF_PAIR_B, st);
   if (A.N % TW == 0 && A.N % TY == 0)
-    k_pair<S, H, COMOV, PASS, true><<<grid, block, 0, st>>>(A);
+    k_pair<S, H, EQ, PASS, true><<<grid, block, 0, st>>>(A);
   else
-    k_pair<S, H, COMOV, PASS, false><<<grid, block, 0, st>>>(A);
+    k_pair<S, H, EQ, PASS, false><<<grid, block, 0, st>>>(A);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
 
-template <typename S, int PASS>
-static int launch_pair(cf_ctx *ctx, const PairArgs<S> &A, cudaStream_t st) {
-  const bool com = ctx->p.equation == CF_EQ_COMOVING_FRW;
-  if (ctx->p.stencil == 13)
-    return com ? launch_pair_t<S, 2, true, PASS>(ctx, A, st) : launch_pair_t<S, 2, false, PASS>(ctx, A, st);
-  return com ? launch_pair_t<S, 1, true, PASS>(ctx, A, st) : launch_pair_t<S, 1, false, PASS>(ctx, A, st);
+template <typename S, int EQ, int PASS>
+static int launch_pair_h(cf_ctx *ctx, const PairArgs<S> &A, cudaStream_t st) {
+  if (ctx->p.stencil == 13) return launch_pair_t<S, 2, EQ, PASS>(ctx, A, st);
+  return launch_pair_t<S, 1, EQ, PASS>(ctx, A, st);
 }
 
-// Stage-time coefficients (and, comoving, the Psi slot) of a paired pass.
+template <typename S, int PASS>
+static int launch_pair(cf_ctx *ctx, const PairArgs<S> &A, cudaStream_t st) {
+  switch (shape_of(ctx->p.equation)) {
+    case EQ_COMOV: return launch_pair_h<S, EQ_COMOV, PASS>(ctx, A, st);
+    case EQ_LAMBDA: return launch_pair_h<S, EQ_LAMBDA, PASS>(ctx, A, st);
+    case EQ_SQRT: return launch_pair_h<S, EQ_SQRT, PASS>(ctx, A, st);
+    case EQ_FIXED: return launch_pair_h<S, EQ_FIXED, PASS>(ctx, A, st);
+    case EQ_APPROX: return launch_pair_h<S, EQ_APPROX, PASS>(ctx, A, st);
+    default: return launch_pair_h<S, EQ_FRW, PASS>(ctx, A, st);
+  }
+}
+
+// Time-independent constants of the equation: lambda, or f_a^2 and 1/f_a^2; the
+// approximate equation's coarse grid.
+static void eq_consts(const cf_ctx *ctx, double *q1, double *q2, const int **cmap, int *M) {
+  *q1 = *q2 = 0.0;
+  if (ctx->p.equation == CF_EQ_LAMBDA_FRW) *q1 = ctx->p.lambda;
+  if (ctx->p.equation == CF_EQ_SQRT_FRW) {
+    *q1 = ctx->p.f_a * ctx->p.f_a;
+    *q2 = 1.0 / (ctx->p.f_a * ctx->p.f_a);
+  }
+  *cmap = ctx->ap_cmap;
+  *M = (int)ctx->p.M;
+}
+
+// The curvature input of a stage at time t: the comoving Psi slot, the fixed Psi
+// plane or the approximate equation's coarse table (none for the others).
+template <typename S>
+static int curvature_at(cf_ctx *ctx, double t, const S **psi, const S **dpsi, cudaStream_t st) {
+  *psi = *dpsi = nullptr;
+  const void *ps = nullptr, *dps = nullptr;
+  switch (ctx->p.equation) {
+    case CF_EQ_COMOVING_FRW: CF_TRY(psi_at(ctx, t, st, &ps, &dps)); break;
+    case CF_EQ_FIXED_CURVATURE_FRW: ps = ctx->fixed_e2m1; break;
+    case CF_EQ_APPROX_COMOVING_FRW: CF_TRY(approx_at(ctx, t, st, &ps)); break;
+    default: break;
+  }
+  *psi = (const S *)ps;
+  *dpsi = (const S *)dps;
+  return CF_OK;
+}
+
+// Stage-time coefficients and curvature input of a paired pass.
 template <typename S>
 static int pair_coeffs(cf_ctx *ctx, double t, double *inv, double *hub3, const S **psi, const S **dpsi,
                        cudaStream_t st) {
   double H;
   stage_coeffs(ctx->p, t, inv, &H);
   *hub3 = 3.0 * H;
-  *psi = *dpsi = nullptr;
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
-    const void *ps, *dps;
-    CF_TRY(psi_at(ctx, t, st, &ps, &dps));
-    *psi = (const S *)ps;
-    *dpsi = (const S *)dps;
-  }
-  return CF_OK;
+  return curvature_at<S>(ctx, t, psi, dpsi, st);
 }
 
 // nsteps RK4 steps as paired-stage passes.  The new phi of pass B alternates
@@ -207,6 +267,7 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
   A.N = (int)ctx->N;
   A.N3 = N3;
   A.m2 = ctx->p.m * ctx->p.m;
+  eq_consts(ctx, &A.q1, &A.q2, &A.cmap, &A.M);
   A.xpi = x + N3;
   A.xlo = (sizeof(S) == 4) ? x + 2 * N3 : nullptr;
   A.acc = (S *)ctx->acc;
@@ -247,14 +308,8 @@ static int fill_stage_coeffs(cf_ctx *ctx, StageArgs<S> &A, double t, cudaStream_
   stage_coeffs(ctx->p, t, &inv, &H);
   A.inv = inv;
   A.hub3 = 3.0 * H;
-  A.psi = A.dpsi = nullptr;
-  if (ctx->p.equation == CF_EQ_COMOVING_FRW) {
-    const void *ps, *dps;
-    CF_TRY(psi_at(ctx, t, st, &ps, &dps));
-    A.psi = (const S *)ps;
-    A.dpsi = (const S *)dps;
-  }
-  return CF_OK;
+  eq_consts(ctx, &A.q1, &A.q2, &A.cmap, &A.M);
+  return curvature_at<S>(ctx, t, &A.psi, &A.dpsi, st);
 }
 
 template <typename S>

@@ -2,8 +2,8 @@
  * cfb200.h -- C ABI of the B200 lattice time-stepping library (libcfb200.so).
  *
  * Scope: the hot path of Cosmic-Fields-Lite -- RK4 time stepping of the
- * Klein-Gordon family on a periodic N^3 lattice (flat, FRW, comoving-curvature
- * coupled), the energy density, and the field / density power spectra that the
+ * Klein-Gordon family on a periodic N^3 lattice (flat, FRW, lambda phi^4,
+ * sqrt potential, fixed and comoving-curvature coupled), the energy density, and the field / density power spectra that the
  * observers save.  Everything runs on one CUDA device; there is no CPU fallback:
  * every call that needs the GPU fails with CF_ERR_CUDA if none is usable.
  *
@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define CFB200_ABI_VERSION 1
+#define CFB200_ABI_VERSION 2
 
 typedef enum cf_status {
   CF_OK = 0,
@@ -52,7 +52,23 @@ typedef enum cf_status {
 typedef enum cf_equation {
   CF_EQ_KG = 0,           /* KleinGordonEquation (src/equations.hpp:36-59) */
   CF_EQ_KG_FRW = 1,       /* KleinGordonEquationInFRW / CudaKleinGordonEquationInFRW */
-  CF_EQ_COMOVING_FRW = 2  /* ComovingCurvatureEquationInFRW / CudaComovingCurvatureEquationInFRW */
+  CF_EQ_COMOVING_FRW = 2, /* ComovingCurvatureEquationInFRW / CudaComovingCurvatureEquationInFRW */
+  /* CudaLambdaEquationInFRW (src/equations_cuda.cuh:36-48, src/equations_cuda.cu:38-76,
+   * :575-607): dphi' = -3H dphi - m^2 phi - lambda phi^3 + a^-2 h^-2 lap phi */
+  CF_EQ_LAMBDA_FRW = 3,
+  /* CudaSqrtPotentialEquationInFRW (src/equations_cuda.cuh:50-62, src/equations_cuda.cu:79-104,
+   * :610-642): V = m^2 f_a^2 (sqrt(1 + phi^2/f_a^2) - 1),
+   * dphi' = -3H dphi - m^2 phi / sqrt(1 + phi^2/f_a^2) + a^-2 h^-2 lap phi */
+  CF_EQ_SQRT_FRW = 4,
+  /* CudaFixedCurvatureEquationInFRW (src/equations_cuda.cuh:64-76, src/equations_cuda.cu:107-136,
+   * :645-675): a time-independent Psi(x) set with cf_set_psi,
+   * dphi' = -3H dphi - e^{2Psi} m^2 phi + e^{4Psi} a^-2 h^-2 lap phi */
+  CF_EQ_FIXED_CURVATURE_FRW = 5,
+  /* CudaApproximateComovingCurvatureEquationInFRW (src/equations_cuda.cuh:92-104,
+   * src/equations_cuda.cu:299-329, :764-815): Psi, dPsi/dt synthesised on a coarse
+   * M^3 grid from the modes of R_fft below M/2 and sampled at the nearest coarse
+   * site, with e^{2Psi} ~ 1 + 2Psi + 2Psi^2 and e^{4Psi} ~ 1 + 4Psi + 8Psi^2 */
+  CF_EQ_APPROX_COMOVING_FRW = 6
 } cf_equation;
 
 typedef enum cf_precision {
@@ -62,7 +78,11 @@ typedef enum cf_precision {
 
 /* Flat parameter block (replaces the reference's POD Param + WorkspaceGeneric
  * field copy, src/workspace.hpp:81-93).  a1, H1, t1, p describe
- * StaticEOSCosmology (src/physics.hpp:15-56); CF_EQ_KG ignores them. */
+ * StaticEOSCosmology (src/physics.hpp:15-56); CF_EQ_KG ignores them.  lambda
+ * (CF_EQ_LAMBDA_FRW), f_a (CF_EQ_SQRT_FRW, > 0; the reference's default is 1)
+ * and M (CF_EQ_APPROX_COMOVING_FRW: M % 8 == 0, M <= N, N % M == 0) are the
+ * workspace fields of the same names (src/workspace.hpp:66-67, :77); other
+ * equations ignore them. */
 typedef struct cf_params {
   int64_t N;
   double L;
@@ -75,6 +95,9 @@ typedef struct cf_params {
   int32_t precision; /* cf_precision */
   int32_t stencil;   /* 7 (reference) or 13 (fourth-order Laplacian) */
   int32_t flags;     /* CF_FLAG_* bits, 0 = defaults */
+  double lambda;     /* quartic coupling */
+  double f_a;        /* scale of the sqrt (monodromy) potential */
+  int64_t M;         /* coarse grid of the approximate comoving-curvature equation */
 } cf_params;
 
 /* Always synthesise Psi / dPsi/dt with the full 3-D C2R, even when R_fft is
@@ -132,6 +155,11 @@ int cf_state_export(cf_ctx *ctx, double *d_xy, const void *d_state, void *stream
  * workspace.R_fft, src/initializer.hpp:200-205), host or device pointer. */
 int cf_set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, void *stream);
 
+/* Psi: the fixed curvature perturbation of CF_EQ_FIXED_CURVATURE_FRW (the
+ * reference's workspace.Psi, N^3 doubles in site order, set by its initializer),
+ * host or device pointer.  Required before stepping that equation. */
+int cf_set_psi(cf_ctx *ctx, const double *Psi, int on_device, void *stream);
+
 /* Psi(x, t) and dPsi/dt(x, t) of the comoving-curvature equation into d_out
  * (2 N^3 doubles: Psi, then dPsi), the fields the right-hand side uses at time t
  * (the reference computes them inside Equation::operator(),
@@ -175,7 +203,9 @@ int cf_scale_sum(cf_ctx *ctx, double *d_out, int n, const double *const *d_in, c
 
 /* ---- observers --------------------------------------------------------------
  * cf_energy_density: Equation::compute_energy_density (src/equations_cuda.cu:537-553,
- *   :733-760) of a device state at time t into d_rho (N^3 doubles).
+ *   :733-760; lambda :591-607 with :332-369; sqrt potential :626-642 with :431-449;
+ *   fixed curvature :660-675 with :451-473; the approximate comoving equation uses
+ *   the full comoving one, :812-815) of a device state at time t into d_rho (N^3 doubles).
  * cf_power_spectrum_s2: compute_power_spectrum (src/fdm3d_cuda.cu:161-176) of an N^3
  *   FP64 field: R2C + deterministic binning into S2 bins.
  * cf_mode_power_spectrum_s2: compute_mode_power_spectrum (src/fdm3d_cuda.cu:144-159)
@@ -187,6 +217,10 @@ int cf_scale_sum(cf_ctx *ctx, double *d_out, int n, const double *const *d_in, c
  * Sums are exact fixed-point integer sums (order independent, bit-reproducible)
  * converted to FP64 once. */
 int cf_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, void *stream);
+/* cf_dot_energy_density: CudaKleinGordonEquationInFRW::compute_dot_energy_density
+ *   (src/equations_cuda.cu:372-424, :556-572), d rho / dt of the state at t into
+ *   d_out (N^3 doubles); CF_EQ_KG_FRW only. */
+int cf_dot_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_out, void *stream);
 int cf_power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, void *stream);
 int cf_mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double *d_out,
                               void *stream);

@@ -23,14 +23,18 @@
  *     whose scale_sum1..6 call cf_scale_sum (replacing
  *     src/odeint_thrust/thrust_operations.cuh:24-353).
  *   - Equation functors: operator()(x, dxdt, t) -> cf_rhs (the stock odeint steppers
- *     then run on the device); compute_energy_density -> cf_energy_density
- *     (src/equations_cuda.cuh:21-103).
+ *     then run on the device); compute_energy_density -> cf_energy_density,
+ *     compute_dot_energy_density -> cf_dot_energy_density (src/equations_cuda.cuh:21-103:
+ *     the KG, FRW, lambda, sqrt-potential, fixed-, comoving- and approximate
+ *     comoving-curvature functors).
  *   - cfb200::fused_rk4: a Stepper (concept as in src/midpoint.hpp:25-101) whose
  *     do_step is ONE cf_rk4_steps call (four fused stage kernels).  It is the path
  *     for the FP32-compensated state (Param field `precision` = CF_FP32_COMP).
  *   - WorkspaceGeneric<DeviceState>(param, initializer): the POD-param + concept
- *     field copy of src/workspace.hpp:20-93.  Optional Param fields `precision` and
- *     `stencil` (long long) select CF_FP32_COMP and the 13-point Laplacian.
+ *     field copy of src/workspace.hpp:20-93 (N, L, m, a1/H1/t1, lambda, f_a, M); the
+ *     initializer fills state, and R_fft or Psi where the equation needs them, on the
+ *     host.  Optional Param fields `precision` and `stencil` (long long) select
+ *     CF_FP32_COMP and the 13-point Laplacian.
  *   - ConstIntervalObserver<Equation, field, density, slices>: the save trigger and
  *     the raw FP64 .dat files of src/observer.hpp:64-126.
  *   - compute_power_spectrum / compute_mode_power_spectrum: src/fdm3d_cuda.cuh:22-31.
@@ -298,6 +302,12 @@ concept HasFRWParameters = requires(Param param) {
   CFB200_TYPE_REQUIREMENT(param.t1, double)
 };
 template <typename Param>
+concept HasLambda = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.lambda, double) };
+template <typename Param>
+concept HasFa = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.f_a, double) };
+template <typename Param>
+concept HasPsiApproximationParameters = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.M, long long int) };
+template <typename Param>
 concept HasPrecision = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.precision, long long int) };
 template <typename Param>
 concept HasStencil = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.stencil, long long int) };
@@ -312,7 +322,9 @@ struct WorkspaceGeneric {
   State state;                 /* filled by the initializer with host data (FP64 [phi|dphi]) */
   double lambda{0};
   double f_a{1.0};
-  std::vector<double> R_fft;   /* host HC array of the comoving curvature (comoving equation) */
+  std::vector<double> Psi;     /* host N^3 fixed curvature (fixed-curvature equation) */
+  std::vector<double> R_fft;   /* host HC array of the comoving curvature (comoving equations) */
+  long long int M = 0;         /* coarse grid of the approximate comoving equation */
   std::vector<double> t_list;
   int precision = CF_FP64;
   int stencil = 7;
@@ -325,6 +337,9 @@ struct WorkspaceGeneric {
       : N(param.N), L(param.L), fft_wrapper((int)param.N) {
     if constexpr (HasFRWParameters<Param>) cosmology = StaticEOSCosmology(param);
     if constexpr (HasMass<Param>) m = param.m;
+    if constexpr (HasLambda<Param>) lambda = param.lambda;
+    if constexpr (HasFa<Param>) f_a = param.f_a;
+    if constexpr (HasPsiApproximationParameters<Param>) M = param.M;
     if constexpr (HasPrecision<Param>) precision = (int)param.precision;
     if constexpr (HasStencil<Param>) stencil = (int)param.stencil;
     initializer(param, *this);
@@ -344,12 +359,20 @@ struct WorkspaceGeneric {
     p.equation = eq;
     p.precision = precision;
     p.stencil = stencil;
+    p.lambda = lambda;
+    p.f_a = f_a;
+    p.M = M;
     ctx = std::make_shared<Context>(p);
     equation = eq;
-    if (eq == CF_EQ_COMOVING_FRW) {
+    if (eq == CF_EQ_COMOVING_FRW || eq == CF_EQ_APPROX_COMOVING_FRW) {
       if (R_fft.size() != (size_t)ctx->info().hc_count)
         throw std::runtime_error("cfb200: comoving-curvature equation needs workspace.R_fft (HC array)");
       check(cf_set_R_fft(ctx->get(), R_fft.data(), 0, ctx->stream()));
+    }
+    if (eq == CF_EQ_FIXED_CURVATURE_FRW) {
+      if (Psi.size() != (size_t)ctx->info().field_count)
+        throw std::runtime_error("cfb200: fixed-curvature equation needs workspace.Psi (N^3 field)");
+      check(cf_set_psi(ctx->get(), Psi.data(), 0, ctx->stream()));
     }
     if (precision != CF_FP64 && state.precision == CF_FP64 && state.size()) {
       State conv(state.size());
@@ -389,6 +412,14 @@ struct DeviceEquation {
     check(cf_energy_density(ws.ctx->get(), ws.state.data(), t, rho.f64(), ws.ctx->stream()));
     return rho;
   }
+
+  /* d rho / dt of workspace.state at time t (CudaKleinGordonEquationInFRW only). */
+  static Vector compute_dot_energy_density(Workspace &ws, const double t) {
+    Vector out((size_t)ws.ctx->info().field_count);
+    out.ctx = ws.ctx;
+    check(cf_dot_energy_density(ws.ctx->get(), ws.state.data(), t, out.f64(), ws.ctx->stream()));
+    return out;
+  }
 };
 
 typedef DeviceEquation<CF_EQ_KG> KleinGordonEquation;
@@ -396,6 +427,10 @@ typedef DeviceEquation<CF_EQ_KG_FRW> KleinGordonEquationInFRW;
 typedef DeviceEquation<CF_EQ_KG_FRW> CudaKleinGordonEquationInFRW;
 typedef DeviceEquation<CF_EQ_COMOVING_FRW> ComovingCurvatureEquationInFRW;
 typedef DeviceEquation<CF_EQ_COMOVING_FRW> CudaComovingCurvatureEquationInFRW;
+typedef DeviceEquation<CF_EQ_LAMBDA_FRW> CudaLambdaEquationInFRW;
+typedef DeviceEquation<CF_EQ_SQRT_FRW> CudaSqrtPotentialEquationInFRW;
+typedef DeviceEquation<CF_EQ_FIXED_CURVATURE_FRW> CudaFixedCurvatureEquationInFRW;
+typedef DeviceEquation<CF_EQ_APPROX_COMOVING_FRW> CudaApproximateComovingCurvatureEquationInFRW;
 
 /* ---- fused RK4 stepper (Stepper concept, src/midpoint.hpp:25-101) ---------- */
 class fused_rk4 {

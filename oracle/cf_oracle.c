@@ -19,9 +19,13 @@
  *   S2 bins: 3*(N/2)^2+1 doubles indexed by s^2 = i^2+j^2+k^2.
  *
  * Equation codes: 0 = KleinGordonEquation (flat), 1 = KleinGordonEquationInFRW,
- * 2 = ComovingCurvatureEquationInFRW.  Stencil: 7 (reference) or 13 (fourth
- * order; no reference counterpart, restated from the standard 5-point
- * second-derivative formula per axis).
+ * 2 = ComovingCurvatureEquationInFRW, and the GPU-only functors of
+ * src/equations_cuda.cu (no CPU twin in the reference; restated from the CUDA
+ * kernels and pinned against the reference's own GPU build, tests/golden/):
+ * 3 = CudaLambdaEquationInFRW, 4 = CudaSqrtPotentialEquationInFRW,
+ * 5 = CudaFixedCurvatureEquationInFRW, 6 = CudaApproximateComovingCurvatureEquationInFRW.
+ * Stencil: 7 (reference) or 13 (fourth order; no reference counterpart,
+ * restated from the standard 5-point second-derivative formula per axis).
  */
 #include <math.h>
 #include <stdint.h>
@@ -40,6 +44,10 @@ typedef struct {
   double a1, H1, t1, p; /* StaticEOSCosmology, src/physics.hpp:15-56 */
   int eq;
   int stencil;
+  double lambda;          /* eq 3: quartic coupling (workspace.lambda) */
+  double f_a;             /* eq 4: sqrt-potential scale (workspace.f_a) */
+  int64_t M;              /* eq 6: coarse grid (workspace.M) */
+  const double *Psi_fixed; /* eq 5: the fixed Psi(x), N^3 (workspace.Psi) */
 } cfo_params;
 
 /* ---- cosmology: src/physics.hpp:34-55 ---------------------------------- */
@@ -102,6 +110,41 @@ void cfo_psi_fields(const cfo_params *P, const double *R_fft, double t, double *
   free(df);
 }
 
+/* eq 6: Psi and dPsi/dt on the coarse M^3 grid at t
+ * (CudaApproximateComovingCurvatureEquationInFRW::operator(), src/equations_cuda.cu:764-809):
+ * the modes of R_fft kept by compute_cutoff_fouriers (src/fdm3d_cuda.cu:118-141,
+ * :206-219: M-grid mode a < M/2 from a, a >= M/2 from N-(M-a), same for b, c from c,
+ * times 1/(N/M)^3), the comoving transfer functions at lattice size M
+ * (src/equations_cuda.cu:209-259) and a 3-D c2r of size M.  Dense M^3 outputs. */
+void cfo_approx_fields(const cfo_params *P, const double *R_fft, double t, double *Psi, double *dPsidt) {
+  const int64_t N = P->N, M = P->M, nhN = N / 2 + 1, nhM = M / 2 + 1;
+  const size_t hcM = (size_t)(2 * M * M * nhM);
+  double *cut = (double *)malloc(sizeof(double) * hcM);
+  double *pf = (double *)malloc(sizeof(double) * hcM);
+  double *df = (double *)malloc(sizeof(double) * hcM);
+  const double scale_diff = (double)N / (double)M;
+  const double scaling = 1.0 / (scale_diff * scale_diff * scale_diff);
+  for (int64_t a = 0; a < M; ++a)
+    for (int64_t b = 0; b < M; ++b)
+      for (int64_t c = 0; c < nhM; ++c) {
+        int64_t aN = (a < M / 2) ? a : (N - (M - a));
+        int64_t bN = (b < M / 2) ? b : (N - (M - b));
+        int64_t oM = 2 * (M * nhM * a + nhM * b + c), oN = 2 * (N * nhN * aN + nhN * bN + c);
+        cut[oM] = R_fft[oN] * scaling;
+        cut[oM + 1] = R_fft[oN + 1] * scaling;
+      }
+  double eta_t = cfo_eta(P, t), H_t = cfo_H(P, t);
+  double factor = (2 * CFO_PI / P->L) * eta_t / sqrt(3);
+  cfo_psi_dpsidt_fft(M, cut, pf, df, factor, H_t);
+  fftw_plan pl = fftw_plan_dft_c2r_3d((int)M, (int)M, (int)M, (fftw_complex *)pf, Psi, FFTW_ESTIMATE);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)pf, Psi);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)df, dPsidt);
+  fftw_destroy_plan(pl);
+  free(cut);
+  free(pf);
+  free(df);
+}
+
 /* Lattice Laplacian times h^2 at site (a,b,c): 7-point (reference
  * src/equations.cpp:94-101 summation order) or 13-point fourth order. */
 static inline double lap_h2(const double *f, int64_t N, int64_t a, int64_t b, int64_t c, int stencil) {
@@ -127,7 +170,13 @@ static inline double lap_h2(const double *f, int64_t N, int64_t a, int64_t b, in
  *   eq 1: src/equations.cpp:71-104 dphi' = -3H dphi - m^2 phi + a^-2 h^-2 lap phi
  *   eq 2: src/equations.cpp:186-261
  *         dphi' = (-3H + 4 dPsi/dt) dphi - e^{2Psi} m^2 phi + e^{4Psi} a^-2 h^-2 lap phi
- * R_fft is used for eq 2 only. */
+ *   eq 3: src/equations_cuda.cu:38-76   ... - m^2 phi - lambda phi^3 + ...
+ *   eq 4: src/equations_cuda.cu:84-104  ... - m^2 phi / sqrt(1 + phi^2 / f_a^2) + ...
+ *   eq 5: src/equations_cuda.cu:112-136 eq 2's form with the fixed Psi and dPsi/dt = 0
+ *   eq 6: src/equations_cuda.cu:299-329 with the coarse fields of cfo_approx_fields,
+ *         sampled at coarse site ((a + s/2) % N) / s per axis, s = N/M, and
+ *         e^{2Psi} -> 1 + 2Psi + 2Psi^2, e^{4Psi} -> 1 + 4Psi + 8Psi^2
+ * R_fft is used for eq 2 and 6 only. */
 void cfo_rhs(const cfo_params *P, const double *x, const double *R_fft, double t, double *dxdt) {
   const int64_t N = P->N, N3 = N * N * N;
   const double m = P->m;
@@ -146,20 +195,51 @@ void cfo_rhs(const cfo_params *P, const double *x, const double *R_fft, double t
     dPsi = (double *)malloc(sizeof(double) * N3);
     cfo_psi_fields(P, R_fft, t, Psi, dPsi);
   }
+  int64_t M = P->M, sd = 1, hs = 0;
+  if (P->eq == 6) {
+    Psi = (double *)malloc(sizeof(double) * M * M * M);
+    dPsi = (double *)malloc(sizeof(double) * M * M * M);
+    cfo_approx_fields(P, R_fft, t, Psi, dPsi);
+    sd = N / M;
+    hs = sd / 2;
+  }
   const double *phi = x, *pi = x + N3;
   for (int64_t a = 0; a < N; ++a)
     for (int64_t b = 0; b < N; ++b)
       for (int64_t c = 0; c < N; ++c) {
         int64_t i = IDX(N, a, b, c);
         double lap = lap_h2(phi, N, a, b, c, P->stencil);
+        double f = phi[i];
         dxdt[i] = pi[i];
-        if (P->eq == 0) {
-          dxdt[N3 + i] = (-1.0) * m * m * phi[i] + inv * lap;
-        } else if (P->eq == 1) {
-          dxdt[N3 + i] = (-3.0) * H_t * pi[i] - m * m * phi[i] + inv * lap;
-        } else {
-          dxdt[N3 + i] = (-3.0 * H_t + 4.0 * dPsi[i]) * pi[i] - exp(2 * Psi[i]) * m * m * phi[i] +
-                         exp(4 * Psi[i]) * inv * lap;
+        switch (P->eq) {
+          case 0:
+            dxdt[N3 + i] = (-1.0) * m * m * f + inv * lap;
+            break;
+          case 1:
+            dxdt[N3 + i] = (-3.0) * H_t * pi[i] - m * m * f + inv * lap;
+            break;
+          case 2:
+            dxdt[N3 + i] = (-3.0 * H_t + 4.0 * dPsi[i]) * pi[i] - exp(2 * Psi[i]) * m * m * f +
+                           exp(4 * Psi[i]) * inv * lap;
+            break;
+          case 3:
+            dxdt[N3 + i] = (-3.0) * H_t * pi[i] - m * m * f - P->lambda * f * f * f + inv * lap;
+            break;
+          case 4:
+            dxdt[N3 + i] = (-3.0) * H_t * pi[i] - m * m * f / sqrt(1.0 + f * f / (P->f_a * P->f_a)) + inv * lap;
+            break;
+          case 5: {
+            double ps = P->Psi_fixed[i];
+            dxdt[N3 + i] = (-3.0) * H_t * pi[i] - exp(2 * ps) * m * m * f + exp(4 * ps) * inv * lap;
+            break;
+          }
+          default: { /* 6 */
+            int64_t j = IDX(M, ((a + hs) % N) / sd, ((b + hs) % N) / sd, ((c + hs) % N) / sd);
+            double ps = Psi[j];
+            dxdt[N3 + i] = (-3.0 * H_t + 4.0 * dPsi[j]) * pi[i] - (1 + 2.0 * ps + 2.0 * ps * ps) * m * m * f +
+                           (1 + 4.0 * ps + 8.0 * ps * ps) * inv * lap;
+            break;
+          }
         }
       }
   free(Psi);
@@ -203,8 +283,12 @@ void cfo_rk4_steps(const cfo_params *P, double *x, const double *R_fft, double t
 
 /* Energy density rho (N^3):
  *   eq 0: src/equations.cpp:38-69, eq 1: :106-138 (inv = h^-2 a^-2),
- *   eq 2: :265-322 (e^{-2Psi} kinetic, e^{2Psi} gradient weights).
- *   rho = 1/2 dphi^2 + 1/2 m^2 phi^2 + 1/8 inv sum_axes (phi_{+1}-phi_{-1})^2 */
+ *   eq 2 and 6: :265-322 (e^{-2Psi} kinetic, e^{2Psi} gradient weights; the
+ *   approximate equation reports the full comoving density, src/equations_cuda.cu:812-815),
+ *   rho = 1/2 dphi^2 + 1/2 m^2 phi^2 + 1/8 inv sum_axes (phi_{+1}-phi_{-1})^2;
+ *   eq 3: src/equations_cuda.cu:332-369 (+ 1/4 lambda phi^4),
+ *   eq 4: :431-449 (potential m^2 f_a^2 (sqrt(1 + phi^2/f_a^2) - 1)),
+ *   eq 5: :451-473 with the fixed Psi. */
 void cfo_energy_density(const cfo_params *P, const double *x, const double *R_fft, double t, double *rho) {
   const int64_t N = P->N, N3 = N * N * N;
   const double m = P->m, h = P->L / N;
@@ -214,7 +298,7 @@ void cfo_energy_density(const cfo_params *P, const double *x, const double *R_ff
     inv = inv / (a_t * a_t);
   }
   double *Psi = NULL;
-  if (P->eq == 2) {
+  if (P->eq == 2 || P->eq == 6) {
     Psi = (double *)malloc(sizeof(double) * N3);
     cfo_psi_fields(P, R_fft, t, Psi, NULL);
   }
@@ -227,14 +311,60 @@ void cfo_energy_density(const cfo_params *P, const double *x, const double *R_ff
         double dy = phi[IDX(N, a, (b + 1) % N, c)] - phi[IDX(N, a, (b + N - 1) % N, c)];
         double dz = phi[IDX(N, a, b, (c + 1) % N)] - phi[IDX(N, a, b, (c + N - 1) % N)];
         double grad = dx * dx + dy * dy + dz * dz;
-        if (P->eq != 2) {
-          rho[i] = 0.5 * (pi[i] * pi[i] + m * m * phi[i] * phi[i] + 0.25 * inv * grad);
-        } else {
-          rho[i] = 0.5 * (exp(-2 * Psi[i]) * pi[i] * pi[i] + m * m * phi[i] * phi[i] +
-                          exp(2 * Psi[i]) * 0.25 * inv * grad);
+        double f = phi[i];
+        switch (P->eq) {
+          case 2:
+          case 6:
+            rho[i] = 0.5 * (exp(-2 * Psi[i]) * pi[i] * pi[i] + m * m * f * f + exp(2 * Psi[i]) * 0.25 * inv * grad);
+            break;
+          case 3:
+            rho[i] = 0.5 * pi[i] * pi[i] + (0.5 / 4.0) * inv * grad + 0.5 * m * m * f * f +
+                     0.25 * P->lambda * f * f * f * f;
+            break;
+          case 4:
+            rho[i] = 0.5 * pi[i] * pi[i] + (0.5 / 4.0) * inv * grad +
+                     m * m * P->f_a * P->f_a * (sqrt(1.0 + f * f / (P->f_a * P->f_a)) - 1.0);
+            break;
+          case 5: {
+            double ps = P->Psi_fixed[i];
+            rho[i] = exp(-2 * ps) * 0.5 * pi[i] * pi[i] + exp(2 * ps) * (0.5 / 4.0) * inv * grad + 0.5 * m * m * f * f;
+            break;
+          }
+          default:
+            rho[i] = 0.5 * (pi[i] * pi[i] + m * m * f * f + 0.25 * inv * grad);
         }
       }
   free(Psi);
+}
+
+/* d rho / dt of KleinGordonEquationInFRW
+ * (CudaKleinGordonEquationInFRW::compute_dot_energy_density, src/equations_cuda.cu:372-424,
+ * :556-572): dphi lap_inv + 1/4 inv sum_e (dphi_{+e} - dphi_{-e})(phi_{+e} - phi_{-e})
+ * - 3H (rho + p), rho = 1/2 dphi^2 + 1/8 inv G + 1/2 m^2 phi^2,
+ * p = 1/2 dphi^2 - 1/2 m^2 phi^2 - 1/24 inv G, G = sum_e (phi_{+e} - phi_{-e})^2. */
+void cfo_dot_energy_density(const cfo_params *P, const double *x, double t, double *out) {
+  const int64_t N = P->N, N3 = N * N * N;
+  const double m = P->m, h = P->L / N;
+  const double a_t = cfo_a(P, t), H_t = cfo_H(P, t);
+  const double inv = 1.0 / (h * h) / (a_t * a_t);
+  const double *phi = x, *pi = x + N3;
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < N; ++c) {
+        int64_t i = IDX(N, a, b, c);
+        int64_t ap = IDX(N, (a + 1) % N, b, c), am = IDX(N, (a + N - 1) % N, b, c);
+        int64_t bp = IDX(N, a, (b + 1) % N, c), bm = IDX(N, a, (b + N - 1) % N, c);
+        int64_t cp = IDX(N, a, b, (c + 1) % N), cm = IDX(N, a, b, (c + N - 1) % N);
+        double f = phi[i];
+        double dx = phi[ap] - phi[am], dy = phi[bp] - phi[bm], dz = phi[cp] - phi[cm];
+        double ex = pi[ap] - pi[am], ey = pi[bp] - pi[bm], ez = pi[cp] - pi[cm];
+        double lap = inv * (-6.0 * f + phi[ap] + phi[am] + phi[bp] + phi[bm] + phi[cp] + phi[cm]);
+        double G = dx * dx + dy * dy + dz * dz;
+        double rho = 0.5 * pi[i] * pi[i] + (0.5 / 4.0) * inv * G + 0.5 * m * m * f * f;
+        double p = 0.5 * pi[i] * pi[i] - 0.5 * m * m * f * f - (1.0 / 4.0 / 6.0) * inv * G;
+        double vt = pi[i] * lap + (1.0 / 4.0) * inv * (ex * dx + ey * dy + ez * dz);
+        out[i] = vt - 3.0 * H_t * (rho + p);
+      }
 }
 
 /* r2c of one N^3 field into HC (fftwWrapper::execute_d2z, src/fftw_wrapper.cpp:24-34). */

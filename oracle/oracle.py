@@ -10,7 +10,9 @@ legs of ``bench.py`` import this module.  It loads
   at build time.
 
 Equation codes: 0 = KleinGordonEquation (flat), 1 = KleinGordonEquationInFRW,
-2 = ComovingCurvatureEquationInFRW.
+2 = ComovingCurvatureEquationInFRW, 3 = CudaLambdaEquationInFRW,
+4 = CudaSqrtPotentialEquationInFRW, 5 = CudaFixedCurvatureEquationInFRW,
+6 = CudaApproximateComovingCurvatureEquationInFRW.
 """
 from __future__ import annotations
 
@@ -31,12 +33,19 @@ class Params(ctypes.Structure):
     """Mirror of ``cfo_params`` in cf_oracle.c."""
 
     _fields_ = [("N", _i64), ("L", _d), ("m", _d), ("a1", _d), ("H1", _d), ("t1", _d),
-                ("p", _d), ("eq", _i), ("stencil", _i)]
+                ("p", _d), ("eq", _i), ("stencil", _i), ("lam", _d), ("f_a", _d), ("M", _i64),
+                ("Psi_fixed", _vp)]
 
 
-def make_params(N, L, m=1.0, eq=1, a1=1.0, H1=0.0, t1=0.0, p=1.0, stencil=7):
-    return Params(int(N), float(L), float(m), float(a1), float(H1), float(t1), float(p),
-                  int(eq), int(stencil))
+def make_params(N, L, m=1.0, eq=1, a1=1.0, H1=0.0, t1=0.0, p=1.0, stencil=7, lam=0.0, f_a=1.0, M=0,
+                psi_fixed=None):
+    """Oracle parameters; ``psi_fixed`` (N^3 FP64, eq 5) is kept alive by the result."""
+    P = Params(int(N), float(L), float(m), float(a1), float(H1), float(t1), float(p),
+               int(eq), int(stencil), float(lam), float(f_a), int(M), None)
+    if psi_fixed is not None:
+        P._psi = np.ascontiguousarray(psi_fixed, dtype=np.float64)
+        P.Psi_fixed = P._psi.ctypes.data
+    return P
 
 
 def _ptr(a):
@@ -66,6 +75,8 @@ def lib():
         L.cfo_rk4_step.argtypes = [P, _vp, _vp, _d, _d]
         L.cfo_rk4_steps.argtypes = [P, _vp, _vp, _d, _d, _i64, _i64]
         L.cfo_energy_density.argtypes = [P, _vp, _vp, _d, _vp]
+        L.cfo_dot_energy_density.argtypes = [P, _vp, _d, _vp]
+        L.cfo_approx_fields.argtypes = [P, _vp, _d, _vp, _vp]
         L.cfo_d2z.argtypes = [_i64, _vp, _vp]
         L.cfo_power_spectrum.argtypes = [_i64, _vp, _vp]
         L.cfo_mode_power_spectrum.argtypes = [_i64, _d, _d, _d, _vp, _vp]
@@ -148,6 +159,22 @@ def energy_density(P, x, t, R_fft=None):
     lib().cfo_energy_density(ctypes.byref(P), _ptr(x), _ptr(R_fft) if R_fft is not None else None,
                              t, _ptr(out))
     return out
+
+
+def dot_energy_density(P, x, t):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty(P.N ** 3)
+    lib().cfo_dot_energy_density(ctypes.byref(P), _ptr(x), t, _ptr(out))
+    return out
+
+
+def approx_fields(P, R_fft, t):
+    """Coarse (M^3) Psi and dPsi/dt of the approximate comoving equation at t."""
+    M3 = P.M ** 3
+    psi = np.empty(M3)
+    dpsi = np.empty(M3)
+    lib().cfo_approx_fields(ctypes.byref(P), _ptr(R_fft), t, _ptr(psi), _ptr(dpsi))
+    return psi, dpsi
 
 
 def d2z(f):

@@ -10,6 +10,11 @@
 //   mode 2: KleinGordonEquationInFRW with cfb200::fused_rk4, FP32-compensated state
 //   mode 3: ComovingCurvatureEquationInFRW with cfb200::fused_rk4 (FP64), R_fft from file
 //   mode 4: KleinGordonEquation (flat) with the stock runge_kutta4_classic
+//   mode 5: CudaLambdaEquationInFRW (lambda = 0.8) with the stock runge_kutta4_classic
+//   mode 6: CudaSqrtPotentialEquationInFRW (f_a = 0.7) with cfb200::fused_rk4
+//   mode 7: CudaFixedCurvatureEquationInFRW with cfb200::fused_rk4, Psi (N^3) from file
+//   mode 8: CudaApproximateComovingCurvatureEquationInFRW (M = N/2) with cfb200::fused_rk4,
+//           R_fft from file
 // Writes out_dir/state.dat (final FP64 state), the observer's spectra files and
 // out_dir/t_list.dat.  The initializer also uses workspace.fft_wrapper the way
 // the reference's initializers do (src/initializer.hpp:204): out_dir/fft_phi0.dat
@@ -26,6 +31,23 @@ struct FRWParam {
   long long int N;
   double L;
   double m;
+  double a1;
+  double H1;
+  double t1;
+  double t_start;
+  double t_end;
+  double t_interval;
+  long long int precision;
+  long long int stencil;
+};
+
+struct FullParam {
+  long long int N;
+  double L;
+  double m;
+  double lambda;
+  double f_a;
+  long long int M;
   double a1;
   double H1;
   double t1;
@@ -63,7 +85,8 @@ static int run(const Param &param, const std::vector<double> &x0, const std::vec
                const std::string &dir) {
   auto init = [&](const auto &p, auto &ws) {
     ws.state.copy_from_host(x0.data(), x0.size());
-    ws.R_fft = R_fft;
+    ws.R_fft = R_fft;  // the optional input file: R_fft (comoving equations) or Psi (fixed curvature)
+    ws.Psi = R_fft;
     const size_t N3 = (size_t)p.N * p.N * p.N;
     cfb200::DeviceState phi;
     phi.copy_from_host(x0.data(), N3);
@@ -119,6 +142,23 @@ int main(int argc, char **argv) {
       case 4: {
         FlatParam q{N, L, 1.0, t0, t1, ti};
         return run<cfb200::KleinGordonEquation, StockRK4>(q, x0, R_fft, dt, dir);
+      }
+      case 5: {
+        FullParam q{N, L, 1.0, 0.8, 1.0, 0, 1.0, 0.5, 1.0, t0, t1, ti, CF_FP64, 7};
+        return run<cfb200::CudaLambdaEquationInFRW, StockRK4>(q, x0, R_fft, dt, dir);
+      }
+      case 6: {
+        FullParam q{N, L, 1.0, 0.0, 0.7, 0, 1.0, 0.5, 1.0, t0, t1, ti, CF_FP64, 7};
+        return run<cfb200::CudaSqrtPotentialEquationInFRW, cfb200::fused_rk4>(q, x0, R_fft, dt, dir);
+      }
+      case 7: {
+        FullParam q{N, L, 1.0, 0.0, 1.0, 0, 1.0, 0.5, 1.0, t0, t1, ti, CF_FP64, 7};
+        return run<cfb200::CudaFixedCurvatureEquationInFRW, cfb200::fused_rk4>(q, x0, R_fft, dt, dir);
+      }
+      case 8: {
+        FullParam q{N, L, 1.0, 0.0, 1.0, N / 2, 1.0, 0.5, 1.0, t0, t1, ti, CF_FP64, 7};
+        return run<cfb200::CudaApproximateComovingCurvatureEquationInFRW, cfb200::fused_rk4>(q, x0, R_fft, dt,
+                                                                                             dir);
       }
       default:
         std::fprintf(stderr, "unknown mode %d\n", mode);

@@ -28,7 +28,11 @@ def test_build_targets_sm100a_only():
 @pytest.mark.parametrize("kw,msg", [
     (dict(N=12), "N = 12"), (dict(N=4), "N = 4"), (dict(stencil=9), "stencil"),
     (dict(equation=7), "equation"), (dict(precision=5), "precision"), (dict(L=-1.0), "L must"),
-    (dict(equation=2, H1=0.0), "conformal"),
+    (dict(equation=2, H1=0.0), "conformal"), (dict(equation=6, H1=0.0, M=8), "conformal"),
+    (dict(equation=4, f_a=0.0), "f_a"), (dict(equation=4, f_a=float("inf")), "f_a"),
+    (dict(equation=3, lam=float("nan")), "lambda"),
+    (dict(equation=6, M=0), "M = 0"), (dict(equation=6, M=12), "M = 12"), (dict(equation=6, M=32), "M = 32"),
+    (dict(N=24, equation=6, M=16), "M = 16"),
 ])
 def test_create_rejects_bad_parameters_on_host(kw, msg):
     args = dict(N=16, L=16.0, m=1.0, equation=1, precision=0, stencil=7, a1=1.0, H1=0.5, t1=1.0)

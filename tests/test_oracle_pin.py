@@ -176,3 +176,42 @@ def test_known_answer_plane_wave_dispersion(stencil):
     w = np.sqrt(m * m + lam)
     y = O.rk4_steps(P, x, 0.0, 0.02, 250)
     assert np.allclose(y[: N ** 3], phi * np.cos(w * 5.0), atol=1e-7)
+
+
+# ---- the GPU-only functors: pinned to the reference's own GPU build ------------
+# tests/golden/ref_gpu_equations.npz holds outputs of src/equations_cuda.cu itself
+# (oracle/ref_gpu_golden.cu, built from the reference sources and run on a GPU;
+# inputs rebuilt bit for bit by tests/golden/ref_gpu_inputs.py).
+
+import sys  # noqa: E402
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+import ref_gpu_inputs as G  # noqa: E402
+
+GPU_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_gpu_equations.npz")
+
+
+def _relmax(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("case", ["lambda", "sqrt", "fixed", "approx", "approx_fullband"])
+def test_restatement_matches_reference_gpu_functors(case):
+    """rhs (operator()), energy density and one runge_kutta4_classic step of the
+    restated equations 3-6 against the reference's GPU functors on the same inputs
+    (1e-12 of the largest value: FP64 rounding of a few operations per site)."""
+    g = np.load(GPU_GOLDEN)
+    P = G.oracle_params(O, case)
+    x, Rf, _ = G.inputs(case)
+    assert _relmax(O.rhs(P, x, G.T, Rf), g[case + "_rhs"]) <= 1e-12
+    if case + "_rho" in g:
+        assert _relmax(O.energy_density(P, x, G.T, Rf), g[case + "_rho"]) <= 1e-12
+    if case + "_step" in g:
+        assert _relmax(O.rk4_steps(P, x, G.T, G.DT, 1, R_fft=Rf), g[case + "_step"]) <= 1e-12
+
+
+def test_restatement_matches_reference_gpu_dot_energy_density():
+    g = np.load(GPU_GOLDEN)["kgfrw_dot_rho"]
+    lat = G.SMALL
+    P = O.make_params(lat["N"], lat["L"], lat["m"], eq=1, **G.FRW)
+    assert _relmax(O.dot_energy_density(P, G.state(lat["N"]), G.T), g) <= 1e-12
