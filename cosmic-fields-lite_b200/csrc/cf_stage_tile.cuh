@@ -273,8 +273,8 @@ __device__ __forceinline__ T kpi_of(T p0, T f0, T lap, const Coupling<S, V> &cp,
       return (-k.hub3.hi + (T)4 * (T)cp.dps.v[v]) * p0 - e2 * k.m2.hi * f0 + e4 * k.inv.hi * lap;
     } else if constexpr (EQ == EQ_LAMBDA) {
       return -k.hub3.hi * p0 - k.m2.hi * f0 - k.q1.hi * f0 * f0 * f0 + k.inv.hi * lap;
-    } else if constexpr (EQ == EQ_SQRT) {
-      return -k.hub3.hi * p0 - k.m2.hi * f0 / sqrt(1.0 + f0 * f0 / k.q1.hi) + k.inv.hi * lap;
+    } else if constexpr (EQ == EQ_SQRT) {  // q2 = 1 / f_a^2
+      return -k.hub3.hi * p0 - k.m2.hi * f0 * rsqrt(1.0 + f0 * f0 * k.q2.hi) + k.inv.hi * lap;
     } else {
       return -k.hub3.hi * p0 - k.m2.hi * f0 + k.inv.hi * lap;
     }
@@ -290,12 +290,14 @@ __device__ __forceinline__ T kpi_of(T p0, T f0, T lap, const Coupling<S, V> &cp,
     } else if constexpr (EQ == EQ_LAMBDA) {
       return -k.hub3.mul(p0) - mf - k.q1.mul(f0 * f0 * f0) + g;
     } else if constexpr (EQ == EQ_SQRT) {
-      // m^2 phi / sqrt(1 + u) = m^2 phi (1 - w), w = u / (s (1 + s)), s = sqrt(1 + u):
-      // the correction is formed relative to m^2 phi, never as a rounded 1 + eps
-      const float u = k.q2.mul(f0 * f0);
-      const float sq = sqrtf(1.0f + u);
-      const float w = u / (sq * (1.0f + sq));
-      return -k.hub3.mul(p0) - fmaf(-w, mf, mf) + g;
+      // m^2 phi / sqrt(y), y = 1 + phi^2 / f_a^2: rsqrtf refined by one Newton step
+      // r <- r + r (1 - y r^2) / 2, which leaves r within a fraction of an ulp of
+      // 1/sqrt(y) (rounding errors that average out, like those of the other terms)
+      const float y = 1.0f + k.q2.mul(f0 * f0);
+      const float r0 = rsqrtf(y);
+      const float e = fmaf(-y * r0, r0, 1.0f);
+      const float r = fmaf(0.5f * r0, e, r0);
+      return -k.hub3.mul(p0) - mf * r + g;
     } else {
       return -k.hub3.mul(p0) - mf + g;
     }

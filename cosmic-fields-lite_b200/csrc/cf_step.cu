@@ -44,7 +44,7 @@ constexpr int TY = 8;   // threads along b
 // whose Psi terms would spill at 64 registers.
 template <typename S, int EQ>
 struct StageMinBlocks {
-  static constexpr int value = EQ == EQ_SQRT ? 3 : ((sizeof(S) == 4 || !EqOf<EQ>::coupled) ? 4 : 1);
+  static constexpr int value = (sizeof(S) == 4 || !EqOf<EQ>::coupled) ? 4 : 1;
 };
 
 template <typename S, int H, int EQ, int STAGE, bool FULL>
@@ -87,23 +87,56 @@ __global__ void __launch_bounds__(TX *TY, (StageMinBlocks<S, EQ>::value)) k_stag
 // 7-point pass B, the pass with the most live values, which takes 2 floats per
 // thread and 4 CTAs/SM without spills (N = 512: 1.71 -> 1.52 ms per step; the
 // other FP32 passes measured slower with 2 floats per thread).
+// (the FP32 fixed-Psi pass B, with one plane fewer, measured 1.32 ms with 16-byte
+// vectors against 1.35 ms with 2 floats; the approximate comoving pass B 1.83 against 1.43)
 template <typename S, int H, int EQ, int PASS>
 struct PairVec {
-  static constexpr int value = (sizeof(S) == 4 && EqOf<EQ>::coupled && H == 1 && PASS == 2) ? 2 : VecT<S>::n;
+  static constexpr int value =
+      (sizeof(S) == 4 && EqOf<EQ>::coupled && EQ != EQ_FIXED && H == 1 && PASS == 2) ? 2 : VecT<S>::n;
 };
 #ifndef CF_PAIR_MB_F32_V2
 #define CF_PAIR_MB_F32_V2 4
 #endif
 
-// The sqrt potential's IEEE square root and division need registers of their
-// own: 7-point floors 3 (pass A) and 2 (pass B) in both storage types, where the
-// uncoupled floors spill (ptxas -v).
+// Floors of the other equation shapes (7-point), measured at N = 512 (ms per pass
+// A / B): sqrt potential FP64 floors 4/3 -> 1.54 / 1.80, 3/2 -> 1.76 / 2.27; FP32
+// 4/3 -> 0.82 / 1.27, 4/4 -> 0.82 / 1.50; FP64 fixed Psi 2 -> 2.31 / 2.31, 3 ->
+// 1.78 / 1.89, 4 -> 1.65 / 1.77; FP64 approximate comoving 2 -> 2.37 / 2.26, 3 ->
+// 1.95 / 2.21, 4 -> 1.91 / 2.60; FP32 fixed Psi pass A 2 / 3 / 4 -> 1.21 / 0.99 /
+// 0.85, FP32 approximate comoving pass A 1.34 / 1.07 / 1.22 (pass B: the FP32
+// comoving floors).
+#ifndef CF_PAIR_MB_SQRT_A
+#define CF_PAIR_MB_SQRT_A 4
+#endif
+#ifndef CF_PAIR_MB_SQRT_B
+#define CF_PAIR_MB_SQRT_B 3
+#endif
+#ifndef CF_PAIR_MB_F64_FIXED
+#define CF_PAIR_MB_F64_FIXED 4
+#endif
+#ifndef CF_PAIR_MB_F64_APPROX_A
+#define CF_PAIR_MB_F64_APPROX_A 4
+#endif
+#ifndef CF_PAIR_MB_F64_APPROX_B
+#define CF_PAIR_MB_F64_APPROX_B 3
+#endif
+#ifndef CF_PAIR_MB_F32_FIXED_A
+#define CF_PAIR_MB_F32_FIXED_A 4
+#endif
+#ifndef CF_PAIR_MB_F32_APPROX_A
+#define CF_PAIR_MB_F32_APPROX_A 3
+#endif
 template <typename S, int H, int EQ, int PASS>
 struct PairMinBlocks {
   static constexpr bool cpl = EqOf<EQ>::coupled;
-  static constexpr int sqrt_h1 = PASS == 1 ? 3 : 2;
+  static constexpr bool fx = EQ == EQ_FIXED || EQ == EQ_APPROX;
+  static constexpr int other =
+      EQ == EQ_SQRT    ? (PASS == 1 ? CF_PAIR_MB_SQRT_A : CF_PAIR_MB_SQRT_B)
+      : sizeof(S) == 4 ? (EQ == EQ_FIXED ? CF_PAIR_MB_F32_FIXED_A : CF_PAIR_MB_F32_APPROX_A)
+      : EQ == EQ_FIXED ? CF_PAIR_MB_F64_FIXED
+                       : (PASS == 1 ? CF_PAIR_MB_F64_APPROX_A : CF_PAIR_MB_F64_APPROX_B);
   static constexpr int value =
-      (EQ == EQ_SQRT && H == 1) ? sqrt_h1 :
+      (H == 1 && (EQ == EQ_SQRT || (fx && (sizeof(S) == 8 || PASS == 1)))) ? other :
       sizeof(S) == 4
           ? (H == 1 ? (PairVec<S, H, EQ, PASS>::value == 2
                            ? CF_PAIR_MB_F32_V2
