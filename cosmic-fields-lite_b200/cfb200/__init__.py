@@ -75,6 +75,9 @@ _SIGS = {
     "cf_scale_sum": ([_vp, _vp, _i, _vp, _vp, _i64, _vp], _i),
     "cf_energy_density": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_dot_energy_density": ([_vp, _vp, _d, _vp, _vp], _i),
+    "cf_white_noise": ([_vp, ctypes.c_uint64, ctypes.c_uint64, _vp, _i64, _vp], _i),
+    "cf_grf": ([_vp, _vp, _vp, _d, _vp, _vp, _vp], _i),
+    "cf_scale_modes": ([_vp, _vp, _vp, _vp, _vp], _i),
     "cf_power_spectrum_s2": ([_vp, _vp, _vp, _vp], _i),
     "cf_mode_power_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_density_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
@@ -278,6 +281,25 @@ class Context:
 
     def s2_counts(self, d_counts, stream=None):
         check(lib().cf_s2_counts(self.h, _ptr(d_counts), _stream(stream)))
+
+    # ---- initial conditions
+    def white_noise(self, d_out, seed, offset=0, n=None, stream=None):
+        """n unit-normal deviates (Philox4x32-10 + Box-Muller) of stream `seed` from `offset`."""
+        n = d_out.numel() if n is None else int(n)
+        check(lib().cf_white_noise(self.h, int(seed), int(offset), _ptr(d_out), n, _stream(stream)))
+
+    def grf(self, d_white, sqrtP_s2, d_out, d_psi=None, psi_scale=0.0, stream=None):
+        """generate_inhomogeneous_gaussian_random_field from the deviates d_white (N^3)."""
+        import numpy as np
+        tab = np.ascontiguousarray(sqrtP_s2, dtype=np.float64)
+        check(lib().cf_grf(self.h, _ptr(d_white), _ptr(d_psi), float(psi_scale), _ptr(tab), _ptr(d_out),
+                           _stream(stream)))
+
+    def scale_modes(self, d_f, scale_s2, d_out, stream=None):
+        """compute_field_with_scaled_fourier_modes with the per-s^2 factor scale_s2."""
+        import numpy as np
+        tab = np.ascontiguousarray(scale_s2, dtype=np.float64)
+        check(lib().cf_scale_modes(self.h, _ptr(d_f), _ptr(tab), _ptr(d_out), _stream(stream)))
 
     # ---- profiling
     def profile(self, on=True):

@@ -66,6 +66,9 @@ int scale_sum(cf_ctx *, double *, int, const double *const *, const double *, in
 int set_R_fft(cf_ctx *, const double *, int, cudaStream_t);
 int energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
 int dot_energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
+int white_noise(cf_ctx *, uint64_t, uint64_t, double *, int64_t, cudaStream_t);
+int grf(cf_ctx *, const double *, const double *, double, const double *, double *, cudaStream_t);
+int scale_modes(cf_ctx *, const double *, const double *, double *, cudaStream_t);
 int power_spectrum_s2(cf_ctx *, const double *, double *, cudaStream_t);
 int mode_power_spectrum_s2(cf_ctx *, const void *, double, double *, cudaStream_t);
 int density_spectrum_s2(cf_ctx *, const void *, double, double *, cudaStream_t);
@@ -277,6 +280,8 @@ int cf_destroy(cf_ctx *ctx) {
   psi_release(ctx);
   approx_release(ctx);
   if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);
+  if (ctx->have_z2d1) cufftDestroy(ctx->plan_z2d1);
+  cudaFree(ctx->ic_table);
   if (ctx->have_d2z2) cufftDestroy(ctx->plan_d2z2);
   cudaFree(ctx->spec_hc);
   cudaFree(ctx->spec_field);
@@ -453,6 +458,54 @@ int cf_dot_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_
   }
   CF_TRY(use_device(ctx));
   return dot_energy_density(ctx, d_state, t, d_out, (cudaStream_t)stream);
+}
+
+int cf_white_noise(cf_ctx *ctx, uint64_t seed, uint64_t offset, double *d_out, int64_t n, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  if (n < 0) {
+    set_error("cf_white_noise: n must be >= 0");
+    return CF_ERR_INVALID;
+  }
+  if (n > 0) CF_TRY(check_ptr(d_out, "d_out", 8));
+  CF_TRY(use_device(ctx));
+  return white_noise(ctx, seed, offset, d_out, n, (cudaStream_t)stream);
+}
+
+static int check_table(const double *h, int64_t n, const char *what) {
+  if (!h) {
+    set_error("%s is NULL", what);
+    return CF_ERR_INVALID;
+  }
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(h[i])) {
+      set_error("%s[%lld] is not finite", what, (long long)i);
+      return CF_ERR_INVALID;
+    }
+  return CF_OK;
+}
+
+int cf_grf(cf_ctx *ctx, const double *d_white, const double *d_psi, double psi_scale, const double *h_sqrtP_s2,
+           double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_white, "d_white"));
+  CF_TRY(check_ptr(d_out, "d_out"));
+  if (d_psi) CF_TRY(check_ptr(d_psi, "d_psi", 8));
+  if (!std::isfinite(psi_scale)) {
+    set_error("psi_scale must be finite");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(check_table(h_sqrtP_s2, ctx->s2_bins, "h_sqrtP_s2"));
+  CF_TRY(use_device(ctx));
+  return grf(ctx, d_white, d_psi, psi_scale, h_sqrtP_s2, d_out, (cudaStream_t)stream);
+}
+
+int cf_scale_modes(cf_ctx *ctx, const double *d_f, const double *h_scale_s2, double *d_out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_f, "d_f"));
+  CF_TRY(check_ptr(d_out, "d_out"));
+  CF_TRY(check_table(h_scale_s2, ctx->s2_bins, "h_scale_s2"));
+  CF_TRY(use_device(ctx));
+  return scale_modes(ctx, d_f, h_scale_s2, d_out, (cudaStream_t)stream);
 }
 
 int cf_power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, void *stream) {

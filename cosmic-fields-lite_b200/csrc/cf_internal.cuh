@@ -125,6 +125,10 @@ struct cf_ctx {
   bool have_d2z1 = false, have_d2z2 = false;
   double *spec_hc = nullptr;    // 2 HC arrays (FP64)
   double *spec_field = nullptr; // N^3 FP64 (energy density scratch)
+  // Initial conditions (cf_init.cu): a Z2D plan and the per-s^2 table of the last call.
+  cufftHandle plan_z2d1 = 0;
+  bool have_z2d1 = false;
+  double *ic_table = nullptr;
   unsigned long long *bins = nullptr;   // 2 * s2_bins words: (lo, hi) fixed point
   unsigned long long *maxbits = nullptr;
   int64_t *s2_counts = nullptr;

@@ -230,6 +230,37 @@ int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stre
 /* Mode multiplicity per S2 bin (exact, the rule of plot_util.py:53-58). */
 int cf_s2_counts(cf_ctx *ctx, int64_t *d_counts, void *stream);
 
+/* ---- initial conditions -------------------------------------------------------
+ * The reference builds its initial fields on the host once, before stepping
+ * (src/initializer.hpp:33-301, src/random_field.cpp:36-89, src/fdm3d.cpp:76-102):
+ * single-threaded normal draws, FFTW transforms, per-mode loops.  These run them
+ * on the device with the context's cuFFT plans.  All arrays are FP64, device,
+ * N^3 fields in site order unless said otherwise.
+ *
+ * cf_white_noise: n unit-normal deviates into d_out, element i a function of
+ *   (seed, offset + i) only: Philox4x32-10 (Salmon et al., SC'11) on the counter
+ *   (offset + i) / 2 with key `seed`, two 53-bit uniforms per counter, Box-Muller
+ *   (cos for even, sin for odd elements).  Any split of a stream into calls gives
+ *   the same deviates.  A stand-in for the reference's std::mt19937 +
+ *   std::normal_distribution stream (src/random_field.cpp:13-33), which is
+ *   sequential; for bit-identical fields a caller draws that stream on the host
+ *   and passes it to cf_grf instead.
+ * cf_grf: generate_inhomogeneous_gaussian_random_field (src/random_field.cpp:36-83)
+ *   from the deviates d_white (N^3, e.g. from cf_white_noise or uploaded):
+ *     out = c2r( sqrtP(s^2) r2c( w / N^3 * exp(psi_scale * Psi) ) ),
+ *   d_psi may be NULL (Psi = 0: generate_gaussian_random_field, :85-89);
+ *   h_sqrtP_s2 is a HOST array of cf_info.s2_bins values sqrt(P(sqrt(s^2) 2 pi / L)),
+ *   the spectrum the reference evaluates per mode.  d_out may equal d_white.
+ * cf_scale_modes: compute_field_with_scaled_fourier_modes (src/fdm3d.cpp:76-102):
+ *     out = c2r( scale(s^2) r2c(f) ),
+ *   h_scale_s2 a HOST array of s2_bins values kernel(sqrt(s^2) 2 pi / L) / N^3
+ *   (the factor the reference applies per mode).  d_out may equal d_f.
+ * Both use the context's spectrum scratch (two HC arrays) and cuFFT plans. */
+int cf_white_noise(cf_ctx *ctx, uint64_t seed, uint64_t offset, double *d_out, int64_t n, void *stream);
+int cf_grf(cf_ctx *ctx, const double *d_white, const double *d_psi, double psi_scale, const double *h_sqrtP_s2,
+           double *d_out, void *stream);
+int cf_scale_modes(cf_ctx *ctx, const double *d_f, const double *h_scale_s2, double *d_out, void *stream);
+
 /* ---- FFT wrapper ---------------------------------------------------------------
  * The reference's cufftWrapperNoBatching (src/cuda_wrapper.cuh:113-130,
  * src/cuda_wrapper.cu:202-255), used through workspace.fft_wrapper by initializers,

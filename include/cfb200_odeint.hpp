@@ -49,7 +49,10 @@
 
 #include <boost/numeric/odeint.hpp>
 #include <cmath>
+#include <complex>
 #include <concepts>
+#include <functional>
+#include <random>
 #include <cstdio>
 #include <fstream>
 #include <memory>
@@ -324,6 +327,7 @@ struct WorkspaceGeneric {
   double f_a{1.0};
   std::vector<double> Psi;     /* host N^3 fixed curvature (fixed-curvature equation) */
   std::vector<double> R_fft;   /* host HC array of the comoving curvature (comoving equations) */
+  DeviceState R_fft_device;    /* or the same array on the device (the GPU initializers fill this) */
   long long int M = 0;         /* coarse grid of the approximate comoving equation */
   std::vector<double> t_list;
   int precision = CF_FP64;
@@ -365,9 +369,13 @@ struct WorkspaceGeneric {
     ctx = std::make_shared<Context>(p);
     equation = eq;
     if (eq == CF_EQ_COMOVING_FRW || eq == CF_EQ_APPROX_COMOVING_FRW) {
-      if (R_fft.size() != (size_t)ctx->info().hc_count)
+      const size_t hc = (size_t)ctx->info().hc_count;
+      if (R_fft_device.size() == hc)
+        check(cf_set_R_fft(ctx->get(), R_fft_device.f64(), 1, ctx->stream()));
+      else if (R_fft.size() == hc)
+        check(cf_set_R_fft(ctx->get(), R_fft.data(), 0, ctx->stream()));
+      else
         throw std::runtime_error("cfb200: comoving-curvature equation needs workspace.R_fft (HC array)");
-      check(cf_set_R_fft(ctx->get(), R_fft.data(), 0, ctx->stream()));
     }
     if (eq == CF_EQ_FIXED_CURVATURE_FRW) {
       if (Psi.size() != (size_t)ctx->info().field_count)
@@ -466,6 +474,226 @@ inline DeviceState compute_mode_power_spectrum(const long long int N, const doub
   check(cf_mode_power_spectrum_s2(ctx.get(), state.data(), a_t, out.f64(), ctx.stream()));
   return out;
 }
+
+/* ---- initial conditions on the device (src/initializer.hpp:33-301,
+ * src/random_field.cpp:13-134, src/fdm3d.cpp:76-102) ----------------------------
+ * The reference's initializers draw from one std::mt19937 + std::normal_distribution
+ * stream and transform on the host.  These draw the SAME stream on the host (so a
+ * seed gives the reference's fields) -- or, when the Param has `noise_seed` >= 0,
+ * counter-based deviates on the device (cf_white_noise; fast at large N, a different
+ * but equally distributed stream) -- and do every transform and per-mode product on
+ * the device (cf_grf, cf_scale_modes). */
+namespace RandomNormal {
+inline std::mt19937 mt{std::random_device{}()};
+inline std::normal_distribution<double> dist{0.0, 1.0};
+inline void set_generator_seed(std::mt19937::result_type seed) { mt = std::mt19937{seed}; }
+inline double generate_random_normal() { return dist(mt); }
+}  // namespace RandomNormal
+
+typedef std::function<double(double)> Spectrum;
+
+/* The spectrum factories of src/random_field.cpp:92-134 (same formulas). */
+inline Spectrum power_law_with_cutoff_given_amplitude_3d(long long N, double L, double sigma, double k_ast,
+                                                         double alpha) {
+  const double pi = 3.14159265358979323846;
+  if (!(alpha >= -3.0) || !(k_ast * L / (2 * pi) > 1.0))
+    throw std::runtime_error("cfb200: power-law spectrum needs alpha >= -3 and k_ast above the box's k_IR");
+  double P_k_ast = alpha == -3.0
+                       ? 2 * pi * pi * sigma * sigma / (k_ast * k_ast * k_ast * log(k_ast * L / (2 * pi)))
+                       : (3 + alpha) * 2 * pi * pi * sigma * sigma * (L * L * L * pow(k_ast * L, alpha)) /
+                             (pow(k_ast * L, alpha + 3) - pow(2 * pi, alpha + 3));
+  P_k_ast *= (N / L) * (N / L) * (N / L);
+  return [=](double k) { return k == 0.0 ? 0.0 : (P_k_ast * (k <= k_ast ? pow(k / k_ast, alpha) : 0.0)); };
+}
+
+inline Spectrum scale_invariant_spectrum_3d(long long N, double L, double A_s) {
+  const double pi = 3.14159265358979323846;
+  const double k0 = 1.0;
+  double P_k0 = A_s / ((k0 * k0 * k0) / (2 * pi * pi));
+  P_k0 *= (N / L) * (N / L) * (N / L);
+  return [=](double k) { return k == 0.0 ? 0.0 : (P_k0 * pow(k / k0, -3)); };
+}
+
+inline Spectrum to_deriv_spectrum(double m, const Spectrum &P_f) {
+  return [m, P_f](double k) { return (k * k + m * m) * P_f(k); };
+}
+
+inline Spectrum to_deriv_spectrum(double m, double a, const Spectrum &P_f) {
+  return [m, a, P_f](double k) { return (k * k / (a * a) + m * m) * P_f(k); };
+}
+
+/* Cosine integral Ci(x), x > 0: the power series gamma + ln x + sum_k (-x^2)^k / (2k (2k)!)
+ * (A&S 5.2.16) up to x = 2; beyond, Ci(x) = -Re E1(ix) with E1 from its continued fraction
+ * (A&S 5.1.22), evaluated by the modified Lentz method.  (The reference evaluates a Pade
+ * approximant; both agree to rounding on the arguments its initializer uses.) */
+inline double cosine_integral(double x) {
+  const double euler = 0.57721566490153286061;
+  if (x <= 2.0) {
+    double sum = 0.0, term = 1.0;
+    for (int k = 1; k < 80; ++k) {
+      term *= -x * x / ((2.0 * k - 1) * (2.0 * k));
+      const double t = term / (2.0 * k);
+      sum += t;
+      if (std::fabs(t) < 1e-18 * std::fabs(sum)) break;
+    }
+    return euler + std::log(x) + sum;
+  }
+  std::complex<double> b(1.0, x), c(1e300, 0.0), d = 1.0 / b, h = d;
+  for (int i = 1; i < 1000; ++i) {
+    const double a = -(double)i * i;
+    b += 2.0;
+    d = 1.0 / (a * d + b);
+    c = b + a / c;
+    const std::complex<double> del = c * d;
+    h *= del;
+    if (std::abs(del - 1.0) < 1e-16) break;
+  }
+  h *= std::complex<double>(std::cos(x), -std::sin(x));
+  return -h.real();
+}
+
+template <typename Param>
+concept HasNoiseSeed = requires(Param param) { CFB200_TYPE_REQUIREMENT(param.noise_seed, long long int) };
+
+/* The deviates of successive fields: the host stream (RandomNormal) or the device
+ * counter stream of `seed`, N^3 per field in the reference's order. */
+class NoiseSource {
+ public:
+  NoiseSource(Context &ctx, long long seed) : ctx_(ctx), seed_(seed) {}
+  void next(DeviceState &out) {
+    const size_t n = (size_t)ctx_.info().field_count;
+    if (seed_ >= 0) {
+      out.resize(n);
+      check(cf_white_noise(ctx_.get(), (uint64_t)seed_, pos_, out.f64(), (int64_t)n, ctx_.stream()));
+    } else {
+      std::vector<double> h(n);
+      for (auto &v : h) v = RandomNormal::generate_random_normal();
+      out.copy_from_host(h.data(), n);
+    }
+    pos_ += n;
+  }
+
+ private:
+  Context &ctx_;
+  long long seed_;
+  uint64_t pos_ = 0;
+};
+
+/* Per-s^2 tables of a spectrum / kernel, with |k| formed as the reference forms it. */
+inline std::vector<double> sqrtP_by_s2(const Context &ctx, const Spectrum &P) {
+  const double pi = 3.14159265358979323846, L = ctx.params().L;
+  std::vector<double> t((size_t)ctx.info().s2_bins);
+  for (size_t s2 = 0; s2 < t.size(); ++s2) t[s2] = sqrt(P(sqrt((double)s2) * 2 * pi / L));  // random_field.cpp:67-68
+  return t;
+}
+
+inline std::vector<double> kernel_by_s2(const Context &ctx, const std::function<double(double)> &kernel) {
+  const double pi = 3.14159265358979323846, L = ctx.params().L;
+  const long long N = ctx.params().N;
+  std::vector<double> t((size_t)ctx.info().s2_bins);
+  for (size_t s2 = 0; s2 < t.size(); ++s2) t[s2] = kernel(sqrt((double)s2) * (2 * pi / L)) / (N * N * N);  // fdm3d.cpp:94
+  return t;
+}
+
+/* generate_inhomogeneous_gaussian_random_field (src/random_field.cpp:36-83): Psi may be
+ * null (generate_gaussian_random_field); the field's modulation is exp(psi_scale Psi). */
+inline DeviceState generate_inhomogeneous_gaussian_random_field(Context &ctx, NoiseSource &noise, const DeviceState *Psi,
+                                                                double psi_scale, const Spectrum &P) {
+  DeviceState f;
+  noise.next(f);
+  const std::vector<double> t = sqrtP_by_s2(ctx, P);
+  check(cf_grf(ctx.get(), f.f64(), Psi ? Psi->f64() : nullptr, Psi ? psi_scale : 0.0, t.data(), f.f64(),
+               ctx.stream()));
+  return f;
+}
+
+/* compute_field_with_scaled_fourier_modes (src/fdm3d.cpp:76-102). */
+inline DeviceState compute_field_with_scaled_fourier_modes(Context &ctx, const DeviceState &f,
+                                                           const std::function<double(double)> &kernel) {
+  DeviceState out(f.size());
+  const std::vector<double> t = kernel_by_s2(ctx, kernel);
+  check(cf_scale_modes(ctx.get(), f.f64(), t.data(), out.f64(), ctx.stream()));
+  return out;
+}
+
+/* A context for the initializers (cuFFT plans and scratch), freed when they return. */
+template <typename Param>
+inline std::shared_ptr<Context> init_context(const Param &param) {
+  cf_params p{};
+  p.N = param.N;
+  p.L = param.L;
+  p.m = param.m;
+  p.a1 = 1.0;
+  p.p = 1.0;
+  p.equation = CF_EQ_KG;
+  p.precision = CF_FP64;
+  p.stencil = 7;
+  p.f_a = 1.0;
+  return std::make_shared<Context>(p);
+}
+
+template <typename Param>
+inline long long noise_seed_of(const Param &param) {
+  if constexpr (HasNoiseSeed<Param>) return param.noise_seed;
+  return -1;
+}
+
+/* perturbed_grf_and_comoving_curvature_fft (src/initializer.hpp:150-206) on the device:
+ * the initializer of the reference driver.  Fills workspace.state ([phi | dphi] FP64)
+ * and workspace.R_fft_device. */
+inline auto perturbed_grf_and_comoving_curvature_fft = [](const auto &param, auto &workspace) {
+  const double pi = 3.14159265358979323846;
+  auto ctx = init_context(param);
+  NoiseSource noise(*ctx, noise_seed_of(param));
+  const double eta_i = workspace.cosmology.eta(param.t_start);
+  const double L = param.L;
+  const double A_s =
+      (-576 * pow(pi, 6) * pow(eta_i, 6) * pow(param.Psi_std_dev, 2)) /
+      (-81 * pow(L, 4) * (pow(L, 2) + 2 * pow(pi, 2) * pow(eta_i, 2)) +
+       L * (81 * pow(L, 5) - 54 * pow(L, 3) * pow(pi, 2) * pow(eta_i, 2) + 48 * L * pow(pi, 4) * pow(eta_i, 4)) *
+           cos((4 * pi * eta_i) / (sqrt(3) * L)) +
+       256 * pow(pi, 6) * pow(eta_i, 6) * cosine_integral((4 * pi * eta_i) / (sqrt(3) * L)) +
+       4 * sqrt(3) * L * pi * eta_i * (27 * pow(L, 4) + 6 * pow(L, 2) * pow(pi, 2) * pow(eta_i, 2) - 16 * pow(pi, 4) * pow(eta_i, 4)) *
+           sin((4 * pi * eta_i) / (sqrt(3) * L)));
+  DeviceState R = generate_inhomogeneous_gaussian_random_field(*ctx, noise, nullptr, 0.0,
+                                                               scale_invariant_spectrum_3d(param.N, L, A_s));
+  auto kernel = [eta_i](double k) {
+    return k == 0.0 ? 0.0
+                    : (6 * sqrt(3) * (-((k * eta_i * cos((k * eta_i) / sqrt(3))) / sqrt(3)) + sin((k * eta_i) / sqrt(3)))) /
+                          (pow(k, 3) * pow(eta_i, 3));
+  };
+  DeviceState Psi = compute_field_with_scaled_fourier_modes(*ctx, R, kernel);
+  const double v = param.k_ast / (param.a1 * param.m);
+  const double alpha_varphi_sqr = 0.5 * (-3 * pow(4 * pow(v, 2) + 5, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
+  const double alpha_dot_varphi_sqr = 0.5 * (25 - 20 * pow(v, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
+  Spectrum P_f = power_law_with_cutoff_given_amplitude_3d(param.N, L, param.varphi_std_dev, param.k_ast, 0);
+  Spectrum P_dtf = to_deriv_spectrum(param.m, P_f);
+  DeviceState varphi = generate_inhomogeneous_gaussian_random_field(*ctx, noise, &Psi, alpha_varphi_sqr, P_f);
+  DeviceState dt_varphi = generate_inhomogeneous_gaussian_random_field(*ctx, noise, &Psi, alpha_dot_varphi_sqr, P_dtf);
+  const size_t N3 = varphi.size();
+  workspace.state.resize(2 * N3);
+  check_cuda(cudaMemcpyAsync(workspace.state.f64(), varphi.f64(), N3 * 8, cudaMemcpyDeviceToDevice, ctx->stream()));
+  check_cuda(cudaMemcpyAsync(workspace.state.f64() + N3, dt_varphi.f64(), N3 * 8, cudaMemcpyDeviceToDevice,
+                             ctx->stream()));
+  workspace.R_fft_device = workspace.fft_wrapper.execute_d2z(R);
+  check_cuda(cudaDeviceSynchronize());
+};
+
+/* unperturbed_grf (src/initializer.hpp:33-44) on the device. */
+inline auto unperturbed_grf = [](const auto &param, auto &workspace) {
+  auto ctx = init_context(param);
+  NoiseSource noise(*ctx, noise_seed_of(param));
+  Spectrum P_f = power_law_with_cutoff_given_amplitude_3d(param.N, param.L, param.varphi_std_dev, param.k_ast, 0);
+  Spectrum P_dtf = to_deriv_spectrum(param.m, P_f);
+  DeviceState varphi = generate_inhomogeneous_gaussian_random_field(*ctx, noise, nullptr, 0.0, P_f);
+  DeviceState dt_varphi = generate_inhomogeneous_gaussian_random_field(*ctx, noise, nullptr, 0.0, P_dtf);
+  const size_t N3 = varphi.size();
+  workspace.state.resize(2 * N3);
+  check_cuda(cudaMemcpyAsync(workspace.state.f64(), varphi.f64(), N3 * 8, cudaMemcpyDeviceToDevice, ctx->stream()));
+  check_cuda(cudaMemcpyAsync(workspace.state.f64() + N3, dt_varphi.f64(), N3 * 8, cudaMemcpyDeviceToDevice,
+                             ctx->stream()));
+  check_cuda(cudaDeviceSynchronize());
+};
 
 /* ---- raw FP64 file output (src/io.cpp:53-62) ------------------------------- */
 inline void write_vector_to_file(const std::vector<double> &v, const std::string &filename) {

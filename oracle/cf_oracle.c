@@ -27,6 +27,7 @@
  * Stencil: 7 (reference) or 13 (fourth order; no reference counterpart,
  * restated from the standard 5-point second-derivative formula per axis).
  */
+#include <complex.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -523,10 +524,60 @@ typedef double (*cfo_spectrum_fn)(double k, const double *args);
 /* generate_inhomogeneous_gaussian_random_field (src/random_field.cpp:36-83):
  * white noise / N^3, times exp(Psi) (Psi may be NULL = 0, scaled by psi_scale),
  * r2c, times sqrt(P(|k|)) per half-complex mode, unnormalised c2r. */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as
+ * 1, 2, 3", SC'11): the counter-based generator behind the product's device white
+ * noise (no reference counterpart).  Ten rounds of two 32x32->64 multiplies by
+ * 0xD2511F53 / 0xCD9E8D57 with the Weyl key schedule 0x9E3779B9 / 0xBB67AE85. */
+void cfo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n1 = (uint32_t)p1, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1,
+             n3 = (uint32_t)p0;
+    c0 = n0, c1 = n1, c2 = n2, c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0, out[1] = c1, out[2] = c2, out[3] = c3;
+}
+
+/* The product's device deviates (cf_white_noise): element g of stream `seed` is deviate
+ * g % 2 of counter g / 2 -- uniforms u1 = (x0:x1 >> 11 + 1/2) 2^-53, u2 = (x2:x3 >> 11) 2^-53,
+ * Box-Muller sqrt(-2 ln u1) (cos 2 pi u2, sin 2 pi u2). */
+void cfo_white_noise(uint64_t seed, uint64_t offset, int64_t n, double *out) {
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t g = offset + (uint64_t)i, ctr = g >> 1;
+    uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0, 0}, k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)}, x[4];
+    cfo_philox4x32_10(c, k, x);
+    uint64_t a = (((uint64_t)x[0] << 32) | x[1]) >> 11, b = (((uint64_t)x[2] << 32) | x[3]) >> 11;
+    double u1 = ((double)a + 0.5) * 0x1.0p-53, u2 = (double)b * 0x1.0p-53;
+    double rad = sqrt(-2.0 * log(u1));
+    out[i] = (g & 1) ? rad * sin(2 * CFO_PI * u2) : rad * cos(2 * CFO_PI * u2);
+  }
+}
+
+/* n consecutive deviates of the stream (RandomNormal::generate_random_normal, src/random_field.cpp:28-31). */
+void cfo_rng_fill(cfo_rng *r, double *out, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) out[i] = cfo_rng_normal(r);
+}
+
+static void grf_core(int64_t N, double L, const double *Psi, double psi_scale, cfo_spectrum_fn P, const double *args,
+                     double *out);
+
 void cfo_grf(cfo_rng *r, int64_t N, double L, const double *Psi, double psi_scale, cfo_spectrum_fn P,
              const double *args, double *out) {
-  const int64_t N3 = N * N * N, nh = N / 2 + 1;
+  const int64_t N3 = N * N * N;
   for (int64_t i = 0; i < N3; ++i) out[i] = (1.0 / (double)N3) * cfo_rng_normal(r);
+  grf_core(N, L, Psi, psi_scale, P, args, out);
+}
+
+/* The same field from given deviates `white` (N^3) instead of the stream. */
+void cfo_grf_white(int64_t N, double L, const double *white, const double *Psi, double psi_scale, int kind,
+                   const double *args, double *out);
+
+static void grf_core(int64_t N, double L, const double *Psi, double psi_scale, cfo_spectrum_fn P, const double *args,
+                     double *out) {
+  const int64_t N3 = N * N * N, nh = N / 2 + 1;
   if (Psi)
     for (int64_t i = 0; i < N3; ++i) out[i] = out[i] * exp(psi_scale * Psi[i]);
   double *hc = (double *)malloc(sizeof(double) * 2 * N * N * nh);
@@ -562,6 +613,25 @@ static double sp_scale_invariant(double k, const double *args) {
   return k == 0.0 ? 0.0 : (args[0] * pow(k / 1.0, -3));
 }
 
+static cfo_spectrum_fn spectrum_of(int kind) {
+  return kind == 0 ? sp_power_law_cutoff : kind == 1 ? sp_deriv_power_law_cutoff : sp_scale_invariant;
+}
+
+/* kind 0: args = {P_k_ast, k_ast, alpha}; 1: {P_k_ast, k_ast, alpha, m}; 2: {P_k0}. */
+void cfo_grf_white(int64_t N, double L, const double *white, const double *Psi, double psi_scale, int kind,
+                   const double *args, double *out) {
+  const int64_t N3 = N * N * N;
+  for (int64_t i = 0; i < N3; ++i) out[i] = (1.0 / (double)N3) * white[i];
+  grf_core(N, L, Psi, psi_scale, spectrum_of(kind), args, out);
+}
+
+/* sqrt(P(sqrt(s^2) 2 pi / L)) for s^2 = 0 .. 3(N/2)^2: the per-mode factor of the GRF. */
+void cfo_sqrtP_table(int64_t N, double L, int kind, const double *args, double *out) {
+  const int64_t n = 3 * (N / 2) * (N / 2) + 1;
+  cfo_spectrum_fn P = spectrum_of(kind);
+  for (int64_t s2 = 0; s2 < n; ++s2) out[s2] = sqrt(P(sqrt((double)s2) * 2 * CFO_PI / L, args));
+}
+
 /* P_k_ast of power_law_with_cutoff_given_amplitude_3d (src/random_field.cpp:92-101). */
 double cfo_power_law_amplitude(int64_t N, double L, double sigma, double k_ast, double alpha) {
   double P = alpha == -3.0
@@ -572,17 +642,35 @@ double cfo_power_law_amplitude(int64_t N, double L, double sigma, double k_ast, 
   return P;
 }
 
-/* Cosine integral Ci(x) = gamma + ln x + sum_{k>=1} (-x^2)^k / (2k (2k)!),
- * the convergent power series (Abramowitz & Stegun 5.2.16), for 0 < x <= 4. */
+/* Cosine integral Ci(x), x > 0.  Up to x = 4: the convergent power series
+ * gamma + ln x + sum_{k>=1} (-x^2)^k / (2k (2k)!) (Abramowitz & Stegun 5.2.16); beyond,
+ * where the series' alternating terms lose digits: Ci(x) = -Re E1(ix) with E1 from its
+ * continued fraction E1(z) = e^{-z} / (z + 1 - 1^2 / (z + 3 - 2^2 / (z + 5 - ...)))
+ * (A&S 5.1.22), evaluated by the modified Lentz method.  (The reference evaluates a
+ * Pade approximant, src/special_function.hpp:4-26; they agree to rounding.) */
 double cfo_ci(double x) {
-  double sum = 0.0, term = 1.0;
-  for (int k = 1; k < 60; ++k) {
-    term *= -x * x / ((2.0 * k - 1) * (2.0 * k));
-    double add = term / (2.0 * k);
-    sum += add;
-    if (fabs(add) < 1e-18 * fabs(sum)) break;
+  if (x <= 2.0) {
+    double sum = 0.0, term = 1.0;
+    for (int k = 1; k < 80; ++k) {
+      term *= -x * x / ((2.0 * k - 1) * (2.0 * k));
+      double add = term / (2.0 * k);
+      sum += add;
+      if (fabs(add) < 1e-18 * fabs(sum)) break;
+    }
+    return 0.57721566490153286061 + log(x) + sum;
   }
-  return 0.57721566490153286061 + log(x) + sum;
+  double complex b = 1.0 + x * I, c = 1e300, d = 1.0 / b, h = d;
+  for (int i = 1; i < 1000; ++i) {
+    double a = -(double)i * i;
+    b += 2.0;
+    d = 1.0 / (a * d + b);
+    c = b + a / c;
+    double complex del = c * d;
+    h *= del;
+    if (cabs(del - 1.0) < 1e-16) break;
+  }
+  h *= cos(x) - sin(x) * I;
+  return -creal(h);
 }
 
 /* Rebuilds the initial state and R_fft of the reference driver
@@ -590,14 +678,18 @@ double cfo_ci(double x) {
  * src/initializer.hpp:150-206): params of src/main.cpp:98-122 with N, L given.
  * state: 2N^3, R_fft: HC.  The amplitude A_s follows initializer.hpp:156-166
  * with Ci evaluated by the series above. */
-void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, double *R_fft) {
+/* Scalars of the reference driver's initializer (src/main.cpp:98-122 parameters,
+ * perturbed_grf_and_comoving_curvature_fft, src/initializer.hpp:150-206). */
+typedef struct {
+  double eta_i, P_k0, alpha_phi, alpha_dphi, args[4];
+} driver_consts;
+
+static driver_consts driver_constants(int64_t N, double L) {
   const double m = 1.0, k_ast = 1.0, varphi_std = 1.0, Psi_std = 0.02, a1 = 1.0, H1 = 0.05;
   const double t1 = 1.0 / (2 * H1), t_start = t1;
   cfo_params P = {N, L, m, a1, H1, t1, 1.0, 2, 7};
-  const int64_t N3 = N * N * N;
-  cfo_rng *r = (cfo_rng *)malloc(sizeof(cfo_rng));
-  cfo_rng_seed(r, seed);
   const double pi = CFO_PI;
+  driver_consts d;
   double eta_i = cfo_eta(&P, t_start);
   double A_s = (-576 * pow(pi, 6) * pow(eta_i, 6) * pow(Psi_std, 2)) /
                (-81 * pow(L, 4) * (pow(L, 2) + 2 * pow(pi, 2) * pow(eta_i, 2)) +
@@ -608,8 +700,50 @@ void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, doubl
                     sin((4 * pi * eta_i) / (sqrt(3) * L)));
   double P_k0 = A_s / ((1.0 * 1.0 * 1.0) / (2 * pi * pi));
   P_k0 *= ((double)N / L) * ((double)N / L) * ((double)N / L);
+  double v = k_ast / (a1 * m);
+  d.eta_i = eta_i;
+  d.P_k0 = P_k0;
+  d.alpha_phi = 0.5 * (-3 * pow(4 * pow(v, 2) + 5, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
+  d.alpha_dphi = 0.5 * (25 - 20 * pow(v, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
+  d.args[0] = cfo_power_law_amplitude(N, L, varphi_std, k_ast, 0);
+  d.args[1] = k_ast;
+  d.args[2] = 0.0;
+  d.args[3] = m;
+  return d;
+}
+
+/* Psi transfer kernel of the initializer (src/initializer.hpp:184-186) over N^3
+ * (the factor compute_field_with_scaled_fourier_modes applies, src/fdm3d.cpp:94). */
+static double driver_kernel_scale(int64_t N, double L, double eta_i, int64_t s2) {
+  const double pi = CFO_PI;
+  double k = sqrt((double)s2) * (2 * pi / L);
+  double kern = k == 0.0 ? 0.0
+                         : (6 * sqrt(3) * (-((k * eta_i * cos((k * eta_i) / sqrt(3))) / sqrt(3)) + sin((k * eta_i) / sqrt(3)))) /
+                               (pow(k, 3) * pow(eta_i, 3));
+  return kern / (double)(N * N * N);
+}
+
+/* The per-s^2 tables and scalars the driver's initializer uses: sqrt P_R, the Psi
+ * kernel / N^3, sqrt P_f, sqrt P_dtf (each 3(N/2)^2+1), alphas = {alpha_phi, alpha_dphi}. */
+void cfo_driver_tables(int64_t N, double L, double *sqrtP_R, double *kern, double *sqrtP_f, double *sqrtP_df,
+                       double *alphas) {
+  driver_consts d = driver_constants(N, L);
+  const int64_t n = 3 * (N / 2) * (N / 2) + 1;
+  cfo_sqrtP_table(N, L, 2, &d.P_k0, sqrtP_R);
+  cfo_sqrtP_table(N, L, 0, d.args, sqrtP_f);
+  cfo_sqrtP_table(N, L, 1, d.args, sqrtP_df);
+  for (int64_t s2 = 0; s2 < n; ++s2) kern[s2] = driver_kernel_scale(N, L, d.eta_i, s2);
+  alphas[0] = d.alpha_phi;
+  alphas[1] = d.alpha_dphi;
+}
+
+void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, double *R_fft) {
+  const int64_t N3 = N * N * N;
+  cfo_rng *r = (cfo_rng *)malloc(sizeof(cfo_rng));
+  cfo_rng_seed(r, seed);
+  driver_consts d = driver_constants(N, L);
   double *R = (double *)malloc(sizeof(double) * N3);
-  cfo_grf(r, N, L, NULL, 0.0, sp_scale_invariant, &P_k0, R);
+  cfo_grf(r, N, L, NULL, 0.0, sp_scale_invariant, &d.P_k0, R);
   /* Psi = compute_field_with_scaled_fourier_modes(R, kernel) (src/fdm3d.cpp:76-102) */
   const int64_t nh = N / 2 + 1;
   double *hc = (double *)malloc(sizeof(double) * 2 * N * N * nh);
@@ -619,11 +753,7 @@ void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, doubl
       for (int64_t c = 0; c < nh; ++c) {
         int64_t as = (a <= N / 2) ? a : (N - a), bs = (b <= N / 2) ? b : (N - b);
         int64_t s2 = as * as + bs * bs + c * c;
-        double k = sqrt((double)s2) * (2 * pi / L);
-        double kern = k == 0.0 ? 0.0
-                               : (6 * sqrt(3) * (-((k * eta_i * cos((k * eta_i) / sqrt(3))) / sqrt(3)) + sin((k * eta_i) / sqrt(3)))) /
-                                     (pow(k, 3) * pow(eta_i, 3));
-        double scale = kern / (double)(N * N * N);
+        double scale = driver_kernel_scale(N, L, d.eta_i, s2);
         int64_t o = 2 * (N * nh * a + nh * b + c);
         hc[o] *= scale;
         hc[o + 1] *= scale;
@@ -632,12 +762,8 @@ void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, doubl
   fftw_plan pl = fftw_plan_dft_c2r_3d((int)N, (int)N, (int)N, (fftw_complex *)hc, Psi, FFTW_ESTIMATE);
   fftw_execute_dft_c2r(pl, (fftw_complex *)hc, Psi);
   fftw_destroy_plan(pl);
-  double v = k_ast / (a1 * m);
-  double alpha_phi = 0.5 * (-3 * pow(4 * pow(v, 2) + 5, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
-  double alpha_dphi = 0.5 * (25 - 20 * pow(v, 2)) / (12 * pow(v, 4) + 50 * pow(v, 2) + 50);
-  double args[4] = {cfo_power_law_amplitude(N, L, varphi_std, k_ast, 0), k_ast, 0.0, m};
-  cfo_grf(r, N, L, Psi, alpha_phi, sp_power_law_cutoff, args, state);
-  cfo_grf(r, N, L, Psi, alpha_dphi, sp_deriv_power_law_cutoff, args, state + N3);
+  cfo_grf(r, N, L, Psi, d.alpha_phi, sp_power_law_cutoff, d.args, state);
+  cfo_grf(r, N, L, Psi, d.alpha_dphi, sp_deriv_power_law_cutoff, d.args, state + N3);
   cfo_d2z(N, R, R_fft);
   free(R);
   free(hc);

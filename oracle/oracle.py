@@ -87,6 +87,14 @@ def lib():
         L.cfo_psi_fields.argtypes = [P, _vp, _d, _vp, _vp]
         L.cfo_psi_dpsidt_fft.argtypes = [_i64, _vp, _vp, _vp, _d, _d]
         L.cfo_driver_initial.argtypes = [_i64, _d, ctypes.c_uint32, _vp, _vp]
+        L.cfo_driver_tables.argtypes = [_i64, _d, _vp, _vp, _vp, _vp, _vp]
+        L.cfo_rng_size.restype = ctypes.c_size_t
+        L.cfo_rng_seed.argtypes = [_vp, ctypes.c_uint32]
+        L.cfo_rng_fill.argtypes = [_vp, _vp, _i64]
+        L.cfo_grf_white.argtypes = [_i64, _d, _vp, _vp, _d, _i, _vp, _vp]
+        L.cfo_sqrtP_table.argtypes = [_i64, _d, _i, _vp, _vp]
+        L.cfo_philox4x32_10.argtypes = [_vp, _vp, _vp]
+        L.cfo_white_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _i64, _vp]
         L.cfo_ci.restype = _d
         L.cfo_ci.argtypes = [_d]
         _lib = L
@@ -242,6 +250,58 @@ def driver_initial(N, L, seed=0):
     R_fft = np.empty(n_hc(N))
     lib().cfo_driver_initial(N, L, seed, _ptr(state), _ptr(R_fft))
     return state, R_fft
+
+
+def normals(seed, n):
+    """The first n deviates of the reference's RandomNormal stream after
+    set_generator_seed(seed) (std::mt19937 + libstdc++ normal_distribution, restated)."""
+    r = ctypes.create_string_buffer(int(lib().cfo_rng_size()))
+    lib().cfo_rng_seed(r, seed)
+    out = np.empty(int(n))
+    lib().cfo_rng_fill(r, _ptr(out), int(n))
+    return out
+
+
+def philox4x32_10(ctr, key):
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.empty(4, dtype=np.uint32)
+    lib().cfo_philox4x32_10(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+def white_noise(seed, offset, n):
+    """The deviates cf_white_noise makes (restated)."""
+    out = np.empty(int(n))
+    lib().cfo_white_noise(int(seed), int(offset), int(n), _ptr(out))
+    return out
+
+
+def grf_white(N, L, white, kind, args, Psi=None, psi_scale=0.0):
+    """generate_inhomogeneous_gaussian_random_field from given deviates; kind 0: power
+    law with cutoff {P_k_ast, k_ast, alpha}, 1: its derivative spectrum {.., m}, 2: scale
+    invariant {P_k0}."""
+    out = np.empty(N ** 3)
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    lib().cfo_grf_white(N, L, _ptr(np.ascontiguousarray(white)), _ptr(Psi) if Psi is not None else None,
+                        psi_scale, kind, _ptr(a), _ptr(out))
+    return out
+
+
+def sqrtP_table(N, L, kind, args):
+    out = np.empty(n_s2(N))
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    lib().cfo_sqrtP_table(N, L, kind, _ptr(a), _ptr(out))
+    return out
+
+
+def driver_tables(N, L):
+    """(sqrtP_R, Psi kernel / N^3, sqrtP_f, sqrtP_dtf, (alpha_phi, alpha_dphi)) of the
+    reference driver's initializer."""
+    t = [np.empty(n_s2(N)) for _ in range(4)]
+    al = np.empty(2)
+    lib().cfo_driver_tables(N, L, *[_ptr(x) for x in t], _ptr(al))
+    return t[0], t[1], t[2], t[3], al
 
 
 # ---------------------------------------------------------------- the reference itself

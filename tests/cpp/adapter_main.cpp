@@ -15,6 +15,11 @@
 //   mode 7: CudaFixedCurvatureEquationInFRW with cfb200::fused_rk4, Psi (N^3) from file
 //   mode 8: CudaApproximateComovingCurvatureEquationInFRW (M = N/2) with cfb200::fused_rk4,
 //           R_fft from file
+//   mode 9: no stepping: the reference driver's initializer run on the device
+//           (cfb200::perturbed_grf_and_comoving_curvature_fft with the driver's parameters,
+//           src/main.cpp:98-122), RandomNormal seeded with <dt> (an integer; noise_seed < 0:
+//           the host stream) or, with <t_start> >= 0, device noise of that seed; writes
+//           out_dir/state.dat and out_dir/R_fft.dat
 // Writes out_dir/state.dat (final FP64 state), the observer's spectra files and
 // out_dir/t_list.dat.  The initializer also uses workspace.fft_wrapper the way
 // the reference's initializers do (src/initializer.hpp:204): out_dir/fft_phi0.dat
@@ -67,6 +72,32 @@ struct FlatParam {
   double t_interval;
 };
 
+struct DriverParam {  // the fields of the reference driver's MyParam that its initializer reads
+  long long int N;
+  double L;
+  double m;
+  double k_ast;
+  double varphi_std_dev;
+  double Psi_std_dev;
+  double a1;
+  double H1;
+  double t1;
+  double t_start;
+  long long int noise_seed;
+};
+
+static int run_init(long long N, double L, unsigned seed, long long noise_seed, const std::string &dir) {
+  DriverParam p{N, L, 1.0, 1.0, 1.0, 0.02, 1.0, 0.05, 1.0 / (2 * 0.05), 1.0 / (2 * 0.05), noise_seed};
+  cfb200::RandomNormal::set_generator_seed(seed);
+  cfb200::WorkspaceGeneric<cfb200::DeviceState> ws(p, cfb200::perturbed_grf_and_comoving_curvature_fft);
+  std::vector<double> h;
+  cfb200::copy_vector(h, ws.state);
+  cfb200::write_vector_to_file(h, dir + "state.dat");
+  cfb200::copy_vector(h, ws.R_fft_device);
+  cfb200::write_vector_to_file(h, dir + "R_fft.dat");
+  return 0;
+}
+
 static std::vector<double> read_file(const std::string &name) {
   std::ifstream f(name, std::ios::binary | std::ios::ate);
   if (!f) {
@@ -118,6 +149,15 @@ int main(int argc, char **argv) {
     return 2;
   }
   const int mode = std::atoi(argv[1]);
+  if (mode == 9) {
+    try {
+      return run_init(std::atoll(argv[2]), std::atof(argv[3]), (unsigned)std::atoll(argv[4]), std::atoll(argv[5]),
+                      argv[9]);
+    } catch (const std::exception &e) {
+      std::fprintf(stderr, "error: %s\n", e.what());
+      return 1;
+    }
+  }
   const long long N = std::atoll(argv[2]);
   const double L = std::atof(argv[3]), dt = std::atof(argv[4]);
   const double t0 = std::atof(argv[5]), t1 = std::atof(argv[6]), ti = std::atof(argv[7]);

@@ -90,3 +90,24 @@ def test_adapter_integrate_const_matches_reference(mode):
     P = O.make_params(N, L, 1.0, eq=eq, **cos, **extra)
     rho_last = O.energy_density(P, got, t_list[-1], Rf)
     assert rel(spectra[-1][2], rho_last[: N * N]) <= 1e-12
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="adapter driver not built (needs Boost.odeint headers)")
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_adapter_device_initializer_matches_reference_initializer():
+    """cfb200::perturbed_grf_and_comoving_curvature_fft (host RandomNormal stream,
+    transforms on the device) against the reference's own CPU initializer
+    (src/initializer.hpp:150-206 compiled in oracle/_ref) with the same seed, at N = 128
+    (the reference's driver parameters carry M = 128 and its workspace asserts N >= M)."""
+    N = 128
+    L, seed = 0.8 * N, 6
+    with tempfile.TemporaryDirectory() as d:
+        out = subprocess.run([BIN, "9", str(N), repr(L), str(seed), "-1", "0", "0", "-", d + "/"],
+                             capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        state = np.fromfile(os.path.join(d, "state.dat"))
+        R_fft = np.fromfile(os.path.join(d, "R_fft.dat"))
+    with tempfile.TemporaryDirectory() as d:
+        want_state, want_R = O.ref_driver_initial(N, L, seed, d, want_state=True)
+    assert np.abs(state - want_state).max() <= 1e-12 * np.abs(want_state).max()
+    assert np.abs(R_fft - want_R).max() <= 1e-12 * np.abs(want_R).max()

@@ -215,3 +215,58 @@ def test_restatement_matches_reference_gpu_dot_energy_density():
     lat = G.SMALL
     P = O.make_params(lat["N"], lat["L"], lat["m"], eq=1, **G.FRW)
     assert _relmax(O.dot_energy_density(P, G.state(lat["N"]), G.T), g) <= 1e-12
+
+
+# ---- initial conditions --------------------------------------------------------
+
+def test_philox_known_answers():
+    """Philox4x32-10 against the known-answer vectors published with the Random123
+    library of Salmon et al. (SC'11): zero, all-ones and pi-digit counters / keys."""
+    assert list(O.philox4x32_10([0, 0, 0, 0], [0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(O.philox4x32_10([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6,
+                                                                         0x6D5451FD]
+    assert list(O.philox4x32_10([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0])) == \
+        [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_white_noise_restatement_is_standard_normal():
+    w = O.white_noise(7, 0, 1 << 20)
+    n = w.size
+    assert abs(w.mean()) < 5 / np.sqrt(n)
+    assert abs(w.var() - 1) < 5 * np.sqrt(2 / n)
+    assert abs((w ** 4).mean() - 3) < 5 * np.sqrt(96 / n)
+    assert np.array_equal(O.white_noise(7, 12345, 100), w[12345:12445])
+
+
+def test_grf_from_the_stream_equals_grf_from_its_deviates():
+    """The reference driver's fields rebuilt from the stream's deviates through the
+    per-s^2 tables (the form the device path takes) equal the per-mode restatement."""
+    N, L = 16, 12.8
+    st, Rf = O.driver_initial(N, L, 3)
+    w = O.normals(3, 3 * N ** 3)
+    tR, kern, tf, tdf, al = O.driver_tables(N, L)
+    a = np.arange(N)
+    a = np.minimum(a, N - a)
+    s2 = a[:, None, None] ** 2 + a[None, :, None] ** 2 + np.arange(N // 2 + 1)[None, None, :] ** 2
+
+    def rt(f, tab):
+        return np.fft.irfftn(np.fft.rfftn(f.reshape(N, N, N)) * tab[s2], s=(N,) * 3, axes=(0, 1, 2)).ravel() * N ** 3
+
+    R = rt(w[: N ** 3] / N ** 3, tR)
+    Psi = rt(R, kern)
+    phi = rt(w[N ** 3: 2 * N ** 3] / N ** 3 * np.exp(al[0] * Psi), tf)
+    assert _relmax(phi, st[: N ** 3]) <= 1e-13
+    assert _relmax(np.fft.rfftn(R.reshape(N, N, N)).ravel().view(float), Rf) <= 1e-13
+
+
+def test_cosine_integral_matches_scipy():
+    """Ci(x) of the driver's A_s (series to x = 2, continued fraction beyond) against
+    scipy.special.sici, absolute error near Ci's zeros."""
+    sici = pytest.importorskip("scipy.special").sici
+    import ctypes
+    L = O.lib()
+    L.cfo_ci.restype = ctypes.c_double
+    L.cfo_ci.argtypes = [ctypes.c_double]
+    for x in np.concatenate([np.linspace(0.05, 2, 40), np.linspace(2.001, 30, 120), [100.0, 1000.0]]):
+        want = sici(x)[1]
+        assert abs(L.cfo_ci(x) - want) <= 1e-15 * max(1.0, abs(want)) + 2e-16, x
