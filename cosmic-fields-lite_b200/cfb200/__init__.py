@@ -82,6 +82,7 @@ _SIGS = {
     "cf_mode_power_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_density_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_s2_to_shells": ([_vp, _vp, _vp, _vp], _i),
+    "cf_density_slices": ([_vp, _vp, _d, _vp, _vp, _vp], _i),
     "cf_s2_counts": ([_vp, _vp, _vp], _i),
     "cf_check_finite": ([_vp, _vp, ctypes.POINTER(_i64), _vp], _i),
     "cf_fft_create": ([_i64, _vp], _i),
@@ -275,6 +276,10 @@ class Context:
 
     def density_spectrum_s2(self, d_state, t, d_out, stream=None):
         check(lib().cf_density_spectrum_s2(self.h, _ptr(d_state), float(t), _ptr(d_out), _stream(stream)))
+
+    def density_slices(self, d_state, t, d_slice=None, d_axis_average=None, stream=None):
+        check(lib().cf_density_slices(self.h, _ptr(d_state), float(t), _ptr(d_slice), _ptr(d_axis_average),
+                                      _stream(stream)))
 
     def s2_to_shells(self, d_shells, d_counts=None, stream=None):
         check(lib().cf_s2_to_shells(self.h, _ptr(d_shells), _ptr(d_counts), _stream(stream)))

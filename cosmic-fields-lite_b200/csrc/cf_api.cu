@@ -67,6 +67,7 @@ int set_R_fft(cf_ctx *, const double *, int, cudaStream_t);
 int energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
 int dot_energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
 int white_noise(cf_ctx *, uint64_t, uint64_t, double *, int64_t, cudaStream_t);
+int density_slices(cf_ctx *, const void *, double, double *, double *, cudaStream_t);
 int grf(cf_ctx *, const double *, const double *, double, const double *, double *, cudaStream_t);
 int scale_modes(cf_ctx *, const double *, const double *, double *, cudaStream_t);
 int power_spectrum_s2(cf_ctx *, const double *, double *, cudaStream_t);
@@ -535,6 +536,17 @@ int cf_density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d
   CF_TRY(check_curvature(ctx));
   CF_TRY(use_device(ctx));
   return density_spectrum_s2(ctx, d_state, t, d_out, (cudaStream_t)stream);
+}
+
+int cf_density_slices(cf_ctx *ctx, const void *d_state, double t, double *d_slice, double *d_axis_average,
+                      void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  if (d_slice) CF_TRY(check_ptr(d_slice, "d_slice", 8));
+  if (d_axis_average) CF_TRY(check_ptr(d_axis_average, "d_axis_average", 8));
+  CF_TRY(check_curvature(ctx));
+  CF_TRY(use_device(ctx));
+  return density_slices(ctx, d_state, t, d_slice, d_axis_average, (cudaStream_t)stream);
 }
 
 int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stream) {

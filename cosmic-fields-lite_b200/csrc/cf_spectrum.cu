@@ -497,6 +497,30 @@ int dot_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_out
   return CF_OK;
 }
 
+// Mean over a of an N^3 field, per (b, c): out[i] = sum_a f[i + a N^2] / N (coalesced in i).
+__global__ void k_axis_mean(const double *__restrict__ f, double *__restrict__ out, long long NN, int N) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += stride) {
+    double acc = 0.0;
+    for (int a = 0; a < N; ++a) acc += f[i + (long long)a * NN];
+    out[i] = acc / (double)N;
+  }
+}
+
+int density_slices(cf_ctx *ctx, const void *d_state, double t, double *d_slice, double *d_avg, cudaStream_t st) {
+  CF_TRY(ensure_spectrum_scratch(ctx, 1));
+  CF_TRY(energy_density(ctx, d_state, t, ctx->spec_field, st));
+  const long long NN = ctx->N * ctx->N;
+  if (d_slice)
+    CF_TRY_CUDA(cudaMemcpyAsync(d_slice, ctx->spec_field, NN * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (d_avg) {
+    ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
+    k_axis_mean<<<grid_for(NN), 256, 0, st>>>(ctx->spec_field, d_avg, NN, (int)ctx->N);
+    CF_LAUNCHED(ctx);
+  }
+  return CF_OK;
+}
+
 int density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d_out, cudaStream_t st) {
   CF_TRY(ensure_spectrum_scratch(ctx, 1));
   CF_TRY(energy_density(ctx, d_state, t, ctx->spec_field, st));

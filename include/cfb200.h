@@ -225,6 +225,12 @@ int cf_power_spectrum_s2(cf_ctx *ctx, const double *d_f, double *d_out, void *st
 int cf_mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double *d_out,
                               void *stream);
 int cf_density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d_out, void *stream);
+/* cf_density_slices: the observer's density slices (src/observer.hpp:110-119) of the
+ *   energy density at t, formed on the device so that only 2 N^2 values cross to the
+ *   host: d_slice (N^2) = rho at a = 0, d_axis_average (N^2) = the mean of rho over a
+ *   (summed in increasing a, then divided by N).  Either output may be NULL. */
+int cf_density_slices(cf_ctx *ctx, const void *d_state, double t, double *d_slice, double *d_axis_average,
+                      void *stream);
 int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stream);
 
 /* Mode multiplicity per S2 bin (exact, the rule of plot_util.py:53-58). */

@@ -48,9 +48,11 @@
 #include <cuda_runtime.h>
 
 #include <boost/numeric/odeint.hpp>
+#include <boost/pfr.hpp>
 #include <cmath>
 #include <complex>
 #include <concepts>
+#include <deque>
 #include <functional>
 #include <random>
 #include <cstdio>
@@ -707,7 +709,138 @@ inline void write_vector_to_filename_template(const std::vector<double> &v, cons
   write_vector_to_file(v, name);
 }
 
-/* ---- observer (src/observer.hpp:64-126) ------------------------------------ */
+/* ---- parameter files (src/param.hpp:40-125) ---------------------------------
+ * The reference saves its POD Param three ways for Python / Mathematica readers
+ * (plot_util.py:17-34): param.dat (the struct's raw bytes), paramNames.txt (one field
+ * name per line) and paramTypes.txt ("Real64" / "Integer64" per line).  Same files
+ * here, field names by Boost.PFR reflection as in the reference. */
+template <typename T>
+inline std::string_view mathematica_format() {
+  if constexpr (std::is_same_v<T, double>) return "Real64";
+  else if constexpr (std::is_same_v<T, long long int>) return "Integer64";
+  else static_assert(sizeof(T) == 0, "Param fields must be double or long long int");
+}
+
+template <typename T>
+inline void save_param_names(const std::string &filename) {
+  std::ofstream out(filename);
+  for (auto name : boost::pfr::names_as_array<T>()) out << name << '\n';
+}
+
+template <typename T>
+inline void save_param_Mathematica_formats(const std::string &filename) {
+  std::ofstream out(filename);
+  boost::pfr::for_each_field(T(), [&](const auto &field) {
+    out << mathematica_format<std::remove_cvref_t<decltype(field)>>() << '\n';
+  });
+}
+
+template <typename T>
+inline void save_param(const T &param, const std::string &filename) {
+  std::ofstream out(filename, std::ios::binary);
+  if (out.is_open()) out.write(reinterpret_cast<const char *>(&param), sizeof(T));
+}
+
+template <typename T>
+inline void save_param_for_Mathematica(const T &param, const std::string &dir) {
+  save_param_names<T>(dir + "paramNames.txt");
+  save_param_Mathematica_formats<T>(dir + "paramTypes.txt");
+  save_param<T>(param, dir + "param.dat");
+}
+
+template <typename T>
+inline void print_param(const T &param) {
+  const auto names = boost::pfr::names_as_array<T>();
+  std::printf("---- The parameters for the simulation ----\n");
+  boost::pfr::for_each_field(param, [&](const auto &field, std::size_t i) {
+    std::printf("%.*s: %.17g\n", (int)names[i].size(), names[i].data(), (double)field);
+  });
+}
+
+inline std::vector<double> load_vector_from_file(const std::string &filename) {
+  std::ifstream file(filename, std::ios::binary | std::ios::ate);
+  std::vector<double> v;
+  if (!file.is_open()) return v;
+  const std::streamsize n = file.tellg();
+  file.seekg(0);
+  v.resize((size_t)n / sizeof(double));
+  file.read(reinterpret_cast<char *>(v.data()), (std::streamsize)(v.size() * sizeof(double)));
+  return v;
+}
+
+/* ---- observer (src/observer.hpp:64-126) ------------------------------------
+ * Same trigger (t >= t_last + t_interval, t == t_end or t == t_start), same files.
+ * Every output is formed on the device (spectra, the density's a = 0 slice and its
+ * mean over a: cf_density_slices), copied into pinned host memory on the workspace's
+ * stream and written once the copy has landed, without stopping the stream: a save's
+ * files are written at the next save, at t == t_end, by flush(), or when the last copy
+ * of the observer goes away (odeint copies observers; the copies share one queue). */
+namespace detail {
+struct ObserverIO {
+  std::shared_ptr<Context> ctx;
+  DeviceState d_out;  // field spectrum | density spectrum | slice | axis average
+  size_t s2 = 0, nn = 0;
+  struct File {
+    std::string name;
+    size_t offset, count;
+  };
+  struct Pending {
+    cudaEvent_t ev;
+    double *host;
+    std::vector<File> files;
+  };
+  std::deque<Pending> pending;
+  std::vector<double *> pool;
+
+  void bind(const std::shared_ptr<Context> &c, long long N) {
+    if (ctx == c) return;
+    drain(true);
+    ctx = c;
+    s2 = (size_t)c->info().s2_bins;
+    nn = (size_t)(N * N);
+    d_out.resize(2 * s2 + 2 * nn);
+    for (double *h : pool) cudaFreeHost(h);
+    pool.clear();
+  }
+  double *take_host() {
+    if (!pool.empty()) {
+      double *h = pool.back();
+      pool.pop_back();
+      return h;
+    }
+    void *h = nullptr;
+    check_cuda(cudaMallocHost(&h, d_out.size() * sizeof(double)));
+    return static_cast<double *>(h);
+  }
+  void write(const Pending &p) {
+    for (const File &f : p.files) {
+      std::ofstream file(f.name, std::ios::binary);
+      if (file.is_open()) file.write(reinterpret_cast<const char *>(p.host + f.offset), f.count * sizeof(double));
+    }
+  }
+  // Writes the saves whose copies have landed, and every save beyond the newest
+  // `keep` (all of them when `all`).
+  void drain(bool all, size_t keep = 0) {
+    while (!pending.empty()) {
+      Pending &p = pending.front();
+      if (!all && pending.size() <= keep && cudaEventQuery(p.ev) == cudaErrorNotReady) break;
+      check_cuda(cudaEventSynchronize(p.ev));
+      write(p);
+      cudaEventDestroy(p.ev);
+      pool.push_back(p.host);
+      pending.pop_front();
+    }
+  }
+  ~ObserverIO() {
+    try {
+      drain(true);
+    } catch (...) {
+    }
+    for (double *h : pool) cudaFreeHost(h);
+  }
+};
+}  // namespace detail
+
 template <typename Equation, bool save_field_spectrum = true, bool save_density_spectrum = true,
           bool save_density = false>
 struct ConstIntervalObserver {
@@ -717,47 +850,49 @@ struct ConstIntervalObserver {
   int idx;
   std::string dir;
   double t_start, t_end, t_interval, t_last;
+  std::shared_ptr<detail::ObserverIO> io = std::make_shared<detail::ObserverIO>();
 
   template <typename Param>
   ConstIntervalObserver(const std::string &dir_, const Param &param, Equation &eqn)
       : workspace(eqn.workspace), idx(0), dir(dir_), t_start(param.t_start), t_end(param.t_end),
         t_interval(param.t_interval), t_last(param.t_start) {}
 
+  /* Writes every pending save's files. */
+  void flush() { io->drain(true); }
+
   void operator()(const State &, double t) {
     if (t >= t_last + t_interval || t == t_end || t == t_start) {
       const long long N = workspace.N;
       Context &ctx = *workspace.ctx;
-      const cf_info &info = ctx.info();
-      std::vector<double> host;
+      io->bind(workspace.ctx, N);
+      cudaStream_t st = ctx.stream();
+      double *d = io->d_out.f64();
+      const size_t s2 = io->s2, nn = io->nn;
+      char name[512];
+      detail::ObserverIO::Pending p{};
+      auto file = [&](const char *fmt, size_t off, size_t count) {
+        std::snprintf(name, sizeof(name), (dir + fmt).c_str(), idx);
+        p.files.push_back({name, off, count});
+      };
       if constexpr (save_field_spectrum) {
-        DeviceState s((size_t)info.s2_bins);
-        check(cf_mode_power_spectrum_s2(ctx.get(), workspace.state.data(), workspace.cosmology.a(t), s.f64(),
-                                        ctx.stream()));
-        check_cuda(cudaStreamSynchronize(ctx.stream()));
-        copy_vector(host, s);
-        write_vector_to_filename_template(host, dir + "varphi_plus_spectrum_%d.dat", idx);
+        check(cf_mode_power_spectrum_s2(ctx.get(), workspace.state.data(), workspace.cosmology.a(t), d, st));
+        file("varphi_plus_spectrum_%d.dat", 0, s2);
       }
       if constexpr (save_density_spectrum) {
-        DeviceState s((size_t)info.s2_bins);
-        check(cf_density_spectrum_s2(ctx.get(), workspace.state.data(), t, s.f64(), ctx.stream()));
-        check_cuda(cudaStreamSynchronize(ctx.stream()));
-        copy_vector(host, s);
-        write_vector_to_filename_template(host, dir + "rho_spectrum_%d.dat", idx);
+        check(cf_density_spectrum_s2(ctx.get(), workspace.state.data(), t, d + s2, st));
+        file("rho_spectrum_%d.dat", s2, s2);
       }
       if constexpr (save_density) {
-        State rho = Equation::compute_energy_density(workspace, t);
-        check_cuda(cudaStreamSynchronize(ctx.stream()));
-        copy_vector(host, rho);
-        std::vector<double> slice(host.begin(), host.begin() + N * N);
-        std::vector<double> avg((size_t)(N * N), 0.0);
-        for (long long i = 0; i < N * N; ++i) {
-          double acc = 0.0;
-          for (long long k = 0; k < N; ++k) acc += host[(size_t)(i + k * N * N)];
-          avg[(size_t)i] = acc / (double)N;
-        }
-        write_vector_to_filename_template(slice, dir + "rho_slice_%d.dat", idx);
-        write_vector_to_filename_template(avg, dir + "rho_axis_average_%d.dat", idx);
+        check(cf_density_slices(ctx.get(), workspace.state.data(), t, d + 2 * s2, d + 2 * s2 + nn, st));
+        file("rho_slice_%d.dat", 2 * s2, nn);
+        file("rho_axis_average_%d.dat", 2 * s2 + nn, nn);
       }
+      p.host = io->take_host();
+      check_cuda(cudaMemcpyAsync(p.host, d, io->d_out.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      check_cuda(cudaEventCreateWithFlags(&p.ev, cudaEventDisableTiming));
+      check_cuda(cudaEventRecord(p.ev, st));
+      io->pending.push_back(std::move(p));
+      io->drain(t == t_end, 2);  // landed saves; at most two in flight
       workspace.t_list.push_back(t);
       t_last = t;
       ++idx;

@@ -20,8 +20,9 @@
 //           src/main.cpp:98-122), RandomNormal seeded with <dt> (an integer; noise_seed < 0:
 //           the host stream) or, with <t_start> >= 0, device noise of that seed; writes
 //           out_dir/state.dat and out_dir/R_fft.dat
-// Writes out_dir/state.dat (final FP64 state), the observer's spectra files and
-// out_dir/t_list.dat.  The initializer also uses workspace.fft_wrapper the way
+// Writes out_dir/state.dat (final FP64 state), the observer's spectra and density
+// files, out_dir/t_list.dat and the parameter files param.dat / paramNames.txt /
+// paramTypes.txt.  The initializer also uses workspace.fft_wrapper the way
 // the reference's initializers do (src/initializer.hpp:204): out_dir/fft_phi0.dat
 // is execute_d2z(phi0), out_dir/fft_roundtrip.dat is execute_z2d of it.
 #include <cstdio>
@@ -129,12 +130,14 @@ static int run(const Param &param, const std::vector<double> &x0, const std::vec
     cfb200::copy_vector(h, back);
     cfb200::write_vector_to_file(h, dir + "fft_roundtrip.dat");
   };
+  cfb200::save_param_for_Mathematica(param, dir);  // src/main.cpp:124
   typename Equation::Workspace workspace(param, init);
   Equation eqn(workspace);
   cfb200::ConstIntervalObserver<Equation, true, true, true> observer(dir, param, eqn);
   Stepper stepper;
   size_t steps = boost::numeric::odeint::integrate_const(stepper, eqn, workspace.state, param.t_start, param.t_end,
                                                           dt, observer);
+  observer.flush();
   std::vector<double> out;
   cfb200::copy_vector(out, workspace.state);
   cfb200::write_vector_to_file(out, dir + "state.dat");

@@ -27,6 +27,18 @@ BIN = os.path.join(ROOT, "tests", "cpp", "_build", "adapter_main")
 FRW = dict(a1=1.0, H1=0.5, t1=1.0)
 
 
+def load_params(project_dir):
+    """The parameter reader of plot_util.py:17-34 (param.dat unpacked by the types in
+    paramTypes.txt, keyed by paramNames.txt)."""
+    import struct
+    raw = open(project_dir + "param.dat", "rb").read()
+    types = open(project_dir + "paramTypes.txt").read().split("\n")[:-1]
+    names = open(project_dir + "paramNames.txt").read().split("\n")[:-1]
+    fmt = "".join({"Integer64": "q", "Real64": "d"}[t] for t in types)
+    vals = struct.unpack_from(fmt, raw)
+    return {names[i]: vals[i] for i in range(len(vals))}
+
+
 def rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
@@ -69,6 +81,8 @@ def test_adapter_integrate_const_matches_reference(mode):
         spectra = [(np.fromfile(os.path.join(d, f"varphi_plus_spectrum_{i}.dat")),
                     np.fromfile(os.path.join(d, f"rho_spectrum_{i}.dat")),
                     np.fromfile(os.path.join(d, f"rho_slice_{i}.dat"))) for i in range(len(t_list))]
+        params = load_params(d + "/")
+        axis_avg = np.fromfile(os.path.join(d, f"rho_axis_average_{len(t_list) - 1}.dat"))
         fk = np.fromfile(os.path.join(d, "fft_phi0.dat")).view(complex)
         back = np.fromfile(os.path.join(d, "fft_roundtrip.dat"))
     # workspace.fft_wrapper as the reference's initializers use it (FP64, unnormalised)
@@ -90,6 +104,10 @@ def test_adapter_integrate_const_matches_reference(mode):
     P = O.make_params(N, L, 1.0, eq=eq, **cos, **extra)
     rho_last = O.energy_density(P, got, t_list[-1], Rf)
     assert rel(spectra[-1][2], rho_last[: N * N]) <= 1e-12
+    assert rel(axis_avg, rho_last.reshape(N, N * N).mean(axis=0)) <= 1e-12
+    # param.dat / paramNames.txt / paramTypes.txt read the way plot_util.py reads them
+    assert params["N"] == N and params["L"] == L and params["t_interval"] == ti
+    assert params["t_start"] == t0 and params["t_end"] == t_end
 
 
 @pytest.mark.skipif(not os.path.exists(BIN), reason="adapter driver not built (needs Boost.odeint headers)")

@@ -385,3 +385,27 @@ def test_linearity_at_full_size_n256():
     for s in (x, y, z):
         c.rk4_steps(s, 1.0, 0.05, 3)
     assert float(torch.linalg.norm(z - (x + 2 * y)) / torch.linalg.norm(z)) <= 1e-14
+
+
+@pytest.mark.parametrize("eq,prec", [(1, cfb200.FP64), (2, cfb200.FP32_COMP)])
+def test_density_slices_match_energy_density(eq, prec):
+    """cf_density_slices: the a = 0 slice and the mean over a of the energy density
+    (the observer's rho_slice / rho_axis_average, src/observer.hpp:110-119)."""
+    N, L = 24, 20.0
+    x, Rf = make_inputs(N, L, eq, 71)
+    c = ctx_for(N, L, eq, prec=prec)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    c.upload(st, x)
+    rho = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
+    c.energy_density(st, 1.3, rho)
+    sl = torch.empty(N * N, dtype=torch.float64, device="cuda")
+    av = torch.empty(N * N, dtype=torch.float64, device="cuda")
+    c.density_slices(st, 1.3, sl, av)
+    r = rho.cpu().numpy()
+    assert np.array_equal(sl.cpu().numpy(), r[: N * N])
+    want = np.zeros(N * N)
+    for a in range(N):  # the summation order of the kernel: increasing a
+        want += r[a * N * N:(a + 1) * N * N]
+    assert np.array_equal(av.cpu().numpy(), want / N)
