@@ -83,6 +83,9 @@ _SIGS = {
     "cf_density_spectrum_s2": ([_vp, _vp, _d, _vp, _vp], _i),
     "cf_s2_to_shells": ([_vp, _vp, _vp, _vp], _i),
     "cf_density_slices": ([_vp, _vp, _d, _vp, _vp, _vp], _i),
+    "cf_wkb_create": ([_vp, _vp, _d, ctypes.POINTER(_vp), _vp], _i),
+    "cf_wkb_evaluate": ([_vp, _d, _vp, _vp], _i),
+    "cf_wkb_destroy": ([_vp], _i),
     "cf_s2_counts": ([_vp, _vp, _vp], _i),
     "cf_check_finite": ([_vp, _vp, ctypes.POINTER(_i64), _vp], _i),
     "cf_fft_create": ([_i64, _vp], _i),
@@ -395,6 +398,30 @@ class FFT:
 
     def inplace_z2d(self, d_inout, stream=None):
         check(lib().cf_fft_inplace_z2d(self.h, _ptr(d_inout), _stream(stream)))
+
+
+class WKB:
+    """cf_wkb: WKB continuation of a KG-FRW state (WKBSolutionForKleinGordonEquationInFRW)."""
+
+    def __init__(self, ctx, d_state, t_i, stream=None):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        check(lib().cf_wkb_create(ctx.h, _ptr(d_state), float(t_i), ctypes.byref(h), _stream(stream)))
+        self.h = h
+
+    def evaluate_at(self, t, d_out, stream=None):
+        check(lib().cf_wkb_evaluate(self.h, float(t), _ptr(d_out), _stream(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cf_wkb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 ENS_PERSISTENT, ENS_BATCHED, ENS_LOOP = 0, 1, 2

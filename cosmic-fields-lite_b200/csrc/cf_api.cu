@@ -68,6 +68,10 @@ int energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
 int dot_energy_density(cf_ctx *, const void *, double, double *, cudaStream_t);
 int white_noise(cf_ctx *, uint64_t, uint64_t, double *, int64_t, cudaStream_t);
 int density_slices(cf_ctx *, const void *, double, double *, double *, cudaStream_t);
+int wkb_create(cf_ctx *, const double *, double, cf_wkb **, cudaStream_t);
+int wkb_evaluate(cf_wkb *, double, double *, cudaStream_t);
+void wkb_destroy(cf_wkb *);
+cf_ctx *wkb_ctx(cf_wkb *);
 int grf(cf_ctx *, const double *, const double *, double, const double *, double *, cudaStream_t);
 int scale_modes(cf_ctx *, const double *, const double *, double *, cudaStream_t);
 int power_spectrum_s2(cf_ctx *, const double *, double *, cudaStream_t);
@@ -547,6 +551,37 @@ int cf_density_slices(cf_ctx *ctx, const void *d_state, double t, double *d_slic
   CF_TRY(check_curvature(ctx));
   CF_TRY(use_device(ctx));
   return density_slices(ctx, d_state, t, d_slice, d_axis_average, (cudaStream_t)stream);
+}
+
+int cf_wkb_create(cf_ctx *ctx, const double *d_state, double t_i, cf_wkb **out, void *stream) {
+  CF_TRY(check_ctx(ctx));
+  CF_TRY(check_ptr(d_state, "d_state"));
+  if (!out || !std::isfinite(t_i) || !(t_i > 0)) {
+    set_error("cf_wkb_create: need out and a finite t_i > 0");
+    return CF_ERR_INVALID;
+  }
+  *out = nullptr;
+  CF_TRY(use_device(ctx));
+  return wkb_create(ctx, d_state, t_i, out, (cudaStream_t)stream);
+}
+
+int cf_wkb_evaluate(cf_wkb *wkb, double t, double *d_out, void *stream) {
+  if (!wkb) {
+    set_error("NULL WKB handle");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(check_ptr(d_out, "d_out"));
+  if (!std::isfinite(t) || !(t > 0)) {
+    set_error("cf_wkb_evaluate: t must be finite and > 0");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(wkb_ctx(wkb)));
+  return wkb_evaluate(wkb, t, d_out, (cudaStream_t)stream);
+}
+
+int cf_wkb_destroy(cf_wkb *wkb) {
+  wkb_destroy(wkb);
+  return CF_OK;
 }
 
 int cf_s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, void *stream) {

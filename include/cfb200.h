@@ -267,6 +267,20 @@ int cf_grf(cf_ctx *ctx, const double *d_white, const double *d_psi, double psi_s
            double *d_out, void *stream);
 int cf_scale_modes(cf_ctx *ctx, const double *d_f, const double *h_scale_s2, double *d_out, void *stream);
 
+/* ---- WKB continuation ------------------------------------------------------------
+ * WKBSolutionForKleinGordonEquationInFRW (src/wkb.hpp:13-27, src/wkb.cpp:5-121): a
+ * KG-FRW state at t_i continued analytically to later times, mode by mode.
+ *   cf_wkb_create: takes the modes of d_state (FP64 [phi | dphi], 2 N^3, device) at t_i
+ *     (the constructor); the context must be CF_EQ_KG_FRW in radiation domination
+ *     (p = 1) with t1 = 1/(2 H1), as the reference asserts, and m > 0.
+ *   cf_wkb_evaluate: the continued state at t into d_out (FP64 2 N^3, device)
+ *     (evaluate_at); returns once the work is done.
+ * The handle keeps the context pointer: destroy it before the context. */
+typedef struct cf_wkb cf_wkb;
+int cf_wkb_create(cf_ctx *ctx, const double *d_state, double t_i, cf_wkb **out, void *stream);
+int cf_wkb_evaluate(cf_wkb *wkb, double t, double *d_out, void *stream);
+int cf_wkb_destroy(cf_wkb *wkb);
+
 /* ---- FFT wrapper ---------------------------------------------------------------
  * The reference's cufftWrapperNoBatching (src/cuda_wrapper.cuh:113-130,
  * src/cuda_wrapper.cu:202-255), used through workspace.fft_wrapper by initializers,

@@ -38,6 +38,9 @@
  *   - ConstIntervalObserver<Equation, field, density, slices>: the save trigger and
  *     the raw FP64 .dat files of src/observer.hpp:64-126.
  *   - compute_power_spectrum / compute_mode_power_spectrum: src/fdm3d_cuda.cuh:22-31.
+ *   - WKBSolutionForKleinGordonEquationInFRW (src/wkb.hpp), the initializers
+ *     perturbed_grf_and_comoving_curvature_fft / unperturbed_grf with RandomNormal
+ *     (src/initializer.hpp, src/random_field.cpp), save_param_for_Mathematica (src/param.hpp).
  *
  * Requirements: C++20, Boost.odeint headers (the reference vendors Boost 1.84),
  * CUDA runtime headers; link libcfb200.so and cudart.
@@ -695,6 +698,44 @@ inline auto unperturbed_grf = [](const auto &param, auto &workspace) {
   check_cuda(cudaMemcpyAsync(workspace.state.f64() + N3, dt_varphi.f64(), N3 * 8, cudaMemcpyDeviceToDevice,
                              ctx->stream()));
   check_cuda(cudaDeviceSynchronize());
+};
+
+/* ---- WKB continuation (src/wkb.hpp:13-27, src/wkb.cpp:5-121) ----------------
+ * Same members and calls as the reference: construct from a workspace whose state is
+ * taken at t_i, then evaluate_at(t) returns the continued FP64 [phi | dphi] on the
+ * device.  Radiation domination with t1 = 1/(2 H1) only, as in the reference. */
+struct WKBSolutionForKleinGordonEquationInFRW {
+  typedef DeviceState Vector;
+  typedef Vector State;
+  typedef WorkspaceGeneric<Vector> Workspace;
+
+  Workspace &workspace;
+  double t_i;
+
+  WKBSolutionForKleinGordonEquationInFRW(Workspace &ws, const double t_i_) : workspace(ws), t_i(t_i_) {
+    if (!ws.ctx) ws.bind(CF_EQ_KG_FRW);
+    const size_t n = 2 * (size_t)ws.ctx->info().field_count;
+    if (ws.state.precision == CF_FP64) {
+      check(cf_wkb_create(ws.ctx->get(), ws.state.f64(), t_i, &h_, ws.ctx->stream()));
+    } else {  // the modes are taken from the FP64 value of an FP32 hi + lo state
+      DeviceState x(n);
+      check(cf_state_export(ws.ctx->get(), x.f64(), ws.state.data(), ws.ctx->stream()));
+      check(cf_wkb_create(ws.ctx->get(), x.f64(), t_i, &h_, ws.ctx->stream()));
+      check_cuda(cudaStreamSynchronize(ws.ctx->stream()));
+    }
+  }
+  ~WKBSolutionForKleinGordonEquationInFRW() { cf_wkb_destroy(h_); }
+  WKBSolutionForKleinGordonEquationInFRW(const WKBSolutionForKleinGordonEquationInFRW &) = delete;
+  WKBSolutionForKleinGordonEquationInFRW &operator=(const WKBSolutionForKleinGordonEquationInFRW &) = delete;
+
+  Vector evaluate_at(const double t) {
+    Vector out(2 * (size_t)workspace.ctx->info().field_count);
+    check(cf_wkb_evaluate(h_, t, out.f64(), workspace.ctx->stream()));
+    return out;
+  }
+
+ private:
+  cf_wkb *h_ = nullptr;
 };
 
 /* ---- raw FP64 file output (src/io.cpp:53-62) ------------------------------- */

@@ -770,3 +770,59 @@ void cfo_driver_initial(int64_t N, double L, uint32_t seed, double *state, doubl
   free(Psi);
   free(r);
 }
+
+/* ---- WKB continuation: WKBSolutionForKleinGordonEquationInFRW, src/wkb.cpp:5-121 ----
+ * Radiation domination with t1 = 1/(2 H1) (the reference asserts both).  Modes of
+ * a^{3/2} phi at t_i, rotated by the phase integral of the effective frequency from
+ * t_i to t_f (the reference's closed form, grouped here by S(t) and U(t)). */
+static double wkb_S(double k2, double a1, double H1, double m, double t) {
+  return sqrt(H1 * (8 * k2 * t + pow(a1, 2) * H1 * (3 + 16 * pow(m, 2) * pow(t, 2))));
+}
+
+double cfo_wkb_phase(double k2, double a1, double H1, double m, double ti, double tf) {
+  const double Sf = wkb_S(k2, a1, H1, m, tf), Si = wkb_S(k2, a1, H1, m, ti);
+  const double Uf = (3 * pow(a1, 2) * H1 + 4 * k2 * tf) / (sqrt(3) * a1 * Sf);
+  const double Ui = (3 * pow(a1, 2) * H1 + 4 * k2 * ti) / (sqrt(3) * a1 * Si);
+  return Sf / (4. * a1 * H1) - Si / (4. * a1 * H1) + (sqrt(3) * log((1 - Uf) / (1 - Ui))) / 8. -
+         (sqrt(3) * log((1 + Uf) / (1 + Ui))) / 8. +
+         (k2 * log((k2 + a1 * m * (4 * a1 * H1 * m * tf + Sf)) / (k2 + a1 * m * (4 * a1 * H1 * m * ti + Si)))) /
+             (4. * pow(a1, 2) * H1 * m);
+}
+
+void cfo_wkb(const cfo_params *P, const double *x, double t_i, double t_f, double *out) {
+  const int64_t N = P->N, N3 = N * N * N, nh = N / 2 + 1, hc = 2 * N * N * nh;
+  const double a1 = P->a1, H1 = P->H1, m = P->m, L = P->L;
+  double *f = (double *)malloc(sizeof(double) * 4 * hc);
+  double *g = f + 2 * hc;
+  cfo_d2z(N, x, f);
+  cfo_d2z(N, x + N3, f + hc);
+  const double ai15 = pow(cfo_a(P, t_i), 1.5), Hi = cfo_H(P, t_i);
+  for (int64_t i = 0; i < hc; ++i) f[i] *= ai15;
+  for (int64_t i = 0; i < hc; ++i) f[hc + i] = ai15 * f[hc + i] + 1.5 * Hi * f[i];
+  for (int64_t a = 0; a < N; ++a)
+    for (int64_t b = 0; b < N; ++b)
+      for (int64_t c = 0; c < nh; ++c) {
+        int64_t as = (a <= N / 2) ? a : (N - a), bs = (b <= N / 2) ? b : (N - b);
+        int64_t s2 = as * as + bs * bs + c * c;
+        double k2 = s2 * pow(2 * CFO_PI / L, 2);
+        int64_t o = 2 * (N * nh * a + nh * b + c);
+        double ph = cfo_wkb_phase(k2, a1, H1, m, t_i, t_f);
+        double w = sqrt(m * m + k2 / (2 * a1 * a1 * H1 * t_i) + 3 / (16 * t_i * t_i));
+        double cv = cos(ph), sv = sin(ph);
+        for (int r = 0; r < 2; ++r) {
+          g[o + r] = f[o + r] * cv + f[hc + o + r] * sv / sqrt(w);
+          g[hc + o + r] = f[hc + o + r] * cv - f[o + r] * sv * sqrt(w);
+        }
+      }
+  fftw_plan pl = fftw_plan_dft_c2r_3d((int)N, (int)N, (int)N, (fftw_complex *)g, out, FFTW_ESTIMATE);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)g, out);
+  fftw_execute_dft_c2r(pl, (fftw_complex *)(g + hc), out + N3);
+  fftw_destroy_plan(pl);
+  const double af15 = pow(cfo_a(P, t_f), 1.5), Hf = cfo_H(P, t_f);
+  for (int64_t i = 0; i < N3; ++i) {
+    double np_ = out[i] / (double)N3, nd = out[N3 + i] / (double)N3;
+    out[i] = np_ / af15;
+    out[N3 + i] = nd / af15 - 1.5 * Hf * np_ / af15;
+  }
+  free(f);
+}

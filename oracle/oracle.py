@@ -95,6 +95,9 @@ def lib():
         L.cfo_sqrtP_table.argtypes = [_i64, _d, _i, _vp, _vp]
         L.cfo_philox4x32_10.argtypes = [_vp, _vp, _vp]
         L.cfo_white_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _i64, _vp]
+        L.cfo_wkb.argtypes = [P, _vp, _d, _d, _vp]
+        L.cfo_wkb_phase.restype = _d
+        L.cfo_wkb_phase.argtypes = [_d, _d, _d, _d, _d, _d]
         L.cfo_ci.restype = _d
         L.cfo_ci.argtypes = [_d]
         _lib = L
@@ -277,6 +280,13 @@ def white_noise(seed, offset, n):
     return out
 
 
+def wkb(P, x, t_i, t_f):
+    """WKBSolutionForKleinGordonEquationInFRW(workspace with state x, t_i).evaluate_at(t_f)."""
+    out = np.empty(2 * P.N ** 3)
+    lib().cfo_wkb(ctypes.byref(P), _ptr(np.ascontiguousarray(x, dtype=np.float64)), t_i, t_f, _ptr(out))
+    return out
+
+
 def grf_white(N, L, white, kind, args, Psi=None, psi_scale=0.0):
     """generate_inhomogeneous_gaussian_random_field from given deviates; kind 0: power
     law with cutoff {P_k_ast, k_ast, alpha}, 1: its derivative spectrum {.., m}, 2: scale
@@ -340,6 +350,15 @@ def ref_energy_density(eq, N, L, m, x, t, a1=1.0, H1=0.0, t1=0.0, R_fft=None, st
     out = np.empty(N ** 3)
     ref(strict).cfr_energy_density(eq, N, L, m, a1, H1, t1, _ptr(np.ascontiguousarray(x)),
                                    _ptr(R_fft) if R_fft is not None else None, t, _ptr(out))
+    return out
+
+
+def ref_wkb(N, L, m, x, t_i, t_f, a1=1.0, H1=0.5, strict=False):
+    """The reference's own WKB continuation (src/wkb.cpp) of state x from t_i to t_f."""
+    R = ref(strict)
+    R.cfr_wkb.argtypes = [ctypes.c_longlong, _d, _d, _d, _d, _d, _vp, _d, _d, _vp]
+    out = np.empty(2 * N ** 3)
+    R.cfr_wkb(N, L, m, a1, H1, 1.0 / (2 * H1), _ptr(np.ascontiguousarray(x)), t_i, t_f, _ptr(out))
     return out
 
 

@@ -3,8 +3,8 @@
  *
  * TEST INFRASTRUCTURE ONLY (oracle).  This file is compiled together with the
  * unmodified reference sources src/equations.cpp, src/fdm3d.cpp,
- * src/fftw_wrapper.cpp, src/random_field.cpp, src/io.cpp, src/eigen_wrapper.cpp
- * (read in place from the reference tree by oracle/Makefile) and the FFTW3
+ * src/fftw_wrapper.cpp, src/random_field.cpp, src/io.cpp, src/eigen_wrapper.cpp,
+ * src/wkb.cpp (read in place from the reference tree by oracle/Makefile) and the FFTW3
  * restatement oracle/fftw_shim.c, into oracle/_ref/libcfref*.so.  Only tests/,
  * the smoke check and bench.py's CPU-baseline / reference legs load it.
  *
@@ -34,6 +34,7 @@
 #include "param.hpp"
 #include "physics.hpp"
 #include "random_field.hpp"
+#include "wkb.hpp"
 #include "workspace.hpp"
 
 namespace {
@@ -279,6 +280,18 @@ void cfr_driver_initial(long long N, double L, unsigned seed, const char *dir, d
   if (R_fft_out) std::memcpy(R_fft_out, workspace.R_fft.data(), sizeof(double) * workspace.R_fft.size());
   ConstIntervalObserver<Equation, true, true, true> observer(d, param, eqn);
   observer(workspace.state, param.t_start);
+}
+
+/* WKBSolutionForKleinGordonEquationInFRW (src/wkb.hpp:13-27, src/wkb.cpp:5-121): the
+ * KG-FRW state x given at t_i, continued to t_f; out = evaluate_at(t_f) (2N^3). */
+void cfr_wkb(long long N, double L, double m, double a1, double H1, double t1, const double *x, double t_i,
+             double t_f, double *out) {
+  HostInit init{x, nullptr, 2 * N * N * N, 2 * N * N * (N / 2 + 1)};
+  FRWParam p{N, L, m, a1, H1, t1, 0, 0, 0};
+  KleinGordonEquationInFRW::Workspace ws(p, init);
+  WKBSolutionForKleinGordonEquationInFRW wkb(ws, t_i);
+  Vec r = wkb.evaluate_at(t_f);
+  std::memcpy(out, r.data(), sizeof(double) * 2 * N * N * N);
 }
 
 }  // extern "C"

@@ -15,6 +15,8 @@
 //   mode 7: CudaFixedCurvatureEquationInFRW with cfb200::fused_rk4, Psi (N^3) from file
 //   mode 8: CudaApproximateComovingCurvatureEquationInFRW (M = N/2) with cfb200::fused_rk4,
 //           R_fft from file
+//   mode 10: cfb200::WKBSolutionForKleinGordonEquationInFRW of in_state at t_start,
+//           evaluated at t_end; writes out_dir/wkb.dat
 //   mode 9: no stepping: the reference driver's initializer run on the device
 //           (cfb200::perturbed_grf_and_comoving_curvature_fft with the driver's parameters,
 //           src/main.cpp:98-122), RandomNormal seeded with <dt> (an integer; noise_seed < 0:
@@ -185,6 +187,16 @@ int main(int argc, char **argv) {
       case 4: {
         FlatParam q{N, L, 1.0, t0, t1, ti};
         return run<cfb200::KleinGordonEquation, StockRK4>(q, x0, R_fft, dt, dir);
+      }
+      case 10: {
+        auto init = [&](const auto &, auto &w) { w.state.copy_from_host(x0.data(), x0.size()); };
+        cfb200::WorkspaceGeneric<cfb200::DeviceState> ws(p, init);
+        cfb200::CudaKleinGordonEquationInFRW eqn(ws);
+        cfb200::WKBSolutionForKleinGordonEquationInFRW wkb(ws, t0);
+        std::vector<double> h;
+        cfb200::copy_vector(h, wkb.evaluate_at(t1));
+        cfb200::write_vector_to_file(h, dir + "wkb.dat");
+        return 0;
       }
       case 5: {
         FullParam q{N, L, 1.0, 0.8, 1.0, 0, 1.0, 0.5, 1.0, t0, t1, ti, CF_FP64, 7};

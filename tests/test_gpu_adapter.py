@@ -129,3 +129,20 @@ def test_adapter_device_initializer_matches_reference_initializer():
         want_state, want_R = O.ref_driver_initial(N, L, seed, d, want_state=True)
     assert np.abs(state - want_state).max() <= 1e-12 * np.abs(want_state).max()
     assert np.abs(R_fft - want_R).max() <= 1e-12 * np.abs(want_R).max()
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="adapter driver not built (needs Boost.odeint headers)")
+def test_adapter_wkb_matches_oracle():
+    """cfb200::WKBSolutionForKleinGordonEquationInFRW(workspace, t_i).evaluate_at(t) (mode 10)."""
+    N, L, ti, tf = 16, 12.8, 3.0, 11.0
+    x = fields.initial_state(N, L, 0.5, 15)
+    x[N ** 3:] = 0.2 * fields.gaussian_field(N, L, 0.5, 16)
+    with tempfile.TemporaryDirectory() as d:
+        xin = os.path.join(d, "x.bin")
+        x.tofile(xin)
+        out = subprocess.run([BIN, "10", str(N), repr(L), "0.1", repr(ti), repr(tf), "1.0", xin, d + "/"],
+                             capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        got = np.fromfile(os.path.join(d, "wkb.dat"))
+    want = O.wkb(O.make_params(N, L, 1.0, eq=1, **FRW), x, ti, tf)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()

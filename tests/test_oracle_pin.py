@@ -270,3 +270,17 @@ def test_cosine_integral_matches_scipy():
     for x in np.concatenate([np.linspace(0.05, 2, 40), np.linspace(2.001, 30, 120), [100.0, 1000.0]]):
         want = sici(x)[1]
         assert abs(L.cfo_ci(x) - want) <= 1e-15 * max(1.0, abs(want)) + 2e-16, x
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("N", [8, 16])
+def test_restatement_matches_reference_wkb(N):
+    """WKBSolutionForKleinGordonEquationInFRW (src/wkb.cpp, compiled in oracle/_ref) against
+    the restatement, both FP64 with the FFTW restatement: <= 1e-13 of the largest value."""
+    from cfb200 import fields
+    L = 0.8 * N
+    x = fields.initial_state(N, L, 0.5, 3)
+    x[N ** 3:] = 0.3 * fields.gaussian_field(N, L, 0.5, 4)
+    P = O.make_params(N, L, 1.0, eq=1, a1=1.0, H1=0.5, t1=1.0)
+    for t_f in (6.0, 40.0):
+        assert _relmax(O.wkb(P, x, 5.0, t_f), O.ref_wkb(N, L, 1.0, x, 5.0, t_f)) <= 1e-13
