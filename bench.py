@@ -41,20 +41,21 @@ WORKLOAD = dict(workload="comoving-curvature KG, radiation FRW, N=512^3, L=512, 
                          "RK4 dt=0.05 from t=1", N=512, L=512.0, m=1.0, dt=0.05, t0=1.0, k_star=0.25,
                 psi_rms=1e-2, k_max=0.5)
 
-# Algorithmic bytes per site and RK4 step of the four fused stage kernels:
-# words moved (state, RK4 accumulator, stage input) per stage 6 + 10 + 10 + 6
-# (FP64) or 6 + 10 + 10 + 12 (FP32-comp, hi + lo state), plus 2 words of
-# Psi, dPsi/dt per stage for the comoving-curvature equation.
-def stage_bytes_per_site(precision, comoving, paired=True):
-    """Algorithmic HBM bytes per site-update of one RK4 step's stage kernels.
-    Paired passes (stages 1+2, 3+4): FP64 6 + 8 words, FP32-comp 6 + 12; four
-    single-stage passes: FP64 32, FP32-comp 38.  Psi, dPsi at four stage times: +8."""
-    if precision == "fp64":
-        words, w = (14 if paired else 32), 8
+# Algorithmic HBM bytes per site and RK4 step, by route.
+def stage_bytes_per_site(precision, comoving, route="step"):
+    """Algorithmic HBM bytes per site-update of one RK4 step.
+    route "step" (one whole-step pass, the 7-point default): the state in and out --
+    FP64 phi, pi (4 words), FP32-comp hi and lo of phi, pi (8 words) -- plus Psi, dPsi
+    at three stage times (+6 words, comoving).  route "pair" (stages 1+2, 3+4; the
+    13-point route): FP64 6 + 8 words, FP32-comp 6 + 12, Psi at four stage times +8.
+    route "stage" (four single-stage passes): FP64 32, FP32-comp 38, +8."""
+    w = 8 if precision == "fp64" else 4
+    if route == "step":
+        words = (4 if precision == "fp64" else 8) + (6 if comoving else 0)
+    elif route == "pair":
+        words = (14 if precision == "fp64" else 18) + (8 if comoving else 0)
     else:
-        words, w = (18 if paired else 38), 4
-    if comoving:
-        words += 8
+        words = (32 if precision == "fp64" else 38) + (8 if comoving else 0)
     return words * w
 
 
@@ -467,12 +468,12 @@ def run_product(args):
     import cfb200
     stage_ms = sum(prof[k][1] for k in cfb200.STEP_KINDS)
     stage_launches = sum(prof[k][0] for k in cfb200.STEP_KINDS)
-    bps = stage_bytes_per_site("fp32comp", True)
+    bps = stage_bytes_per_site("fp32comp", True, "step")
     achieved = bps * N ** 3 * args.steps / (stage_ms * 1e-3) / 1e9
-    # DRAM bytes per site-update of the two passes from an ncu capture at N = 256
+    # DRAM bytes per site-update of the whole-step pass from an ncu capture at N = 256
     # (inputs 10x L2), scaled by the sites a launch processes
-    traffic = traffic_from_profiles("pair_kernels_n256.md")
-    roofline = {"bound": "hbm", "kernel": "k_pair (paired RK4 stages 1+2 and 3+4, FP32-comp, comoving)",
+    traffic = traffic_from_profiles("step_kernel_n256.md")
+    roofline = {"bound": "hbm", "kernel": "k_step (one pass per RK4 step, FP32-comp, comoving, 7-point)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
                 "traffic": (traffic * N ** 3 * args.steps / stage_launches) if traffic else None,
@@ -508,7 +509,7 @@ def run_product(args):
         c2, s2_ = make_case(N, L, prec, stencil, com)
         t2, _, p2 = time_steps(c2, s2_, ks, args.warmup, profile=True)
         sm = sum(p2[k][1] for k in cfb200.STEP_KINDS)
-        bb = stage_bytes_per_site(prec, com)
+        bb = stage_bytes_per_site(prec, com, "step" if stencil == 7 else "pair")
         secondary[name] = {"value": world * N ** 3 * ks / (max_over_ranks(t2, pg) * 1e-3),
                            "ms_per_step": t2 / ks,
                            "stage_kernels_gbs": bb * N ** 3 * ks / (sm * 1e-3) / 1e9}

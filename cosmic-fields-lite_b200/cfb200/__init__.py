@@ -29,6 +29,7 @@ EQ_LAMBDA_FRW, EQ_SQRT_FRW, EQ_FIXED_CURVATURE_FRW, EQ_APPROX_COMOVING_FRW = 3, 
 FP64, FP32_COMP = 0, 1
 FLAG_FULL_PSI_FFT = 1
 FLAG_STAGE_KERNELS = 2
+FLAG_PAIR_KERNELS = 4
 PSI_NONE, PSI_FULL, PSI_PRUNED, PSI_PRUNED_FUSED = 0, 1, 2, 3
 
 
@@ -119,8 +120,8 @@ _SIGS = {
 }
 
 PROF_KINDS = ["stage1", "stage2", "stage3", "stage4", "psi_transfer", "psi_fft", "spectrum", "other", "pair_a",
-              "pair_b"]
-STEP_KINDS = ("stage1", "stage2", "stage3", "stage4", "pair_a", "pair_b")
+              "pair_b", "step"]
+STEP_KINDS = ("stage1", "stage2", "stage3", "stage4", "pair_a", "pair_b", "step")
 
 
 class cf_profile(ctypes.Structure):

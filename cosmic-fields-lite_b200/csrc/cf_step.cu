@@ -1,10 +1,11 @@
 // cf_step.cu -- fused RK4 stage kernels (the hot path), cf_rhs, cf_scale_sum.
 //
 // One RK4 step (stepper/runge_kutta4_classic.hpp:88-138) is four stages.  By
-// default cf_rk4_steps runs them as two paired-stage passes (stages 1+2, 3+4;
-// cf_pair_tile.cuh), which keep the intermediate stage inputs out of HBM; the
-// four single-stage kernels remain for CF_FLAG_STAGE_KERNELS, the adjoint's
-// recompute and the ensembles.  A single-stage kernel makes ONE pass over HBM:
+// default cf_rk4_steps runs a 7-point step as one whole-step pass (k_step,
+// cf_step_tile.cuh) and a 13-point step as two paired-stage passes (stages 1+2,
+// 3+4; cf_pair_tile.cuh); both keep the intermediate stage inputs out of HBM and
+// give the same bits.  The four single-stage kernels remain for
+// CF_FLAG_STAGE_KERNELS, the adjoint's recompute and the persistent ensemble kernel.  A single-stage kernel makes ONE pass over HBM:
 // it streams its stage input y through a 2.5-D blocked stencil and fuses the
 // odeint linear combinations (thrust_operations::scale_sum2 / scale_sum5) into
 // the same pass:
@@ -32,6 +33,7 @@
 #include "cf_internal.cuh"
 #include "cf_pair_tile.cuh"
 #include "cf_stage_tile.cuh"
+#include "cf_step_tile.cuh"
 
 namespace cfb {
 
@@ -335,6 +337,120 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
   return CF_OK;
 }
 
+// ---- whole-step passes (7-point) -------------------------------------------
+// CTA shape per storage type, measured at N = 512 (ms per step, KG-FRW / comoving
+// step kernel): FP32 32 x 8 threads (128 x 8 sites, 2 CTAs/SM) 1.34 / 2.13 against
+// 16 x 16 1.41 / 2.22 and 16 x 8 (3 CTAs/SM) 1.59 / 2.41; FP64 16 x 8 threads (32 x 8
+// sites, 3 CTAs/SM) 1.71 / 3.14 against 32 x 8 1.85 / 3.19 and 16 x 16 1.81 / 3.32.
+template <typename S>
+struct StepShape;
+template <>
+struct StepShape<float> {
+  static constexpr int TX = 32, TY = 8, MB = 2;
+};
+template <>
+struct StepShape<double> {
+  static constexpr int TX = 16, TY = 8, MB = 3;
+};
+
+template <typename S, int EQ, bool FULL>
+__global__ void __launch_bounds__(StepShape<S>::TX *StepShape<S>::TY, StepShape<S>::MB)
+    k_step(const StepArgs<S> A) {
+  extern __shared__ __align__(16) unsigned char step_smem[];
+  constexpr int TXs = StepShape<S>::TX, TYs = StepShape<S>::TY;
+  using SM = StepSmem<S, TXs, TYs>;
+  const int a_begin = blockIdx.z * A.a_chunk;
+  step_tile<S, EQ, TXs, TYs, FULL>(A, blockIdx.x * SM::TW, blockIdx.y * TYs, a_begin,
+                                   min(a_begin + A.a_chunk, A.N), reinterpret_cast<S *>(step_smem));
+}
+
+// Planes per CTA: each chunk re-reads 4 halo planes, so chunks are long where the
+// grid stays several waves deep.
+static int step_a_chunk(int N, int tiles_xy) {
+  int chunk = 64;
+  while (chunk > 4 && (long long)tiles_xy * ((N + chunk - 1) / chunk) < 148LL * 6) chunk /= 2;
+  return chunk;
+}
+
+template <typename S, int EQ, bool FULL>
+static int launch_step_k(cf_ctx *ctx, const StepArgs<S> &A, dim3 grid, cudaStream_t st) {
+  using SM = StepSmem<S, StepShape<S>::TX, StepShape<S>::TY>;
+  constexpr size_t bytes = (size_t)SM::count * sizeof(S);
+  static unsigned long long attr_set = 0;  // devices on which this instantiation may use > 48 KB
+  const unsigned long long bit = 1ull << (ctx->device & 63);
+  if (!(attr_set & bit)) {
+    CF_TRY_CUDA(cudaFuncSetAttribute(k_step<S, EQ, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    attr_set |= bit;
+  }
+  k_step<S, EQ, FULL><<<grid, dim3(StepShape<S>::TX, StepShape<S>::TY), bytes, st>>>(A);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+template <typename S, int EQ>
+static int launch_step_t(cf_ctx *ctx, const StepArgs<S> &A0, cudaStream_t st) {
+  using SM = StepSmem<S, StepShape<S>::TX, StepShape<S>::TY>;
+  constexpr int TYs = StepShape<S>::TY;
+  StepArgs<S> A = A0;
+  unsigned gx = ceil_div(A.N, SM::TW), gy = ceil_div(A.N, TYs);
+  A.a_chunk = step_a_chunk(A.N, (int)(gx * gy));
+  dim3 grid(gx, gy, ceil_div(A.N, A.a_chunk));
+  ProfScope ps(ctx, CF_PROF_STEP, st);
+  if (A.N % SM::TW == 0 && A.N % TYs == 0) return launch_step_k<S, EQ, true>(ctx, A, grid, st);
+  return launch_step_k<S, EQ, false>(ctx, A, grid, st);
+}
+
+template <typename S>
+static int launch_step(cf_ctx *ctx, const StepArgs<S> &A, cudaStream_t st) {
+  switch (shape_of(ctx->p.equation)) {
+    case EQ_COMOV: return launch_step_t<S, EQ_COMOV>(ctx, A, st);
+    case EQ_LAMBDA: return launch_step_t<S, EQ_LAMBDA>(ctx, A, st);
+    case EQ_SQRT: return launch_step_t<S, EQ_SQRT>(ctx, A, st);
+    case EQ_FIXED: return launch_step_t<S, EQ_FIXED>(ctx, A, st);
+    case EQ_APPROX: return launch_step_t<S, EQ_APPROX>(ctx, A, st);
+    default: return launch_step_t<S, EQ_FRW>(ctx, A, st);
+  }
+}
+
+// nsteps RK4 steps as whole-step passes.  The new phi and pi alternate between the
+// state's planes and the ya scratch; after an odd number of steps they are copied back.
+template <typename S>
+static int rk4_steps_fused_t(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
+                             cudaStream_t st) {
+  CF_TRY(ensure_rk4_scratch(ctx));
+  const long long N3 = ctx->N3;
+  S *x = (S *)d_state;
+  S *buf[2] = {x, (S *)ctx->ya};
+  int cur = 0;
+  StepArgs<S> A{};
+  A.N = (int)ctx->N;
+  A.N3 = N3;
+  A.m2 = ctx->p.m * ctx->p.m;
+  eq_consts(ctx, &A.q1, &A.q2, &A.cmap, &A.M);
+  A.xlo = (sizeof(S) == 4) ? x + 2 * N3 : nullptr;
+  A.dt2 = dt / 2.0;
+  A.dt = dt;
+  A.dt6 = dt / 6.0;
+  for (int64_t j = 0; j < nsteps; ++j) {
+    const double t = t0 + (double)(step0 + j) * dt;
+    const double ts[3] = {t, t + dt / 2.0, t + dt};
+    for (int k = 0; k < 3; ++k) {
+      double H;
+      stage_coeffs(ctx->p, ts[k], &A.inv[k], &H);
+      A.hub3[k] = 3.0 * H;
+      CF_TRY(curvature_at<S>(ctx, ts[k], &A.psi[k], &A.dpsi[k], st));
+    }
+    A.xphi = buf[cur];
+    A.xpi = buf[cur] + N3;
+    A.ophi = buf[cur ^ 1];
+    A.opi = buf[cur ^ 1] + N3;
+    CF_TRY(launch_step<S>(ctx, A, st));
+    cur ^= 1;
+  }
+  if (cur) CF_TRY_CUDA(cudaMemcpyAsync(x, buf[1], 2 * N3 * sizeof(S), cudaMemcpyDeviceToDevice, st));
+  return CF_OK;
+}
+
 template <typename S>
 static int fill_stage_coeffs(cf_ctx *ctx, StageArgs<S> &A, double t, cudaStream_t st) {
   double inv, H;
@@ -467,12 +583,16 @@ int rk4_step_buffers(cf_ctx *ctx, void *d_state, void *acc, void *ya, void *yb, 
 }
 
 int rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, cudaStream_t st) {
-  const bool single = (ctx->p.flags & CF_FLAG_STAGE_KERNELS) != 0;
-  if (ctx->p.precision == CF_FP32_COMP)
-    return single ? rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
-                  : rk4_steps_pairs_t<float>(ctx, d_state, t0, dt, step0, nsteps, st);
-  return single ? rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st)
-                : rk4_steps_pairs_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
+  const int f = ctx->p.flags;
+  const bool f32 = ctx->p.precision == CF_FP32_COMP;
+  if (f & CF_FLAG_STAGE_KERNELS)
+    return f32 ? rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
+               : rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
+  if ((f & CF_FLAG_PAIR_KERNELS) || ctx->p.stencil != 7)
+    return f32 ? rk4_steps_pairs_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
+               : rk4_steps_pairs_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
+  return f32 ? rk4_steps_fused_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
+             : rk4_steps_fused_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
 }
 
 int rhs(cf_ctx *ctx, const double *d_x, double *d_dxdt, double t, cudaStream_t st) {

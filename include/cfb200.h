@@ -104,9 +104,13 @@ typedef struct cf_params {
  * band-limited (the pruned synthesis is used by default when R_fft is exactly
  * zero outside a small box of modes; both give the same fields to rounding). */
 #define CF_FLAG_FULL_PSI_FFT 1
-/* cf_rk4_steps runs each step as four single-stage passes instead of two
- * paired-stage passes (stages 1+2, 3+4); both give bit-identical states. */
+/* cf_rk4_steps runs each step as four single-stage passes instead of the default
+ * route; every route gives bit-identical states. */
 #define CF_FLAG_STAGE_KERNELS 2
+/* cf_rk4_steps runs each 7-point step as two paired-stage passes (stages 1+2, 3+4)
+ * instead of one whole-step pass (the default for the 7-point stencil; the 13-point
+ * stencil always takes the paired passes). */
+#define CF_FLAG_PAIR_KERNELS 4
 
 typedef struct cf_ctx cf_ctx;
 
@@ -172,7 +176,7 @@ int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream);
  * stage times t, t+dt/2, t+dt/2, t+dt (stepper/runge_kutta4_classic.hpp:88-138).
  * Replaces 4 x Equation::operator() + 3 x scale_sum2 + scale_sum5 per step
  * (src/equations_cuda.cu:522-534, :678-731; src/odeint_thrust/thrust_operations.cu:238-313)
- * by four fused stage kernels, one HBM pass each. */
+ * by one HBM pass per step (7-point stencil) or two (13-point); see CF_FLAG_*. */
 int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
                  void *stream);
 
@@ -398,7 +402,8 @@ typedef enum cf_prof_kind {
   CF_PROF_OTHER = 7,
   CF_PROF_PAIR_A = 8,       /* paired-stage passes: stages 1+2, stages 3+4 */
   CF_PROF_PAIR_B = 9,
-  CF_PROF_KINDS = 10
+  CF_PROF_STEP = 10,        /* whole-step pass (all four stages) */
+  CF_PROF_KINDS = 11
 } cf_prof_kind;
 
 typedef struct cf_profile {

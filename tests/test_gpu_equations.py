@@ -235,3 +235,32 @@ def test_dot_energy_density_matches_reference_gpu():
     out = torch.empty(lat["N"] ** 3, dtype=torch.float64, device="cuda")
     c.dot_energy_density(dev(G.state(lat["N"])), G.T, out)
     assert relmax(out.cpu().numpy(), g) <= 1e-12
+
+
+@pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
+@pytest.mark.parametrize("N,nsteps", [(64, 3), (40, 2), (16, 3), (8, 1)])
+@pytest.mark.parametrize("eq", [0, 1, 2, 3, 4, 5, 6])
+def test_whole_step_pass_equals_paired_passes_bitwise(eq, N, nsteps, prec):
+    """The default 7-point route (one whole-step pass per RK4 step) against the paired
+    passes (CF_FLAG_PAIR_KERNELS): bit-identical states for every equation, storage
+    type, full (N = 64) and ragged (N = 40) tiles, lattices smaller than a tile and odd
+    and even step counts."""
+    L = 0.9 * N
+    out = []
+    for flags in (0, cfb200.FLAG_PAIR_KERNELS):
+        if eq in EQS:
+            c, x, _, _, _ = setup(N, L, eq, prec=prec, flags=flags, seed=23, M=8)
+        else:
+            x = fields.initial_state(N, L, 0.5, 23)
+            x[N ** 3:] = 0.3 * fields.gaussian_field(N, L, 0.5, 24)
+            c = cfb200.Context(N, L, m=1.0, equation=eq, precision=prec, flags=flags, **(FRW if eq else {}))
+            if eq == 2:
+                c.set_R_fft(fields.curvature_R_fft(N, L, 2.0, 1e-2, 2 * np.pi / L * 3, seed=25), on_device=False)
+        st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+        c.upload(st, x)
+        c.rk4_steps(st, 1.0, 0.07, nsteps)
+        got = np.empty_like(x)
+        c.download(got, st)
+        torch.cuda.synchronize()
+        out.append(got)
+    assert np.array_equal(out[0], out[1])
