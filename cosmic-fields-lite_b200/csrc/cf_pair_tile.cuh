@@ -100,7 +100,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
   using T = typename Arith<S>::T;
   const StageCoef<T> k1c{Coef<T>(A.m2), Coef<T>(A.inv1), Coef<T>(A.hub3_1), Coef<T>(A.q1), Coef<T>(A.q2)};
   const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(A.inv2), Coef<T>(A.hub3_2), Coef<T>(A.q1), Coef<T>(A.q2)};
-  const Coef<T> cw(A.cw), cy(A.cy);
+  const Coef<T> cw(A.cw), cy(A.cy), c6(A.dt6);
   const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
 
   auto load_w = [&](long long off) -> Pack<S, V> {
@@ -116,7 +116,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
   if (act) {
 #pragma unroll
     for (int j = 0; j < 2 * H; ++j) {
-      const long long off = NN * ((a_begin - H + j + N) % N) + rowoff;
+      const long long off = NN * wrap_n(a_begin - H + j, N) + rowoff;
       qu[j + 1] = ldv<S, V>(uphi + off);
       qw[j + 1] = load_w(off);
     }
@@ -129,10 +129,10 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
       qu[j] = qu[j + 1];
       qw[j] = qw[j + 1];
     }
-    Pack<S, V> p0v, xp, xq, cp, cq, lp, lq;
+    Pack<S, V> p0v, xp, xq, cp, cq, lp{}, lq{};
     Coupling<S, V> cpl1, cpl2;
     if (act) {
-      const long long head = NN * ((a + H) % N) + rowoff;
+      const long long head = NN * wrap_n(a + H, N) + rowoff;
       qu[2 * H] = ldv<S, V>(uphi + head);
       qw[2 * H] = load_w(head);
       p0v = ldv<S, V>(upi + site);
@@ -177,7 +177,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
         if (pass == 0 && (ty < H || ty >= tye - H)) r = (ty < H) ? ty : ty + 2 * H;
         if (pass == 1 && ty < H && ty >= tye - H) r = ty + 2 * H;
         if (r >= 0) {
-          const int gb = (b0 - H + r + N) % N;
+          const int gb = wrap_n(b0 - H + r, N);
           const long long off = NN * a + (long long)N * gb + c;
           const Pack<S, V> hu = ldv<S, V>(uphi + off);
           const Pack<S, V> hw = load_w(off);
@@ -193,14 +193,14 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
     for (int i = tid; i < sre * 2 * H; i += TXv * TYv) {
       const int r = i / (2 * H);
       const int j = i % (2 * H);
-      const int gb = (b0 - H + r + N) % N;
+      const int gb = wrap_n(b0 - H + r, N);
       int col, gc;
       if (j < H) {
         col = j;
-        gc = (c0 - H + j + N) % N;
+        gc = wrap_n(c0 - H + j, N);
       } else {
         col = twe + H + (j - H);
-        gc = (c0 + twe + (j - H)) % N;
+        gc = wrap_n(c0 + twe + (j - H), N);
       }
       const long long off = NN * a + (long long)N * gb + gc;
       smu[r * SP + col] = uphi[off];
@@ -242,20 +242,9 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
         o3.v[v] = (S)cy.fma(p1, f0);  // yb = x + dt/2 k2  (x = u in pass A)
         o4.v[v] = (S)cy.fma(k2pi, p0);
       } else {
-        const double ip = A.dt6 * (double)((T)c1phi + p1);  // x += dt/6 (acc + k4)
-        const double iq = A.dt6 * (double)((T)c1pi + k2pi);
-        if constexpr (sizeof(S) == 8) {
-          o1.v[v] = (S)((double)xp.v[v] + ip);
-          o2.v[v] = (S)((double)xq.v[v] + iq);
-        } else {
-          const double np = ((double)xp.v[v] + (double)lp.v[v]) + ip;
-          const double nq = ((double)xq.v[v] + (double)lq.v[v]) + iq;
-          const float hp = (float)np, hq = (float)nq;
-          o1.v[v] = hp;
-          o2.v[v] = hq;
-          o3.v[v] = (float)(np - (double)hp);
-          o4.v[v] = (float)(nq - (double)hq);
-        }
+        // x += dt/6 (acc + k4)
+        state_update(xp.v[v], lp.v[v], (T)c1phi + p1, c6, o1.v[v], o3.v[v]);
+        state_update(xq.v[v], lq.v[v], (T)c1pi + k2pi, c6, o2.v[v], o4.v[v]);
       }
     }
     if constexpr (PASS == 1) {

@@ -115,13 +115,18 @@ struct StageArgs {
   double dt6;   // dt / 6
 };
 
+// Periodic index for i in [-N, 2N): two compares instead of an integer division by
+// N.  Every wrapped index of the tile kernels lies within H <= 2 sites of the
+// lattice (halo rows and columns of an active tile, planes a - H .. a + H).
+__device__ __forceinline__ int wrap_n(int i, int N) { return i < 0 ? i + N : (i >= N ? i - N : i); }
+
 // Arithmetic type of the stage evaluations: FP64 for FP64 storage; FP32 for
 // FP32_COMP, whose stage inputs and accumulator are FP32 words anyway.  In FP32
 // every rounding must be unbiased, or it acts like a changed time step or mass
 // and the error grows with time: coefficients (dt/2, dt/6, h^-2 a^-2, 3H, m^2)
 // enter as hi + lo pairs, e^{2 Psi} as 1 + expm1f (never rounded as 1 + eps),
-// and the state update x += dt/6 (acc + k4) is formed in FP64 and kept as the
-// hi + lo pair.
+// and the state update x += dt/6 (acc + k4) is formed without rounding error on
+// the hi + lo pair (comp_update).
 template <typename S>
 struct Arith {
   using T = S;
@@ -146,6 +151,32 @@ struct Coef<float> {
   // add + c v
   __device__ __forceinline__ float fma(float v, float add) const { return add + fmaf(hi, v, lo * v); }
 };
+
+// FP32_COMP state update hi + lo + c s as a normalised hi + lo pair, in FP32 alone:
+// the product c s exactly as p + pe (FMA), hi + p exactly as t + e (TwoSum, Knuth),
+// the small parts added, and the pair renormalised (Fast2Sum, |t| >= |e|).  The
+// explicit round-to-nearest intrinsics keep the compiler from contracting or
+// reassociating the error terms.
+__device__ __forceinline__ void comp_update(float hi, float lo, float s, const Coef<float> &c, float &oh,
+                                            float &ol) {
+  const float p = __fmul_rn(c.hi, s);
+  const float pe = __fmaf_rn(c.lo, s, __fmaf_rn(c.hi, s, -p));
+  const float t = __fadd_rn(hi, p);
+  const float z = __fsub_rn(t, hi);
+  const float e = __fadd_rn(__fadd_rn(__fsub_rn(hi, __fsub_rn(t, z)), __fsub_rn(p, z)), __fadd_rn(lo, pe));
+  oh = __fadd_rn(t, e);
+  ol = __fsub_rn(e, __fsub_rn(oh, t));
+}
+
+// x += dt/6 s (RK4's last combination): FP64 directly; FP32_COMP on the hi + lo pair.
+__device__ __forceinline__ void state_update(double x, double, double s, const Coef<double> &c6, double &ox,
+                                             double &) {
+  ox = x + c6.hi * s;
+}
+__device__ __forceinline__ void state_update(float hi, float lo, float s, const Coef<float> &c6, float &oh,
+                                             float &ol) {
+  comp_update(hi, lo, s, c6, oh, ol);
+}
 
 // e^{2 Psi} and e^{4 Psi} from the Psi slot's e^{2 Psi} - 1 (FP64).
 __device__ __forceinline__ void psi_factors(double e2m1, double &e2, double &e4) {
@@ -350,23 +381,23 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
   const S *pi_in = A.yin + N3;
   using T = typename Arith<S>::T;
   const StageCoef<T> kc{Coef<T>(A.m2), Coef<T>(A.inv), Coef<T>(A.hub3), Coef<T>(A.q1), Coef<T>(A.q2)};
-  const Coef<T> cy(A.cy);
+  const Coef<T> cy(A.cy), c6(A.dt6);
   const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
 
   Pack<S> q[2 * H + 1];
   if (act) {
 #pragma unroll
-    for (int j = 0; j < 2 * H; ++j) q[j + 1] = ldv(phi_in + NN * ((a_begin - H + j + N) % N) + rowoff);
+    for (int j = 0; j < 2 * H; ++j) q[j + 1] = ldv(phi_in + NN * wrap_n(a_begin - H + j, N) + rowoff);
   }
 
   for (int a = a_begin; a < a_end; ++a) {
     const long long site = NN * a + rowoff;
 #pragma unroll
     for (int j = 0; j < 2 * H; ++j) q[j] = q[j + 1];
-    Pack<S> pi0, xp, xq, cp, cq, lp, lq;
+    Pack<S> pi0, xp, xq, cp, cq, lp{}, lq{};
     Coupling<S, V> cpl;
     if (act) {
-      q[2 * H] = ldv(phi_in + NN * ((a + H) % N) + rowoff);
+      q[2 * H] = ldv(phi_in + NN * wrap_n(a + H, N) + rowoff);
       pi0 = ldv(pi_in + site);
       if constexpr (STAGE == 2 || STAGE == 3 || STAGE == 4) {
         xp = ldv_rw(A.x + site);
@@ -393,7 +424,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
       // halo rows: H above the tile and H below its active height, interior columns
       if (ty < H || ty >= tye - H) {
         const int r = (ty < H) ? ty : ty + 2 * H;
-        const int gb = (b0 - H + r + N) % N;
+        const int gb = wrap_n(b0 - H + r, N);
         const Pack<S> h = ldv(phi_in + NN * a + (long long)N * gb + c);
 #pragma unroll
         for (int v = 0; v < V; ++v) sm[r * SP + H + tx * V + v] = h.v[v];
@@ -401,7 +432,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
       // (a thread that is both in the top and the bottom band, tye < 2H, writes its bottom row below)
       if (ty < H && ty >= tye - H) {
         const int r = ty + 2 * H;
-        const int gb = (b0 - H + r + N) % N;
+        const int gb = wrap_n(b0 - H + r, N);
         const Pack<S> h = ldv(phi_in + NN * a + (long long)N * gb + c);
 #pragma unroll
         for (int v = 0; v < V; ++v) sm[r * SP + H + tx * V + v] = h.v[v];
@@ -411,14 +442,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
     for (int i = tid; i < sre * 2 * H; i += TXv * TYv) {
       const int r = i / (2 * H);
       const int j = i % (2 * H);
-      const int gb = (b0 - H + r + N) % N;
+      const int gb = wrap_n(b0 - H + r, N);
       int col, gc;
       if (j < H) {
         col = j;
-        gc = (c0 - H + j + N) % N;
+        gc = wrap_n(c0 - H + j, N);
       } else {
         col = twe + H + (j - H);
-        gc = (c0 + twe + (j - H)) % N;
+        gc = wrap_n(c0 + twe + (j - H), N);
       }
       sm[r * SP + col] = phi_in[NN * a + (long long)N * gb + gc];
     }
@@ -449,20 +480,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
         o_phi.v[v] = (S)cy.fma(kphi, (T)xp.v[v]);
         o_pi.v[v] = (S)cy.fma(kpi, (T)xq.v[v]);
       } else {  // STAGE 4
-        const double ip = A.dt6 * (double)((T)cp.v[v] + kphi);
-        const double iq = A.dt6 * (double)((T)cq.v[v] + kpi);
-        if constexpr (sizeof(S) == 8) {
-          xp.v[v] = (S)((double)xp.v[v] + ip);
-          xq.v[v] = (S)((double)xq.v[v] + iq);
-        } else {
-          const double np = ((double)xp.v[v] + (double)lp.v[v]) + ip;
-          const double nq = ((double)xq.v[v] + (double)lq.v[v]) + iq;
-          const float hp = (float)np, hq = (float)nq;
-          xp.v[v] = hp;
-          xq.v[v] = hq;
-          lp.v[v] = (float)(np - (double)hp);
-          lq.v[v] = (float)(nq - (double)hq);
-        }
+        state_update(xp.v[v], lp.v[v], (T)cp.v[v] + kphi, c6, xp.v[v], lp.v[v]);
+        state_update(xq.v[v], lq.v[v], (T)cq.v[v] + kpi, c6, xq.v[v], lq.v[v]);
       }
     }
     if constexpr (STAGE == 0) {

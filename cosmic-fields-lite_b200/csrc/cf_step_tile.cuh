@@ -184,6 +184,7 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
   const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(A.inv[1]), Coef<T>(A.hub3[1]), Coef<T>(A.q1), Coef<T>(A.q2)};
   const StageCoef<T> k4c{Coef<T>(A.m2), Coef<T>(A.inv[2]), Coef<T>(A.hub3[2]), Coef<T>(A.q1), Coef<T>(A.q2)};
   const Coef<T> ch(A.dt2), cf(A.dt);
+  const Coef<T> c6(A.dt6);
   const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
   auto s4 = [&](int p) { return (p - a_begin + 4) & 3; };
   auto s3 = [&](int p) { return (p - a_begin + 3) % 3; };
@@ -194,7 +195,7 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
 
   // copies of plane p (x_phi, x_pi; tile and 2-ring) into slot s4(p)
   auto issue = [&](int p) {
-    const long long poff = NN * ((p % N + N) % N);
+    const long long poff = NN * wrap_n(p, N);
     S *xf = XF + s4(p) * SM::P2, *xp = XP + s4(p) * SM::P2;
     if (act) {
       cp_async_16(xf + own2, A.xphi + poff + rowoff);
@@ -202,15 +203,15 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     }
     if (ty < 4 && colact) {  // ring rows: 2 above the tile, 2 below its active height
       const int r2 = ty < 2 ? ty : tye + ty;
-      const long long off = poff + (long long)N * ((b0 - 2 + r2 + 2 * N) % N) + c;
+      const long long off = poff + (long long)N * wrap_n(b0 - 2 + r2, N) + c;
       cp_async_16(xf + r2 * SP + O + tx * V, A.xphi + off);
       cp_async_16(xp + r2 * SP + O + tx * V, A.xpi + off);
     }
     for (int i = NT - 1 - tid; i < (tye + 4) * 2; i += NT) {  // ring columns (the last warps): pairs
       const int r2 = i >> 1, side = i & 1;
-      const int gc = side ? (c0 + twe) % N : (c0 - 2 + N) % N;
+      const int gc = wrap_n(side ? c0 + twe : c0 - 2, N);
       const int col = side ? O + twe : O - 2;
-      const long long off = poff + (long long)N * ((b0 - 2 + r2 + 2 * N) % N) + gc;
+      const long long off = poff + (long long)N * wrap_n(b0 - 2 + r2, N) + gc;
       if constexpr (sizeof(S) == 8) {
         cp_async_16(xf + r2 * SP + col, A.xphi + off);
         cp_async_16(xp + r2 * SP + col, A.xpi + off);
@@ -245,6 +246,36 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     }
   };
 
+  // Stages 1-2 at one ring site (r1, col) of the 1-ring plane q (col in the row's
+  // shared-memory coordinates): writes its yb_phi, yc_phi
+  auto ring_site = [&](int q, int qm, long long qoff, S *yb, S *yc, int r1, int col) {
+    const int o2 = (r1 + 1) * SP + col;
+    const int gb = wrap_n(b0 - 1 + r1, N), gc = wrap_n(c0 + col - O, N);
+    const long long site = qoff + (long long)N * gb + gc;
+    Coupling<S, 1> ct, ch2;
+    if constexpr (EqOf<EQ>::coupled) {
+      coupling_at<EQ, S>(ct, A.psi[0], A.dpsi[0], site, A.cmap, A.M, qm, gb, gc);
+      if constexpr (EQ == EQ_FIXED)
+        ch2 = ct;
+      else
+        coupling_at<EQ, S>(ch2, A.psi[1], A.dpsi[1], site, A.cmap, A.M, qm, gb, gc);
+    }
+    const S *f0p = XF + s4(q) * SM::P2, *fmp = XF + s4(q - 1) * SM::P2, *fpp = XF + s4(q + 1) * SM::P2;
+    const S *x0p = XP + s4(q) * SM::P2, *xmp = XP + s4(q - 1) * SM::P2, *xpp = XP + s4(q + 1) * SM::P2;
+    const Star<T> fs{(T)f0p[o2], (T)fpp[o2], (T)fmp[o2], (T)f0p[o2 + SP], (T)f0p[o2 - SP], (T)f0p[o2 + 1],
+                     (T)f0p[o2 - 1]};
+    const Star<T> ps{(T)x0p[o2], (T)xpp[o2], (T)xmp[o2], (T)x0p[o2 + SP], (T)x0p[o2 - SP], (T)x0p[o2 + 1],
+                     (T)x0p[o2 - 1]};
+    const T f0 = fs.f0, p0 = ps.f0;
+    const T k1 = kpi_of<EQ, S, 1>(p0, f0, lap_of(fs), ct, 0, k1c);
+    const S yapi = (S)ch.fma(k1, p0);
+    const Star<T> ya = ya_star<S, T>(fs, ps, ch);
+    const T k2 = kpi_of<EQ, S, 1>((T)yapi, ya.f0, lap_of(ya), ch2, 0, k2c);
+    const S bpi = (S)ch.fma(k2, p0);
+    yb[r1 * SP + col] = (S)ch.fma((T)yapi, f0);
+    yc[r1 * SP + col] = (S)cf.fma((T)bpi, f0);
+  };
+
   issue(a_begin - 2);
   cp_async_commit();
   for (int p = a_begin - 2; p <= a_end + 1; ++p) {
@@ -256,7 +287,7 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     // ---- phase 1 on plane q = p - 1: the tile and its 1-ring
     const int q = p - 1;
     if (q >= a_begin - 1) {
-      const int qm = (q % N + N) % N;
+      const int qm = wrap_n(q, N);
       const long long qoff = NN * qm;
       S *yb = YB + s3(q) * SM::P1, *yc = YC + s3(q) * SM::P1;
       if (act) {  // own sites
@@ -280,7 +311,7 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
       }
       if (ty < 2 && colact) {  // ring rows of the 1-ring plane: b0 - 1 and b0 + tye
         const int r1 = ty == 0 ? 0 : tye + 1;
-        const int gb = (b0 - 1 + r1 + 2 * N) % N;
+        const int gb = wrap_n(b0 - 1 + r1, N);
         const long long site = qoff + (long long)N * gb + c;
         Coupling<S, V> ct, ch2;
         if constexpr (EqOf<EQ>::coupled) {
@@ -304,34 +335,8 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
       }
       // ring columns of the 1-ring plane (corners included): scalars, on the last warps
       // (the first warp takes the ring rows)
-      for (int i = NT - 1 - tid; i < (tye + 2) * 2; i += NT) {
-        const int r1 = i >> 1, col = (i & 1) ? O + twe : O - 1;
-        const int o2 = (r1 + 1) * SP + col;
-        const int gb = (b0 - 1 + r1 + 2 * N) % N, gc = (i & 1) ? (c0 + twe) % N : (c0 - 1 + N) % N;
-        const long long site = qoff + (long long)N * gb + gc;
-        Coupling<S, 1> ct, ch2;
-        if constexpr (EqOf<EQ>::coupled) {
-          coupling_at<EQ, S>(ct, A.psi[0], A.dpsi[0], site, A.cmap, A.M, qm, gb, gc);
-          if constexpr (EQ == EQ_FIXED)
-            ch2 = ct;
-          else
-            coupling_at<EQ, S>(ch2, A.psi[1], A.dpsi[1], site, A.cmap, A.M, qm, gb, gc);
-        }
-        const S *f0p = XF + s4(q) * SM::P2, *fmp = XF + s4(q - 1) * SM::P2, *fpp = XF + s4(q + 1) * SM::P2;
-        const S *x0p = XP + s4(q) * SM::P2, *xmp = XP + s4(q - 1) * SM::P2, *xpp = XP + s4(q + 1) * SM::P2;
-        const Star<T> fs{(T)f0p[o2], (T)fpp[o2], (T)fmp[o2], (T)f0p[o2 + SP], (T)f0p[o2 - SP], (T)f0p[o2 + 1],
-                         (T)f0p[o2 - 1]};
-        const Star<T> ps{(T)x0p[o2], (T)xpp[o2], (T)xmp[o2], (T)x0p[o2 + SP], (T)x0p[o2 - SP], (T)x0p[o2 + 1],
-                         (T)x0p[o2 - 1]};
-        const T f0 = fs.f0, p0 = ps.f0;
-        const T k1 = kpi_of<EQ, S, 1>(p0, f0, lap_of(fs), ct, 0, k1c);
-        const S yapi = (S)ch.fma(k1, p0);
-        const Star<T> ya = ya_star<S, T>(fs, ps, ch);
-        const T k2 = kpi_of<EQ, S, 1>((T)yapi, ya.f0, lap_of(ya), ch2, 0, k2c);
-        const S bpi = (S)ch.fma(k2, p0);
-        yb[r1 * SP + col] = (S)ch.fma((T)yapi, f0);
-        yc[r1 * SP + col] = (S)cf.fma((T)bpi, f0);
-      }
+      for (int i = NT - 1 - tid; i < (tye + 2) * 2; i += NT)
+        ring_site(q, qm, qoff, yb, yc, i >> 1, (i & 1) ? O + twe : O - 1);
     }
     __syncthreads();  // yb_phi, yc_phi of plane q ready
 
@@ -340,7 +345,7 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     // issued after this); DL entries are written and read by the owning thread only.
     const int r = p - 2;
     if (r >= a_begin && act) {
-      const int rm = (r % N + N) % N;
+      const int rm = wrap_n(r, N);
       const long long roff = NN * rm;
       Coupling<S, V> cth, cd;
       if constexpr (EqOf<EQ>::coupled) {
@@ -357,7 +362,8 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
       RowStar<S, V, SP> B, C;
       B.load(YB + s3(r) * SM::P1, YB + s3(r - 1) * SM::P1, YB + s3(r + 1) * SM::P1, own1);
       C.load(YC + s3(r) * SM::P1, YC + s3(r - 1) * SM::P1, YC + s3(r + 1) * SM::P1, own1);
-      Pack<S, V> lp, lq, o1, o2, o3, o4;
+      Pack<S, V> o1, o2, o3, o4;
+      Pack<S, V> lp{}, lq{};
       if constexpr (sizeof(S) == 4) {
         lp = ldv_rw<S, V>(A.xlo + roff + rowoff);
         lq = ldv_rw<S, V>(A.xlo + N3 + roff + rowoff);
@@ -372,20 +378,8 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
         const S ycpi = (S)cf.fma(k3, (T)xpi.v[v]);
         const Star<T> cs = C.template at<T>(v);
         const T k4 = kpi_of<EQ, S, V>((T)ycpi, cs.f0, lap_of(cs), cd, v, k4c);
-        const double ip = A.dt6 * (double)((T)c1phi + (T)ycpi);
-        const double iq = A.dt6 * (double)((T)c1pi + k4);
-        if constexpr (sizeof(S) == 8) {
-          o1.v[v] = (S)((double)xphi.v[v] + ip);
-          o2.v[v] = (S)((double)xpi.v[v] + iq);
-        } else {
-          const double np = ((double)xphi.v[v] + (double)lp.v[v]) + ip;
-          const double nq = ((double)xpi.v[v] + (double)lq.v[v]) + iq;
-          const float hp = (float)np, hq = (float)nq;
-          o1.v[v] = hp;
-          o2.v[v] = hq;
-          o3.v[v] = (float)(np - (double)hp);
-          o4.v[v] = (float)(nq - (double)hq);
-        }
+        state_update(xphi.v[v], lp.v[v], (T)c1phi + (T)ycpi, c6, o1.v[v], o3.v[v]);
+        state_update(xpi.v[v], lq.v[v], (T)c1pi + k4, c6, o2.v[v], o4.v[v]);
       }
       stv(A.ophi + roff + rowoff, o1);
       stv(A.opi + roff + rowoff, o2);
