@@ -104,6 +104,10 @@ struct cf_ctx {
   bool pc_fused = false;
   void *pr_wN = nullptr;
   void *pr_twM = nullptr;  // pass-1 twiddles e^{2 pi i k2 m1 / (N/2)}, [m1][k2]
+  // Pass B as one kernel (FP32, power-of-two N, 32..1024): its four-step twiddles
+  // e^{2 pi i k2 m1 / N}, [m1][k2]; no plan_pb then.
+  bool pb_fused = false;
+  void *pr_twB = nullptr;
 
   // Fixed curvature: e^{2 Psi(x)} - 1 of cf_set_psi, N^3 of the storage type.
   void *fixed_e2m1 = nullptr;

@@ -402,6 +402,144 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
   }
 }
 
+// ---- pass B as one kernel: pruned lines -> full lines -----------------------
+// For FP32 storage and power-of-two N (32..1024) the C2C of pass B reads the
+// pass-A lines at their 2Kb+1 non-zero b-frequencies only (pz_a[f][k][jj][a]) and
+// writes the full lines pz_b[f][k][a][b] once: no zero-padded copy (k_prune_b)
+// and no library pass over the zeros.  The N-point inverse DFT is split
+// N = R1 x R2 as in pass C (k = k2 + R2 k1, m = m1 + R1 m2):
+//   pass 1: for each k2, an R1-point DFT over k1 -- zero outside the k1 rows
+//           [0, B) and [R1 - B, R1), B = ceil((Kb+1)/R2) -- times e^{2 pi i k2 m1 / N};
+//   pass 2: for each m1, an R2-point DFT over k2, giving z[m1 + R1 m2].
+// A CTA takes LINES consecutive a of one (f, k): the input tile Y[jj][line] is
+// read with the lines fastest (coalesced along a), the intermediate sits in
+// shared memory as T[m1][k2][line] (odd m1 stride), and pass 2 stores along b.
+template <typename S, int R1, int R2, int LINES, int B>
+__global__ void __launch_bounds__(R2 *LINES) k_pass_b_fft(const S *__restrict__ pa, S *__restrict__ pb,
+                                                         const typename Cplx<S>::T *__restrict__ twN, int N, int Kb,
+                                                         int Kc, const __grid_constant__ Tw32<S> tw) {
+  using C = typename Cplx<S>::T;
+  constexpr int TS = R2 * LINES + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *T = reinterpret_cast<C *>(smraw);  // [R1][TS]
+  C *TW = T + R1 * TS;                  // [R1][R2]: e^{2 pi i k2 m1 / N}
+  C *Ys = TW + R1 * R2;                 // [2Kb+1][LINES]
+  const int nj = 2 * Kb + 1;
+  const int a0 = blockIdx.x * LINES, k = blockIdx.y, f = blockIdx.z;
+  const long long fk = (long long)f * (Kc + 1) + k;
+  const C *src = reinterpret_cast<const C *>(pa) + fk * nj * N + a0;
+  for (int i = threadIdx.x; i < R1 * R2; i += blockDim.x) TW[i] = twN[i];
+  for (int i = threadIdx.x; i < nj * LINES; i += blockDim.x) {
+    const int jj = i / LINES, l = i - jj * LINES;
+    Ys[i] = src[(long long)jj * N + l];
+  }
+  __syncthreads();
+  for (int task = threadIdx.x; task < R2 * LINES; task += blockDim.x) {
+    const int k2 = task / LINES, l = task - k2 * LINES;
+    C v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      const int kk = k2 + R2 * k1;
+      C z{(S)0, (S)0};
+      if (k1 >= B && k1 < R1 - B) {
+        // outside the band's rows: zero
+      } else if (kk <= Kb) {
+        z = Ys[kk * LINES + l];  // b-frequency kk
+      } else if (kk >= N - Kb) {
+        z = Ys[(kk - N + nj) * LINES + l];  // b-frequency kk - N
+      }
+      v[k1] = z;
+    }
+    dft_inv<S, R1>(v, tw);
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+      C y = v[m1];
+      if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
+      T[m1 * TS + k2 * LINES + l] = y;
+    }
+  }
+  __syncthreads();
+  C *dst = reinterpret_cast<C *>(pb) + (fk * N + a0) * N;
+  for (int task = threadIdx.x; task < R1 * LINES; task += blockDim.x) {
+    const int l = task / R1, m1 = task - l * R1;
+    C u[R2];
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[m1 * TS + k2 * LINES + l];
+    dft_inv<S, R2>(u, tw);
+    C *row = dst + (long long)l * N;
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
+  }
+}
+
+// Pass-B shapes (N = R1 x R2, LINES lines per CTA, R2 x LINES threads).
+struct PbShape {
+  int R1, R2, lines;
+};
+static bool pb_shape(long long N, size_t word, PbShape *sh) {
+  if (word != 4 || N < 32 || N > 1024 || (N & (N - 1))) return false;
+  switch (N) {
+    case 32: *sh = PbShape{8, 4, 16}; break;
+    case 64: *sh = PbShape{8, 8, 16}; break;
+    case 128: *sh = PbShape{16, 8, 16}; break;
+    case 256: *sh = PbShape{16, 16, 16}; break;
+    case 512: *sh = PbShape{32, 16, 16}; break;
+    default: *sh = PbShape{32, 32, 8}; break;
+  }
+  return true;
+}
+static size_t pb_fused_smem(const cf_ctx *ctx, const PbShape &sh) {
+  return ((size_t)sh.R1 * (sh.R2 * sh.lines + 1) + (size_t)sh.R1 * sh.R2 + (size_t)(2 * ctx->Kb + 1) * sh.lines) * 2 *
+         ctx->word;
+}
+
+template <typename S, int R1, int R2, int LINES, int B>
+static int launch_pb_fused_b(cf_ctx *ctx, size_t smem, cudaStream_t st) {
+  using C = typename Cplx<S>::T;
+  auto kern = k_pass_b_fft<S, R1, R2, LINES, B>;
+  if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Tw32<S> tw;
+  for (int e = 0; e < 16; ++e) {
+    const double ang = 2.0 * 3.14159265358979323846 * e / 32.0;
+    tw.w[e] = C{(S)std::cos(ang), (S)std::sin(ang)};
+  }
+  const int N = (int)ctx->N;
+  kern<<<dim3(N / LINES, ctx->Kc + 1, 2), R2 * LINES, smem, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b,
+                                                                   (const C *)ctx->pr_twB, N, ctx->Kb, ctx->Kc, tw);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+// The smallest compiled band B >= ceil((Kb+1)/R2) (2, 3, 4, 6 or all rows).
+template <typename S, int R1, int R2, int LINES>
+static int launch_pb_fused_t(cf_ctx *ctx, size_t smem, cudaStream_t st) {
+  const int need = (ctx->Kb + 1 + R2 - 1) / R2;
+  if constexpr (R1 >= 16) {
+    if (need <= 2) return launch_pb_fused_b<S, R1, R2, LINES, 2>(ctx, smem, st);
+    if (need <= 3) return launch_pb_fused_b<S, R1, R2, LINES, 3>(ctx, smem, st);
+    if (need <= 4) return launch_pb_fused_b<S, R1, R2, LINES, 4>(ctx, smem, st);
+    if (need <= 6) return launch_pb_fused_b<S, R1, R2, LINES, 6>(ctx, smem, st);
+  }
+  return launch_pb_fused_b<S, R1, R2, LINES, R1 / 2>(ctx, smem, st);
+}
+
+static int launch_pb_fused(cf_ctx *ctx, cudaStream_t st) {
+  PbShape sh;
+  if (!pb_shape(ctx->N, ctx->word, &sh)) return set_error("fused pass B: unsupported N"), CF_ERR_INVALID;
+  const size_t smem = pb_fused_smem(ctx, sh);
+#define CF_PB(r1, r2, ln) \
+  if (sh.R1 == r1 && sh.R2 == r2 && sh.lines == ln) return launch_pb_fused_t<float, r1, r2, ln>(ctx, smem, st);
+  CF_PB(8, 4, 16)
+  CF_PB(8, 8, 16)
+  CF_PB(16, 8, 16)
+  CF_PB(16, 16, 16)
+  CF_PB(32, 16, 16)
+  CF_PB(32, 32, 8)
+#undef CF_PB
+  set_error("fused pass B: no kernel for R1=%d R2=%d lines=%d", sh.R1, sh.R2, sh.lines);
+  return CF_ERR_INVALID;
+}
+
 // Psi -> e^{2 Psi} - 1 in place after a cuFFT C2R (the slot's first field).
 static int psi_to_e2m1(cf_ctx *ctx, void *f, cudaStream_t st) {
   ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
@@ -568,10 +706,11 @@ static void free_pruned(cf_ctx *ctx) {
   cudaFree(ctx->pz_b);
   cudaFree(ctx->pr_wN);
   cudaFree(ctx->pr_twM);
+  cudaFree(ctx->pr_twB);
   cufftDestroy(ctx->plan_pa);
-  cufftDestroy(ctx->plan_pb);
+  if (!ctx->pb_fused) cufftDestroy(ctx->plan_pb);
   if (!ctx->pc_fused) cufftDestroy(ctx->plan_pc);
-  ctx->pz_a = ctx->pz_b = ctx->pr_wN = ctx->pr_twM = nullptr;
+  ctx->pz_a = ctx->pz_b = ctx->pr_wN = ctx->pr_twM = ctx->pr_twB = nullptr;
   ctx->have_pruned = false;
 }
 
@@ -595,9 +734,28 @@ static int ensure_pruned(cf_ctx *ctx) {
   CF_TRY_CUFFT(cufftCreate(&ctx->plan_pa));
   CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pa, 1, n1, nullptr, 1, N, nullptr, 1, N, dp ? CUFFT_Z2Z : CUFFT_C2C,
                                    2 * nk * nj, &work));
-  CF_TRY_CUFFT(cufftCreate(&ctx->plan_pb));
-  CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pb, 1, n1, nullptr, 1, N, nullptr, 1, N, dp ? CUFFT_Z2Z : CUFFT_C2C,
-                                   2 * nk * N, &work));
+  PbShape bsh;
+  ctx->pb_fused = pb_shape(N, ctx->word, &bsh) && pb_fused_smem(ctx, bsh) <= kPcFusedSmemMax;
+  if (ctx->pb_fused) {
+    // pass-B four-step twiddles e^{2 pi i k2 m1 / N}, laid out [m1][k2] (FP32)
+    std::vector<float> t(2 * N);
+    for (int m1 = 0; m1 < bsh.R1; ++m1)
+      for (int k2 = 0; k2 < bsh.R2; ++k2) {
+        const double ang = 2.0 * 3.14159265358979323846 * (double)((long long)k2 * m1 % N) / (double)N;
+        t[2 * (m1 * bsh.R2 + k2)] = (float)std::cos(ang);
+        t[2 * (m1 * bsh.R2 + k2) + 1] = (float)std::sin(ang);
+      }
+    if (cudaMalloc(&ctx->pr_twB, (size_t)N * cb) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMalloc of the pass-B twiddles failed");
+      return CF_ERR_NOMEM;
+    }
+    CF_TRY_CUDA(cudaMemcpy(ctx->pr_twB, t.data(), (size_t)N * cb, cudaMemcpyHostToDevice));
+  } else {
+    CF_TRY_CUFFT(cufftCreate(&ctx->plan_pb));
+    CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pb, 1, n1, nullptr, 1, N, nullptr, 1, N, dp ? CUFFT_Z2Z : CUFFT_C2C,
+                                     2 * nk * N, &work));
+  }
   PcShape sh;
   ctx->pc_fused = pc_shape(N, ctx->word, &sh) && pc_fused_smem(ctx, sh) <= kPcFusedSmemMax;
   if (ctx->pc_fused) {
@@ -664,13 +822,16 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
     else
       CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pa, (cufftComplex *)ctx->pz_a, (cufftComplex *)ctx->pz_a, CUFFT_INVERSE));
   }
-  {
-    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
-    k_prune_b<S><<<dim3((N + 255) / 256, N, 2 * (Kc + 1)), 256, 0, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b, N, Kb,
-                                                                         Kc);
-    CF_LAUNCHED(ctx);
-  }
-  {
+  if (ctx->pb_fused) {
+    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    CF_TRY(launch_pb_fused(ctx, st));
+  } else {
+    {
+      ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+      k_prune_b<S><<<dim3((N + 255) / 256, N, 2 * (Kc + 1)), 256, 0, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b, N,
+                                                                           Kb, Kc);
+      CF_LAUNCHED(ctx);
+    }
     ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
     CF_TRY_CUFFT(cufftSetStream(ctx->plan_pb, st));
     if (ctx->word == 8)

@@ -143,6 +143,41 @@ def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or,
         assert rel(b[sl], want) <= tol
 
 
+@pytest.mark.parametrize("N,K", [(512, 41), (1024, 40)])
+def test_pruned_psi_at_full_size_equals_full_c2r(N, K):
+    """FP32 storage at the benchmark's sizes, R_fft band-limited to a box of
+    |i|, |j|, k <= K: the pruned route -- pass B and pass C each as one kernel, split
+    32 x 16 at N = 512 and 32 x 32 at N = 1024 -- against the forced full 3-D C2R,
+    compared on the device, 2e-6 of the largest value (FP32 rounding of two FFT
+    orderings)."""
+    L = float(N)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(17)
+    hc = torch.fft.rfftn(torch.randn((N, N, N), generator=g, device="cuda", dtype=torch.float64))
+    i = torch.arange(N, device="cuda")
+    far = torch.minimum(i, N - i) > K
+    hc[far] = 0
+    hc[:, far] = 0
+    hc[:, :, K + 1:] = 0
+    Rf = torch.view_as_real(hc * (1e-2 / N ** 1.5)).reshape(-1).contiguous()
+    del hc
+    got = {}
+    for flags in (0, cfb200.FLAG_FULL_PSI_FFT):
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, flags=flags, **FRW)
+        c.set_R_fft(Rf, on_device=True)
+        assert c.info.psi_route == (cfb200.PSI_PRUNED_FUSED if flags == 0 else cfb200.PSI_FULL)
+        out = torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
+        c.psi_fields(1.3, out)
+        torch.cuda.synchronize()
+        got[flags] = out
+        c.close()
+        torch.cuda.empty_cache()
+    a, b = got[0], got[cfb200.FLAG_FULL_PSI_FFT]
+    for sl in (slice(0, N ** 3), slice(N ** 3, None)):
+        err = float((a[sl] - b[sl]).abs().max() / b[sl].abs().max())
+        assert err <= 2e-6, err
+
+
 @pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
 @pytest.mark.parametrize("eq", [0, 1, 2])
 @pytest.mark.parametrize("stencil", [7, 13])
