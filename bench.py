@@ -364,9 +364,9 @@ def ensemble_bench(steps=100, per_segment=50):
     L = N, m ~ U[0.5, 2] (seed 12345), GRF initial fields (k* = 0.5, <phi^2> = 1,
     dphi = 0, seeds 1000 + i), FP32-comp, 7-point, dt = 0.1 from t = 1, density
     spectra every 50 steps.  The same `steps` are timed as CUDA-graph replays of
-    one interval (the batched per-stage launches, or the persistent kernel) + the
-    spectra, as direct batched launches, and as one launch per stage per member
-    (the single-instance path)."""
+    one interval (the batched whole-step launches, one per step, or the persistent
+    kernel) + the spectra, as direct batched launches, and as one whole-step launch
+    per step per member (the single-instance path)."""
     import numpy as np
     import torch
 

@@ -12,8 +12,10 @@
 //                      gives up with CF_ERR_TIMEOUT instead of hanging) before the
 //                      next stage.  Stage coefficients come from a per-step table
 //                      in device memory, so a captured graph replays it.
-//   CF_ENS_BATCHED     two launches per step over the whole work list: the paired
-//                      passes of cf_rk4_steps (stages 1+2, 3+4; cf_pair_tile.cuh).
+//   CF_ENS_BATCHED     the passes of cf_rk4_steps over the whole work list: one
+//                      whole-step launch per step for the 7-point stencil
+//                      (cf_step_tile.cuh), the two paired passes (stages 1+2, 3+4;
+//                      cf_pair_tile.cuh) for the 13-point one.
 //   CF_ENS_LOOP        the same passes, one launch per member (the single-instance path).
 //
 // cf_ensemble_run_graph captures one observer interval -- the batched launches
@@ -36,6 +38,7 @@
 #include "cf_internal.cuh"
 #include "cf_pair_tile.cuh"
 #include "cf_stage_tile.cuh"
+#include "cf_step_tile.cuh"
 
 namespace cfb {
 
@@ -288,6 +291,88 @@ __global__ void k_counter_add(long long *c, long long v) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *c += v;
 }
 
+// Whole-step tiles of the 7-point ensembles (threads along c x along b, CTAs/SM):
+// shape 0 is cf_rk4_steps' own (FP32 128 x 8 sites, FP64 32 x 8), shape 1 a
+// narrower, taller tile for members whose N is not a multiple of the wide one
+// (FP32 64 x 16, FP64 16 x 16).
+constexpr int ENS_STEP_SHAPES = 2;
+template <typename S, int SS>
+struct EnsStepShape;
+template <>
+struct EnsStepShape<float, 0> {
+  static constexpr int TX = 32, TY = 8, MB = 2;
+};
+template <>
+struct EnsStepShape<float, 1> {
+  static constexpr int TX = 16, TY = 16, MB = 2;
+};
+template <>
+struct EnsStepShape<double, 0> {
+  static constexpr int TX = 16, TY = 8, MB = 3;
+};
+template <>
+struct EnsStepShape<double, 1> {
+  static constexpr int TX = 8, TY = 16, MB = 3;
+};
+template <typename S, int SS>
+constexpr size_t ens_step_smem() {
+  return (size_t)StepSmem<S, EnsStepShape<S, SS>::TX, EnsStepShape<S, SS>::TY>::count * sizeof(S);
+}
+
+// One RK4 step of one work item as cf_rk4_steps' whole-step pass, with the same
+// coefficients (1/h^2 / a^2 and 3H at t, t + dt/2, t + dt from the step table).
+// Within a run, step j reads phi, pi from x for even j and from ya for odd j and
+// writes the other buffer; the lo words stay in x; a run of odd length ends with
+// k_ens_xy_back.
+template <typename S, int SS>
+__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY, EnsStepShape<S, SS>::MB)
+    k_ens_step(const EnsArgs E, int step_off) {
+  using SH = EnsStepShape<S, SS>;
+  extern __shared__ __align__(16) unsigned char ens_step_sm[];
+  const EnsItem it = E.items[blockIdx.x];
+  const EnsMember mb = E.members[it.member];
+  const long long step = *E.step_counter + step_off;
+  S *x = (S *)mb.x, *ya = (S *)mb.ya;
+  S *cur = (step_off & 1) ? ya : x, *nxt = (step_off & 1) ? x : ya;
+  StepArgs<S> A{};
+  A.xphi = cur;
+  A.xpi = cur + mb.N3;
+  A.ophi = nxt;
+  A.opi = nxt + mb.N3;
+  A.xlo = (sizeof(S) == 4) ? x + 2 * mb.N3 : nullptr;
+  A.N = mb.N;
+  A.N3 = mb.N3;
+  A.m2 = mb.m2;
+  const int idx[3] = {0, 1, 3};  // stage times t, t + dt/2, t + dt
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const EnsCoef c = E.coef[4 * step + idx[k]];
+    A.inv[k] = mb.inv_scale / c.a2;
+    A.hub3[k] = c.hub3;
+  }
+  A.dt2 = E.dt / 2.0;
+  A.dt = E.dt;
+  A.dt6 = E.dt / 6.0;
+  step_tile<S, EQ_FRW, SH::TX, SH::TY, false>(A, it.c0, it.b0, it.a_begin, it.a_end, reinterpret_cast<S *>(ens_step_sm));
+}
+
+// phi and pi back from ya to x over one whole-step work item's sites.
+template <typename S, int SS>
+__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY) k_ens_xy_back(const EnsArgs E) {
+  constexpr int V = VecT<S>::n, TW = EnsStepShape<S, SS>::TX * V;
+  const EnsItem it = E.items[blockIdx.x];
+  const EnsMember mb = E.members[it.member];
+  const int N = mb.N;
+  const int c = it.c0 + threadIdx.x * V, b = it.b0 + threadIdx.y;
+  if (threadIdx.x * V >= min(TW, N - it.c0) || b >= N) return;
+  const long long NN = (long long)N * N;
+  for (int a = it.a_begin; a < it.a_end; ++a) {
+    const long long site = NN * a + (long long)N * b + c;
+    stv((S *)mb.x + site, ldv((const S *)mb.ya + site));
+    stv((S *)mb.x + mb.N3 + site, ldv((const S *)mb.ya + mb.N3 + site));
+  }
+}
+
 // Batched energy density of the members of one size class (blockIdx.y = member in class).
 template <typename S>
 __global__ void k_ens_energy(const EnsMember *members, const int *class_members, double *rho, int N, double a2) {
@@ -331,6 +416,10 @@ struct cf_ensemble {
   cfb::EnsItem *d_items = nullptr;
   std::map<int, std::pair<int, int>> tune;  // N -> (shape, a_chunk)
   int shape = 0;                            // shape used by the persistent kernel
+  // whole-step work list of the 7-point batched and loop schedules
+  std::vector<cfb::EnsItem> sitems;
+  cfb::EnsItem *d_sitems = nullptr;
+  int sshape = 0, schunk = 32;
   // time table
   cfb::EnsCoef *d_coef = nullptr;
   long long coef_cap = 0;
@@ -398,6 +487,36 @@ static int upload_items(cf_ensemble *E) {
   CF_TRY_CUDA(cudaMalloc(&E->d_items, sizeof(EnsItem) * E->items.size()));
   CF_TRY_CUDA(cudaMemcpy(E->d_items, E->items.data(), sizeof(EnsItem) * E->items.size(), cudaMemcpyHostToDevice));
   return CF_OK;
+}
+
+// Whole-step items: tiles of step shape E->sshape, a-chunks of E->schunk planes;
+// the CTA shared memory of that shape is allowed above 48 KB here (before any capture).
+template <typename S, int SS>
+static int step_items_t(cf_ensemble *E) {
+  using SH = EnsStepShape<S, SS>;
+  constexpr int TW = SH::TX * VecT<S>::n;
+  E->sitems.clear();
+  for (int i = 0; i < E->count; ++i) {
+    const int N = E->hm[i].N;
+    for (int a = 0; a < N; a += E->schunk)
+      for (int b = 0; b < N; b += SH::TY)
+        for (int c = 0; c < N; c += TW) E->sitems.push_back({i, c, b, a, std::min(a + E->schunk, N), SS});
+  }
+  std::stable_sort(E->sitems.begin(), E->sitems.end(),
+                   [&](const EnsItem &x, const EnsItem &y) { return E->hm[x.member].N > E->hm[y.member].N; });
+  CF_TRY_CUDA(cudaFuncSetAttribute(k_ens_step<S, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)ens_step_smem<S, SS>()));
+  cudaFree(E->d_sitems);
+  E->d_sitems = nullptr;
+  CF_TRY_CUDA(cudaMalloc(&E->d_sitems, sizeof(EnsItem) * E->sitems.size()));
+  CF_TRY_CUDA(cudaMemcpy(E->d_sitems, E->sitems.data(), sizeof(EnsItem) * E->sitems.size(), cudaMemcpyHostToDevice));
+  return CF_OK;
+}
+
+static int build_step_items(cf_ensemble *E) {
+  if (E->stencil != 7) return CF_OK;
+  if (E->word == 4) return E->sshape ? step_items_t<float, 1>(E) : step_items_t<float, 0>(E);
+  return E->sshape ? step_items_t<double, 1>(E) : step_items_t<double, 0>(E);
 }
 
 static int ensure_coef(cf_ensemble *E, double t0, double dt, long long nsteps_total, cudaStream_t st) {
@@ -495,6 +614,54 @@ static int pair_steps(cf_ensemble *E, size_t i0, size_t i1, long long nsteps, do
   return CF_OK;
 }
 
+// One whole-step launch over step items [i0, i1) (BACK: phi, pi back from ya to x).
+template <typename S, int SS, bool BACK>
+static int launch_items_step(cf_ensemble *E, size_t i0, size_t i1, int step_off, double dt, cudaStream_t st) {
+  EnsArgs A{};
+  A.members = E->dm;
+  A.items = E->d_sitems + i0;
+  A.n_items = (int)(i1 - i0);
+  A.coef = E->d_coef;
+  A.step_counter = E->d_step;
+  A.dt = dt;
+  const dim3 block(EnsStepShape<S, SS>::TX, EnsStepShape<S, SS>::TY);
+  if constexpr (BACK)
+    k_ens_xy_back<S, SS><<<A.n_items, block, 0, st>>>(A);
+  else
+    k_ens_step<S, SS><<<A.n_items, block, ens_step_smem<S, SS>(), st>>>(A, step_off);
+  CF_TRY_CUDA(cudaGetLastError());
+  E->launches++;
+  return CF_OK;
+}
+
+// nsteps whole steps over step items [i0, i1) (BATCHED: all of them; LOOP: member by
+// member), steps from the device step counter; phi, pi back to x after an odd count.
+template <typename S, int SS>
+static int step_steps_t(cf_ensemble *E, bool loop, long long nsteps, double dt, cudaStream_t st) {
+  std::vector<std::pair<size_t, size_t>> ranges;
+  if (!loop) {
+    ranges.push_back({0, E->sitems.size()});
+  } else {  // each member's items are contiguous
+    for (size_t i0 = 0; i0 < E->sitems.size();) {
+      size_t i1 = i0;
+      while (i1 < E->sitems.size() && E->sitems[i1].member == E->sitems[i0].member) ++i1;
+      ranges.push_back({i0, i1});
+      i0 = i1;
+    }
+  }
+  for (long long j = 0; j < nsteps; ++j)
+    for (auto &r : ranges) CF_TRY((launch_items_step<S, SS, false>(E, r.first, r.second, (int)j, dt, st)));
+  if (nsteps & 1)
+    for (auto &r : ranges) CF_TRY((launch_items_step<S, SS, true>(E, r.first, r.second, 0, dt, st)));
+  return CF_OK;
+}
+
+static int step_steps(cf_ensemble *E, bool loop, long long nsteps, double dt, cudaStream_t st) {
+  if (E->word == 4)
+    return E->sshape ? step_steps_t<float, 1>(E, loop, nsteps, dt, st) : step_steps_t<float, 0>(E, loop, nsteps, dt, st);
+  return E->sshape ? step_steps_t<double, 1>(E, loop, nsteps, dt, st) : step_steps_t<double, 0>(E, loop, nsteps, dt, st);
+}
+
 template <typename S, int H, int SHAPE>
 static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, double dt, cudaStream_t st) {
   CF_TRY_CUDA(cudaMemcpyAsync(E->d_step, &step0, sizeof(long long), cudaMemcpyHostToDevice, st));
@@ -511,6 +678,7 @@ static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, do
     }
     return CF_OK;
   }
+  if (H == 1) return step_steps(E, mode == CF_ENS_LOOP, nsteps, dt, st);
   if (mode == CF_ENS_BATCHED) return pair_steps<S, H, SHAPE>(E, 0, E->items.size(), nsteps, dt, st);
   // CF_ENS_LOOP: the single-instance path, member by member (each member's
   // items are contiguous in the work list)
@@ -557,7 +725,9 @@ static int batched_launches(cf_ensemble *E, long long steps, double dt, cudaStre
 static int segment(cf_ensemble *E, int mode, long long steps, double dt, cudaStream_t st) {
   int s;
   if (mode == CF_ENS_BATCHED) {
-    if (E->word == 4)
+    if (E->stencil == 7)
+      s = step_steps(E, false, steps, dt, st);
+    else if (E->word == 4)
       s = E->stencil == 13 ? batched_launches<float, 2>(E, steps, dt, st) : batched_launches<float, 1>(E, steps, dt, st);
     else
       s = E->stencil == 13 ? batched_launches<double, 2>(E, steps, dt, st)
@@ -729,6 +899,7 @@ int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out) {
   cudaMemset(E->d_step, 0, sizeof(long long));
   build_items(E);
   int s = upload_items(E);
+  if (s == CF_OK) s = build_step_items(E);
   if (s != CF_OK) {
     cf_ensemble_destroy(E);
     return s;
@@ -744,6 +915,7 @@ int cf_ensemble_destroy(cf_ensemble *E) {
   for (void *a : E->allocs) cudaFree(a);
   cudaFree(E->dm);
   cudaFree(E->d_items);
+  cudaFree(E->d_sitems);
   cudaFree(E->d_coef);
   cudaFree(E->d_step);
   cudaFree(E->d_bar);
@@ -767,7 +939,7 @@ int cf_ensemble_info(const cf_ensemble *E, int64_t *spectra_total, int64_t *work
     for (int i = 0; i < E->count; ++i) off += 3 * (E->hm[i].N / 2) * (E->hm[i].N / 2) + 1;
     *spectra_total = off;
   }
-  if (work_items) *work_items = (int64_t)E->items.size();
+  if (work_items) *work_items = (int64_t)(E->stencil == 7 ? E->sitems.size() : E->items.size());
   return CF_OK;
 }
 
@@ -914,6 +1086,39 @@ int cf_ensemble_autotune(cf_ensemble *E, double t0, double dt, int64_t steps, vo
   CF_TRY_CUDA(cudaEventCreate(&b));
   float best = 1e30f;
   int best_shape = 0, best_chunk = 16;
+  if (E->stencil == 7) {  // the whole-step work list of the batched schedule
+    const int schunks[3] = {16, 32, 64};
+    for (int shape = 0; shape < ENS_STEP_SHAPES; ++shape)
+      for (int ch : schunks) {
+        E->sshape = shape;
+        E->schunk = ch;
+        CF_TRY(build_step_items(E));
+        CF_TRY(step_steps(E, false, 1, dt, st));  // warm
+        CF_TRY_CUDA(cudaEventRecord(a, st));
+        CF_TRY(step_steps(E, false, steps, dt, st));
+        CF_TRY_CUDA(cudaEventRecord(b, st));
+        CF_TRY_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        CF_TRY_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if (ms < best) {
+          best = ms;
+          best_shape = shape;
+          best_chunk = ch;
+        }
+      }
+    E->sshape = best_shape;
+    E->schunk = best_chunk;
+    CF_TRY(build_step_items(E));
+    if (E->gexec) {
+      cudaGraphExecDestroy(E->gexec);
+      E->gexec = nullptr;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (h_shape) *h_shape = best_shape;
+    if (h_a_chunk) *h_a_chunk = best_chunk;
+    return CF_OK;
+  }
   const int chunks[3] = {8, 16, 32};
   for (int shape = 0; shape < ENS_SHAPES; ++shape)
     for (int ch : chunks) {

@@ -352,19 +352,23 @@ int cf_shell_amplitude_gradient(cf_ctx *ctx, const double *d_lambda_phi, const d
  * per process (src/main.cpp:82-196).
  *   CF_ENS_PERSISTENT: one cooperative kernel for all nsteps (grid barriers between
  *     stages; a barrier that waits too long returns CF_ERR_TIMEOUT, never hangs).
- *   CF_ENS_BATCHED: two launches per step over all members (the paired-stage
- *     passes of cf_rk4_steps: stages 1+2, 3+4).
+ *   CF_ENS_BATCHED: the passes of cf_rk4_steps over all members: one whole-step
+ *     launch per step (7-point), two paired-stage launches per step (13-point:
+ *     stages 1+2, 3+4).
  *   CF_ENS_LOOP: the same passes, one launch per member (single-instance path).
  * cf_ensemble_run_graph: nsegments observer intervals of steps_per_segment steps from
  *   t0 (absolute steps 0..): a CUDA graph of one interval -- the persistent kernel
- *   (mode CF_ENS_PERSISTENT) or the 4 * steps_per_segment batched launches (mode
+ *   (mode CF_ENS_PERSISTENT) or the batched launches of steps_per_segment steps (mode
  *   CF_ENS_BATCHED), each reading its step from a device counter that the graph
  *   advances -- is captured once and replayed per segment; when d_spectra is non-NULL the members' density
  *   spectra (S2 bins, concatenated member by member, cf_ensemble_info gives the
  *   per-segment length) at each segment end follow each replay.  Needs a
  *   non-default stream.
  * cf_ensemble_autotune: times tile shapes and a-chunk lengths on the members
- *   (overwrites their states: tune before uploading initial data). */
+ *   (of the whole-step work list for the 7-point stencil, of the paired-stage /
+ *   persistent one for the 13-point; overwrites their states: tune before
+ *   uploading initial data). cf_ensemble_info's work_items counts the items of the
+ *   batched schedule. */
 typedef enum cf_ens_mode { CF_ENS_PERSISTENT = 0, CF_ENS_BATCHED = 1, CF_ENS_LOOP = 2 } cf_ens_mode;
 typedef struct cf_ensemble cf_ensemble;
 int cf_ensemble_create(const cf_params *members, int count, cf_ensemble **out);
