@@ -344,24 +344,33 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
 // sites, 3 CTAs/SM) 1.71 / 3.14 against 32 x 8 1.85 / 3.19 and 16 x 16 1.81 / 3.32.
 template <typename S>
 struct StepShape;
+// RW: two ring warps beside the own rows (step_tile RINGW), measured at N = 512
+// (ms per step, step kernel, comoving / KG-FRW): FP32 1.876 / 1.191 against 1.975 /
+// 1.195 without; FP64 2.883 / 1.731 against 2.942 / 1.721; bit-identical.
 template <>
 struct StepShape<float> {
   static constexpr int TX = 32, TY = 8, MB = 2;
+  static constexpr bool RW = true;
 };
 template <>
 struct StepShape<double> {
   static constexpr int TX = 16, TY = 8, MB = 3;
+  static constexpr bool RW = true;
 };
+template <typename S>
+constexpr int step_threads_y() {
+  return StepShape<S>::TY + (StepShape<S>::RW ? 2 : 0);
+}
 
 template <typename S, int EQ, bool FULL>
-__global__ void __launch_bounds__(StepShape<S>::TX *StepShape<S>::TY, StepShape<S>::MB)
+__global__ void __launch_bounds__(StepShape<S>::TX *step_threads_y<S>(), StepShape<S>::MB)
     k_step(const StepArgs<S> A) {
   extern __shared__ __align__(16) unsigned char step_smem[];
   constexpr int TXs = StepShape<S>::TX, TYs = StepShape<S>::TY;
   using SM = StepSmem<S, TXs, TYs>;
   const int a_begin = blockIdx.z * A.a_chunk;
-  step_tile<S, EQ, TXs, TYs, FULL>(A, blockIdx.x * SM::TW, blockIdx.y * TYs, a_begin,
-                                   min(a_begin + A.a_chunk, A.N), reinterpret_cast<S *>(step_smem));
+  step_tile<S, EQ, TXs, TYs, FULL, StepShape<S>::RW>(A, blockIdx.x * SM::TW, blockIdx.y * TYs, a_begin,
+                                                     min(a_begin + A.a_chunk, A.N), reinterpret_cast<S *>(step_smem));
 }
 
 // Planes per CTA: each chunk re-reads 4 halo planes, so chunks are long where the
@@ -382,7 +391,7 @@ static int launch_step_k(cf_ctx *ctx, const StepArgs<S> &A, dim3 grid, cudaStrea
     CF_TRY_CUDA(cudaFuncSetAttribute(k_step<S, EQ, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     attr_set |= bit;
   }
-  k_step<S, EQ, FULL><<<grid, dim3(StepShape<S>::TX, StepShape<S>::TY), bytes, st>>>(A);
+  k_step<S, EQ, FULL><<<grid, dim3(StepShape<S>::TX, step_threads_y<S>()), bytes, st>>>(A);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }

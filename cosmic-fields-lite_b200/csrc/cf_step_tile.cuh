@@ -161,11 +161,18 @@ __device__ __forceinline__ Star<T> ya_star(const Star<T> &f, const Star<T> &p, c
                  (T)w_of((S)f.cm, (S)p.cm, ch)};
 }
 
-template <typename S, int EQ, int TXv, int TYv, bool FULL = false>
+// RINGW: the CTA has two more thread rows (ring warps, ty = TYv and TYv + 1) beside the
+// TYv rows of own sites.  They copy the ring rows and columns, form the two ring rows
+// of phase 1 while the own rows form theirs, and form the ring columns of plane q
+// after the second barrier, while the own rows run phase 2 on plane r: phase 2 reads
+// plane q = r + 1 at own sites only (its a-neighbour), and q's ring is first read by
+// phase 2 one plane later.  Without RINGW the first two own rows take the ring rows
+// and the last threads the ring columns, both before the second barrier.
+template <typename S, int EQ, int TXv, int TYv, bool FULL = false, bool RINGW = false>
 __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, int a_begin, int a_end, S *smem) {
   using SM = StepSmem<S, TXv, TYv>;
   using T = typename Arith<S>::T;
-  constexpr int V = SM::V, TW = SM::TW, O = SM::O, SP = SM::SP, NT = TXv * TYv, PD = SM::PD;
+  constexpr int V = SM::V, TW = SM::TW, O = SM::O, SP = SM::SP, NT = TXv * (TYv + (RINGW ? 2 : 0)), PD = SM::PD;
   S *XF = smem;               // x_phi, 4 planes of P2
   S *XP = XF + 4 * SM::P2;    // x_pi,  4 planes of P2
   S *YB = XP + 4 * SM::P2;    // yb_phi, 3 planes of P1
@@ -201,7 +208,17 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
       cp_async_16(xf + own2, A.xphi + poff + rowoff);
       cp_async_16(xp + own2, A.xpi + poff + rowoff);
     }
-    if (ty < 4 && colact) {  // ring rows: 2 above the tile, 2 below its active height
+    if constexpr (RINGW) {  // ring rows: ring warp 0 the 2 above the tile, ring warp 1 the 2 below
+      if (ty >= TYv && colact) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int r2 = ty == TYv ? k : tye + 2 + k;
+          const long long off = poff + (long long)N * wrap_n(b0 - 2 + r2, N) + c;
+          cp_async_16(xf + r2 * SP + O + tx * V, A.xphi + off);
+          cp_async_16(xp + r2 * SP + O + tx * V, A.xpi + off);
+        }
+      }
+    } else if (ty < 4 && colact) {  // ring rows: 2 above the tile, 2 below its active height
       const int r2 = ty < 2 ? ty : tye + ty;
       const long long off = poff + (long long)N * wrap_n(b0 - 2 + r2, N) + c;
       cp_async_16(xf + r2 * SP + O + tx * V, A.xphi + off);
@@ -309,8 +326,9 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
         sts<S, V>(dl + PD + od, vap);
         sts<S, V>(dl + 2 * PD + od, vpp);
       }
-      if (ty < 2 && colact) {  // ring rows of the 1-ring plane: b0 - 1 and b0 + tye
-        const int r1 = ty == 0 ? 0 : tye + 1;
+      // ring rows of the 1-ring plane: b0 - 1 and b0 + tye
+      if ((RINGW ? ty >= TYv : ty < 2) && colact) {
+        const int r1 = ty == (RINGW ? TYv : 0) ? 0 : tye + 1;
         const int gb = wrap_n(b0 - 1 + r1, N);
         const long long site = qoff + (long long)N * gb + c;
         Coupling<S, V> ct, ch2;
@@ -334,11 +352,25 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
         sts<S, V>(yc + r1 * SP + O + tx * V, vc);
       }
       // ring columns of the 1-ring plane (corners included): scalars, on the last warps
-      // (the first warp takes the ring rows)
-      for (int i = NT - 1 - tid; i < (tye + 2) * 2; i += NT)
-        ring_site(q, qm, qoff, yb, yc, i >> 1, (i & 1) ? O + twe : O - 1);
+      // (the first warp takes the ring rows); with RINGW after the barrier below
+      if constexpr (!RINGW)
+        for (int i = NT - 1 - tid; i < (tye + 2) * 2; i += NT)
+          ring_site(q, qm, qoff, yb, yc, i >> 1, (i & 1) ? O + twe : O - 1);
     }
-    __syncthreads();  // yb_phi, yc_phi of plane q ready
+    __syncthreads();  // yb_phi, yc_phi of plane q ready (with RINGW: its own sites and ring rows)
+
+    // ---- RINGW: the ring columns of plane q, beside phase 2.  They read x of planes
+    // q-1..q+1 (slot s4(q-1) is refilled by the next iteration's copies: its ring
+    // columns by the same last warp, after the __syncwarp) and write YB / YC of plane
+    // q at ring columns, which phase 2 below does not read.
+    if constexpr (RINGW) {
+      if (q >= a_begin - 1) {
+        const int qm = wrap_n(q, N);
+        for (int i = NT - 1 - tid; i < (tye + 2) * 2; i += NT)
+          ring_site(q, qm, NN * qm, YB + s3(q) * SM::P1, YC + s3(q) * SM::P1, i >> 1, (i & 1) ? O + twe : O - 1);
+      }
+      __syncwarp();
+    }
 
     // ---- phase 2 on plane r = p - 2 (own sites): stages 3 and 4, the update.  Its x_phi,
     // x_pi are still staged (slot s4(r) is next refilled by the copies of plane r + 4,
