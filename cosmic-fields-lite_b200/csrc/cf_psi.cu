@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -402,6 +403,104 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
   }
 }
 
+// Pass C as a persistent kernel (FP64 storage; pc_persistent).  A CTA walks tiles (f, a, ROWS rows of b) with
+// stride gridDim.x; the twiddles e^{2 pi i k2 m1 / M} and w^k are staged once per
+// CTA, and the next tile's band rows X[k][b0 .. b0 + ROWS) are copied into shared
+// memory by cp.async while the current tile runs its second radix pass, so the
+// tile's global loads are not waited on at its start.  The arithmetic is pass 1 /
+// pass 2 of k_prune_c_fft; Z[k] = X[k] + i X[k] w^k is formed in pass 1 from the
+// staged X.
+__device__ __forceinline__ void pc_cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <typename S, int R1, int R2, int ROWS, int B>
+__global__ void __launch_bounds__(256) k_prune_c_fft_p(const S *__restrict__ pb, S *__restrict__ out,
+                                                       const typename Cplx<S>::T *__restrict__ wN,
+                                                       const typename Cplx<S>::T *__restrict__ twM, int N, int Kc,
+                                                       int ntiles, const __grid_constant__ Tw32<S> tw) {
+  using C = typename Cplx<S>::T;
+  constexpr int M = R1 * R2;  // N == 2 M
+  constexpr int TS = R2 * ROWS + 1;
+  constexpr int CPR = ROWS * (int)sizeof(C) / 16;  // 16-byte copies per band row of a tile
+  static_assert(ROWS * sizeof(C) % 16 == 0, "tile rows");
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *XR = reinterpret_cast<C *>(smraw);  // [Kc+1][ROWS]: X[k] of the tile (16-byte aligned)
+  C *T = XR + (Kc + 1) * ROWS;           // [R1][TS]
+  C *TW = T + R1 * TS;                   // [R1][R2]: e^{2 pi i k2 m1 / M}
+  C *WK = TW + M;                        // [Kc+1]: w^k = e^{2 pi i k / N}
+  const int nb = N / ROWS;
+  auto issue = [&](int tile) {
+    const int bt = tile % nb, a = (tile / nb) % N, f = tile / (nb * N);
+    const C *src = reinterpret_cast<const C *>(pb) + ((long long)f * (Kc + 1) * N + a) * N + (long long)bt * ROWS;
+    for (int i = threadIdx.x; i < (Kc + 1) * CPR; i += blockDim.x) {
+      const int k = i / CPR, j = i - k * CPR;
+      pc_cp_async16(reinterpret_cast<unsigned char *>(XR + k * ROWS) + 16 * j,
+                    reinterpret_cast<const unsigned char *>(src + (long long)k * N * N) + 16 * j);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  for (int i = threadIdx.x; i < M; i += blockDim.x) TW[i] = twM[i];
+  for (int i = threadIdx.x; i <= Kc; i += blockDim.x) WK[i] = wN[i];
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int bt = tile % nb, a = (tile / nb) % N, f = tile / (nb * N);
+    const int b0 = bt * ROWS;
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();  // the tile's X (everyone's copies); the last tile's pass 2 is done with T
+    for (int task = threadIdx.x; task < R2 * ROWS; task += blockDim.x) {
+      const int k2 = task / ROWS, r = task - k2 * ROWS;
+      C v[R1];
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) {
+        const int k = k2 + R2 * k1;
+        C z{(S)0, (S)0};
+        if (k1 >= B && k1 < R1 - B) {
+          // outside the band's rows: zero
+        } else if (k <= Kc) {
+          C x = XR[k * ROWS + r];
+          if (k == 0) x.y = (S)0;
+          const C xp = c_mul_i(c_mul(x, WK[k]));
+          z = c_add(x, xp);  // X + i X w^k
+        } else if (k >= M - Kc) {
+          const int j = M - k;
+          const C x = XR[j * ROWS + r];
+          const C xp = c_mul_i(c_mul(x, WK[j]));
+          const C d = c_sub(x, xp);  // conj(X - i X w^j)
+          z = C{d.x, -d.y};
+        }
+        v[k1] = z;
+      }
+      dft_inv<S, R1>(v, tw);
+#pragma unroll
+      for (int m1 = 0; m1 < R1; ++m1) {
+        C y = v[m1];
+        if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
+        T[m1 * TS + k2 * ROWS + r] = y;
+      }
+    }
+    __syncthreads();  // T complete; every read of the tile's X is done
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+    for (int task = threadIdx.x; task < R1 * ROWS; task += blockDim.x) {
+      const int r = task / R1, m1 = task - r * R1;
+      C u[R2];
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[m1 * TS + k2 * ROWS + r];
+      dft_inv<S, R2>(u, tw);
+      C *row = reinterpret_cast<C *>(out) + ((long long)(f * N + a) * N + b0 + r) * M;
+#pragma unroll
+      for (int m2 = 0; m2 < R2; ++m2) {
+        C o = u[m2];
+        if (f == 0) o = C{e2m1_of(o.x), e2m1_of(o.y)};  // the slot holds e^{2 Psi} - 1
+        row[m1 + R1 * m2] = o;
+      }
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // ---- pass B as one kernel: pruned lines -> full lines -----------------------
 // For FP32 storage and power-of-two N (32..1024) the C2C of pass B reads the
 // pass-A lines at their 2Kb+1 non-zero b-frequencies only (pz_a[f][k][jj][a]) and
@@ -575,7 +674,15 @@ static bool pc_shape(long long N, size_t word, PcShape *sh) {
   *sh = PcShape{R1, R2, rows};
   return true;
 }
+// Pass C kernel per storage type, measured at N = 512 (Psi synthesis per RK4 step,
+// two refreshes): FP64 k_prune_c_fft_p 1.79 ms against k_prune_c_fft 2.08; FP32
+// k_prune_c_fft 0.90 ms against k_prune_c_fft_p 0.91 (0.92 with 5 CTAs/SM forced).
+// Both give the same bits.
+static bool pc_persistent(const cf_ctx *ctx) { return ctx->word == 8; }
 static size_t pc_fused_smem(const cf_ctx *ctx, const PcShape &sh) {
+  if (pc_persistent(ctx))  // X, T, TW, w^k
+    return ((size_t)(ctx->Kc + 1) * sh.rows + (size_t)sh.R1 * (sh.R2 * sh.rows + 1) + (size_t)sh.R1 * sh.R2 +
+            (size_t)(ctx->Kc + 1)) * 2 * ctx->word;
   return ((size_t)sh.R1 * (sh.R2 * sh.rows + 1) + (size_t)sh.R1 * sh.R2 + 2 * (size_t)(ctx->Kc + 1) * sh.rows) * 2 *
          ctx->word;
 }
@@ -583,16 +690,28 @@ static size_t pc_fused_smem(const cf_ctx *ctx, const PcShape &sh) {
 template <typename S, int R1, int R2, int ROWS, int B>
 static int launch_pc_fused_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
   using C = typename Cplx<S>::T;
-  auto kern = k_prune_c_fft<S, R1, R2, ROWS, B>;
-  if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Tw32<S> tw;
   for (int e = 0; e < 16; ++e) {
     const double ang = 2.0 * 3.14159265358979323846 * e / 32.0;
     tw.w[e] = C{(S)std::cos(ang), (S)std::sin(ang)};
   }
   const int N = (int)ctx->N;
-  kern<<<dim3(N / ROWS, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)out, (const C *)ctx->pr_wN,
-                                                 (const C *)ctx->pr_twM, N, ctx->Kc, tw);
+  if constexpr (sizeof(S) == 8) {  // pc_persistent: one CTA per resident slot
+    auto kern = k_prune_c_fft_p<S, R1, R2, ROWS, B>;
+    if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int sms = 0, per_sm = 0;
+    CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    const int ntiles = 2 * N * (N / ROWS);
+    const int grid = std::max(1, std::min(ntiles, sms * std::max(per_sm, 1)));
+    kern<<<grid, 256, smem, st>>>((const S *)ctx->pz_b, (S *)out, (const C *)ctx->pr_wN, (const C *)ctx->pr_twM, N,
+                                  ctx->Kc, ntiles, tw);
+  } else {
+    auto kern = k_prune_c_fft<S, R1, R2, ROWS, B>;
+    if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<dim3(N / ROWS, N, 2), 256, smem, st>>>((const S *)ctx->pz_b, (S *)out, (const C *)ctx->pr_wN,
+                                                   (const C *)ctx->pr_twM, N, ctx->Kc, tw);
+  }
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
