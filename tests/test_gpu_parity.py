@@ -143,13 +143,15 @@ def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or,
         assert rel(b[sl], want) <= tol
 
 
-@pytest.mark.parametrize("N,K", [(512, 41), (1024, 40)])
-def test_pruned_psi_at_full_size_equals_full_c2r(N, K):
-    """FP32 storage at the benchmark's sizes, R_fft band-limited to a box of
-    |i|, |j|, k <= K: the pruned route -- pass B and pass C each as one kernel, split
-    32 x 16 at N = 512 and 32 x 32 at N = 1024 -- against the forced full 3-D C2R,
-    compared on the device, 2e-6 of the largest value (FP32 rounding of two FFT
-    orderings)."""
+@pytest.mark.parametrize("N,K,prec,tol", [(512, 41, cfb200.FP32_COMP, 2e-6), (1024, 40, cfb200.FP32_COMP, 2e-6),
+                                          (512, 41, cfb200.FP64, 1e-12)])
+def test_pruned_psi_at_full_size_equals_full_c2r(N, K, prec, tol):
+    """The benchmark's sizes, R_fft band-limited to a box of |i|, |j|, k <= K: the
+    pruned route against the forced full 3-D C2R, compared on the device as a
+    fraction of the largest value.  FP32 storage: pass B and pass C each as one
+    kernel (pass B split 32 x 16 at N = 512 and 32 x 32 at N = 1024), 2e-6 (FP32
+    rounding of two FFT orderings).  FP64 storage: pass C as the persistent
+    kernel (16 x 16 at N = 512), 1e-12."""
     L = float(N)
     g = torch.Generator(device="cuda")
     g.manual_seed(17)
@@ -163,7 +165,7 @@ def test_pruned_psi_at_full_size_equals_full_c2r(N, K):
     del hc
     got = {}
     for flags in (0, cfb200.FLAG_FULL_PSI_FFT):
-        c = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, flags=flags, **FRW)
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=prec, flags=flags, **FRW)
         c.set_R_fft(Rf, on_device=True)
         assert c.info.psi_route == (cfb200.PSI_PRUNED_FUSED if flags == 0 else cfb200.PSI_FULL)
         out = torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
@@ -175,7 +177,7 @@ def test_pruned_psi_at_full_size_equals_full_c2r(N, K):
     a, b = got[0], got[cfb200.FLAG_FULL_PSI_FFT]
     for sl in (slice(0, N ** 3), slice(N ** 3, None)):
         err = float((a[sl] - b[sl]).abs().max() / b[sl].abs().max())
-        assert err <= 2e-6, err
+        assert err <= tol, err
 
 
 @pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
