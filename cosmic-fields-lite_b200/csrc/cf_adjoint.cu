@@ -423,10 +423,11 @@ int state_export(cf_ctx *, double *, const void *, cudaStream_t);
 int adjoint_forward(cf_adjoint *a, void *d_state, double t0, double dt, cudaStream_t st) {
   a->t0 = t0;
   a->dt = dt;
-  for (int64_t n = 0; n < a->nsteps; ++n) {
-    if (n % a->every == 0)
-      CF_TRY_CUDA(cudaMemcpyAsync(a->ckpt[n / a->every], d_state, a->state_bytes, cudaMemcpyDeviceToDevice, st));
-    CF_TRY(rk4_steps(a->ctx, d_state, t0, dt, n, 1, st));
+  // one call per checkpoint segment: the steps are those of single-step calls (same
+  // kernels, times t0 + n dt), without a state copy-back after every step
+  for (int64_t n0 = 0; n0 < a->nsteps; n0 += a->every) {
+    CF_TRY_CUDA(cudaMemcpyAsync(a->ckpt[n0 / a->every], d_state, a->state_bytes, cudaMemcpyDeviceToDevice, st));
+    CF_TRY(rk4_steps(a->ctx, d_state, t0, dt, n0, std::min<int64_t>(a->every, a->nsteps - n0), st));
   }
   a->have_forward = true;
   return CF_OK;
