@@ -178,6 +178,27 @@ def test_known_answer_plane_wave_dispersion(stencil):
     assert np.allclose(y[: N ** 3], phi * np.cos(w * 5.0), atol=1e-7)
 
 
+@pytest.mark.parametrize("stencil,order", [(7, 2), (13, 4)])
+def test_laplacian_convergence_order_on_a_plane_wave(stencil, order):
+    """The 7-point Laplacian converges as h^2 and the 13-point one as h^4: on
+    cos(2 pi (a + 2 b + 3 c) / N) with L fixed, the right-hand side's pi part
+    (flat KG, m = 0: h^-2 Delta_h phi) approaches -(2 pi / L)^2 (1 + 4 + 9) phi,
+    and halving h divides the error by 2^order."""
+    L = 8.0
+    errs = []
+    for N in (16, 32, 64):
+        i = np.arange(N)
+        A, Bb, Cc = np.meshgrid(i, i, i, indexing="ij")
+        phi = np.cos(2 * np.pi * (A + 2 * Bb + 3 * Cc) / N).ravel()
+        x = np.concatenate([phi, np.zeros(N ** 3)])
+        P = O.make_params(N, L, 0.0, eq=0, stencil=stencil)
+        lap = O.rhs(P, x, 0.0, None)[N ** 3:]
+        exact = -(2 * np.pi / L) ** 2 * 14.0 * phi
+        errs.append(float(np.abs(lap - exact).max() / np.abs(exact).max()))
+    rates = [np.log2(errs[k] / errs[k + 1]) for k in range(2)]
+    assert all(abs(r - order) < 0.15 for r in rates), (errs, rates)
+
+
 # ---- the GPU-only functors: pinned to the reference's own GPU build ------------
 # tests/golden/ref_gpu_equations.npz holds outputs of src/equations_cuda.cu itself
 # (oracle/ref_gpu_golden.cu, built from the reference sources and run on a GPU;
