@@ -4,13 +4,14 @@
 Workload (the configuration the headline metric is quoted on): the
 comoving-curvature-coupled Klein-Gordon equation in radiation-dominated FRW
 (a1 = 1, H1 = 0.5, t1 = 1, so a = t^1/2), N = 512, L = 512, m = 1, FP32 hi+lo
-compensated state with FP64 arithmetic, 7-point Laplacian, RK4 dt = 0.05 from
-t = 1.  phi(0) is a Gaussian random field (k* = 0.25, <phi^2> = 1), dphi(0) = 0;
+compensated state (stage arithmetic in FP32 with hi + lo coefficients, an
+error-free FP32 state update; FP64 background, reductions and spectra),
+7-point Laplacian, RK4 dt = 0.05 from t = 1.  phi(0) is a Gaussian random field (k* = 0.25, <phi^2> = 1), dphi(0) = 0;
 R is a k^-3 field with cutoff k_max = 0.5 normalised to rms Psi = 1e-2.
 Seeded synthetic inputs; no dataset is involved.
 
-One bench step = one RK4 step of the whole lattice (4 fused stage kernels and
-the Psi / dPsi refreshes at the two new stage times).  The state (1 GB) and all
+One bench step = one RK4 step of the whole lattice (one whole-step pass and the
+Psi / dPsi refreshes at the two new stage times).  The state (1 GB) and all
 RK4 buffers are far larger than the 126 MB L2, so no L2 flush is needed between
 steps.  Times are CUDA events on the stepping stream, max over ranks.
 

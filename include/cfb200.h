@@ -73,7 +73,9 @@ typedef enum cf_equation {
 
 typedef enum cf_precision {
   CF_FP64 = 0,      /* state stored and stepped in FP64 */
-  CF_FP32_COMP = 1  /* state stored as FP32 hi + FP32 compensation, arithmetic in FP64 */
+  CF_FP32_COMP = 1  /* state stored as FP32 hi + FP32 lo; stage inputs, accumulator and stage
+                       arithmetic in FP32 (coefficients as hi + lo pairs, the state update
+                       error-free on the hi + lo pair); a(t), H(t), reductions and spectra FP64 */
 } cf_precision;
 
 /* Flat parameter block (replaces the reference's POD Param + WorkspaceGeneric

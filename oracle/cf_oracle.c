@@ -66,6 +66,7 @@ double cfo_eta(const cfo_params *P, double t) {
 void cfo_psi_dpsidt_fft(int64_t N, const double *R_fft, double *Psi_fft, double *dPsidt_fft,
                         double factor, double H_t) {
   const int64_t nh = N / 2 + 1;
+#pragma omp parallel for schedule(static)
   for (int64_t a = 0; a < N; ++a)
     for (int64_t b = 0; b < N; ++b)
       for (int64_t c = 0; c < nh; ++c) {
@@ -205,6 +206,8 @@ void cfo_rhs(const cfo_params *P, const double *x, const double *R_fft, double t
     hs = sd / 2;
   }
   const double *phi = x, *pi = x + N3;
+  /* sites are independent: the a-planes are spread over OpenMP threads (same bits) */
+#pragma omp parallel for schedule(static)
   for (int64_t a = 0; a < N; ++a)
     for (int64_t b = 0; b < N; ++b)
       for (int64_t c = 0; c < N; ++c) {
@@ -259,13 +262,17 @@ void cfo_rk4_step(const cfo_params *P, double *x, const double *R_fft, double t,
   double *k2 = k1 + n, *k3 = k2 + n, *k4 = k3 + n, *y = k4 + n;
   const double dh = dt / 2.0, th = t + dh;
   cfo_rhs(P, x, R_fft, t, k1);
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < n; ++i) y[i] = 1.0 * x[i] + dh * k1[i];
   cfo_rhs(P, y, R_fft, th, k2);
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < n; ++i) y[i] = 1.0 * x[i] + dh * k2[i];
   cfo_rhs(P, y, R_fft, th, k3);
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < n; ++i) y[i] = 1.0 * x[i] + dt * k3[i];
   cfo_rhs(P, y, R_fft, t + dt, k4);
   const double dt6 = dt / 6.0, dt3 = dt / 3.0;
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < n; ++i)
     x[i] = 1.0 * x[i] + dt6 * k1[i] + dt3 * k2[i] + dt3 * k3[i] + dt6 * k4[i];
   free(k1);
@@ -304,6 +311,7 @@ void cfo_energy_density(const cfo_params *P, const double *x, const double *R_ff
     cfo_psi_fields(P, R_fft, t, Psi, NULL);
   }
   const double *phi = x, *pi = x + N3;
+#pragma omp parallel for schedule(static)
   for (int64_t a = 0; a < N; ++a)
     for (int64_t b = 0; b < N; ++b)
       for (int64_t c = 0; c < N; ++c) {

@@ -8,14 +8,16 @@ full-array sum; for the rho slice / axis average the first 4096 values and the
 sum.  The parity tests rebuild the same quantities with the oracles and compare
 on exactly these entries.
 
-Usage: python tests/golden/make_golden.py [path/to/reference]
+Usage: python tests/golden/make_golden.py <path/to/reference tree>
 """
 import os
 import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: make_golden.py <path/to/reference tree>")
+ref = sys.argv[1]
 src = os.path.join(ref, "output", "Growth_and_FS")
 out = {}
 for name in ["initial_R_spectrum", "initial_Psi_spectrum", "rho_spectrum_0", "varphi_plus_spectrum_0",

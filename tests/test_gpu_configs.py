@@ -1,0 +1,158 @@
+"""Parity at the benchmark configurations' own sizes.
+
+The fixtures in tests/golden/ were made by the reference's own CPU build
+(src/equations.cpp + Eigen + Boost.odeint RK4 + ConstIntervalObserver, FP64) and
+cross-checked against the C restatement (tests/golden/make_config_fixtures.py):
+
+* config 1: KleinGordonEquationInFRW, N = 256, L = 256, m = 1, radiation era,
+  RK4 dt = 0.05 for 1000 steps from t = 1, both observer spectra every
+  dt_save = 5 (src/observer.hpp:87-125), the spectra and a phi plane after the
+  last step;
+* config 2: ComovingCurvatureEquationInFRW, N = 512, L = 512, m = 1, 3 steps,
+  the density and mode power spectra and a phi plane.
+
+The inputs are regenerated here from their seeds (numpy) and checked against the
+checksums stored with the fixture before anything is compared.
+
+Tolerances (relative): FP64 fields and spectra <= 1e-12 (per bin over the bins
+>= 1e-10 of the largest); FP32_COMP density spectrum <= 1e-6 per bin after 1000
+steps (the FP32 hi + lo state's error budget), fields <= 1e-6.
+"""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import cfb200  # noqa: E402
+import oracle as O  # noqa: E402
+from cfb200 import fields  # noqa: E402
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FRW = dict(a1=1.0, H1=0.5, t1=1.0)
+FLOOR = 1e-10  # bins below FLOOR x the largest bin are not compared per bin
+
+
+def per_bin(a, b, floor=FLOOR):
+    a, b = np.asarray(a), np.asarray(b)
+    big = np.abs(b) >= floor * np.abs(b).max()
+    return float(np.max(np.abs(a[big] - b[big]) / np.abs(b[big])))
+
+
+def norm_rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+
+def _same_input(x, want):
+    got = np.array([x.sum(), (x * x).sum()])
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-12 * abs(want[1])), (got, want)
+
+
+def _shells(N, s2):
+    return O.shells_from_s2(N, s2)[0]
+
+
+@pytest.fixture(scope="module")
+def config1():
+    g = dict(np.load(os.path.join(GOLD, "config1_kgfrw_n256.npz")))
+    N = int(g["N"])
+    x0 = fields.initial_state(N, float(g["L"]), float(g["k_star"]), seed=int(g["seed"]))
+    _same_input(x0, g["input_checksum"])
+    return g, x0
+
+
+@pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP], ids=["fp64", "fp32comp"])
+def test_config1_kgfrw_n256_1000_steps_matches_reference(config1, prec):
+    """Both observer spectra at every save (unit shells) and, after step 1000, both
+    s^2 spectra and the a = 0 planes of phi and dphi against the reference's own
+    CPU run of the same configuration."""
+    g, x0 = config1
+    N, L, m, dt, t0 = int(g["N"]), float(g["L"]), float(g["m"]), float(g["dt"]), float(g["t0"])
+    P = O.make_params(N, L, m, eq=1, **FRW)
+    ctx = cfb200.Context(N, L, m=m, equation=cfb200.EQ_KG_FRW, precision=prec, stencil=7, **FRW)
+    st = torch.empty(ctx.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    ctx.upload(st, x0)
+    rho = torch.empty(ctx.info.s2_bins, dtype=torch.float64, device="cuda")
+    mode = torch.empty_like(rho)
+    fp64 = prec == cfb200.FP64
+    tol_spec = 1e-12 if fp64 else 1e-6
+    done, worst = 0, {"rho": 0.0, "varphi_plus": 0.0}
+    for i, (s, ts) in enumerate(zip(g["steps"], g["t_list"])):
+        ctx.rk4_steps(st, t0, dt, int(s) - done, step0=done)
+        done = int(s)
+        ctx.density_spectrum_s2(st, float(ts), rho)
+        ctx.mode_power_spectrum_s2(st, O.a_of_t(P, float(ts)), mode)
+        torch.cuda.synchronize()
+        for name, d in (("rho", rho), ("varphi_plus", mode)):
+            e = per_bin(_shells(N, d.cpu().numpy()), g[name + "_shells"][i])
+            worst[name] = max(worst[name], e)
+    nsteps = int(g["nsteps"])
+    ctx.rk4_steps(st, t0, dt, nsteps - done, step0=done)
+    t1 = float(g["t_final"])
+    ctx.density_spectrum_s2(st, t1, rho)
+    ctx.mode_power_spectrum_s2(st, O.a_of_t(P, t1), mode)
+    xs = np.empty(2 * N ** 3)
+    ctx.download(xs, st)
+    torch.cuda.synchronize()
+    e_rho = per_bin(rho.cpu().numpy(), g["rho_s2_final"])
+    e_mode = per_bin(mode.cpu().numpy(), g["varphi_plus_s2_final"])
+    e_phi = norm_rel(xs[: N * N], g["phi_plane0"])
+    e_dphi = norm_rel(xs[N ** 3: N ** 3 + N * N], g["dphi_plane0"])
+    print(f"config1 {'fp64' if fp64 else 'fp32comp'}: shells worst per bin rho {worst['rho']:.3e} "
+          f"varphi_plus {worst['varphi_plus']:.3e}; after {nsteps} steps s2 per bin rho {e_rho:.3e} "
+          f"varphi_plus {e_mode:.3e}; phi plane {e_phi:.3e}, dphi plane {e_dphi:.3e}")
+    assert worst["rho"] <= tol_spec and worst["varphi_plus"] <= tol_spec, worst
+    assert e_rho <= tol_spec and e_mode <= tol_spec, (e_rho, e_mode)
+    tol_f = 1e-12 if fp64 else 1e-6
+    assert e_phi <= tol_f and e_dphi <= tol_f, (e_phi, e_dphi)
+    ctx.close()
+
+
+@pytest.fixture(scope="module")
+def config2():
+    g = dict(np.load(os.path.join(GOLD, "config2_comoving_n512.npz")))
+    N, L = int(g["N"]), float(g["L"])
+    x0 = fields.initial_state(N, L, float(g["k_star"]), seed=int(g["seed"]))
+    _same_input(x0, g["input_checksum"])
+    eta0 = 2.0 * float(g["t0"]) ** 0.5
+    Rf = fields.curvature_R_fft(N, L, eta0, float(g["psi_rms"]), float(g["k_max"]), seed=int(g["R_seed"]))
+    _same_input(Rf, g["R_checksum"])
+    return g, x0, Rf
+
+
+@pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP], ids=["fp64", "fp32comp"])
+def test_config2_comoving_n512_matches_reference(config2, prec):
+    """The comoving-curvature equation at N = 512 (pruned Psi synthesis, whole-step
+    pass): density and mode power spectra and the a = 0 planes after 3 steps
+    against the reference's own CPU run."""
+    g, x0, Rf = config2
+    N, L, m, dt, t0 = int(g["N"]), float(g["L"]), float(g["m"]), float(g["dt"]), float(g["t0"])
+    ctx = cfb200.Context(N, L, m=m, equation=cfb200.EQ_COMOVING_FRW, precision=prec, stencil=7, **FRW)
+    ctx.set_R_fft(Rf, on_device=False)
+    st = torch.empty(ctx.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    ctx.upload(st, x0)
+    ctx.rk4_steps(st, t0, dt, int(g["nsteps"]))
+    t1 = float(g["t_final"])
+    rho = torch.empty(ctx.info.s2_bins, dtype=torch.float64, device="cuda")
+    mode = torch.empty_like(rho)
+    ctx.density_spectrum_s2(st, t1, rho)
+    P = O.make_params(N, L, m, eq=2, **FRW)
+    ctx.mode_power_spectrum_s2(st, O.a_of_t(P, t1), mode)
+    xs = np.empty(2 * N ** 3)
+    ctx.download(xs, st)
+    torch.cuda.synchronize()
+    route = int(ctx.info.psi_route)
+    e_rho = per_bin(rho.cpu().numpy(), g["rho_s2"])
+    e_sh = per_bin(_shells(N, rho.cpu().numpy()), g["rho_shells"])
+    e_mode = per_bin(mode.cpu().numpy(), g["varphi_plus_s2"])
+    e_phi = norm_rel(xs[: N * N], g["phi_plane0"])
+    e_dphi = norm_rel(xs[N ** 3: N ** 3 + N * N], g["dphi_plane0"])
+    fp64 = prec == cfb200.FP64
+    print(f"config2 {'fp64' if fp64 else 'fp32comp'} (psi route {route}): s2 per bin rho {e_rho:.3e}, "
+          f"shells {e_sh:.3e}, varphi_plus {e_mode:.3e}; phi plane {e_phi:.3e}, dphi plane {e_dphi:.3e}")
+    tol = 1e-12 if fp64 else 1e-6
+    assert max(e_rho, e_sh, e_mode) <= tol, (e_rho, e_sh, e_mode)
+    assert e_phi <= tol and e_dphi <= tol, (e_phi, e_dphi)
+    ctx.close()
