@@ -19,9 +19,15 @@
 //    buffer entry before reading it.  Calls whose GPU work overlaps (other
 //    streams, other host threads) race on the array and must be serialised by
 //    the caller.
-//  - The first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//  - The array is reserved when the library's device code is first loaded on a
+//    device.  With lazy module loading (the default since CUDA 12.2) that is the
+//    first call of this entry point there, so an application that hands its free
+//    device memory to its own pool makes one call first -- a call with
+//    nsteps = 0 does only this -- or runs with CUDA_MODULE_LOADING=EAGER.
+//  - A call outside stream capture looks up the array's device address
+//    (cudaGetSymbolAddress) with the context's device current, so the address
+//    stays right after a cudaDeviceReset; a call during capture uses the address
+//    of the last call outside capture, so make one such call before capturing.
 //  - Flat and FRW Klein-Gordon only: the comoving-curvature equation needs the
 //    Psi buffers and cuFFT plans, which allocate.
 
@@ -48,16 +54,20 @@ constexpr int kMaxDevices = 64;
 static void *g_scratch_dev[kMaxDevices];
 static std::mutex g_scratch_mu;
 
-// Device address of g_noalloc_scratch on the current device (looked up once per device).
-static int scratch_address(void **out) {
+// Device address of g_noalloc_scratch on the current device: looked up afresh
+// outside stream capture (a cudaDeviceReset may have moved it), the last address
+// seen on this device during capture.
+static int scratch_address(cudaStream_t st, void **out) {
   int dev = 0;
   CF_TRY_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("cf_rk4_steps_noalloc: device ordinal %d out of range", dev);
     return CF_ERR_INVALID;
   }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CF_TRY_CUDA(cudaStreamIsCapturing(st, &cs));
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_dev[dev]) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -65,6 +75,10 @@ static int scratch_address(void **out) {
       return CF_ERR_CUDA;
     }
     g_scratch_dev[dev] = p;
+  } else if (!g_scratch_dev[dev]) {
+    set_error("cf_rk4_steps_noalloc: first call on device %d made during stream capture; make one call "
+              "(nsteps = 0 suffices) before capturing", dev);
+    return CF_ERR_INVALID;
   }
   *out = g_scratch_dev[dev];
   return CF_OK;
@@ -100,11 +114,18 @@ extern "C" int cf_rk4_steps_noalloc(cf_ctx *ctx, void *d_state, double t0, doubl
               (long long)ctx->N, 3 * buf, kNoAllocScratchBytes);
     return CF_ERR_INVALID;
   }
+  // the context's device for the call; the caller's current device afterwards
+  int prev = 0;
+  CF_TRY_CUDA(cudaGetDevice(&prev));
+  struct Restore {
+    int dev;
+    ~Restore() { cudaSetDevice(dev); }
+  } restore{prev};
   CF_TRY_CUDA(cudaSetDevice(ctx->device));
-  void *base = nullptr;
-  CF_TRY(scratch_address(&base));
-  char *p = static_cast<char *>(base);
   cudaStream_t st = (cudaStream_t)stream;
+  void *base = nullptr;
+  CF_TRY(scratch_address(st, &base));
+  char *p = static_cast<char *>(base);
   for (int64_t j = 0; j < nsteps; ++j) {
     const double t = t0 + (double)(step0 + j) * dt;
     CF_TRY(rk4_step_buffers(ctx, d_state, p, p + buf, p + 2 * buf, t, dt, st));

@@ -266,6 +266,22 @@ __device__ __forceinline__ double e2m1_of(double psi) {
   return fma(q, x * x, x);
 }
 
+// The same for a pair of FP32 values (a complex entry of pass C's output) with the
+// sm_100 paired FP32 instructions (FADD2 / FMUL2 / FFMA2): one instruction per Horner
+// step for both values, each component rounded exactly as the scalar form above.
+__device__ __forceinline__ float2 e2m1_pair(float2 psi) {
+  const float2 x = __fadd2_rn(psi, psi);  // 2 psi, exact
+  if (fabsf(x.x) > 0.25f || fabsf(x.y) > 0.25f) return make_float2(e2m1_of(psi.x), e2m1_of(psi.y));
+  float2 q = make_float2(1.0f / 5040.0f, 1.0f / 5040.0f);
+  q = __ffma2_rn(q, x, make_float2(1.0f / 720.0f, 1.0f / 720.0f));
+  q = __ffma2_rn(q, x, make_float2(1.0f / 120.0f, 1.0f / 120.0f));
+  q = __ffma2_rn(q, x, make_float2(1.0f / 24.0f, 1.0f / 24.0f));
+  q = __ffma2_rn(q, x, make_float2(1.0f / 6.0f, 1.0f / 6.0f));
+  q = __ffma2_rn(q, x, make_float2(0.5f, 0.5f));
+  return __ffma2_rn(q, __fmul2_rn(x, x), x);
+}
+__device__ __forceinline__ double2 e2m1_pair(double2 psi) { return make_double2(e2m1_of(psi.x), e2m1_of(psi.y)); }
+
 template <typename S>
 __global__ void k_psi_to_e2m1(S *__restrict__ f, long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -293,6 +309,10 @@ template <typename C>
 __device__ __forceinline__ C c_mul_i(C a) {
   return C{-a.y, a.x};
 }
+// FP32 complex sums as one sm_100 paired instruction (FADD2) each: per component the
+// same round-to-nearest sum as the scalar form.
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 
 __host__ __device__ constexpr int bit_reverse(int i, int R) {
   int r = 0;
@@ -397,7 +417,7 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
 #pragma unroll
     for (int m2 = 0; m2 < R2; ++m2) {
       C o = u[m2];
-      if (f == 0) o = C{e2m1_of(o.x), e2m1_of(o.y)};  // the slot holds e^{2 Psi} - 1
+      if (f == 0) o = e2m1_pair(o);  // the slot holds e^{2 Psi} - 1
       row[m1 + R1 * m2] = o;
     }
   }
@@ -493,12 +513,190 @@ __global__ void __launch_bounds__(256) k_prune_c_fft_p(const S *__restrict__ pb,
 #pragma unroll
       for (int m2 = 0; m2 < R2; ++m2) {
         C o = u[m2];
-        if (f == 0) o = C{e2m1_of(o.x), e2m1_of(o.y)};  // the slot holds e^{2 Psi} - 1
+        if (f == 0) o = e2m1_pair(o);  // the slot holds e^{2 Psi} - 1
         row[m1 + R1 * m2] = o;
       }
     }
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ---- pass C, one warp per row group (FP32, N = 256, 512, 1024) --------------
+// The same four-step arithmetic as k_prune_c_fft without a CTA barrier: a warp owns
+// RW = 32 / R1 consecutive rows of one (f, a) plane and does everything for them --
+// copies the rows' Kc + 1 band entries into its own shared memory by cp.async (one
+// tile ahead, double-buffered), forms i X w^k, runs pass 1 (lane = (row, k2)) and
+// pass 2 (lane = (row, m1)) through a warp-private transpose with only __syncwarp
+// between them, and stores along the output rows.  Persistent: warps walk the tiles
+// (f, a, row group) with stride = warps in the grid, adjacent warps on adjacent rows
+// (their 8- or 16-byte input copies share sectors through L1).
+template <int R1, int R2, int B>
+__global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict__ pb, float *__restrict__ out,
+                                                     const float2 *__restrict__ wN, const float2 *__restrict__ twM,
+                                                     int N, int Kc, long long ntiles,
+                                                     const __grid_constant__ Tw32<float> tw) {
+  constexpr int M = R1 * R2;  // N == 2 M
+  constexpr int RW = 32 / R1;
+  constexpr int TP = R2 + 1;  // transpose row pitch (complex), odd: pass-2 reads free of bank conflicts
+  static_assert(RW >= 1 && R2 <= R1, "shape");
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *TW = reinterpret_cast<float2 *>(smraw);  // [R1][R2]: e^{2 pi i k2 m1 / M}
+  float2 *WK = TW + M;                             // [Kc+1]: w^k
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kn = Kc + 1;
+  const int xw = ((kn * RW + 1) & ~1);  // complex per X buffer, even (16-byte aligned)
+  float2 *W = WK + ((kn + 1) & ~1) + (size_t)warp * (3 * xw + RW * R1 * TP);
+  float2 *X0 = W, *XP = W + 2 * xw, *T = W + 3 * xw;  // X: 2 buffers [k][r]; XP [k][r]; T [r][m1][TP]
+  for (int i = threadIdx.x; i < M; i += blockDim.x) TW[i] = twM[i];
+  for (int i = threadIdx.x; i < kn; i += blockDim.x) WK[i] = wN[i];
+  __syncthreads();  // the only CTA barrier: the shared twiddles
+
+  const int groups = N / RW;  // row groups per (f, a) plane
+  const long long stride = (long long)gridDim.x * (blockDim.x >> 5);
+  long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+  auto issue = [&](long long t, float2 *dst) {
+    const int g = (int)(t % groups);
+    const long long fa = t / groups;  // f * N + a
+    const int a = (int)(fa % N), f = (int)(fa / N);
+    const float2 *src = reinterpret_cast<const float2 *>(pb) + ((long long)f * kn * N + a) * N + (long long)g * RW;
+    for (int k = lane; k < kn; k += 32) {
+      const unsigned d = (unsigned)__cvta_generic_to_shared(dst + k * RW);
+      if constexpr (RW == 2)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + (long long)k * N * N)
+                     : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src + (long long)k * N * N)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int buf = 0;
+  if (tile < ntiles) issue(tile, X0);
+  for (; tile < ntiles; tile += stride) {
+    if (tile + stride < ntiles) {
+      issue(tile + stride, X0 + (buf ^ 1) * xw);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncwarp();  // the tile's band entries (every lane's copies)
+    const float2 *X = X0 + buf * xw;
+    const int g = (int)(tile % groups);
+    const long long fa = tile / groups;
+    // i X w^k (X[0] by its real part: the Hermitian projection of every C2R)
+    for (int i = lane; i < kn * RW; i += 32) {
+      const int k = i / RW;
+      float2 x = X[i];
+      if (k == 0) x.y = 0.0f;
+      XP[i] = c_mul_i(c_mul(x, WK[k]));
+    }
+    __syncwarp();
+    // pass 1: lane (r, k2), an R1-point DFT over the band rows k1, times e^{2 pi i k2 m1 / M}
+    {
+      const int r = lane / R1, k2 = lane % R1;
+      if (k2 < R2) {
+        float2 v[R1];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+          const int k = k2 + R2 * k1;
+          float2 z = make_float2(0.0f, 0.0f);
+          if (k1 >= B && k1 < R1 - B) {
+            // outside the band's rows: zero
+          } else if (k <= Kc) {
+            float2 x = X[k * RW + r];
+            if (k == 0) x.y = 0.0f;
+            z = c_add(x, XP[k * RW + r]);  // X + i X w^k
+          } else if (k >= M - Kc) {
+            const int j = M - k;
+            const float2 d = c_sub(X[j * RW + r], XP[j * RW + r]);  // conj(X - i X w^j)
+            z = make_float2(d.x, -d.y);
+          }
+          v[k1] = z;
+        }
+        dft_inv<float, R1>(v, tw);
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) {
+          float2 y = v[m1];
+          if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
+          T[(r * R1 + m1) * TP + k2] = y;
+        }
+      }
+    }
+    __syncwarp();
+    // pass 2: lane (r, m1), an R2-point DFT over k2, giving z[m1 + R1 m2] of row r
+    {
+      const int r = lane / R1, m1 = lane % R1;
+      float2 u[R2];
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[(r * R1 + m1) * TP + k2];
+      dft_inv<float, R2>(u, tw);
+      const bool field0 = fa < N;  // f == 0: the slot holds e^{2 Psi} - 1
+      float2 *row = reinterpret_cast<float2 *>(out) + (fa * N + (long long)g * RW + r) * M;
+#pragma unroll
+      for (int m2 = 0; m2 < R2; ++m2) {
+        float2 o = u[m2];
+        if (field0) o = e2m1_pair(o);
+        row[m1 + R1 * m2] = o;
+      }
+    }
+    __syncwarp();  // T, XP and this X buffer are free for the next tile
+    buf ^= 1;
+  }
+}
+
+static bool pc_warp_shape(long long N, size_t word, int *R1, int *R2) {
+  if (word != 4) return false;
+  switch (N) {
+    case 256: *R1 = 16, *R2 = 8; return true;
+    case 512: *R1 = 16, *R2 = 16; return true;
+    case 1024: *R1 = 32, *R2 = 16; return true;
+    default: return false;
+  }
+}
+static size_t pc_warp_smem(int Kc, int R1, int R2) {
+  const int RW = 32 / R1, kn = Kc + 1, xw = (kn * RW + 1) & ~1;
+  return ((size_t)R1 * R2 + ((kn + 1) & ~1) + 8 * (size_t)(3 * xw + RW * R1 * (R2 + 1))) * sizeof(float2);
+}
+
+template <int R1, int R2, int B>
+static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+  auto kern = k_prune_c_warp<R1, R2, B>;
+  if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Tw32<float> tw;
+  for (int e = 0; e < 16; ++e) {
+    const double ang = 2.0 * 3.14159265358979323846 * e / 32.0;
+    tw.w[e] = float2{(float)std::cos(ang), (float)std::sin(ang)};
+  }
+  int sms = 0, per_sm = 0;
+  CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+  const int N = (int)ctx->N;
+  const long long ntiles = 2LL * N * (N / (32 / R1));
+  const long long grid = std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)sms * std::max(per_sm, 1)));
+  kern<<<(unsigned)grid, 256, smem, st>>>((const float *)ctx->pz_b, (float *)out, (const float2 *)ctx->pr_wN,
+                                          (const float2 *)ctx->pr_twM, N, ctx->Kc, ntiles, tw);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+// The smallest compiled band B >= ceil((Kc+1)/R2).
+template <int R1, int R2>
+static int launch_pc_warp_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+  const int need = (ctx->Kc + 1 + R2 - 1) / R2;
+  if (need <= 2) return launch_pc_warp_b<R1, R2, 2>(ctx, out, smem, st);
+  if (need <= 3) return launch_pc_warp_b<R1, R2, 3>(ctx, out, smem, st);
+  if (need <= 4) return launch_pc_warp_b<R1, R2, 4>(ctx, out, smem, st);
+  if (need <= 6) return launch_pc_warp_b<R1, R2, 6>(ctx, out, smem, st);
+  return launch_pc_warp_b<R1, R2, R1 / 2>(ctx, out, smem, st);
+}
+
+static int launch_pc_warp(cf_ctx *ctx, void *out, cudaStream_t st) {
+  int R1 = 0, R2 = 0;
+  if (!pc_warp_shape(ctx->N, ctx->word, &R1, &R2)) return set_error("warp pass C: unsupported N"), CF_ERR_INVALID;
+  const size_t smem = pc_warp_smem(ctx->Kc, R1, R2);
+  if (R1 == 16 && R2 == 8) return launch_pc_warp_t<16, 8>(ctx, out, smem, st);
+  if (R1 == 16 && R2 == 16) return launch_pc_warp_t<16, 16>(ctx, out, smem, st);
+  return launch_pc_warp_t<32, 16>(ctx, out, smem, st);
 }
 
 // ---- pass B as one kernel: pruned lines -> full lines -----------------------
@@ -961,6 +1159,10 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
   }
   if (ctx->pc_fused) {
     ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+    int R1 = 0, R2 = 0;
+    if (!(ctx->p.flags & CF_FLAG_PSI_CTA_PASS_C) && pc_warp_shape(ctx->N, ctx->word, &R1, &R2) &&
+        pc_warp_smem(ctx->Kc, R1, R2) <= kPcFusedSmemMax)
+      return launch_pc_warp(ctx, out, st);
     return launch_pc_fused<S>(ctx, out, st);
   }
   {

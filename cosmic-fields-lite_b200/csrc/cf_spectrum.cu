@@ -32,24 +32,28 @@ namespace cfb {
 enum EdKind : int { ED_QUAD = 0, ED_LAMBDA = 1, ED_SQRT = 2, ED_CURV = 3 };
 
 template <typename S, int ED>
-__global__ void k_energy(const S *__restrict__ x, const S *__restrict__ xlo, const S *__restrict__ psi,
-                         double *__restrict__ rho, int N, double m2, double inv, double q) {
+__global__ void __launch_bounds__(128) k_energy(const S *__restrict__ x, const S *__restrict__ xlo,
+                                                const S *__restrict__ psi, double *__restrict__ rho, int N, double m2,
+                                                double inv, double q) {
+  // one lattice row (a, b) per block, threads along c: the row's neighbour rows are
+  // found once, only c wraps per site
   const long long N3 = (long long)N * N * N;
   const long long NN = (long long)N * N;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  const int a = (int)(blockIdx.x / (unsigned)N), b = (int)(blockIdx.x - (unsigned)a * (unsigned)N);
+  const long long row = NN * a + (long long)N * b;
+  const long long rap = NN * (a + 1 == N ? 0 : a + 1) + (long long)N * b;
+  const long long ram = NN * (a == 0 ? N - 1 : a - 1) + (long long)N * b;
+  const long long rbp = NN * a + (long long)N * (b + 1 == N ? 0 : b + 1);
+  const long long rbm = NN * a + (long long)N * (b == 0 ? N - 1 : b - 1);
   auto phi = [&](long long i) -> double {
     double v = (double)x[i];
     if (xlo) v += (double)xlo[i];
     return v;
   };
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N3; i += stride) {
-    const int c = (int)(i % N);
-    const int b = (int)((i / N) % N);
-    const int a = (int)(i / NN);
-    const long long ap = NN * ((a + 1) % N) + (long long)N * b + c, am = NN * ((a + N - 1) % N) + (long long)N * b + c;
-    const long long bp = NN * a + (long long)N * ((b + 1) % N) + c, bm = NN * a + (long long)N * ((b + N - 1) % N) + c;
-    const long long cp = NN * a + (long long)N * b + (c + 1) % N, cm = NN * a + (long long)N * b + (c + N - 1) % N;
-    const double dx = phi(ap) - phi(am), dy = phi(bp) - phi(bm), dz = phi(cp) - phi(cm);
+  for (int c = threadIdx.x; c < N; c += blockDim.x) {
+    const long long i = row + c;
+    const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
+    const double dx = phi(rap + c) - phi(ram + c), dy = phi(rbp + c) - phi(rbm + c), dz = phi(row + cp) - phi(row + cm);
     const double grad = dx * dx + dy * dy + dz * dz;
     const double f = phi(i);
     double p = (double)x[N3 + i];
@@ -170,18 +174,75 @@ __device__ __forceinline__ void decode_mode(int N, long long i, int &c, long lon
   s2 = as * as + bs * bs + (long long)c * c;
 }
 
-__global__ void k_spec_max(const SpecIn A, long long pairs, unsigned long long *maxbits) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
+// ---- orbits of the binning ---------------------------------------------------
+// The HC rows (a, b) whose modes share s^2 at every c: a in {as, N - as}, b in
+// {bs, N - bs} and, for as != bs, the same with a and b swapped, 0 <= as <= bs <=
+// N/2 -- up to 8 rows, and every row lies in exactly one orbit.  A warp takes one
+// orbit and its lanes the c values, so the reads are coalesced along c; a lane sums
+// the 128-bit fixed-point words of its modes in registers and adds the sum to the
+// bin with one pair of 64-bit atomics.  Integer addition is associative, so a bin
+// is the same integer as with one atomic pair per mode, at an eighth of the atomics
+// (a quarter on the axes).
+struct Orbit {
+  int as, bs, na, nb, n;  // na, nb: 1 on an axis (0 or N/2), else 2; n rows
+  long long ab2;          // as^2 + bs^2
+};
+
+__device__ __forceinline__ long long orbit_count(int N) { return (long long)(N / 2 + 1) * (N / 2 + 2) / 2; }
+
+// Orbit o = bs (bs + 1) / 2 + as (0 <= as <= bs <= N/2).
+__device__ __forceinline__ bool orbit_of(int N, long long o, Orbit &ob) {
+  const int h = N / 2;
+  if (o >= orbit_count(N)) return false;
+  int bs = (int)((sqrt(8.0 * (double)o + 1.0) - 1.0) * 0.5);
+  while ((long long)(bs + 1) * (bs + 2) / 2 <= o) ++bs;
+  while ((long long)bs * (bs + 1) / 2 > o) --bs;
+  ob.as = (int)(o - (long long)bs * (bs + 1) / 2);
+  ob.bs = bs;
+  ob.na = (ob.as == 0 || ob.as == h) ? 1 : 2;
+  ob.nb = (bs == 0 || bs == h) ? 1 : 2;
+  ob.n = ob.na * ob.nb * (ob.as != bs ? 2 : 1);
+  ob.ab2 = (long long)ob.as * ob.as + (long long)bs * bs;
+  return true;
+}
+
+// Row a N + b of the orbit's r-th row (r < n): first a in {as, N - as} with b in {bs,
+// N - bs}, then (as != bs) a in {bs, N - bs} with b in {as, N - as}.
+__device__ __forceinline__ long long orbit_row(const Orbit &ob, int r, int N) {
+  const int m = ob.na * ob.nb;
+  int a, b;
+  if (r < m) {
+    const int i = ob.nb == 2 ? r >> 1 : r, j = ob.nb == 2 ? r & 1 : 0;
+    a = i ? N - ob.as : ob.as;
+    b = j ? N - ob.bs : ob.bs;
+  } else {
+    const int q = r - m;
+    const int i = ob.na == 2 ? q >> 1 : q, j = ob.na == 2 ? q & 1 : 0;
+    a = i ? N - ob.bs : ob.bs;
+    b = j ? N - ob.as : ob.as;
+  }
+  return (long long)a * N + b;
+}
+
+// Largest weighted mode value (blockIdx.y: batch entry, HC arrays hc_count apart).
+__global__ void __launch_bounds__(256) k_spec_max(SpecIn A, long long hc_count, unsigned long long *maxbits) {
+  A.f += (long long)blockIdx.y * hc_count;
+  Orbit ob;
+  if (!orbit_of(A.N, (long long)blockIdx.x * 8 + (threadIdx.x >> 5), ob)) return;  // whole warps
+  const int nh = A.N / 2 + 1;
+  long long rows[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) rows[r] = r < ob.n ? orbit_row(ob, r, A.N) * nh : 0;
   double m = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
-    int c;
-    long long s2;
-    decode_mode(A.N, i, c, s2);
-    m = fmax(m, mode_value(A, i, c, s2));
+  for (int c = threadIdx.x & 31; c < nh; c += 32) {
+    const long long s2 = ob.ab2 + (long long)c * c;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      if (r < ob.n) m = fmax(m, mode_value(A, rows[r] + c, c, s2));
   }
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
   // non-negative doubles order like their bit patterns
-  if ((threadIdx.x & 31) == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(m));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits + blockIdx.y, (unsigned long long)__double_as_longlong(m));
 }
 
 // Power-of-two exponent e with (max * entries) * 2^e <= 2^126.
@@ -193,23 +254,54 @@ __device__ __forceinline__ int fixed_exponent(unsigned long long maxbits, long l
   return 126 - ex;
 }
 
-__global__ void k_spec_bin(const SpecIn A, long long pairs, const unsigned long long *maxbits,
-                           unsigned long long *bins) {
-  const int e = fixed_exponent(*maxbits, pairs);
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
-    int c;
-    long long s2;
-    decode_mode(A.N, i, c, s2);
-    const double y = ldexp(mode_value(A, i, c, s2), e);
-    const unsigned long long hi = __double2ull_rz(ldexp(y, -64));
-    const unsigned long long lo = __double2ull_rz(y - ldexp((double)hi, 64));
-    unsigned long long carry = 0;
-    if (lo) {
-      const unsigned long long old = atomicAdd(&bins[2 * s2], lo);
-      carry = (old + lo < old) ? 1ull : 0ull;
-    }
-    if (hi + carry) atomicAdd(&bins[2 * s2 + 1], hi + carry);
+// One mode value as a 128-bit fixed-point word (lo, hi) at scale 2^e, truncated.
+__device__ __forceinline__ void to_fixed(double v, int e, unsigned long long &lo, unsigned long long &hi) {
+  const double y = ldexp(v, e);
+  hi = __double2ull_rz(ldexp(y, -64));
+  lo = __double2ull_rz(y - ldexp((double)hi, 64));
+}
+
+// (lo, hi) += (l, h), 128-bit.
+__device__ __forceinline__ void add128(unsigned long long &lo, unsigned long long &hi, unsigned long long l,
+                                       unsigned long long h) {
+  const unsigned long long nl = lo + l;
+  hi += h + (nl < lo ? 1ull : 0ull);
+  lo = nl;
+}
+
+__device__ __forceinline__ void atomic_add128(unsigned long long *bin, unsigned long long lo, unsigned long long hi) {
+  unsigned long long carry = 0;
+  if (lo) {
+    const unsigned long long old = atomicAdd(bin, lo);
+    carry = (old + lo < old) ? 1ull : 0ull;
+  }
+  if (hi + carry) atomicAdd(bin + 1, hi + carry);
+}
+
+// Bins of the weighted mode values (blockIdx.y: batch entry; bins 2 nb words apart).
+__global__ void __launch_bounds__(256) k_spec_bin(SpecIn A, long long hc_count, long long pairs,
+                                                  const unsigned long long *maxbits, unsigned long long *bins,
+                                                  long long nb) {
+  A.f += (long long)blockIdx.y * hc_count;
+  bins += 2 * nb * (long long)blockIdx.y;
+  Orbit ob;
+  if (!orbit_of(A.N, (long long)blockIdx.x * 8 + (threadIdx.x >> 5), ob)) return;
+  const int e = fixed_exponent(maxbits[blockIdx.y], pairs);
+  const int nh = A.N / 2 + 1;
+  long long rows[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) rows[r] = r < ob.n ? orbit_row(ob, r, A.N) * nh : 0;
+  for (int c = threadIdx.x & 31; c < nh; c += 32) {
+    const long long s2 = ob.ab2 + (long long)c * c;
+    unsigned long long lo = 0, hi = 0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      if (r < ob.n) {
+        unsigned long long l, h;
+        to_fixed(mode_value(A, rows[r] + c, c, s2), e, l, h);
+        add128(lo, hi, l, h);
+      }
+    atomic_add128(bins + 2 * s2, lo, hi);
   }
 }
 
@@ -252,57 +344,14 @@ __global__ void k_shells(const unsigned long long *bins, const unsigned long lon
   }
 }
 
-__global__ void k_s2_counts(int N, long long pairs, unsigned long long *counts) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
-    int c;
-    long long s2;
-    decode_mode(N, i, c, s2);
-    atomicAdd(&counts[s2], (c == 0 || 2 * c == N) ? 1ull : 2ull);
-  }
+__global__ void __launch_bounds__(256) k_s2_counts(int N, unsigned long long *counts) {
+  Orbit ob;
+  if (!orbit_of(N, (long long)blockIdx.x * 8 + (threadIdx.x >> 5), ob)) return;
+  for (int c = threadIdx.x & 31; c <= N / 2; c += 32)
+    atomicAdd(&counts[ob.ab2 + (long long)c * c], (unsigned long long)ob.n * ((c == 0 || 2 * c == N) ? 1ull : 2ull));
 }
 
 // ---- batched binning (blockIdx.y = batch entry; used by ensembles) ----------
-__global__ void k_specb_max(const double *hc, long long hc_count, int N, long long pairs, unsigned long long *maxbits) {
-  SpecIn A{};
-  A.f = hc + (long long)blockIdx.y * hc_count;
-  A.N = N;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  double m = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
-    int c;
-    long long s2;
-    decode_mode(N, i, c, s2);
-    m = fmax(m, mode_value(A, i, c, s2));
-  }
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(maxbits + blockIdx.y, (unsigned long long)__double_as_longlong(m));
-}
-
-__global__ void k_specb_bin(const double *hc, long long hc_count, int N, long long pairs,
-                            const unsigned long long *maxbits, unsigned long long *bins, long long nb) {
-  SpecIn A{};
-  A.f = hc + (long long)blockIdx.y * hc_count;
-  A.N = N;
-  unsigned long long *bb = bins + 2 * nb * blockIdx.y;
-  const int e = fixed_exponent(maxbits[blockIdx.y], pairs);
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
-    int c;
-    long long s2;
-    decode_mode(N, i, c, s2);
-    const double y = ldexp(mode_value(A, i, c, s2), e);
-    const unsigned long long hi = __double2ull_rz(ldexp(y, -64));
-    const unsigned long long lo = __double2ull_rz(y - ldexp((double)hi, 64));
-    unsigned long long carry = 0;
-    if (lo) {
-      const unsigned long long old = atomicAdd(&bb[2 * s2], lo);
-      carry = (old + lo < old) ? 1ull : 0ull;
-    }
-    if (hi + carry) atomicAdd(&bb[2 * s2 + 1], hi + carry);
-  }
-}
-
 __global__ void k_specb_final(const unsigned long long *bins, const unsigned long long *maxbits, long long pairs,
                               double *out, long long nb) {
   const int e = fixed_exponent(maxbits[blockIdx.y], pairs);
@@ -313,15 +362,24 @@ __global__ void k_specb_final(const unsigned long long *bins, const unsigned lon
     o[s] = fixed_to_double(bb[2 * s], bb[2 * s + 1], e);
 }
 
+// Blocks of 8 warps, one orbit per warp.
+static unsigned orbit_blocks(int N) {
+  const long long norb = (long long)(N / 2 + 1) * (N / 2 + 2) / 2;
+  return (unsigned)((norb + 7) / 8);
+}
+
 int bin_batched(const double *hc, int N, int batch, unsigned long long *maxbits, unsigned long long *bins, double *out,
                 long long nb, cudaStream_t st, cf_ctx *) {
   const long long hc_count = 2LL * N * N * (N / 2 + 1), pairs = hc_count / 2;
   CF_TRY_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned long long) * batch, st));
   CF_TRY_CUDA(cudaMemsetAsync(bins, 0, sizeof(unsigned long long) * 2 * nb * batch, st));
-  const unsigned gx = (unsigned)std::min<long long>((pairs + 255) / 256, 148LL * 8);
-  k_specb_max<<<dim3(gx, batch), 256, 0, st>>>(hc, hc_count, N, pairs, maxbits);
+  SpecIn A{};
+  A.f = hc;
+  A.N = N;
+  const unsigned gx = orbit_blocks(N);
+  k_spec_max<<<dim3(gx, batch), 256, 0, st>>>(A, hc_count, maxbits);
   CF_TRY_CUDA(cudaGetLastError());
-  k_specb_bin<<<dim3(gx, batch), 256, 0, st>>>(hc, hc_count, N, pairs, maxbits, bins, nb);
+  k_spec_bin<<<dim3(gx, batch), 256, 0, st>>>(A, hc_count, pairs, maxbits, bins, nb);
   CF_TRY_CUDA(cudaGetLastError());
   const unsigned gf = (unsigned)std::min<long long>((nb + 255) / 256, 148LL * 8);
   k_specb_final<<<dim3(gf, batch), 256, 0, st>>>(bins, maxbits, pairs, out, nb);
@@ -354,7 +412,7 @@ int ensure_spectrum_scratch(cf_ctx *ctx, int nfields) {
       return CF_ERR_NOMEM;
     }
     CF_TRY_CUDA(cudaMemset(ctx->s2_counts, 0, (size_t)ctx->s2_bins * sizeof(int64_t)));
-    k_s2_counts<<<grid_for(hc / 2), 256>>>((int)ctx->N, (long long)(hc / 2), (unsigned long long *)ctx->s2_counts);
+    k_s2_counts<<<orbit_blocks((int)ctx->N), 256>>>((int)ctx->N, (unsigned long long *)ctx->s2_counts);
     CF_LAUNCHED(ctx);
     CF_TRY_CUDA(cudaMemset(ctx->bins, 0, 2 * (size_t)ctx->s2_bins * sizeof(unsigned long long)));
     CF_TRY_CUDA(cudaMemset(ctx->maxbits, 0, sizeof(unsigned long long)));
@@ -392,9 +450,9 @@ static int bin_spectrum(cf_ctx *ctx, bool mode, double a_t, double *d_out, cudaS
   ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
   CF_TRY_CUDA(cudaMemsetAsync(ctx->maxbits, 0, sizeof(unsigned long long), st));
   CF_TRY_CUDA(cudaMemsetAsync(ctx->bins, 0, 2 * (size_t)ctx->s2_bins * sizeof(unsigned long long), st));
-  k_spec_max<<<grid_for(pairs), 256, 0, st>>>(A, pairs, ctx->maxbits);
+  k_spec_max<<<orbit_blocks(A.N), 256, 0, st>>>(A, 0, ctx->maxbits);
   CF_LAUNCHED(ctx);
-  k_spec_bin<<<grid_for(pairs), 256, 0, st>>>(A, pairs, ctx->maxbits, ctx->bins);
+  k_spec_bin<<<orbit_blocks(A.N), 256, 0, st>>>(A, 0, pairs, ctx->maxbits, ctx->bins, ctx->s2_bins);
   CF_LAUNCHED(ctx);
   if (d_out) {
     k_spec_final<<<grid_for(ctx->s2_bins), 256, 0, st>>>(ctx->bins, ctx->maxbits, pairs, d_out, ctx->s2_bins);
@@ -444,7 +502,7 @@ static void launch_energy(cf_ctx *ctx, const void *d_state, const void *psi, dou
                           double q, cudaStream_t st) {
   const long long N3 = ctx->N3;
   const S *x = (const S *)d_state;
-  k_energy<S, ED><<<grid_for(N3), 256, 0, st>>>(x, sizeof(S) == 4 ? x + 2 * N3 : nullptr, (const S *)psi, d_rho,
+  k_energy<S, ED><<<(unsigned)(ctx->N * ctx->N), 128, 0, st>>>(x, sizeof(S) == 4 ? x + 2 * N3 : nullptr, (const S *)psi, d_rho,
                                                 (int)ctx->N, m2, inv, q);
 }
 

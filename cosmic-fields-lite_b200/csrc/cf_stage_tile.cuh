@@ -21,6 +21,8 @@
 
 #include <cuda_runtime.h>
 
+#include "cf_f32x2.cuh"
+
 namespace cfb {
 
 // A thread's consecutive sites along c, moved as one vector: V = 4 floats or 2
@@ -146,26 +148,19 @@ template <>
 struct Coef<float> {
   float hi, lo;
   __host__ __device__ Coef(double c) : hi((float)c), lo((float)(c - (double)(float)c)) {}
-  // c v with the product's error random (hi v + lo v)
-  __device__ __forceinline__ float mul(float v) const { return fmaf(hi, v, lo * v); }
+  // c v with the product's error random (hi v + lo v); the same operations as c_mul /
+  // c_fma of cf_f32x2.cuh
+  __device__ __forceinline__ float mul(float v) const { return __fmaf_rn(hi, v, __fmul_rn(lo, v)); }
   // add + c v
-  __device__ __forceinline__ float fma(float v, float add) const { return add + fmaf(hi, v, lo * v); }
+  __device__ __forceinline__ float fma(float v, float add) const { return __fadd_rn(add, mul(v)); }
+  __device__ __forceinline__ CoefL<float> lane() const { return CoefL<float>{hi, lo}; }
 };
 
-// FP32_COMP state update hi + lo + c s as a normalised hi + lo pair, in FP32 alone:
-// the product c s exactly as p + pe (FMA), hi + p exactly as t + e (TwoSum, Knuth),
-// the small parts added, and the pair renormalised (Fast2Sum, |t| >= |e|).  The
-// explicit round-to-nearest intrinsics keep the compiler from contracting or
-// reassociating the error terms.
+// FP32_COMP state update hi + lo + c s as a normalised hi + lo pair (comp_update_f32 of
+// cf_f32x2.cuh: error-free product and TwoSum, the small parts added, Fast2Sum).
 __device__ __forceinline__ void comp_update(float hi, float lo, float s, const Coef<float> &c, float &oh,
                                             float &ol) {
-  const float p = __fmul_rn(c.hi, s);
-  const float pe = __fmaf_rn(c.lo, s, __fmaf_rn(c.hi, s, -p));
-  const float t = __fadd_rn(hi, p);
-  const float z = __fsub_rn(t, hi);
-  const float e = __fadd_rn(__fadd_rn(__fsub_rn(hi, __fsub_rn(t, z)), __fsub_rn(p, z)), __fadd_rn(lo, pe));
-  oh = __fadd_rn(t, e);
-  ol = __fsub_rn(e, __fsub_rn(oh, t));
+  comp_update_f32<float>(hi, lo, s, c.lane(), oh, ol);
 }
 
 // x += dt/6 s (RK4's last combination): FP64 directly; FP32_COMP on the hi + lo pair.
@@ -191,7 +186,24 @@ __device__ __forceinline__ void psi_factors(double e2m1, double &e2, double &e4)
 template <typename S, int H, int SP, int V, typename T = typename Arith<S>::T>
 __device__ __forceinline__ T lap_at(const Pack<S, V> (&q)[2 * H + 1], const S *sm, int row, int col, int v) {
   const T f0 = (T)q[H].v[v];
-  if constexpr (H == 1) {
+  if constexpr (sizeof(T) == 4) {  // FP32: the fixed operation order of cf_f32x2.cuh
+    if constexpr (H == 1) {
+      return lap7_f32<float>(f0, q[2].v[v], q[0].v[v], sm[(row + 1) * SP + col], sm[(row - 1) * SP + col],
+                             sm[row * SP + col + 1], sm[row * SP + col - 1]);
+    } else {
+      float s1 = p_add(q[3].v[v], q[1].v[v]);
+      s1 = p_add(s1, sm[(row + 1) * SP + col]);
+      s1 = p_add(s1, sm[(row - 1) * SP + col]);
+      s1 = p_add(s1, sm[row * SP + col + 1]);
+      s1 = p_add(s1, sm[row * SP + col - 1]);
+      float s2 = p_add(q[4].v[v], q[0].v[v]);
+      s2 = p_add(s2, sm[(row + 2) * SP + col]);
+      s2 = p_add(s2, sm[(row - 2) * SP + col]);
+      s2 = p_add(s2, sm[row * SP + col + 2]);
+      s2 = p_add(s2, sm[row * SP + col - 2]);
+      return lap13_f32<float>(f0, s1, s2);
+    }
+  } else if constexpr (H == 1) {
     const T s = (T)-6 * f0 + (T)q[2].v[v] + (T)q[0].v[v] + (T)sm[(row + 1) * SP + col] + (T)sm[(row - 1) * SP + col];
     return s + ((T)sm[row * SP + col + 1] + (T)sm[row * SP + col - 1]);
   } else {
@@ -309,29 +321,13 @@ __device__ __forceinline__ T kpi_of(T p0, T f0, T lap, const Coupling<S, V> &cp,
     } else {
       return -k.hub3.hi * p0 - k.m2.hi * f0 + k.inv.hi * lap;
     }
-  } else {
-    const float mf = k.m2.mul(f0);
-    const float g = k.inv.mul(lap);
-    if constexpr (EQ == EQ_COMOV || EQ == EQ_FIXED || EQ == EQ_APPROX) {
-      const float e2m1 = (float)cp.ps.v[v];
-      // e^{4Psi} - 1 = (e^{2Psi} - 1)(e^{2Psi} + 1); the approximate equation's own quadratic
-      const float e4m1 = (EQ == EQ_APPROX) ? (float)cp.ps4.v[v] : e2m1 * (e2m1 + 2.0f);
-      const float fr = (EQ == EQ_FIXED) ? -k.hub3.mul(p0) : 4.0f * (float)cp.dps.v[v] * p0 - k.hub3.mul(p0);
-      return fr - fmaf(e2m1, mf, mf) + fmaf(e4m1, g, g);
-    } else if constexpr (EQ == EQ_LAMBDA) {
-      return -k.hub3.mul(p0) - mf - k.q1.mul(f0 * f0 * f0) + g;
-    } else if constexpr (EQ == EQ_SQRT) {
-      // m^2 phi / sqrt(y), y = 1 + phi^2 / f_a^2: rsqrtf refined by one Newton step
-      // r <- r + r (1 - y r^2) / 2, which leaves r within a fraction of an ulp of
-      // 1/sqrt(y) (rounding errors that average out, like those of the other terms)
-      const float y = 1.0f + k.q2.mul(f0 * f0);
-      const float r0 = rsqrtf(y);
-      const float e = fmaf(-y * r0, r0, 1.0f);
-      const float r = fmaf(0.5f * r0, e, r0);
-      return -k.hub3.mul(p0) - mf * r + g;
-    } else {
-      return -k.hub3.mul(p0) - mf + g;
-    }
+  } else {  // FP32: kpi_f32 of cf_f32x2.cuh, one site
+    const StageCoefL<float> kl{k.m2.lane(), k.inv.lane(), k.hub3.lane(), k.q1.lane(), k.q2.lane()};
+    float ps = 0.0f, dps = 0.0f, ps4 = 0.0f;
+    if constexpr (EqOf<EQ>::coupled) ps = (float)cp.ps.v[v];
+    if constexpr (EQ == EQ_COMOV || EQ == EQ_APPROX) dps = (float)cp.dps.v[v];
+    if constexpr (EQ == EQ_APPROX) ps4 = (float)cp.ps4.v[v];
+    return kpi_f32<EQ, float>(p0, f0, lap, ps, dps, ps4, kl);
   }
 }
 

@@ -79,8 +79,12 @@ struct StepSmem {
 // 7-point Laplacian sum in the order of lap_at: (-6 f0 + a+ + a- + b+ + b-) + (c+ + c-)
 template <typename T>
 __device__ __forceinline__ T lap7(T f0, T ap, T am, T bp, T bm, T cp, T cm) {
-  const T s = (T)-6 * f0 + ap + am + bp + bm;
-  return s + (cp + cm);
+  if constexpr (sizeof(T) == 4) {
+    return lap7_f32<float>(f0, ap, am, bp, bm, cp, cm);
+  } else {
+    const T s = (T)-6 * f0 + ap + am + bp + bm;
+    return s + (cp + cm);
+  }
 }
 
 // Curvature values of one site (a ring site of phase 1).
@@ -107,6 +111,11 @@ __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// A hint that brings `bytes` (a multiple of 16, 16-byte aligned, inside an allocation)
+// from global memory into L2 without occupying registers or shared memory.
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -152,6 +161,39 @@ __device__ __forceinline__ T lap_of(const Star<T> &s) {
   return lap7<T>(s.f0, s.ap, s.am, s.bp, s.bm, s.cp, s.cm);
 }
 
+// FP32: the stencil of sites (2l, 2l+1) of a row's four as lane pairs (cf_f32x2.cuh).
+// The c-neighbours pair across the vector: lane 0 takes (c1, c2) and (l, c0), lane 1
+// (c3, r) and (c1, c2).
+template <int SP>
+__device__ __forceinline__ Star<float2> star2(const RowStar<float, 4, SP> &R, int l) {
+  const int v = 2 * l;
+  return Star<float2>{make_float2(R.c.v[v], R.c.v[v + 1]), make_float2(R.a.v[v], R.a.v[v + 1]),
+                      make_float2(R.b.v[v], R.b.v[v + 1]), make_float2(R.n.v[v], R.n.v[v + 1]),
+                      make_float2(R.s.v[v], R.s.v[v + 1]),
+                      make_float2(R.c.v[v + 1], l == 0 ? R.c.v[2] : R.r),
+                      make_float2(l == 0 ? R.l : R.c.v[1], R.c.v[v])};
+}
+__device__ __forceinline__ float2 lap_of2(const Star<float2> &s) {
+  return lap7_f32<float2>(s.f0, s.ap, s.am, s.bp, s.bm, s.cp, s.cm);
+}
+template <int V>
+__device__ __forceinline__ float2 lane2(const Pack<float, V> &p, int l) {
+  return make_float2(p.v[2 * l], p.v[2 * l + 1]);
+}
+template <int V>
+__device__ __forceinline__ void set2(Pack<float, V> &p, int l, float2 x) {
+  p.v[2 * l] = x.x;
+  p.v[2 * l + 1] = x.y;
+}
+// The curvature lanes of a stage (ps, dps, ps4 of kpi_f32; zero where the equation has none).
+template <int EQ, int V>
+__device__ __forceinline__ void coupling2(const Coupling<float, V> &c, int l, float2 &ps, float2 &dps, float2 &ps4) {
+  ps = dps = ps4 = make_float2(0.0f, 0.0f);
+  if constexpr (EqOf<EQ>::coupled) ps = lane2(c.ps, l);
+  if constexpr (EQ == EQ_COMOV || EQ == EQ_APPROX) dps = lane2(c.dps, l);
+  if constexpr (EQ == EQ_APPROX) ps4 = lane2(c.ps4, l);
+}
+
 // ya_phi = x_phi + dt/2 x_pi at each point of a stencil (the stored stage input of the
 // paired kernels, formed here where it is needed).
 template <typename S, typename T>
@@ -192,6 +234,11 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
   const StageCoef<T> k4c{Coef<T>(A.m2), Coef<T>(A.inv[2]), Coef<T>(A.hub3[2]), Coef<T>(A.q1), Coef<T>(A.q2)};
   const Coef<T> ch(A.dt2), cf(A.dt);
   const Coef<T> c6(A.dt6);
+  // FP32: the same coefficients as lane pairs for the paired arithmetic
+  const C2 M2p = coef_f32x2(A.m2), Q1p = coef_f32x2(A.q1), Q2p = coef_f32x2(A.q2);
+  const C2 INVp[3] = {coef_f32x2(A.inv[0]), coef_f32x2(A.inv[1]), coef_f32x2(A.inv[2])};
+  const C2 HUBp[3] = {coef_f32x2(A.hub3[0]), coef_f32x2(A.hub3[1]), coef_f32x2(A.hub3[2])};
+  const C2 CHp = coef_f32x2(A.dt2), CFp = coef_f32x2(A.dt), C6p = coef_f32x2(A.dt6);
   const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
   auto s4 = [&](int p) { return (p - a_begin + 4) & 3; };
   auto s3 = [&](int p) { return (p - a_begin + 3) % 3; };
@@ -246,20 +293,44 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     RowStar<S, V, SP> F, P;
     F.load(XF + s4(q) * SM::P2, XF + s4(q - 1) * SM::P2, XF + s4(q + 1) * SM::P2, o2);
     P.load(XP + s4(q) * SM::P2, XP + s4(q - 1) * SM::P2, XP + s4(q + 1) * SM::P2, o2);
+    if constexpr (sizeof(S) == 4) {  // two sites per paired FP32 instruction, same bits
+      const StageCoefL<float2> K1{M2p, INVp[0], HUBp[0], Q1p, Q2p}, K2{M2p, INVp[1], HUBp[1], Q1p, Q2p};
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const Star<T> fs = F.template at<T>(v), ps = P.template at<T>(v);
-      const T f0 = fs.f0, p0 = ps.f0;
-      const T k1 = kpi_of<EQ, S, V>(p0, f0, lap_of(fs), ct, v, k1c);
-      const S yapi = (S)ch.fma(k1, p0);
-      const Star<T> ya = ya_star<S, T>(fs, ps, ch);
-      const T k2 = kpi_of<EQ, S, V>((T)yapi, ya.f0, lap_of(ya), ch2, v, k2c);
-      const S bpi = (S)ch.fma(k2, p0);
-      yb.v[v] = (S)ch.fma((T)yapi, f0);
-      yc.v[v] = (S)cf.fma((T)bpi, f0);
-      ybpi.v[v] = bpi;
-      aphi.v[v] = (S)((T)(S)p0 + (T)2 * (T)yapi);
-      api.v[v] = (S)((T)(S)k1 + (T)2 * k2);
+      for (int l = 0; l < V / 2; ++l) {
+        const Star<float2> fs = star2(F, l), ps = star2(P, l);
+        const float2 f0 = fs.f0, p0 = ps.f0;
+        float2 c_ps, c_dps, c_ps4;
+        coupling2<EQ>(ct, l, c_ps, c_dps, c_ps4);
+        const float2 k1 = kpi_f32<EQ, float2>(p0, f0, lap_of2(fs), c_ps, c_dps, c_ps4, K1);
+        const float2 yapi = c_fma(CHp, k1, p0);
+        const Star<float2> ya{c_fma(CHp, ps.f0, fs.f0), c_fma(CHp, ps.ap, fs.ap), c_fma(CHp, ps.am, fs.am),
+                              c_fma(CHp, ps.bp, fs.bp), c_fma(CHp, ps.bm, fs.bm), c_fma(CHp, ps.cp, fs.cp),
+                              c_fma(CHp, ps.cm, fs.cm)};
+        coupling2<EQ>(ch2, l, c_ps, c_dps, c_ps4);
+        const float2 k2 = kpi_f32<EQ, float2>(yapi, ya.f0, lap_of2(ya), c_ps, c_dps, c_ps4, K2);
+        const float2 bpi = c_fma(CHp, k2, p0);
+        set2(yb, l, c_fma(CHp, yapi, f0));
+        set2(yc, l, c_fma(CFp, bpi, f0));
+        set2(ybpi, l, bpi);
+        set2(aphi, l, p_fma(p_splat<float2>(2.0f), yapi, p0));
+        set2(api, l, p_fma(p_splat<float2>(2.0f), k2, k1));
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const Star<T> fs = F.template at<T>(v), ps = P.template at<T>(v);
+        const T f0 = fs.f0, p0 = ps.f0;
+        const T k1 = kpi_of<EQ, S, V>(p0, f0, lap_of(fs), ct, v, k1c);
+        const S yapi = (S)ch.fma(k1, p0);
+        const Star<T> ya = ya_star<S, T>(fs, ps, ch);
+        const T k2 = kpi_of<EQ, S, V>((T)yapi, ya.f0, lap_of(ya), ch2, v, k2c);
+        const S bpi = (S)ch.fma(k2, p0);
+        yb.v[v] = (S)ch.fma((T)yapi, f0);
+        yc.v[v] = (S)cf.fma((T)bpi, f0);
+        ybpi.v[v] = bpi;
+        aphi.v[v] = (S)((T)(S)p0 + (T)2 * (T)yapi);
+        api.v[v] = (S)((T)(S)k1 + (T)2 * k2);
+      }
     }
   };
 
@@ -293,10 +364,46 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     yc[r1 * SP + col] = (S)cf.fma((T)bpi, f0);
   };
 
+  // L2 prefetch of the rows of plane p that phase 1 (curvature at t, t + dt/2, two
+  // planes later) and phase 2 (curvature at t + dt/2, t + dt and the lo words, three
+  // planes later) load straight from global memory: one thread per row and array, so
+  // those loads wait on L2 rather than HBM.
+  auto prefetch_plane = [&](int p) {
+    if (tx != 0 || !colact) return;
+    const bool own = ty < TYv;
+    if (own ? ty >= tye : !RINGW) return;
+    const int gb = own ? b : wrap_n(ty == TYv ? b0 - 1 : b0 + tye, N);
+    const long long off = NN * wrap_n(p, N) + (long long)N * gb + c0;
+    const unsigned bytes = (unsigned)(twe * sizeof(S));
+    if constexpr (EqOf<EQ>::psi_plane) {
+      prefetch_l2(A.psi[0] + off, bytes);
+      if constexpr (EQ != EQ_FIXED) {
+        prefetch_l2(A.psi[1] + off, bytes);
+        if (own) prefetch_l2(A.psi[2] + off, bytes);
+      }
+    }
+    if constexpr (EqOf<EQ>::dpsi_plane) {
+      prefetch_l2(A.dpsi[0] + off, bytes);
+      prefetch_l2(A.dpsi[1] + off, bytes);
+      if (own) prefetch_l2(A.dpsi[2] + off, bytes);
+    }
+    if constexpr (sizeof(S) == 4) {
+      if (own) {
+        prefetch_l2(A.xlo + off, bytes);
+        prefetch_l2(A.xlo + N3 + off, bytes);
+      }
+    }
+  };
+
   issue(a_begin - 2);
   cp_async_commit();
+  prefetch_plane(a_begin - 2);
+  prefetch_plane(a_begin - 1);
   for (int p = a_begin - 2; p <= a_end + 1; ++p) {
-    if (p + 1 <= a_end + 1) issue(p + 1);
+    if (p + 1 <= a_end + 1) {
+      issue(p + 1);
+      prefetch_plane(p + 1);
+    }
     cp_async_commit();
     cp_async_wait_one();  // this thread's copies of plane p have landed
     __syncthreads();      // everyone's; and phase 2 of the last plane is done with YB / YC
@@ -400,6 +507,30 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
         lp = ldv_rw<S, V>(A.xlo + roff + rowoff);
         lq = ldv_rw<S, V>(A.xlo + N3 + roff + rowoff);
       }
+      if constexpr (sizeof(S) == 4) {  // two sites per paired FP32 instruction, same bits
+        const StageCoefL<float2> K2{M2p, INVp[1], HUBp[1], Q1p, Q2p}, K4{M2p, INVp[2], HUBp[2], Q1p, Q2p};
+#pragma unroll
+        for (int l = 0; l < V / 2; ++l) {
+          const Star<float2> bs = star2(B, l);
+          const float2 p0 = lane2(ybpi, l);
+          float2 c_ps, c_dps, c_ps4;
+          coupling2<EQ>(cth, l, c_ps, c_dps, c_ps4);
+          const float2 k3 = kpi_f32<EQ, float2>(p0, bs.f0, lap_of2(bs), c_ps, c_dps, c_ps4, K2);
+          const float2 c1phi = p_fma(p_splat<float2>(2.0f), p0, lane2(aphi, l));
+          const float2 c1pi = p_fma(p_splat<float2>(2.0f), k3, lane2(api, l));
+          const float2 ycpi = c_fma(CFp, k3, lane2(xpi, l));
+          const Star<float2> cs = star2(C, l);
+          coupling2<EQ>(cd, l, c_ps, c_dps, c_ps4);
+          const float2 k4 = kpi_f32<EQ, float2>(ycpi, cs.f0, lap_of2(cs), c_ps, c_dps, c_ps4, K4);
+          float2 h1, l1, h2, l2;
+          comp_update_f32<float2>(lane2(xphi, l), lane2(lp, l), p_add(c1phi, ycpi), C6p, h1, l1);
+          comp_update_f32<float2>(lane2(xpi, l), lane2(lq, l), p_add(c1pi, k4), C6p, h2, l2);
+          set2(o1, l, h1);
+          set2(o3, l, l1);
+          set2(o2, l, h2);
+          set2(o4, l, l2);
+        }
+      } else
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const Star<T> bs = B.template at<T>(v);

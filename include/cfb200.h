@@ -113,6 +113,10 @@ typedef struct cf_params {
  * instead of one whole-step pass (the default for the 7-point stencil; the 13-point
  * stencil always takes the paired passes). */
 #define CF_FLAG_PAIR_KERNELS 4
+/* FP32 storage: the pruned Psi synthesis's last pass (the length-N C2R of every row)
+ * runs as the CTA-per-tile kernel instead of the default warp-per-row-group kernel
+ * (N = 256, 512, 1024); both compute the same values. */
+#define CF_FLAG_PSI_CTA_PASS_C 8
 
 typedef struct cf_ctx cf_ctx;
 
@@ -192,9 +196,15 @@ int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0
  * anything else is rejected (CF_ERR_INVALID / CF_ERR_UNSUPPORTED).  All calls on
  * a device share the array, which keeps the last call's contents (nothing needs
  * clearing: each step writes every entry before reading it); calls whose GPU work
- * overlaps race and must be serialised by the caller.  The first call on a device
- * looks up the array's device address with that device current: make it before
- * any stream capture.  Calls no cudaMalloc, cudaFree or allocating library routine. */
+ * overlaps race and must be serialised by the caller.  With lazy module loading
+ * (the CUDA default) the array is reserved on a device by the first call there:
+ * an application that gives its free device memory to its own pool makes one call
+ * first (nsteps = 0 only reserves the array and resolves its address) or sets
+ * CUDA_MODULE_LOADING=EAGER.  Calls outside stream capture look the array's
+ * address up afresh (valid after a cudaDeviceReset); calls during capture reuse
+ * the last address, so make one call before capturing.  The caller's current
+ * device is restored on return.  Calls no cudaMalloc, cudaFree or allocating
+ * library routine. */
 int cf_rk4_steps_noalloc(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
                          void *stream);
 

@@ -8,7 +8,8 @@ FFTW3 restatement of oracle/fftw_shim.c) and cross-checked against the C
 restatement (oracle/liboracle.so); both figures are stored in the file.
 
     python tests/golden/make_config_fixtures.py config1
-        -> tests/golden/config1_kgfrw_n256.npz
+        -> tests/golden/config1_kgfrw_n256.npz (with the reference's own -ffast-math /
+           strict-FP spread as floor_* entries; `config1-floor` adds only those)
     python tests/golden/make_config_fixtures.py config2
         -> tests/golden/config2_comoving_n512.npz
 
@@ -27,8 +28,8 @@ config2: ComovingCurvatureEquationInFRW (src/equations.cpp:186-261), same
   0.25, seed = 2), dphi(0) = 0; R_fft = fields.curvature_R_fft(512, 512, eta(1) =
   2, psi_rms = 1e-2, k_max = 0.5, seed = 3) (the k^-3 spectrum with cutoff).
   RK4 dt = 0.05 from t = 1 for 3 steps.  Stored: the density power spectrum (s^2
-  bins and unit shells) and the mode power spectrum at t = 1.15, the a = 0 planes
-  of phi and dphi, input checksums.
+  bins and unit shells) and the mode power spectrum (unit shells) at t = 1.15, the
+  first 64 rows of the a = 0 planes of phi and dphi, input checksums.
 
 The reference build must exist (make -C oracle ref REF=<reference tree>).
 """
@@ -120,11 +121,46 @@ def config2(out):
     rho_r = O.power_spectrum(O.energy_density(P, y, t1, Rf))
     cross = max(rel_max(y, xr), rel_max(rho_r, rho))
     print(f"restatement vs reference build: {cross:.3e}", flush=True)
-    N2 = N * N
+    R = 64 * N  # the first 64 rows of the a = 0 plane
     np.savez(out, N=N, L=L, m=m, dt=dt, t0=t0, nsteps=nsteps, k_star=0.25, seed=2, R_seed=3, psi_rms=1e-2,
              k_max=0.5, input_checksum=checksum(x0), R_checksum=checksum(Rf), t_final=t1,
-             rho_s2=rho, rho_shells=shells(N, rho), varphi_plus_s2=mode,
-             phi_plane0=xr[:N2], dphi_plane0=xr[N ** 3:N ** 3 + N2], restatement_vs_reference=cross)
+             rho_s2=rho, rho_shells=shells(N, rho), varphi_plus_shells=shells(N, mode),
+             phi_rows=xr[:R], dphi_rows=xr[N ** 3:N ** 3 + R], restatement_vs_reference=cross)
+
+
+def config1_floor(path):
+    """The reference's own noise floor at config 1: its -O2 build without -ffast-math
+    (oracle/_ref/libcfref_strict.so) against the fixture's -ffast-math build, per
+    metric, added to the fixture as floor_*."""
+    g = dict(np.load(path))
+    N, L, m, dt, t0, nsteps = int(g["N"]), float(g["L"]), float(g["m"]), float(g["dt"]), float(g["t0"]), int(g["nsteps"])
+    x0 = fields.initial_state(N, L, float(g["k_star"]), seed=int(g["seed"]))
+    t = time.time()
+    xs, sp = O.ref_integrate(1, N, L, m, x0, t0, t0 + (nsteps + 0.5) * dt, dt, t_interval=float(g["t_list"][1] - t0),
+                             observe=True, strict=True, **FRW)
+    print(f"strict reference build: {time.time() - t:.0f} s", flush=True)
+    P = O.make_params(N, L, m, eq=1, **FRW)
+    t1 = float(g["t_final"])
+    rho = O.ref_power_spectrum(O.ref_energy_density(1, N, L, m, xs, t1, strict=True, **FRW), strict=True)
+    mode = O.ref_mode_power_spectrum(N, L, m, O.a_of_t(P, t1), xs, strict=True)
+
+    def per_bin(a, b, floor=1e-10):
+        big = np.abs(b) >= floor * np.abs(b).max()
+        return float(np.max(np.abs(a[big] - b[big]) / np.abs(b[big])))
+
+    def norm_rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    N2 = N * N
+    g["floor_rho_s2_final"] = per_bin(rho, g["rho_s2_final"])
+    g["floor_varphi_plus_s2_final"] = per_bin(mode, g["varphi_plus_s2_final"])
+    g["floor_rho_shells"] = max(per_bin(shells(N, a), b) for a, b in zip(sp["rho"], g["rho_shells"]))
+    g["floor_varphi_plus_shells"] = max(per_bin(shells(N, a), b)
+                                        for a, b in zip(sp["varphi_plus"], g["varphi_plus_shells"]))
+    g["floor_phi_plane0"] = norm_rel(xs[:N2], g["phi_plane0"])
+    g["floor_dphi_plane0"] = norm_rel(xs[N ** 3:N ** 3 + N2], g["dphi_plane0"])
+    print({k: float(v) for k, v in g.items() if k.startswith("floor_")}, flush=True)
+    np.savez(path, **g)
 
 
 if __name__ == "__main__":
@@ -133,6 +169,9 @@ if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "config1"
     if which == "config1":
         config1(os.path.join(HERE, "config1_kgfrw_n256.npz"))
+        config1_floor(os.path.join(HERE, "config1_kgfrw_n256.npz"))
+    elif which == "config1-floor":
+        config1_floor(os.path.join(HERE, "config1_kgfrw_n256.npz"))
     elif which == "config2":
         config2(os.path.join(HERE, "config2_comoving_n512.npz"))
     else:

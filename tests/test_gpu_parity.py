@@ -446,3 +446,27 @@ def test_density_slices_match_energy_density(eq, prec):
     for a in range(N):  # the summation order of the kernel: increasing a
         want += r[a * N * N:(a + 1) * N * N]
     assert np.array_equal(av.cpu().numpy(), want / N)
+
+
+@pytest.mark.parametrize("stencil,order", [(7, 2), (13, 4)])
+def test_gpu_laplacian_convergence_order_on_a_plane_wave(stencil, order):
+    """The device stencils' own convergence order (the oracle twin is in
+    test_oracle_pin.py): cf_rhs (FP64, flat KG, m = 0) on cos(2 pi (a + 2b + 3c) / N)
+    with L fixed approaches -(2 pi / L)^2 14 phi as h^2 (7-point) and h^4 (13-point)."""
+    L = 8.0
+    errs = []
+    for N in (16, 32, 64):
+        i = np.arange(N)
+        A, Bb, Cc = np.meshgrid(i, i, i, indexing="ij")
+        phi = np.cos(2 * np.pi * (A + 2 * Bb + 3 * Cc) / N).ravel()
+        x = dev(np.concatenate([phi, np.zeros(N ** 3)]))
+        c = ctx_for(N, L, 0, stencil=stencil, m=0.0)
+        out = torch.empty_like(x)
+        c.rhs(x, out, 0.0)
+        torch.cuda.synchronize()
+        lap = out[N ** 3:].cpu().numpy()
+        exact = -(2 * np.pi / L) ** 2 * 14.0 * phi
+        errs.append(float(np.abs(lap - exact).max() / np.abs(exact).max()))
+        c.close()
+    rates = [np.log2(errs[k] / errs[k + 1]) for k in range(2)]
+    assert all(abs(r - order) < 0.15 for r in rates), (errs, rates)

@@ -6,10 +6,13 @@ of context allocations.
 
 Checked through the C ABI against the allocating entry point cf_rk4_steps on
 the same inputs: two calls in a row (the second continuing the first), both
-precisions, flat and FRW equations; the same kernels run, so the states must be
-identical (tolerance 1e-15 relative, as the fused-vs-odeint check in
-test_gpu_parity.py).  Sizes beyond the array and the comoving-curvature equation
-are rejected with a clear error.  This file is collected last.
+precisions, both stencils, flat and FRW equations.  The routes differ -- the
+no-allocation entry point runs the four single-stage kernels, cf_rk4_steps the
+whole-step pass (7-point) or the paired passes (13-point) -- but every route forms
+and rounds each value identically, so the states must be bit-identical.  A call
+with nsteps = 0 is accepted and changes nothing.  Sizes beyond the array and the
+comoving-curvature equation are rejected with a clear error.  This file is
+collected last.
 """
 import ctypes
 
@@ -42,22 +45,27 @@ def _rel(a, b):
     return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
 
 
+@pytest.mark.parametrize("stencil", [7, 13])
 @pytest.mark.parametrize("eq", [cfb200.EQ_KG, cfb200.EQ_KG_FRW])
 @pytest.mark.parametrize("prec,N", [(cfb200.FP64, 64), (cfb200.FP64, 80), (cfb200.FP32_COMP, 96)])
-def test_noalloc_matches_allocating_stepper_on_two_calls(eq, prec, N):
+def test_noalloc_matches_allocating_stepper_on_two_calls(eq, prec, N, stencil):
     L = float(N)
     cos = FRW if eq == cfb200.EQ_KG_FRW else {}
-    ctx = cfb200.Context(N, L, m=1.0, equation=eq, precision=prec, **cos)
+    ctx = cfb200.Context(N, L, m=1.0, equation=eq, precision=prec, stencil=stencil, **cos)
     x = fields.initial_state(N, L, 0.5, seed=N + eq)
     a = torch.empty(ctx.info.state_bytes // 8, dtype=torch.float64, device="cuda")
     ctx.upload(a, x)
     b = a.clone()
     t0, dt = (1.0 if cos else 0.0), 0.05
+    # a zero-step call reserves the array and resolves its address, nothing else
+    assert _run_noalloc(ctx, b, t0, dt, 0, 0) == cfb200.CF_OK, cfb200.lib().cf_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
     for call, (step0, n) in enumerate([(0, 4), (4, 3)]):
         ctx.rk4_steps(a, t0, dt, n, step0=step0)
         assert _run_noalloc(ctx, b, t0, dt, n, step0) == cfb200.CF_OK, cfb200.lib().cf_last_error()
         torch.cuda.synchronize()
-        assert _rel(b, a) <= 1e-15, (call, _rel(b, a))
+        assert torch.equal(a, b), (call, _rel(b, a))
     ctx.close()
 
 
