@@ -218,7 +218,7 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     set_error("stencil must be 7 or 13, got %d", p.stencil);
     return CF_ERR_INVALID;
   }
-  if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS | CF_FLAG_PAIR_KERNELS)) {
+  if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS | CF_FLAG_PAIR_KERNELS | CF_FLAG_PSI_CTA_PASS_C)) {
     set_error("unknown flags 0x%x", (unsigned)p.flags);
     return CF_ERR_INVALID;
   }

@@ -6,12 +6,14 @@
 // the same fused RK4 passes as cf_rk4_steps, applied to a work list of (member,
 // b-tile, c-tile, a-chunk) items.  Three schedules:
 //
-//   CF_ENS_PERSISTENT  one cooperative kernel for all steps over the four
-//                      single-stage tiles (cf_stage_tile.cuh): each CTA takes work
-//                      items of a stage, then a grid barrier (bounded spin:
-//                      gives up with CF_ERR_TIMEOUT instead of hanging) before the
-//                      next stage.  Stage coefficients come from a per-step table
-//                      in device memory, so a captured graph replays it.
+//   CF_ENS_PERSISTENT  one cooperative kernel for all steps: each CTA takes work
+//                      items from a shared counter -- whole-step items for the
+//                      7-point stencil (cf_step_tile.cuh), single-stage items for
+//                      the 13-point one (cf_stage_tile.cuh) -- then a grid barrier
+//                      (bounded spin: gives up with CF_ERR_TIMEOUT instead of
+//                      hanging) before the next step (stage).  Stage coefficients
+//                      come from a per-step table in device memory, so a captured
+//                      graph replays it.
 //   CF_ENS_BATCHED     the passes of cf_rk4_steps over the whole work list: one
 //                      whole-step launch per step for the 7-point stencil
 //                      (cf_step_tile.cuh), the two paired passes (stages 1+2, 3+4;
@@ -325,13 +327,10 @@ constexpr size_t ens_step_smem() {
 // writes the other buffer; the lo words stay in x; a run of odd length ends with
 // k_ens_xy_back.
 template <typename S, int SS>
-__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY, EnsStepShape<S, SS>::MB)
-    k_ens_step(const EnsArgs E, int step_off) {
+__device__ __forceinline__ void ens_step_item(const EnsArgs &E, const EnsItem &it, long long step, int step_off,
+                                              S *sm) {
   using SH = EnsStepShape<S, SS>;
-  extern __shared__ __align__(16) unsigned char ens_step_sm[];
-  const EnsItem it = E.items[blockIdx.x];
   const EnsMember mb = E.members[it.member];
-  const long long step = *E.step_counter + step_off;
   S *x = (S *)mb.x, *ya = (S *)mb.ya;
   S *cur = (step_off & 1) ? ya : x, *nxt = (step_off & 1) ? x : ya;
   StepArgs<S> A{};
@@ -353,14 +352,21 @@ __global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::
   A.dt2 = E.dt / 2.0;
   A.dt = E.dt;
   A.dt6 = E.dt / 6.0;
-  step_tile<S, EQ_FRW, SH::TX, SH::TY, false>(A, it.c0, it.b0, it.a_begin, it.a_end, reinterpret_cast<S *>(ens_step_sm));
+  step_tile<S, EQ_FRW, SH::TX, SH::TY, false>(A, it.c0, it.b0, it.a_begin, it.a_end, sm);
+}
+
+template <typename S, int SS>
+__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY, EnsStepShape<S, SS>::MB)
+    k_ens_step(const EnsArgs E, int step_off) {
+  extern __shared__ __align__(16) unsigned char ens_step_sm[];
+  ens_step_item<S, SS>(E, E.items[blockIdx.x], *E.step_counter + step_off, step_off,
+                       reinterpret_cast<S *>(ens_step_sm));
 }
 
 // phi and pi back from ya to x over one whole-step work item's sites.
 template <typename S, int SS>
-__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY) k_ens_xy_back(const EnsArgs E) {
+__device__ __forceinline__ void ens_xy_back_item(const EnsArgs &E, const EnsItem &it) {
   constexpr int V = VecT<S>::n, TW = EnsStepShape<S, SS>::TX * V;
-  const EnsItem it = E.items[blockIdx.x];
   const EnsMember mb = E.members[it.member];
   const int N = mb.N;
   const int c = it.c0 + threadIdx.x * V, b = it.b0 + threadIdx.y;
@@ -370,6 +376,46 @@ __global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::
     const long long site = NN * a + (long long)N * b + c;
     stv((S *)mb.x + site, ldv((const S *)mb.ya + site));
     stv((S *)mb.x + mb.N3 + site, ldv((const S *)mb.ya + mb.N3 + site));
+  }
+}
+
+template <typename S, int SS>
+__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY) k_ens_xy_back(const EnsArgs E) {
+  ens_xy_back_item<S, SS>(E, E.items[blockIdx.x]);
+}
+
+// The persistent form of the 7-point ensemble step (CF_ENS_PERSISTENT): one
+// cooperative launch for all steps, CTAs taking whole-step work items from a shared
+// counter (the items differ in cost: edge tiles, a-chunk remainders) and meeting at
+// one bounded grid barrier per RK4 step -- every item of step j reads the buffer the
+// items of step j - 1 wrote; a run of odd length ends with phi, pi back in x.
+template <typename S, int SS>
+__global__ void __launch_bounds__(EnsStepShape<S, SS>::TX *EnsStepShape<S, SS>::TY, EnsStepShape<S, SS>::MB)
+    k_ens_persistent_step(const EnsArgs E) {
+  extern __shared__ __align__(16) unsigned char ens_step_sm[];
+  __shared__ int next;
+  const long long step0 = *E.step_counter;
+  for (int j = 0; j < E.nsteps; ++j) {
+    for (;;) {
+      if (threadIdx.x == 0 && threadIdx.y == 0) next = (int)atomicAdd(E.work, 1u);
+      __syncthreads();
+      const int i = next;
+      if (i >= E.n_items) break;
+      // step_tile synchronises the CTA before it returns, so every thread has read
+      // `next` before thread 0 overwrites it
+      ens_step_item<S, SS>(E, E.items[i], step0 + j, j, reinterpret_cast<S *>(ens_step_sm));
+    }
+    if (!grid_barrier(E)) return;
+  }
+  if (E.nsteps & 1) {
+    for (;;) {
+      if (threadIdx.x == 0 && threadIdx.y == 0) next = (int)atomicAdd(E.work, 1u);
+      __syncthreads();
+      const int i = next;
+      if (i >= E.n_items) break;
+      ens_xy_back_item<S, SS>(E, E.items[i]);
+      __syncthreads();
+    }
   }
 }
 
@@ -453,6 +499,7 @@ struct cf_ensemble {
   long long spin_limit = 1LL << 24;
   int64_t launches = 0;
   int coop_blocks = 0;
+  int coop_blocks_step = 0;  // resident CTAs of the persistent whole-step kernel
 };
 
 namespace cfb {
@@ -506,6 +553,9 @@ static int step_items_t(cf_ensemble *E) {
                    [&](const EnsItem &x, const EnsItem &y) { return E->hm[x.member].N > E->hm[y.member].N; });
   CF_TRY_CUDA(cudaFuncSetAttribute(k_ens_step<S, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)ens_step_smem<S, SS>()));
+  CF_TRY_CUDA(cudaFuncSetAttribute(k_ens_persistent_step<S, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)ens_step_smem<S, SS>()));
+  E->coop_blocks_step = 0;
   cudaFree(E->d_sitems);
   E->d_sitems = nullptr;
   CF_TRY_CUDA(cudaMalloc(&E->d_sitems, sizeof(EnsItem) * E->sitems.size()));
@@ -579,6 +629,49 @@ static int launch_persistent(cf_ensemble *E, int nsteps, double dt, cudaStream_t
   CF_TRY_CUDA(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), block, args, 0, st));
   E->launches++;
   return CF_OK;
+}
+
+// The persistent whole-step kernel over all step items (7-point), cooperative launch.
+template <typename S, int SS>
+static int launch_persistent_step_t(cf_ensemble *E, int nsteps, double dt, cudaStream_t st) {
+  auto kern = k_ens_persistent_step<S, SS>;
+  const dim3 block(EnsStepShape<S, SS>::TX, EnsStepShape<S, SS>::TY);
+  const size_t smem = ens_step_smem<S, SS>();
+  if (!E->coop_blocks_step) {
+    int per_sm = 0, dev = 0, sms = 0;
+    CF_TRY_CUDA(cudaGetDevice(&dev));
+    CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)(block.x * block.y), smem));
+    if (per_sm < 1) return ens_fail("ensemble: persistent whole-step kernel does not fit on an SM");
+    E->coop_blocks_step = per_sm * sms;
+  }
+  EnsArgs A{};
+  A.members = E->dm;
+  A.items = E->d_sitems;
+  A.n_items = (int)E->sitems.size();
+  A.coef = E->d_coef;
+  A.step_counter = E->d_step;
+  A.nsteps = nsteps;
+  A.dt = dt;
+  A.bar_count = E->d_bar;
+  A.bar_gen = E->d_bar + 1;
+  A.work = E->d_bar + 2;
+  A.err = E->d_err;
+  A.bar_extra = E->bar_extra;
+  A.spin_limit = E->spin_limit;
+  void *args[] = {(void *)&A};
+  const int blocks = std::min(E->coop_blocks_step, A.n_items);
+  CF_TRY_CUDA(cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), block, args, smem, st));
+  E->launches++;
+  return CF_OK;
+}
+
+static int launch_persistent_step(cf_ensemble *E, int nsteps, double dt, cudaStream_t st) {
+  if (E->word == 4)
+    return E->sshape ? launch_persistent_step_t<float, 1>(E, nsteps, dt, st)
+                     : launch_persistent_step_t<float, 0>(E, nsteps, dt, st);
+  return E->sshape ? launch_persistent_step_t<double, 1>(E, nsteps, dt, st)
+                   : launch_persistent_step_t<double, 0>(E, nsteps, dt, st);
 }
 
 // One launch over work items [i0, i1): paired pass PASS (1, 2), or (PASS 0) phi
@@ -668,7 +761,10 @@ static int run_t(cf_ensemble *E, int mode, long long step0, long long nsteps, do
   if (mode == CF_ENS_PERSISTENT) {
     CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 3 * sizeof(unsigned), st));
     CF_TRY_CUDA(cudaMemsetAsync(E->d_err, 0, sizeof(int), st));
-    CF_TRY(launch_persistent<S, H, SHAPE>(E, (int)nsteps, dt, st));
+    if (H == 1)
+      CF_TRY(launch_persistent_step(E, (int)nsteps, dt, st));
+    else
+      CF_TRY((launch_persistent<S, H, SHAPE>(E, (int)nsteps, dt, st)));
     int err = 0;
     CF_TRY_CUDA(cudaMemcpyAsync(&err, E->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CF_TRY_CUDA(cudaStreamSynchronize(st));
@@ -739,7 +835,9 @@ static int segment(cf_ensemble *E, int mode, long long steps, double dt, cudaStr
     return CF_OK;
   }
   CF_TRY_CUDA(cudaMemsetAsync(E->d_bar, 0, 3 * sizeof(unsigned), st));
-  if (E->word == 4) {
+  if (E->stencil == 7) {
+    s = launch_persistent_step(E, (int)steps, dt, st);
+  } else if (E->word == 4) {
     if (E->stencil == 13)
       s = E->shape ? launch_persistent<float, 2, 1>(E, (int)steps, dt, st)
                    : launch_persistent<float, 2, 0>(E, (int)steps, dt, st);

@@ -143,6 +143,29 @@ def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or,
         assert rel(b[sl], want) <= tol
 
 
+@pytest.mark.parametrize("N,k_max", [(256, 0.3), (256, 0.6), (512, 0.5), (1024, 0.5)])
+def test_warp_pass_c_equals_cta_pass_c(N, k_max):
+    """FP32 storage, N = 256, 512, 1024: the last pass of the pruned synthesis as
+    one warp per row group (the default) and as one CTA per tile
+    (CF_FLAG_PSI_CTA_PASS_C) do the same arithmetic in the same order, so Psi and
+    dPsi/dt are bit-identical."""
+    L = float(N)
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=37, use_torch=True)
+    got = {}
+    for flags in (0, cfb200.FLAG_PSI_CTA_PASS_C):
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, flags=flags, **FRW)
+        c.set_R_fft(Rf, on_device=True)
+        assert c.info.psi_route == cfb200.PSI_PRUNED_FUSED
+        out = torch.empty(2 * N ** 3, dtype=torch.float64, device="cuda")
+        c.psi_fields(1.3, out)
+        torch.cuda.synchronize()
+        got[flags] = out
+        c.close()
+    assert torch.equal(got[0], got[cfb200.FLAG_PSI_CTA_PASS_C])
+    del got
+    torch.cuda.empty_cache()
+
+
 @pytest.mark.parametrize("N,K,prec,tol", [(512, 41, cfb200.FP32_COMP, 2e-6), (1024, 40, cfb200.FP32_COMP, 2e-6),
                                           (512, 41, cfb200.FP64, 1e-12)])
 def test_pruned_psi_at_full_size_equals_full_c2r(N, K, prec, tol):
