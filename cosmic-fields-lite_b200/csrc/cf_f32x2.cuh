@@ -80,17 +80,21 @@ __device__ __forceinline__ L lap7_f32(L f0, L ap, L am, L bp, L bm, L cp, L cm) 
   return p_add(s, p_add(cp, cm));
 }
 
-// 13-point 4th-order Laplacian sum (times h^2) from the six first and the six second
-// neighbours (each summed a+, a-, b+, b-, c+, c-): (16 s1 - s2 - 90 f0) / 12.
+// 13-point 4th-order Laplacian sum times 12 h^2 from the six first and the six second
+// neighbours (each summed a+, a-, b+, b-, c+, c-): 16 s1 - s2 - 90 f0.  The 1/12 goes
+// into the stage's h^-2 a^-2 coefficient instead (lap_coef_f32), saving a division and a
+// rounding; every FP32 13-point route does the same.
 template <typename L>
 __device__ __forceinline__ L lap13_f32(L f0, L s1, L s2) {
-  L r = p_fma(p_splat<L>(16.0f), s1, p_neg(s2));
-  r = p_fma(p_splat<L>(-90.0f), f0, r);
-  if constexpr (sizeof(L) == 4) {
-    return __fdiv_rn(r, 12.0f);
-  } else {
-    return make_float2(__fdiv_rn(r.x, 12.0f), __fdiv_rn(r.y, 12.0f));
-  }
+  const L r = p_fma(p_splat<L>(16.0f), s1, p_neg(s2));
+  return p_fma(p_splat<L>(-90.0f), f0, r);
+}
+
+// The coefficient of the Laplacian sum in the FP32 stage arithmetic: h^-2 a^-2, and
+// h^-2 a^-2 / 12 for the 13-point stencil (whose sum lap13_f32 leaves times 12).
+template <int H>
+__host__ __device__ inline double lap_coef_f32(double inv) {
+  return H == 2 ? inv / 12.0 : inv;
 }
 
 // pi component of the right-hand side (src/equations_cuda.cu:15-36 FRW, :38-76

@@ -98,8 +98,11 @@ __device__ __forceinline__ void pair_tile(const PairArgs<S> &A, int c0, int b0, 
   const S *upi = A.upi;
   const S *xphi = A.xphi;  // w's base phi (pass A: the same array as uphi)
   using T = typename Arith<S>::T;
-  const StageCoef<T> k1c{Coef<T>(A.m2), Coef<T>(A.inv1), Coef<T>(A.hub3_1), Coef<T>(A.q1), Coef<T>(A.q2)};
-  const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(A.inv2), Coef<T>(A.hub3_2), Coef<T>(A.q1), Coef<T>(A.q2)};
+  // FP32: the 13-point sum comes times 12 (lap13_f32), its 1/12 rides on the coefficient
+  const double inv1 = sizeof(T) == 4 ? lap_coef_f32<H>(A.inv1) : A.inv1;
+  const double inv2 = sizeof(T) == 4 ? lap_coef_f32<H>(A.inv2) : A.inv2;
+  const StageCoef<T> k1c{Coef<T>(A.m2), Coef<T>(inv1), Coef<T>(A.hub3_1), Coef<T>(A.q1), Coef<T>(A.q2)};
+  const StageCoef<T> k2c{Coef<T>(A.m2), Coef<T>(inv2), Coef<T>(A.hub3_2), Coef<T>(A.q1), Coef<T>(A.q2)};
   const Coef<T> cw(A.cw), cy(A.cy), c6(A.dt6);
   const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
 

@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(256) k_prune_c_fft_p(const S *__restrict__ pb,
 template <int R1, int R2, int B>
 __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict__ pb, float *__restrict__ out,
                                                      const float2 *__restrict__ wN, const float2 *__restrict__ twM,
-                                                     int N, int Kc, long long ntiles,
+                                                     int N, int Kc, int ntiles, int log2_groups, int log2_n,
                                                      const __grid_constant__ Tw32<float> tw) {
   constexpr int M = R1 * R2;  // N == 2 M
   constexpr int RW = 32 / R1;
@@ -551,22 +551,22 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
   for (int i = threadIdx.x; i < kn; i += blockDim.x) WK[i] = wN[i];
   __syncthreads();  // the only CTA barrier: the shared twiddles
 
-  const int groups = N / RW;  // row groups per (f, a) plane
-  const long long stride = (long long)gridDim.x * (blockDim.x >> 5);
-  long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
-  auto issue = [&](long long t, float2 *dst) {
-    const int g = (int)(t % groups);
-    const long long fa = t / groups;  // f * N + a
-    const int a = (int)(fa % N), f = (int)(fa / N);
-    const float2 *src = reinterpret_cast<const float2 *>(pb) + ((long long)f * kn * N + a) * N + (long long)g * RW;
-    for (int k = lane; k < kn; k += 32) {
-      const unsigned d = (unsigned)__cvta_generic_to_shared(dst + k * RW);
+  // tile t = (f N + a) groups + g, groups = N / RW row groups per plane (powers of two)
+  const int gmask = (1 << log2_groups) - 1, nmask = (1 << log2_n) - 1;
+  const long long NN = (long long)N * N;
+  const int stride = gridDim.x * (blockDim.x >> 5);
+  int tile = blockIdx.x * (blockDim.x >> 5) + warp;
+  auto issue = [&](int t, float2 *dst) {
+    const int g = t & gmask, fa = t >> log2_groups;
+    const int a = fa & nmask, f = fa >> log2_n;
+    const float2 *src = reinterpret_cast<const float2 *>(pb) + ((long long)f * kn * N + a) * N + g * RW + lane * NN;
+    const unsigned d0 = (unsigned)__cvta_generic_to_shared(dst + lane * RW);
+    for (int k = lane; k < kn; k += 32, src += 32 * NN) {
+      const unsigned d = d0 + (unsigned)((k - lane) * RW * sizeof(float2));
       if constexpr (RW == 2)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + (long long)k * N * N)
-                     : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
       else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src + (long long)k * N * N)
-                     : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
@@ -581,8 +581,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
     }
     __syncwarp();  // the tile's band entries (every lane's copies)
     const float2 *X = X0 + buf * xw;
-    const int g = (int)(tile % groups);
-    const long long fa = tile / groups;
+    const int g = tile & gmask, fa = tile >> log2_groups;
     // i X w^k (X[0] by its real part: the Hermitian projection of every C2R)
     for (int i = lane; i < kn * RW; i += 32) {
       const int k = i / RW;
@@ -631,7 +630,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
       for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[(r * R1 + m1) * TP + k2];
       dft_inv<float, R2>(u, tw);
       const bool field0 = fa < N;  // f == 0: the slot holds e^{2 Psi} - 1
-      float2 *row = reinterpret_cast<float2 *>(out) + (fa * N + (long long)g * RW + r) * M;
+      float2 *row = reinterpret_cast<float2 *>(out) + ((long long)fa * N + g * RW + r) * M;
 #pragma unroll
       for (int m2 = 0; m2 < R2; ++m2) {
         float2 o = u[m2];
@@ -670,11 +669,14 @@ static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st
   int sms = 0, per_sm = 0;
   CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
   CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
-  const int N = (int)ctx->N;
-  const long long ntiles = 2LL * N * (N / (32 / R1));
-  const long long grid = std::max(1LL, std::min<long long>((ntiles + 7) / 8, (long long)sms * std::max(per_sm, 1)));
+  const int N = (int)ctx->N, groups = N / (32 / R1);
+  const int ntiles = 2 * N * groups;
+  int log2_n = 0, log2_g = 0;
+  while ((1 << log2_n) < N) ++log2_n;
+  while ((1 << log2_g) < groups) ++log2_g;
+  const int grid = std::max(1, std::min((ntiles + 7) / 8, sms * std::max(per_sm, 1)));
   kern<<<(unsigned)grid, 256, smem, st>>>((const float *)ctx->pz_b, (float *)out, (const float2 *)ctx->pr_wN,
-                                          (const float2 *)ctx->pr_twM, N, ctx->Kc, ntiles, tw);
+                                          (const float2 *)ctx->pr_twM, N, ctx->Kc, ntiles, log2_g, log2_n, tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }

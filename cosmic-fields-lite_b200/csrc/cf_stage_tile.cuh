@@ -181,8 +181,9 @@ __device__ __forceinline__ void psi_factors(double e2m1, double &e2, double &e4)
 
 // Laplacian sum (times h^2) at (row, col) of a staged plane whose a-neighbours
 // are q[0..2H] (q[H] the plane itself): 7-point for H = 1, 13-point 4th order for
-// H = 2 (src/fdm3d_cuda.cu:20-83).  The single-stage and the paired-stage tiles
-// both form it here, so their sums round identically.
+// H = 2 (src/fdm3d_cuda.cu:20-83; in FP32 the 13-point sum comes times 12, see
+// lap13_f32).  The single-stage and the paired-stage tiles both form it here, so
+// their sums round identically.
 template <typename S, int H, int SP, int V, typename T = typename Arith<S>::T>
 __device__ __forceinline__ T lap_at(const Pack<S, V> (&q)[2 * H + 1], const S *sm, int row, int col, int v) {
   const T f0 = (T)q[H].v[v];
@@ -376,7 +377,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs<S> &A, int c0, int b0
   const S *phi_in = A.yin;
   const S *pi_in = A.yin + N3;
   using T = typename Arith<S>::T;
-  const StageCoef<T> kc{Coef<T>(A.m2), Coef<T>(A.inv), Coef<T>(A.hub3), Coef<T>(A.q1), Coef<T>(A.q2)};
+  // FP32: the 13-point sum comes times 12 (lap13_f32), its 1/12 rides on the coefficient
+  const double invc = sizeof(T) == 4 ? lap_coef_f32<H>(A.inv) : A.inv;
+  const StageCoef<T> kc{Coef<T>(A.m2), Coef<T>(invc), Coef<T>(A.hub3), Coef<T>(A.q1), Coef<T>(A.q2)};
   const Coef<T> cy(A.cy), c6(A.dt6);
   const CoarseCols<V> cc = coarse_cols<EQ, V>(A.cmap, act, b, c);
 

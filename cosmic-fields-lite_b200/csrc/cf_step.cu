@@ -1,11 +1,13 @@
 // cf_step.cu -- fused RK4 stage kernels (the hot path), cf_rhs, cf_scale_sum.
 //
 // One RK4 step (stepper/runge_kutta4_classic.hpp:88-138) is four stages.  By
-// default cf_rk4_steps runs a 7-point step as one whole-step pass (k_step,
-// cf_step_tile.cuh) and a 13-point step as two paired-stage passes (stages 1+2,
-// 3+4; cf_pair_tile.cuh); both keep the intermediate stage inputs out of HBM and
-// give the same bits.  The four single-stage kernels remain for
-// CF_FLAG_STAGE_KERNELS, the adjoint's recompute and the persistent ensemble kernel.  A single-stage kernel makes ONE pass over HBM:
+// default cf_rk4_steps runs a step as one whole-step pass -- k_step
+// (cf_step_tile.cuh) for the 7-point stencil, k_step13 (cf_step13_tile.cuh) for the
+// 13-point one in FP32 -- and an FP64 13-point step as two paired-stage passes
+// (stages 1+2, 3+4; cf_pair_tile.cuh); all keep the intermediate stage inputs out of
+// HBM and give the same bits.  The four single-stage kernels remain for
+// CF_FLAG_STAGE_KERNELS, the adjoint's recompute, cf_rk4_steps_noalloc and the
+// 13-point persistent ensemble kernel.  A single-stage kernel makes ONE pass over HBM:
 // it streams its stage input y through a 2.5-D blocked stencil and fuses the
 // odeint linear combinations (thrust_operations::scale_sum2 / scale_sum5) into
 // the same pass:
@@ -22,9 +24,10 @@
 // cf_stage_tile.cuh: a CTA of 32 x 8 threads owns a (b, c) tile of 8 rows x 64
 // (FP64) or 128 (FP32) columns and marches along a over a chunk of planes.
 //
-// Storage: S = double (CF_FP64) or float (CF_FP32_COMP).  Arithmetic is FP64 in
-// both; in FP32_COMP the state x is an FP32 hi + FP32 lo pair that stage 4 updates
-// as a compensated sum, while acc and the stage inputs y are single FP32 words.
+// Storage: S = double (CF_FP64) or float (CF_FP32_COMP).  FP64 storage steps in
+// FP64.  In FP32_COMP the state x is an FP32 hi + FP32 lo pair that stage 4 updates
+// error-free, acc and the stage inputs y are single FP32 words, and the stage
+// arithmetic is FP32 with hi + lo coefficients (cf_f32x2.cuh).
 
 #include <cuda_runtime.h>
 
@@ -33,6 +36,7 @@
 #include "cf_internal.cuh"
 #include "cf_pair_tile.cuh"
 #include "cf_stage_tile.cuh"
+#include "cf_step13_tile.cuh"
 #include "cf_step_tile.cuh"
 
 namespace cfb {
@@ -409,8 +413,58 @@ static int launch_step_t(cf_ctx *ctx, const StepArgs<S> &A0, cudaStream_t st) {
   return launch_step_k<S, EQ, false>(ctx, A, grid, st);
 }
 
+// ---- whole-step passes, 13-point stencil (FP32 storage) -------------------
+// 64 x 8 sites per CTA, two ring warps, 108 KB of shared memory: 2 CTAs per SM.
+constexpr int S13_TX = 32, S13_TY = 8;
+
+template <int EQ, bool FULL>
+__global__ void __launch_bounds__(S13_TX *(S13_TY + 2), 2) k_step13(const StepArgs<float> A) {
+  extern __shared__ __align__(16) unsigned char step13_smem[];
+  using SM = Step13Smem<S13_TX, S13_TY>;
+  const int a_begin = blockIdx.z * A.a_chunk;
+  step13_tile<EQ, S13_TX, S13_TY, FULL>(A, blockIdx.x * SM::TW, blockIdx.y * S13_TY, a_begin,
+                                        min(a_begin + A.a_chunk, A.N), reinterpret_cast<float *>(step13_smem));
+}
+
+template <int EQ, bool FULL>
+static int launch_step13_k(cf_ctx *ctx, const StepArgs<float> &A, dim3 grid, cudaStream_t st) {
+  using SM = Step13Smem<S13_TX, S13_TY>;
+  constexpr size_t bytes = (size_t)SM::count * sizeof(float);
+  static unsigned long long attr_set = 0;  // devices on which this instantiation may use > 48 KB
+  const unsigned long long bit = 1ull << (ctx->device & 63);
+  if (!(attr_set & bit)) {
+    CF_TRY_CUDA(cudaFuncSetAttribute(k_step13<EQ, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    attr_set |= bit;
+  }
+  k_step13<EQ, FULL><<<grid, dim3(S13_TX, S13_TY + 2), bytes, st>>>(A);
+  CF_LAUNCHED(ctx);
+  return CF_OK;
+}
+
+template <int EQ>
+static int launch_step13_t(cf_ctx *ctx, const StepArgs<float> &A0, cudaStream_t st) {
+  using SM = Step13Smem<S13_TX, S13_TY>;
+  StepArgs<float> A = A0;
+  const unsigned gx = ceil_div(A.N, SM::TW), gy = ceil_div(A.N, S13_TY);
+  A.a_chunk = step_a_chunk(A.N, (int)(gx * gy));
+  const dim3 grid(gx, gy, ceil_div(A.N, A.a_chunk));
+  ProfScope ps(ctx, CF_PROF_STEP, st);
+  if (A.N % SM::TW == 0 && A.N % S13_TY == 0) return launch_step13_k<EQ, true>(ctx, A, grid, st);
+  return launch_step13_k<EQ, false>(ctx, A, grid, st);
+}
+
 template <typename S>
 static int launch_step(cf_ctx *ctx, const StepArgs<S> &A, cudaStream_t st) {
+  if constexpr (sizeof(S) == 4) {
+    if (ctx->p.stencil == 13) {  // the equations without curvature planes (rk4_steps routes the others)
+      switch (shape_of(ctx->p.equation)) {
+        case EQ_LAMBDA: return launch_step13_t<EQ_LAMBDA>(ctx, A, st);
+        case EQ_SQRT: return launch_step13_t<EQ_SQRT>(ctx, A, st);
+        case EQ_FRW: return launch_step13_t<EQ_FRW>(ctx, A, st);
+        default: return set_error("13-point whole-step pass: curvature-coupled equation"), CF_ERR_INVALID;
+      }
+    }
+  }
   switch (shape_of(ctx->p.equation)) {
     case EQ_COMOV: return launch_step_t<S, EQ_COMOV>(ctx, A, st);
     case EQ_LAMBDA: return launch_step_t<S, EQ_LAMBDA>(ctx, A, st);
@@ -597,7 +651,14 @@ int rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, i
   if (f & CF_FLAG_STAGE_KERNELS)
     return f32 ? rk4_steps_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
                : rk4_steps_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
-  if ((f & CF_FLAG_PAIR_KERNELS) || ctx->p.stencil != 7)
+  // 13-point stencil: the whole-step pass for FP32 storage and the equations without
+  // curvature planes; the paired passes for FP64 and for the curvature-coupled
+  // equations, where they measured faster (N = 512, FP32_COMP, ms per step: KG-FRW
+  // whole-step 2.17 / paired 2.55; comoving 3.86 / 3.81, with an L2 prefetch of the
+  // curvature rows 4.45 / 3.81)
+  const int shape = shape_of(ctx->p.equation);
+  const bool coupled = shape == EQ_COMOV || shape == EQ_FIXED || shape == EQ_APPROX;
+  if ((f & CF_FLAG_PAIR_KERNELS) || (ctx->p.stencil != 7 && (!f32 || coupled)))
     return f32 ? rk4_steps_pairs_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)
                : rk4_steps_pairs_t<double>(ctx, d_state, t0, dt, step0, nsteps, st);
   return f32 ? rk4_steps_fused_t<float>(ctx, d_state, t0, dt, step0, nsteps, st)

@@ -364,31 +364,32 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
     yc[r1 * SP + col] = (S)cf.fma((T)bpi, f0);
   };
 
-  // L2 prefetch of the rows of plane p that phase 1 (curvature at t, t + dt/2, two
-  // planes later) and phase 2 (curvature at t + dt/2, t + dt and the lo words, three
-  // planes later) load straight from global memory: one thread per row and array, so
-  // those loads wait on L2 rather than HBM.
-  auto prefetch_plane = [&](int p) {
+  // L2 prefetch, one plane ahead, of what phases 1 and 2 load straight from global
+  // memory: the curvature at t and t + dt/2 of plane p for phase 1 (own and ring rows),
+  // and the curvature at t + dt and the lo words of plane p for phase 2 (own rows).  One
+  // thread per row and array issues it, so those loads wait on L2 rather than HBM; a
+  // lead of one plane (a few microseconds) covers the HBM latency without leaving the
+  // lines in L2 long enough to be evicted.
+  auto prefetch_rows = [&](int p, bool phase1) {
     if (tx != 0 || !colact) return;
     const bool own = ty < TYv;
-    if (own ? ty >= tye : !RINGW) return;
+    if (own ? ty >= tye : (!RINGW || !phase1)) return;
     const int gb = own ? b : wrap_n(ty == TYv ? b0 - 1 : b0 + tye, N);
     const long long off = NN * wrap_n(p, N) + (long long)N * gb + c0;
     const unsigned bytes = (unsigned)(twe * sizeof(S));
-    if constexpr (EqOf<EQ>::psi_plane) {
-      prefetch_l2(A.psi[0] + off, bytes);
-      if constexpr (EQ != EQ_FIXED) {
-        prefetch_l2(A.psi[1] + off, bytes);
-        if (own) prefetch_l2(A.psi[2] + off, bytes);
+    if (phase1) {
+      if constexpr (EqOf<EQ>::psi_plane) {
+        prefetch_l2(A.psi[0] + off, bytes);
+        if constexpr (EQ != EQ_FIXED) prefetch_l2(A.psi[1] + off, bytes);
       }
-    }
-    if constexpr (EqOf<EQ>::dpsi_plane) {
-      prefetch_l2(A.dpsi[0] + off, bytes);
-      prefetch_l2(A.dpsi[1] + off, bytes);
-      if (own) prefetch_l2(A.dpsi[2] + off, bytes);
-    }
-    if constexpr (sizeof(S) == 4) {
-      if (own) {
+      if constexpr (EqOf<EQ>::dpsi_plane) {
+        prefetch_l2(A.dpsi[0] + off, bytes);
+        prefetch_l2(A.dpsi[1] + off, bytes);
+      }
+    } else {
+      if constexpr (EqOf<EQ>::psi_plane && EQ != EQ_FIXED) prefetch_l2(A.psi[2] + off, bytes);
+      if constexpr (EqOf<EQ>::dpsi_plane) prefetch_l2(A.dpsi[2] + off, bytes);
+      if constexpr (sizeof(S) == 4) {
         prefetch_l2(A.xlo + off, bytes);
         prefetch_l2(A.xlo + N3 + off, bytes);
       }
@@ -397,14 +398,12 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
 
   issue(a_begin - 2);
   cp_async_commit();
-  prefetch_plane(a_begin - 2);
-  prefetch_plane(a_begin - 1);
   for (int p = a_begin - 2; p <= a_end + 1; ++p) {
-    if (p + 1 <= a_end + 1) {
-      issue(p + 1);
-      prefetch_plane(p + 1);
-    }
+    if (p + 1 <= a_end + 1) issue(p + 1);
     cp_async_commit();
+    // phase 1 takes plane p next iteration, phase 2 plane p - 1
+    if (p >= a_begin - 1 && p <= a_end) prefetch_rows(p, true);
+    if (p - 1 >= a_begin && p - 1 <= a_end - 1) prefetch_rows(p - 1, false);
     cp_async_wait_one();  // this thread's copies of plane p have landed
     __syncthreads();      // everyone's; and phase 2 of the last plane is done with YB / YC
 
@@ -464,7 +463,14 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
         for (int i = NT - 1 - tid; i < (tye + 2) * 2; i += NT)
           ring_site(q, qm, qoff, yb, yc, i >> 1, (i & 1) ? O + twe : O - 1);
     }
-    __syncthreads();  // yb_phi, yc_phi of plane q ready (with RINGW: its own sites and ring rows)
+    // Without ring warps the ring columns of plane q are formed above by the last warps,
+    // and the barrier makes them visible before phase 2.  With ring warps nothing after
+    // this point needs another thread's phase-1 result of this iteration: phase 2 of
+    // plane r reads plane q = r + 1 only at the thread's own sites (its a-neighbour,
+    // written by the same thread above) and plane r in full (formed last iteration,
+    // visible since the barrier at the top); the ring warps' ring columns of plane q
+    // read x only.  The barrier at the top of the next iteration orders all of it.
+    if constexpr (!RINGW) __syncthreads();
 
     // ---- RINGW: the ring columns of plane q, beside phase 2.  They read x of planes
     // q-1..q+1 (slot s4(q-1) is refilled by the next iteration's copies: its ring

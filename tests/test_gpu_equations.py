@@ -99,17 +99,19 @@ def test_rk4_matches_oracle(eq, stencil, prec, tol):
     assert rel(got[N ** 3:], want[N ** 3:]) <= tol
 
 
+@pytest.mark.parametrize("stencil", [7, 13])
 @pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
 @pytest.mark.parametrize("N", [64, 40])
 @pytest.mark.parametrize("eq", sorted(EQS))
-def test_pair_equals_stage_kernels_bitwise(eq, N, prec):
-    """Paired-stage passes (default) and the four single-stage kernels
-    (CF_FLAG_STAGE_KERNELS) give bit-identical states, odd and even step counts,
-    full tiles (N = 64) and ragged ones (N = 40)."""
+def test_pair_equals_stage_kernels_bitwise(eq, N, prec, stencil):
+    """The default route (the whole-step pass; for the 13-point stencil the
+    paired passes in FP64 and for the curvature-coupled equations) and the four
+    single-stage kernels (CF_FLAG_STAGE_KERNELS) give bit-identical states, odd and
+    even step counts, full tiles (N = 64) and ragged ones (N = 40)."""
     L = 0.9 * N
     out = []
     for flags in (0, cfb200.FLAG_STAGE_KERNELS):
-        c, x, _, _, _ = setup(N, L, eq, prec=prec, flags=flags, seed=21, M=8)
+        c, x, _, _, _ = setup(N, L, eq, prec=prec, stencil=stencil, flags=flags, seed=21, M=8)
         st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
         c.upload(st, x)
         c.rk4_steps(st, 1.0, 0.07, 3)
