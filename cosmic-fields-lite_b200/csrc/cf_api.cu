@@ -81,6 +81,8 @@ int s2_to_shells(cf_ctx *, double *, int64_t *, cudaStream_t);
 int s2_counts(cf_ctx *, int64_t *, cudaStream_t);
 int state_export(cf_ctx *, double *, const void *, cudaStream_t);
 int state_import(cf_ctx *, void *, const double *, cudaStream_t);
+int state_upload_host(cf_ctx *, void *, const double *, cudaStream_t);
+int state_download_host(cf_ctx *, double *, const void *, cudaStream_t);
 int check_finite(cf_ctx *, const void *, int64_t *, cudaStream_t);
 int adjoint_create(cf_ctx *, int64_t, int64_t, cf_adjoint **);
 void adjoint_destroy(cf_adjoint *);
@@ -293,6 +295,8 @@ int cf_destroy(cf_ctx *ctx) {
   cudaFree(ctx->bins);
   cudaFree(ctx->maxbits);
   cudaFree(ctx->s2_counts);
+  cudaFree(ctx->stage);
+  if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
   delete ctx;
   return CF_OK;
 }
@@ -326,15 +330,7 @@ int cf_state_upload(cf_ctx *ctx, void *d_state, const double *h_xy, void *stream
     CF_TRY_CUDA(cudaMemcpyAsync(d_state, h_xy, bytes, cudaMemcpyHostToDevice, st));
     return CF_OK;
   }
-  double *tmp = nullptr;
-  if (cudaMallocAsync((void **)&tmp, bytes, st) != cudaSuccess) {
-    set_error("cudaMallocAsync staging buffer failed");
-    return CF_ERR_NOMEM;
-  }
-  CF_TRY_CUDA(cudaMemcpyAsync(tmp, h_xy, bytes, cudaMemcpyHostToDevice, st));
-  int s = state_import(ctx, d_state, tmp, st);
-  CF_TRY_CUDA(cudaFreeAsync(tmp, st));
-  return s;
+  return state_upload_host(ctx, d_state, h_xy, st);
 }
 
 int cf_state_download(cf_ctx *ctx, double *h_xy, const void *d_state, void *stream) {
@@ -348,15 +344,7 @@ int cf_state_download(cf_ctx *ctx, double *h_xy, const void *d_state, void *stre
     CF_TRY_CUDA(cudaMemcpyAsync(h_xy, d_state, bytes, cudaMemcpyDeviceToHost, st));
     return CF_OK;
   }
-  double *tmp = nullptr;
-  if (cudaMallocAsync((void **)&tmp, bytes, st) != cudaSuccess) {
-    set_error("cudaMallocAsync staging buffer failed");
-    return CF_ERR_NOMEM;
-  }
-  int s = state_export(ctx, tmp, d_state, st);
-  if (s == CF_OK) CF_TRY_CUDA(cudaMemcpyAsync(h_xy, tmp, bytes, cudaMemcpyDeviceToHost, st));
-  CF_TRY_CUDA(cudaFreeAsync(tmp, st));
-  return s;
+  return state_download_host(ctx, h_xy, d_state, st);
 }
 
 int cf_state_import(cf_ctx *ctx, void *d_state, const double *d_xy, void *stream) {

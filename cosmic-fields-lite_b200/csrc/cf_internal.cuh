@@ -135,6 +135,12 @@ struct cf_ctx {
   double *ic_table = nullptr;
   unsigned long long *bins = nullptr;   // 2 * s2_bins words: (lo, hi) fixed point
   unsigned long long *maxbits = nullptr;
+  long long spec_mult = 0;  // scale multiplier of the last binning (bin_spectrum)
+  // Host <-> device transfers of an FP32_COMP state (cf_state_upload / download):
+  // two FP64 chunks used in turn, and the event that ends the last transfer.
+  double *stage = nullptr;
+  cudaEvent_t stage_ev = nullptr;
+  bool stage_used = false;
   int64_t *s2_counts = nullptr;
 
   // Profiling (cf_profile_enable): pending event pairs and per-kind totals.

@@ -269,6 +269,17 @@ __device__ __forceinline__ double e2m1_of(double psi) {
 // The same for a pair of FP32 values (a complex entry of pass C's output) with the
 // sm_100 paired FP32 instructions (FADD2 / FMUL2 / FFMA2): one instruction per Horner
 // step for both values, each component rounded exactly as the scalar form above.
+// e2m1_poly_pair: the polynomial alone, for values the caller has range-checked.
+__device__ __forceinline__ float2 e2m1_poly_pair(float2 psi) {
+  const float2 x = __fadd2_rn(psi, psi);  // 2 psi, exact
+  float2 q = make_float2(1.0f / 5040.0f, 1.0f / 5040.0f);
+  q = __ffma2_rn(q, x, make_float2(1.0f / 720.0f, 1.0f / 720.0f));
+  q = __ffma2_rn(q, x, make_float2(1.0f / 120.0f, 1.0f / 120.0f));
+  q = __ffma2_rn(q, x, make_float2(1.0f / 24.0f, 1.0f / 24.0f));
+  q = __ffma2_rn(q, x, make_float2(1.0f / 6.0f, 1.0f / 6.0f));
+  q = __ffma2_rn(q, x, make_float2(0.5f, 0.5f));
+  return __ffma2_rn(q, __fmul2_rn(x, x), x);
+}
 __device__ __forceinline__ float2 e2m1_pair(float2 psi) {
   const float2 x = __fadd2_rn(psi, psi);  // 2 psi, exact
   if (fabsf(x.x) > 0.25f || fabsf(x.y) > 0.25f) return make_float2(e2m1_of(psi.x), e2m1_of(psi.y));
@@ -313,6 +324,11 @@ __device__ __forceinline__ C c_mul_i(C a) {
 // same round-to-nearest sum as the scalar form.
 __device__ __forceinline__ float2 c_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+// FP32 complex product as FMUL2 + FFMA2: re = fma(a.x, b.x, rn(-a.y b.y)), im = fma(a.x,
+// b.y, rn(a.y b.x)) -- a fixed rounding, whatever contraction the compiler would pick.
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(a.x, a.x), b, __fmul2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x)));
+}
 
 __host__ __device__ constexpr int bit_reverse(int i, int R) {
   int r = 0;
@@ -323,29 +339,55 @@ __host__ __device__ constexpr int bit_reverse(int i, int R) {
   return r;
 }
 
+// Bit k set for the rows k < B and k >= R - B of an R-point DFT's input: the band of
+// a pruned line, whose other rows are zero.
+__host__ __device__ constexpr unsigned band_mask(int R, int B) {
+  return 2 * B >= R ? (R == 32 ? 0xffffffffu : (1u << R) - 1u) : ((1u << B) - 1u) | (((1u << B) - 1u) << (R - B));
+}
+
 // In-register R-point inverse DFT (e^{+2 pi i k m / R}), natural order in and out.
-template <typename S, int R>
+// NZ: bit k clear where the caller knows v[k] is zero.  Radix-2 butterflies with a
+// zero operand reduce to copies and negations (u + 0 = u, 0 + t = t and 0 - t = -t
+// exactly), decided at compile time once the loops are unrolled; the non-zero values
+// are bit-identical to the full butterfly network's.
+template <typename S, int R, unsigned NZ = 0xffffffffu>
 __device__ __forceinline__ void dft_inv(typename Cplx<S>::T (&v)[R], const Tw32<S> &tw) {
   static_assert(R >= 2 && R <= 32 && (R & (R - 1)) == 0, "radix");
   using C = typename Cplx<S>::T;
   C a[R];
+  bool nz[R];
 #pragma unroll
-  for (int i = 0; i < R; ++i) a[i] = v[bit_reverse(i, R)];
+  for (int i = 0; i < R; ++i) {
+    a[i] = v[bit_reverse(i, R)];
+    nz[i] = (NZ >> bit_reverse(i, R)) & 1u;
+  }
 #pragma unroll
   for (int len = 2; len <= R; len *= 2) {
 #pragma unroll
     for (int i = 0; i < R; i += len) {
 #pragma unroll
       for (int j = 0; j < len / 2; ++j) {
+        const int p = i + j, q = i + j + len / 2;
+        if (!nz[q]) {  // t = 0
+          a[q] = a[p];
+          nz[q] = nz[p];
+          continue;
+        }
         const int e = j * (32 / len);  // e^{2 pi i j / len} = e^{2 pi i e / 32}
-        C t = a[i + j + len / 2];
+        C t = a[q];
         if (e == 8)
           t = c_mul_i(t);
         else if (e != 0)
           t = c_mul(t, tw.w[e]);
-        const C u = a[i + j];
-        a[i + j] = c_add(u, t);
-        a[i + j + len / 2] = c_sub(u, t);
+        if (!nz[p]) {  // u = 0
+          a[p] = t;
+          a[q] = C{-t.x, -t.y};
+          nz[p] = true;
+        } else {
+          const C u = a[p];
+          a[p] = c_add(u, t);
+          a[q] = c_sub(u, t);
+        }
       }
     }
   }
@@ -354,8 +396,9 @@ __device__ __forceinline__ void dft_inv(typename Cplx<S>::T (&v)[R], const Tw32<
 }
 
 // B: Z is zero outside the k1 rows [0, B) and [R1 - B, R1) (the band |k| <= Kc
-// with B = ceil((Kc+1)/R2)); as a template argument those zeros are constants
-// and the pass-1 DFT drops the work on them.  B = R1/2 keeps every row.
+// with B = ceil((Kc+1)/R2)); as a template argument it gives the pass-1 DFT its
+// zero mask (band_mask), so the butterflies on those rows reduce to copies.
+// B = R1/2 keeps every row.
 template <typename S, int R1, int R2, int ROWS, int B>
 __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S *__restrict__ out,
                                                      const typename Cplx<S>::T *__restrict__ wN,
@@ -398,7 +441,7 @@ __global__ void __launch_bounds__(256) k_prune_c_fft(const S *__restrict__ pb, S
       }
       v[k1] = z;
     }
-    dft_inv<S, R1>(v, tw);
+    dft_inv<S, R1, band_mask(R1, B)>(v, tw);
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
       C y = v[m1];
@@ -493,7 +536,7 @@ __global__ void __launch_bounds__(256) k_prune_c_fft_p(const S *__restrict__ pb,
         }
         v[k1] = z;
       }
-      dft_inv<S, R1>(v, tw);
+      dft_inv<S, R1, band_mask(R1, B)>(v, tw);
 #pragma unroll
       for (int m1 = 0; m1 < R1; ++m1) {
         C y = v[m1];
@@ -523,30 +566,41 @@ __global__ void __launch_bounds__(256) k_prune_c_fft_p(const S *__restrict__ pb,
 
 // ---- pass C, one warp per row group (FP32, N = 256, 512, 1024) --------------
 // The same four-step arithmetic as k_prune_c_fft without a CTA barrier: a warp owns
-// RW = 32 / R1 consecutive rows of one (f, a) plane and does everything for them --
+// RW = 32 / R2 consecutive rows of one (f, a) plane and does everything for them --
 // copies the rows' Kc + 1 band entries into its own shared memory by cp.async (one
-// tile ahead, double-buffered), forms i X w^k, runs pass 1 (lane = (row, k2)) and
-// pass 2 (lane = (row, m1)) through a warp-private transpose with only __syncwarp
+// tile ahead, double-buffered), runs pass 1 with one lane per (row, k2) -- every lane
+// busy -- forming X + i X w^k from the staged X as it loads, then pass 2 with RW R1 / 32
+// (row, m1) tasks per lane through a warp-private transpose, with only __syncwarp
 // between them, and stores along the output rows.  Persistent: warps walk the tiles
-// (f, a, row group) with stride = warps in the grid, adjacent warps on adjacent rows
-// (their 8- or 16-byte input copies share sectors through L1).
+// (f, a, row group) with stride = warps in the grid, adjacent warps on adjacent rows.
+//
+// Shared layout per warp: X[buf][r][XPP] (XPP = 8 mod 16 complex, so the two rows a
+// half-warp reads when R2 = 8 sit on disjoint banks) and T[r][RP] with T[r] = [m1][TP],
+// TP = R2 + 1 odd (pass-2 reads free of bank conflicts) and RP = R2 mod 16 where R2 < 16.
+__host__ __device__ constexpr int pc_xpp(int kn) { return ((kn + 7) & ~15) + 8; }
+__host__ __device__ constexpr int pc_rp(int R1, int R2) {
+  return R2 >= 16 ? R1 * (R2 + 1) : R1 * (R2 + 1) + ((R2 - (R1 * (R2 + 1)) % 16) + 16) % 16;
+}
+
 template <int R1, int R2, int B>
 __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict__ pb, float *__restrict__ out,
                                                      const float2 *__restrict__ wN, const float2 *__restrict__ twM,
-                                                     int N, int Kc, int ntiles, int log2_groups, int log2_n,
-                                                     const __grid_constant__ Tw32<float> tw) {
+                                                     int N, int Kc, int tile0, int ntiles, int log2_groups,
+                                                     int log2_n, const __grid_constant__ Tw32<float> tw) {
   constexpr int M = R1 * R2;  // N == 2 M
-  constexpr int RW = 32 / R1;
-  constexpr int TP = R2 + 1;  // transpose row pitch (complex), odd: pass-2 reads free of bank conflicts
-  static_assert(RW >= 1 && R2 <= R1, "shape");
+  constexpr int RW = 32 / R2;
+  constexpr int TP = R2 + 1;
+  constexpr int RP = pc_rp(R1, R2);
+  constexpr int P2 = RW * R1 / 32;  // pass-2 tasks per lane
+  static_assert(R2 <= R1 && 32 % R2 == 0 && (RW * R1) % 32 == 0, "shape");
   extern __shared__ __align__(16) unsigned char smraw[];
   float2 *TW = reinterpret_cast<float2 *>(smraw);  // [R1][R2]: e^{2 pi i k2 m1 / M}
   float2 *WK = TW + M;                             // [Kc+1]: w^k
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kn = Kc + 1;
-  const int xw = ((kn * RW + 1) & ~1);  // complex per X buffer, even (16-byte aligned)
-  float2 *W = WK + ((kn + 1) & ~1) + (size_t)warp * (3 * xw + RW * R1 * TP);
-  float2 *X0 = W, *XP = W + 2 * xw, *T = W + 3 * xw;  // X: 2 buffers [k][r]; XP [k][r]; T [r][m1][TP]
+  const int xpp = pc_xpp(kn), xw = RW * xpp;  // complex per X buffer
+  float2 *W = WK + ((kn + 1) & ~1) + (size_t)warp * (2 * xw + RW * RP);
+  float2 *X0 = W, *T = W + 2 * xw;
   for (int i = threadIdx.x; i < M; i += blockDim.x) TW[i] = twM[i];
   for (int i = threadIdx.x; i < kn; i += blockDim.x) WK[i] = wN[i];
   __syncthreads();  // the only CTA barrier: the shared twiddles
@@ -555,18 +609,19 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
   const int gmask = (1 << log2_groups) - 1, nmask = (1 << log2_n) - 1;
   const long long NN = (long long)N * N;
   const int stride = gridDim.x * (blockDim.x >> 5);
-  int tile = blockIdx.x * (blockDim.x >> 5) + warp;
+  int tile = tile0 + blockIdx.x * (blockDim.x >> 5) + warp;  // tiles [tile0, ntiles)
   auto issue = [&](int t, float2 *dst) {
     const int g = t & gmask, fa = t >> log2_groups;
     const int a = fa & nmask, f = fa >> log2_n;
     const float2 *src = reinterpret_cast<const float2 *>(pb) + ((long long)f * kn * N + a) * N + g * RW + lane * NN;
-    const unsigned d0 = (unsigned)__cvta_generic_to_shared(dst + lane * RW);
+    const unsigned d0 = (unsigned)__cvta_generic_to_shared(dst + lane);
     for (int k = lane; k < kn; k += 32, src += 32 * NN) {
-      const unsigned d = d0 + (unsigned)((k - lane) * RW * sizeof(float2));
-      if constexpr (RW == 2)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-      else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+      const unsigned d = d0 + (unsigned)((k - lane) * sizeof(float2));
+#pragma unroll
+      for (int r = 0; r < RW; ++r)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d + (unsigned)(r * xpp * sizeof(float2))),
+                     "l"(src + r)
+                     : "memory");
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
@@ -582,63 +637,73 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
     __syncwarp();  // the tile's band entries (every lane's copies)
     const float2 *X = X0 + buf * xw;
     const int g = tile & gmask, fa = tile >> log2_groups;
-    // i X w^k (X[0] by its real part: the Hermitian projection of every C2R)
-    for (int i = lane; i < kn * RW; i += 32) {
-      const int k = i / RW;
-      float2 x = X[i];
-      if (k == 0) x.y = 0.0f;
-      XP[i] = c_mul_i(c_mul(x, WK[k]));
-    }
-    __syncwarp();
     // pass 1: lane (r, k2), an R1-point DFT over the band rows k1, times e^{2 pi i k2 m1 / M}
     {
-      const int r = lane / R1, k2 = lane % R1;
-      if (k2 < R2) {
-        float2 v[R1];
+      const int r = lane / R2, k2 = lane % R2;
+      const float2 *Xr = X + r * xpp;
+      float2 v[R1];
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) {
-          const int k = k2 + R2 * k1;
-          float2 z = make_float2(0.0f, 0.0f);
-          if (k1 >= B && k1 < R1 - B) {
-            // outside the band's rows: zero
-          } else if (k <= Kc) {
-            float2 x = X[k * RW + r];
-            if (k == 0) x.y = 0.0f;
-            z = c_add(x, XP[k * RW + r]);  // X + i X w^k
-          } else if (k >= M - Kc) {
-            const int j = M - k;
-            const float2 d = c_sub(X[j * RW + r], XP[j * RW + r]);  // conj(X - i X w^j)
+      for (int k1 = 0; k1 < R1; ++k1) {
+        // rows k1 < B hold k <= R2 B - 1 <= M/2 - 1 < M - Kc, rows k1 >= R1 - B hold
+        // k >= M/2 > Kc (Kc < M/2): each band half tests its own side only
+        const int k = k2 + R2 * k1;
+        float2 z = make_float2(0.0f, 0.0f);
+        if (k1 < B) {
+          if (k <= Kc) {
+            float2 x = Xr[k];
+            if (k == 0) x.y = 0.0f;  // X[0] by its real part: the Hermitian projection of every C2R
+            z = c_add(x, c_mul_i(c_mul(x, WK[k])));  // X + i X w^k
+          }
+        } else if (k1 >= R1 - B) {
+          const int j = M - k;
+          if (j <= Kc) {
+            const float2 x = Xr[j];
+            const float2 d = c_sub(x, c_mul_i(c_mul(x, WK[j])));  // conj(X - i X w^j)
             z = make_float2(d.x, -d.y);
           }
-          v[k1] = z;
         }
-        dft_inv<float, R1>(v, tw);
+        v[k1] = z;
+      }
+      dft_inv<float, R1, band_mask(R1, B)>(v, tw);
+      float2 *Tr = T + r * RP + k2;
 #pragma unroll
-        for (int m1 = 0; m1 < R1; ++m1) {
-          float2 y = v[m1];
-          if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
-          T[(r * R1 + m1) * TP + k2] = y;
-        }
+      for (int m1 = 0; m1 < R1; ++m1) {
+        float2 y = v[m1];
+        if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
+        Tr[m1 * TP] = y;
       }
     }
     __syncwarp();
-    // pass 2: lane (r, m1), an R2-point DFT over k2, giving z[m1 + R1 m2] of row r
-    {
-      const int r = lane / R1, m1 = lane % R1;
+    // pass 2: task (r, m1), an R2-point DFT over k2, giving z[m1 + R1 m2] of row r
+    const bool field0 = fa < N;  // f == 0: the slot holds e^{2 Psi} - 1
+#pragma unroll 1
+    for (int p = 0; p < P2; ++p) {
+      const int task = lane + 32 * p;
+      const int r = task / R1, m1 = task % R1;
       float2 u[R2];
+      const float2 *Tr = T + r * RP + m1 * TP;
 #pragma unroll
-      for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[(r * R1 + m1) * TP + k2];
+      for (int k2 = 0; k2 < R2; ++k2) u[k2] = Tr[k2];
       dft_inv<float, R2>(u, tw);
-      const bool field0 = fa < N;  // f == 0: the slot holds e^{2 Psi} - 1
       float2 *row = reinterpret_cast<float2 *>(out) + ((long long)fa * N + g * RW + r) * M;
+      if (field0) {
+        // one range test for the lane's R2 values: all inside |2 Psi| <= 1/4 takes the
+        // polynomial directly; otherwise e2m1_pair decides per value as everywhere else
+        float mx = 0.0f;
 #pragma unroll
-      for (int m2 = 0; m2 < R2; ++m2) {
-        float2 o = u[m2];
-        if (field0) o = e2m1_pair(o);
-        row[m1 + R1 * m2] = o;
+        for (int m2 = 0; m2 < R2; ++m2) mx = fmaxf(mx, fmaxf(fabsf(u[m2].x), fabsf(u[m2].y)));
+        if (2.0f * mx <= 0.25f) {
+#pragma unroll
+          for (int m2 = 0; m2 < R2; ++m2) u[m2] = e2m1_poly_pair(u[m2]);
+        } else {
+#pragma unroll
+          for (int m2 = 0; m2 < R2; ++m2) u[m2] = e2m1_pair(u[m2]);
+        }
       }
+#pragma unroll
+      for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
     }
-    __syncwarp();  // T, XP and this X buffer are free for the next tile
+    __syncwarp();  // T and this X buffer are free for the next tile
     buf ^= 1;
   }
 }
@@ -653,12 +718,12 @@ static bool pc_warp_shape(long long N, size_t word, int *R1, int *R2) {
   }
 }
 static size_t pc_warp_smem(int Kc, int R1, int R2) {
-  const int RW = 32 / R1, kn = Kc + 1, xw = (kn * RW + 1) & ~1;
-  return ((size_t)R1 * R2 + ((kn + 1) & ~1) + 8 * (size_t)(3 * xw + RW * R1 * (R2 + 1))) * sizeof(float2);
+  const int RW = 32 / R2, kn = Kc + 1;
+  return ((size_t)R1 * R2 + ((kn + 1) & ~1) + 8 * (size_t)(2 * RW * pc_xpp(kn) + RW * pc_rp(R1, R2))) * sizeof(float2);
 }
 
 template <int R1, int R2, int B>
-static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st, int f0, int nf) {
   auto kern = k_prune_c_warp<R1, R2, B>;
   if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Tw32<float> tw;
@@ -669,36 +734,37 @@ static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st
   int sms = 0, per_sm = 0;
   CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
   CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
-  const int N = (int)ctx->N, groups = N / (32 / R1);
-  const int ntiles = 2 * N * groups;
+  const int N = (int)ctx->N, groups = N / (32 / R2);
+  const int tile0 = f0 * N * groups, ntiles = (f0 + nf) * N * groups;  // fields [f0, f0 + nf)
   int log2_n = 0, log2_g = 0;
   while ((1 << log2_n) < N) ++log2_n;
   while ((1 << log2_g) < groups) ++log2_g;
-  const int grid = std::max(1, std::min((ntiles + 7) / 8, sms * std::max(per_sm, 1)));
+  const int grid = std::max(1, std::min((ntiles - tile0 + 7) / 8, sms * std::max(per_sm, 1)));
   kern<<<(unsigned)grid, 256, smem, st>>>((const float *)ctx->pz_b, (float *)out, (const float2 *)ctx->pr_wN,
-                                          (const float2 *)ctx->pr_twM, N, ctx->Kc, ntiles, log2_g, log2_n, tw);
+                                          (const float2 *)ctx->pr_twM, N, ctx->Kc, tile0, ntiles, log2_g, log2_n,
+                                          tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
 
 // The smallest compiled band B >= ceil((Kc+1)/R2).
 template <int R1, int R2>
-static int launch_pc_warp_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st) {
+static int launch_pc_warp_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st, int f0, int nf) {
   const int need = (ctx->Kc + 1 + R2 - 1) / R2;
-  if (need <= 2) return launch_pc_warp_b<R1, R2, 2>(ctx, out, smem, st);
-  if (need <= 3) return launch_pc_warp_b<R1, R2, 3>(ctx, out, smem, st);
-  if (need <= 4) return launch_pc_warp_b<R1, R2, 4>(ctx, out, smem, st);
-  if (need <= 6) return launch_pc_warp_b<R1, R2, 6>(ctx, out, smem, st);
-  return launch_pc_warp_b<R1, R2, R1 / 2>(ctx, out, smem, st);
+  if (need <= 2) return launch_pc_warp_b<R1, R2, 2>(ctx, out, smem, st, f0, nf);
+  if (need <= 3) return launch_pc_warp_b<R1, R2, 3>(ctx, out, smem, st, f0, nf);
+  if (need <= 4) return launch_pc_warp_b<R1, R2, 4>(ctx, out, smem, st, f0, nf);
+  if (need <= 6) return launch_pc_warp_b<R1, R2, 6>(ctx, out, smem, st, f0, nf);
+  return launch_pc_warp_b<R1, R2, R1 / 2>(ctx, out, smem, st, f0, nf);
 }
 
-static int launch_pc_warp(cf_ctx *ctx, void *out, cudaStream_t st) {
+static int launch_pc_warp(cf_ctx *ctx, void *out, cudaStream_t st, int f0 = 0, int nf = 2) {
   int R1 = 0, R2 = 0;
   if (!pc_warp_shape(ctx->N, ctx->word, &R1, &R2)) return set_error("warp pass C: unsupported N"), CF_ERR_INVALID;
   const size_t smem = pc_warp_smem(ctx->Kc, R1, R2);
-  if (R1 == 16 && R2 == 8) return launch_pc_warp_t<16, 8>(ctx, out, smem, st);
-  if (R1 == 16 && R2 == 16) return launch_pc_warp_t<16, 16>(ctx, out, smem, st);
-  return launch_pc_warp_t<32, 16>(ctx, out, smem, st);
+  if (R1 == 16 && R2 == 8) return launch_pc_warp_t<16, 8>(ctx, out, smem, st, f0, nf);
+  if (R1 == 16 && R2 == 16) return launch_pc_warp_t<16, 16>(ctx, out, smem, st, f0, nf);
+  return launch_pc_warp_t<32, 16>(ctx, out, smem, st, f0, nf);
 }
 
 // ---- pass B as one kernel: pruned lines -> full lines -----------------------
@@ -716,7 +782,7 @@ static int launch_pc_warp(cf_ctx *ctx, void *out, cudaStream_t st) {
 template <typename S, int R1, int R2, int LINES, int B>
 __global__ void __launch_bounds__(R2 *LINES) k_pass_b_fft(const S *__restrict__ pa, S *__restrict__ pb,
                                                          const typename Cplx<S>::T *__restrict__ twN, int N, int Kb,
-                                                         int Kc, const __grid_constant__ Tw32<S> tw) {
+                                                         int Kc, int f0, const __grid_constant__ Tw32<S> tw) {
   using C = typename Cplx<S>::T;
   constexpr int TS = R2 * LINES + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -724,7 +790,7 @@ __global__ void __launch_bounds__(R2 *LINES) k_pass_b_fft(const S *__restrict__ 
   C *TW = T + R1 * TS;                  // [R1][R2]: e^{2 pi i k2 m1 / N}
   C *Ys = TW + R1 * R2;                 // [2Kb+1][LINES]
   const int nj = 2 * Kb + 1;
-  const int a0 = blockIdx.x * LINES, k = blockIdx.y, f = blockIdx.z;
+  const int a0 = blockIdx.x * LINES, k = blockIdx.y, f = f0 + (int)blockIdx.z;
   const long long fk = (long long)f * (Kc + 1) + k;
   const C *src = reinterpret_cast<const C *>(pa) + fk * nj * N + a0;
   for (int i = threadIdx.x; i < R1 * R2; i += blockDim.x) TW[i] = twN[i];
@@ -749,7 +815,7 @@ __global__ void __launch_bounds__(R2 *LINES) k_pass_b_fft(const S *__restrict__ 
       }
       v[k1] = z;
     }
-    dft_inv<S, R1>(v, tw);
+    dft_inv<S, R1, band_mask(R1, B)>(v, tw);
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
       C y = v[m1];
@@ -782,7 +848,7 @@ static bool pb_shape(long long N, size_t word, PbShape *sh) {
     case 64: *sh = PbShape{8, 8, 16}; break;
     case 128: *sh = PbShape{16, 8, 16}; break;
     case 256: *sh = PbShape{16, 16, 16}; break;
-    case 512: *sh = PbShape{32, 16, 16}; break;
+    case 512: *sh = PbShape{32, 16, 8}; break;  // 8 lines: 42 KB of shared memory, 5 CTAs per SM
     default: *sh = PbShape{32, 32, 8}; break;
   }
   return true;
@@ -793,7 +859,7 @@ static size_t pb_fused_smem(const cf_ctx *ctx, const PbShape &sh) {
 }
 
 template <typename S, int R1, int R2, int LINES, int B>
-static int launch_pb_fused_b(cf_ctx *ctx, size_t smem, cudaStream_t st) {
+static int launch_pb_fused_b(cf_ctx *ctx, size_t smem, cudaStream_t st, int f0, int nf) {
   using C = typename Cplx<S>::T;
   auto kern = k_pass_b_fft<S, R1, R2, LINES, B>;
   if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -803,36 +869,36 @@ static int launch_pb_fused_b(cf_ctx *ctx, size_t smem, cudaStream_t st) {
     tw.w[e] = C{(S)std::cos(ang), (S)std::sin(ang)};
   }
   const int N = (int)ctx->N;
-  kern<<<dim3(N / LINES, ctx->Kc + 1, 2), R2 * LINES, smem, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b,
-                                                                   (const C *)ctx->pr_twB, N, ctx->Kb, ctx->Kc, tw);
+  kern<<<dim3(N / LINES, ctx->Kc + 1, nf), R2 * LINES, smem, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b,
+                                                                    (const C *)ctx->pr_twB, N, ctx->Kb, ctx->Kc, f0, tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
 
 // The smallest compiled band B >= ceil((Kb+1)/R2) (2, 3, 4, 6 or all rows).
 template <typename S, int R1, int R2, int LINES>
-static int launch_pb_fused_t(cf_ctx *ctx, size_t smem, cudaStream_t st) {
+static int launch_pb_fused_t(cf_ctx *ctx, size_t smem, cudaStream_t st, int f0, int nf) {
   const int need = (ctx->Kb + 1 + R2 - 1) / R2;
   if constexpr (R1 >= 16) {
-    if (need <= 2) return launch_pb_fused_b<S, R1, R2, LINES, 2>(ctx, smem, st);
-    if (need <= 3) return launch_pb_fused_b<S, R1, R2, LINES, 3>(ctx, smem, st);
-    if (need <= 4) return launch_pb_fused_b<S, R1, R2, LINES, 4>(ctx, smem, st);
-    if (need <= 6) return launch_pb_fused_b<S, R1, R2, LINES, 6>(ctx, smem, st);
+    if (need <= 2) return launch_pb_fused_b<S, R1, R2, LINES, 2>(ctx, smem, st, f0, nf);
+    if (need <= 3) return launch_pb_fused_b<S, R1, R2, LINES, 3>(ctx, smem, st, f0, nf);
+    if (need <= 4) return launch_pb_fused_b<S, R1, R2, LINES, 4>(ctx, smem, st, f0, nf);
+    if (need <= 6) return launch_pb_fused_b<S, R1, R2, LINES, 6>(ctx, smem, st, f0, nf);
   }
-  return launch_pb_fused_b<S, R1, R2, LINES, R1 / 2>(ctx, smem, st);
+  return launch_pb_fused_b<S, R1, R2, LINES, R1 / 2>(ctx, smem, st, f0, nf);
 }
 
-static int launch_pb_fused(cf_ctx *ctx, cudaStream_t st) {
+static int launch_pb_fused(cf_ctx *ctx, cudaStream_t st, int f0 = 0, int nf = 2) {
   PbShape sh;
   if (!pb_shape(ctx->N, ctx->word, &sh)) return set_error("fused pass B: unsupported N"), CF_ERR_INVALID;
   const size_t smem = pb_fused_smem(ctx, sh);
 #define CF_PB(r1, r2, ln) \
-  if (sh.R1 == r1 && sh.R2 == r2 && sh.lines == ln) return launch_pb_fused_t<float, r1, r2, ln>(ctx, smem, st);
+  if (sh.R1 == r1 && sh.R2 == r2 && sh.lines == ln) return launch_pb_fused_t<float, r1, r2, ln>(ctx, smem, st, f0, nf);
   CF_PB(8, 4, 16)
   CF_PB(8, 8, 16)
   CF_PB(16, 8, 16)
   CF_PB(16, 16, 16)
-  CF_PB(32, 16, 16)
+  CF_PB(32, 16, 8)
   CF_PB(32, 32, 8)
 #undef CF_PB
   set_error("fused pass B: no kernel for R1=%d R2=%d lines=%d", sh.R1, sh.R2, sh.lines);
@@ -1141,6 +1207,9 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
     else
       CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pa, (cufftComplex *)ctx->pz_a, (cufftComplex *)ctx->pz_a, CUFFT_INVERSE));
   }
+  int R1w = 0, R2w = 0;
+  const bool warp_c = ctx->pc_fused && !(ctx->p.flags & CF_FLAG_PSI_CTA_PASS_C) &&
+                      pc_warp_shape(ctx->N, ctx->word, &R1w, &R2w) && pc_warp_smem(ctx->Kc, R1w, R2w) <= kPcFusedSmemMax;
   if (ctx->pb_fused) {
     ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
     CF_TRY(launch_pb_fused(ctx, st));
@@ -1161,10 +1230,7 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
   }
   if (ctx->pc_fused) {
     ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
-    int R1 = 0, R2 = 0;
-    if (!(ctx->p.flags & CF_FLAG_PSI_CTA_PASS_C) && pc_warp_shape(ctx->N, ctx->word, &R1, &R2) &&
-        pc_warp_smem(ctx->Kc, R1, R2) <= kPcFusedSmemMax)
-      return launch_pc_warp(ctx, out, st);
+    if (warp_c) return launch_pc_warp(ctx, out, st);
     return launch_pc_fused<S>(ctx, out, st);
   }
   {

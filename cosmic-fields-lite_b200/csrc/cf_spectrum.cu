@@ -3,11 +3,13 @@
 // The reference bins |f_k|^2 into s^2 bins with FP64 atomicAdd, whose result
 // depends on the order the atomics land in (src/fdm3d_cuda.cu:3-27, comment at
 // :25).  Here every mode value is converted to a 128-bit fixed-point integer
-// whose scale is a power of two chosen from the (order-independent) maximum
-// mode value, and the bins accumulate those integers with 64-bit integer
-// atomics (carry propagated to the high word).  Integer addition is
-// associative, so the bins are bit-reproducible, and the sums are exact up to
-// the fixed-point resolution (2^-126 of an upper bound on any bin).
+// whose scale is a power of two chosen from an order-independent upper bound on
+// any bin -- the largest mode value times the entry count (a max pass over the
+// modes), or for the density spectrum N^5 times the largest row sum of rho^2,
+// formed by the energy pass itself (Parseval) -- and the bins accumulate those
+// integers with 64-bit integer atomics (carry propagated to the high word).
+// Integer addition is associative, so the bins are bit-reproducible, and the
+// sums are exact up to the fixed-point resolution (2^-126 of the bound).
 // Unit-width |k| shells are then exact integer regroupings of the s^2 bins.
 
 #include <cuda_runtime.h>
@@ -31,12 +33,17 @@ namespace cfb {
 // the same value without the cancellation of sqrt(1 + u) - 1 at small u.
 enum EdKind : int { ED_QUAD = 0, ED_LAMBDA = 1, ED_SQRT = 2, ED_CURV = 3 };
 
+// With `rowmax` set, the block also forms its row's sum of rho^2 (fixed order: the
+// thread's c values in turn, then a shuffle tree, then the warps in turn) and folds it
+// into *rowmax with an integer max of the bit pattern; N^2 times the largest row sum
+// bounds sum_x rho^2, which Parseval turns into a bound on every spectrum bin.
 template <typename S, int ED>
 __global__ void __launch_bounds__(128) k_energy(const S *__restrict__ x, const S *__restrict__ xlo,
                                                 const S *__restrict__ psi, double *__restrict__ rho, int N, double m2,
-                                                double inv, double q) {
+                                                double inv, double q, unsigned long long *__restrict__ rowmax) {
   // one lattice row (a, b) per block, threads along c: the row's neighbour rows are
   // found once, only c wraps per site
+  double ss = 0.0;
   const long long N3 = (long long)N * N * N;
   const long long NN = (long long)N * N;
   const int a = (int)(blockIdx.x / (unsigned)N), b = (int)(blockIdx.x - (unsigned)a * (unsigned)N);
@@ -58,16 +65,29 @@ __global__ void __launch_bounds__(128) k_energy(const S *__restrict__ x, const S
     const double f = phi(i);
     double p = (double)x[N3 + i];
     if (xlo) p += (double)xlo[N3 + i];
+    double r;
     if constexpr (ED == ED_CURV) {
       const double e2 = 1.0 + (double)psi[i];
-      rho[i] = 0.5 * (p * p / e2 + m2 * f * f + e2 * 0.25 * inv * grad);
+      r = 0.5 * (p * p / e2 + m2 * f * f + e2 * 0.25 * inv * grad);
     } else if constexpr (ED == ED_LAMBDA) {
-      rho[i] = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad) + 0.25 * q * f * f * f * f;
+      r = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad) + 0.25 * q * f * f * f * f;
     } else if constexpr (ED == ED_SQRT) {  // q = 1 / f_a^2
-      rho[i] = 0.5 * (p * p + 0.25 * inv * grad) + m2 * f * f / (sqrt(1.0 + f * f * q) + 1.0);
+      r = 0.5 * (p * p + 0.25 * inv * grad) + m2 * f * f / (sqrt(1.0 + f * f * q) + 1.0);
     } else {
-      rho[i] = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad);
+      r = 0.5 * (p * p + m2 * f * f + 0.25 * inv * grad);
     }
+    rho[i] = r;
+    ss += r * r;
+  }
+  if (!rowmax) return;  // uniform over the block
+  __shared__ double part[4];
+  for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = ss;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double t = ((part[0] + part[1]) + part[2]) + part[3];
+    // non-negative doubles order like their bit patterns
+    atomicMax(rowmax, (unsigned long long)__double_as_longlong(t));
   }
 }
 
@@ -437,8 +457,13 @@ int ensure_spectrum_scratch(cf_ctx *ctx, int nfields) {
 }
 
 // Bins the HC data already in ctx->spec_hc (1 field, or phi/dphi for the mode spectrum).
-static int bin_spectrum(cf_ctx *ctx, bool mode, double a_t, double *d_out, cudaStream_t st) {
-  const long long pairs = ctx->hc_count / 2;
+// bound_mult = 0: a max pass finds the largest weighted mode value and the scale bounds
+// it times the HC entry count.  bound_mult > 0: ctx->maxbits already holds a value m
+// with m * bound_mult >= the sum of all weighted mode values.
+static int bin_spectrum(cf_ctx *ctx, bool mode, double a_t, double *d_out, cudaStream_t st,
+                        long long bound_mult = 0) {
+  const long long pairs = bound_mult > 0 ? bound_mult : ctx->hc_count / 2;
+  ctx->spec_mult = pairs;
   SpecIn A{};
   A.f = ctx->spec_hc;
   A.g = mode ? ctx->spec_hc + ctx->hc_count : nullptr;
@@ -448,10 +473,12 @@ static int bin_spectrum(cf_ctx *ctx, bool mode, double a_t, double *d_out, cudaS
   A.m2 = ctx->p.m * ctx->p.m;
   A.a2 = a_t * a_t;
   ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
-  CF_TRY_CUDA(cudaMemsetAsync(ctx->maxbits, 0, sizeof(unsigned long long), st));
   CF_TRY_CUDA(cudaMemsetAsync(ctx->bins, 0, 2 * (size_t)ctx->s2_bins * sizeof(unsigned long long), st));
-  k_spec_max<<<orbit_blocks(A.N), 256, 0, st>>>(A, 0, ctx->maxbits);
-  CF_LAUNCHED(ctx);
+  if (bound_mult <= 0) {
+    CF_TRY_CUDA(cudaMemsetAsync(ctx->maxbits, 0, sizeof(unsigned long long), st));
+    k_spec_max<<<orbit_blocks(A.N), 256, 0, st>>>(A, 0, ctx->maxbits);
+    CF_LAUNCHED(ctx);
+  }
   k_spec_bin<<<orbit_blocks(A.N), 256, 0, st>>>(A, 0, pairs, ctx->maxbits, ctx->bins, ctx->s2_bins);
   CF_LAUNCHED(ctx);
   if (d_out) {
@@ -499,23 +526,25 @@ int mode_power_spectrum_s2(cf_ctx *ctx, const void *d_state, double a_t, double 
 
 template <typename S, int ED>
 static void launch_energy(cf_ctx *ctx, const void *d_state, const void *psi, double *d_rho, double m2, double inv,
-                          double q, cudaStream_t st) {
+                          double q, unsigned long long *rowmax, cudaStream_t st) {
   const long long N3 = ctx->N3;
   const S *x = (const S *)d_state;
-  k_energy<S, ED><<<(unsigned)(ctx->N * ctx->N), 128, 0, st>>>(x, sizeof(S) == 4 ? x + 2 * N3 : nullptr, (const S *)psi, d_rho,
-                                                (int)ctx->N, m2, inv, q);
+  k_energy<S, ED><<<(unsigned)(ctx->N * ctx->N), 128, 0, st>>>(x, sizeof(S) == 4 ? x + 2 * N3 : nullptr,
+                                                               (const S *)psi, d_rho, (int)ctx->N, m2, inv, q, rowmax);
 }
 
 template <int ED>
 static void launch_energy_p(cf_ctx *ctx, const void *d_state, const void *psi, double *d_rho, double m2, double inv,
-                            double q, cudaStream_t st) {
+                            double q, unsigned long long *rowmax, cudaStream_t st) {
   if (ctx->p.precision == CF_FP32_COMP)
-    launch_energy<float, ED>(ctx, d_state, psi, d_rho, m2, inv, q, st);
+    launch_energy<float, ED>(ctx, d_state, psi, d_rho, m2, inv, q, rowmax, st);
   else
-    launch_energy<double, ED>(ctx, d_state, psi, d_rho, m2, inv, q, st);
+    launch_energy<double, ED>(ctx, d_state, psi, d_rho, m2, inv, q, rowmax, st);
 }
 
-int energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, cudaStream_t st) {
+// `rowmax` (optional, zeroed by the caller): receives the largest row sum of rho^2.
+static int energy_density_b(cf_ctx *ctx, const void *d_state, double t, double *d_rho, unsigned long long *rowmax,
+                            cudaStream_t st) {
   double inv, H;
   stage_coeffs(ctx->p, t, &inv, &H);
   const double m2 = ctx->p.m * ctx->p.m;
@@ -527,15 +556,19 @@ int energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, cu
   if (eq == CF_EQ_FIXED_CURVATURE_FRW) ps = ctx->fixed_e2m1;
   ProfScope prof(ctx, CF_PROF_SPECTRUM, st);
   if (ps)
-    launch_energy_p<ED_CURV>(ctx, d_state, ps, d_rho, m2, inv, 0.0, st);
+    launch_energy_p<ED_CURV>(ctx, d_state, ps, d_rho, m2, inv, 0.0, rowmax, st);
   else if (eq == CF_EQ_LAMBDA_FRW)
-    launch_energy_p<ED_LAMBDA>(ctx, d_state, nullptr, d_rho, m2, inv, ctx->p.lambda, st);
+    launch_energy_p<ED_LAMBDA>(ctx, d_state, nullptr, d_rho, m2, inv, ctx->p.lambda, rowmax, st);
   else if (eq == CF_EQ_SQRT_FRW)
-    launch_energy_p<ED_SQRT>(ctx, d_state, nullptr, d_rho, m2, inv, 1.0 / (ctx->p.f_a * ctx->p.f_a), st);
+    launch_energy_p<ED_SQRT>(ctx, d_state, nullptr, d_rho, m2, inv, 1.0 / (ctx->p.f_a * ctx->p.f_a), rowmax, st);
   else
-    launch_energy_p<ED_QUAD>(ctx, d_state, nullptr, d_rho, m2, inv, 0.0, st);
+    launch_energy_p<ED_QUAD>(ctx, d_state, nullptr, d_rho, m2, inv, 0.0, rowmax, st);
   CF_LAUNCHED(ctx);
   return CF_OK;
+}
+
+int energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_rho, cudaStream_t st) {
+  return energy_density_b(ctx, d_state, t, d_rho, nullptr, st);
 }
 
 int dot_energy_density(cf_ctx *ctx, const void *d_state, double t, double *d_out, cudaStream_t st) {
@@ -579,15 +612,25 @@ int density_slices(cf_ctx *ctx, const void *d_state, double t, double *d_slice, 
   return CF_OK;
 }
 
+// The fixed-point scale comes from the energy pass: by Parseval the weighted HC
+// values of rho sum to N^3 sum_x rho^2 <= N^5 max_row sum_c rho^2, so no bin can
+// exceed that bound, and the binning needs no pass of its own to find a maximum.
 int density_spectrum_s2(cf_ctx *ctx, const void *d_state, double t, double *d_out, cudaStream_t st) {
   CF_TRY(ensure_spectrum_scratch(ctx, 1));
-  CF_TRY(energy_density(ctx, d_state, t, ctx->spec_field, st));
-  return power_spectrum_s2(ctx, ctx->spec_field, d_out, st);
+  CF_TRY_CUDA(cudaMemsetAsync(ctx->maxbits, 0, sizeof(unsigned long long), st));
+  CF_TRY(energy_density_b(ctx, d_state, t, ctx->spec_field, ctx->maxbits, st));
+  CF_TRY_CUFFT(cufftSetStream(ctx->plan_d2z1, st));
+  {
+    ProfScope ps(ctx, CF_PROF_SPECTRUM, st);
+    CF_TRY_CUFFT(cufftExecD2Z(ctx->plan_d2z1, (cufftDoubleReal *)ctx->spec_field, (cufftDoubleComplex *)ctx->spec_hc));
+  }
+  const long long N = ctx->N;
+  return bin_spectrum(ctx, false, 1.0, d_out, st, N * N * N * N * N);
 }
 
 int s2_to_shells(cf_ctx *ctx, double *d_shells, int64_t *d_counts, cudaStream_t st) {
   CF_TRY(ensure_spectrum_scratch(ctx, 0));
-  k_shells<<<grid_for(ctx->shells, 128), 128, 0, st>>>(ctx->bins, ctx->maxbits, ctx->hc_count / 2,
+  k_shells<<<grid_for(ctx->shells, 128), 128, 0, st>>>(ctx->bins, ctx->maxbits, ctx->spec_mult,
                                                        (const long long *)ctx->s2_counts, d_shells,
                                                        (long long *)d_counts, ctx->s2_bins, ctx->shells);
   CF_LAUNCHED(ctx);
@@ -621,6 +664,77 @@ int state_import(cf_ctx *ctx, void *d_state, const double *d_xy, cudaStream_t st
   k_import_f32<<<grid_for(n2), 256, 0, st>>>(d_xy, (float *)d_state, n2);
   CF_LAUNCHED(ctx);
   return CF_OK;
+}
+
+// ---- host <-> device state transfer of the FP32_COMP layout ------------------
+// The FP64 [phi | pi] host array goes through two device chunks of the context
+// (allocated once, kStageChunk doubles each) in turn: a chunk's copy and its
+// conversion are ordered on the caller's stream, and chunk i + 2 reuses chunk i's
+// buffer after its conversion.  An event recorded after the last chunk orders the
+// next transfer, on whatever stream it runs, behind this one.
+__global__ void k_import_f32_part(const double *__restrict__ in, float *__restrict__ s, long long n2, long long off,
+                                  long long len) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
+    const double v = in[i];
+    const float h = (float)v;
+    s[off + i] = h;
+    s[n2 + off + i] = (float)(v - (double)h);
+  }
+}
+
+__global__ void k_export_f32_part(const float *__restrict__ s, double *__restrict__ out, long long n2, long long off,
+                                  long long len) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride)
+    out[i] = (double)s[off + i] + (double)s[n2 + off + i];
+}
+
+static constexpr long long kStageChunk = 16LL << 20;  // doubles per chunk (128 MB)
+
+static int stage_begin(cf_ctx *ctx, cudaStream_t st) {
+  if (!ctx->stage) {
+    if (cudaMalloc(&ctx->stage, 2 * kStageChunk * sizeof(double)) != cudaSuccess) {
+      ctx->stage = nullptr;
+      set_error("cudaMalloc state staging chunks failed");
+      return CF_ERR_NOMEM;
+    }
+    CF_TRY_CUDA(cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming));
+  }
+  if (ctx->stage_used) CF_TRY_CUDA(cudaStreamWaitEvent(st, ctx->stage_ev, 0));
+  return CF_OK;
+}
+
+static int stage_end(cf_ctx *ctx, cudaStream_t st) {
+  CF_TRY_CUDA(cudaEventRecord(ctx->stage_ev, st));
+  ctx->stage_used = true;
+  return CF_OK;
+}
+
+int state_upload_host(cf_ctx *ctx, void *d_state, const double *h_xy, cudaStream_t st) {
+  CF_TRY(stage_begin(ctx, st));
+  const long long n2 = 2 * ctx->N3;
+  for (long long off = 0, i = 0; off < n2; off += kStageChunk, ++i) {
+    const long long len = std::min(kStageChunk, n2 - off);
+    double *buf = ctx->stage + (i & 1) * kStageChunk;
+    CF_TRY_CUDA(cudaMemcpyAsync(buf, h_xy + off, len * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_import_f32_part<<<grid_for(len), 256, 0, st>>>(buf, (float *)d_state, n2, off, len);
+    CF_LAUNCHED(ctx);
+  }
+  return stage_end(ctx, st);
+}
+
+int state_download_host(cf_ctx *ctx, double *h_xy, const void *d_state, cudaStream_t st) {
+  CF_TRY(stage_begin(ctx, st));
+  const long long n2 = 2 * ctx->N3;
+  for (long long off = 0, i = 0; off < n2; off += kStageChunk, ++i) {
+    const long long len = std::min(kStageChunk, n2 - off);
+    double *buf = ctx->stage + (i & 1) * kStageChunk;
+    k_export_f32_part<<<grid_for(len), 256, 0, st>>>((const float *)d_state, buf, n2, off, len);
+    CF_LAUNCHED(ctx);
+    CF_TRY_CUDA(cudaMemcpyAsync(h_xy + off, buf, len * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  return stage_end(ctx, st);
 }
 
 int check_finite(cf_ctx *ctx, const void *d_state, int64_t *h_bad, cudaStream_t st) {

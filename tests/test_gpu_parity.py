@@ -325,6 +325,46 @@ def test_power_spectrum_s2_matches_oracle_and_reference(N):
         assert rel(got, O.ref_power_spectrum(f)) <= 1e-12
 
 
+@pytest.mark.parametrize("eq,prec", [(1, cfb200.FP64), (1, cfb200.FP32_COMP), (2, cfb200.FP32_COMP)])
+def test_density_spectrum_equals_power_spectrum_of_energy_density(eq, prec):
+    """The density spectrum takes its fixed-point scale from the energy pass (a Parseval
+    bound) instead of a max pass: per bin it is the power spectrum of the energy density
+    to the fixed-point resolution, and the shells regroup its own bins."""
+    N, L = 48, 38.4
+    x, Rf = make_inputs(N, L, eq, 21)
+    c = ctx_for(N, L, eq, prec)
+    if Rf is not None:
+        c.set_R_fft(Rf, on_device=False)
+    st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+    c.upload(st, x)
+    t = 2.5
+    rho = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
+    c.energy_density(st, t, rho)
+    a = torch.empty(O.n_s2(N), dtype=torch.float64, device="cuda")
+    b = torch.empty_like(a)
+    c.power_spectrum_s2(rho, a)
+    c.density_spectrum_s2(st, t, b)
+    sh = torch.empty(O.n_shells(N), dtype=torch.float64, device="cuda")
+    c.s2_to_shells(sh, None)
+    A, B = a.cpu().numpy(), b.cpu().numpy()
+    # both are truncations of the same FP64 mode values; a value loses less than one
+    # fixed-point unit, 2^-125 of the scale bound: (largest mode value) x (HC entries)
+    # for the power spectrum, N^5 x (largest row sum of rho^2) for the density spectrum;
+    # the conversion of a bin's 128-bit sum back to FP64 rounds (< 2 ulp)
+    counts = torch.empty(O.n_s2(N), dtype=torch.int64, device="cuda")
+    c.s2_counts(counts)
+    r = rho.cpu().numpy().reshape(N * N, N)
+    bound_a = A.max() * N * N * (N // 2 + 1)
+    bound_b = float(N) ** 5 * (r * r).sum(axis=1).max()
+    tol = counts.cpu().numpy() * 2.0 ** -125 * (bound_a + bound_b) + 4 * np.finfo(float).eps * A
+    bad = np.nonzero(np.abs(A - B) > tol)[0]
+    assert bad.size == 0, [(int(s), A[s], B[s], tol[s]) for s in bad[:8]]
+    big = A >= 1e-6 * A.max()
+    assert np.max(np.abs(A - B)[big] / A[big]) <= 1e-15
+    want_sh, _ = O.shells_from_s2(N, B)
+    assert np.max(np.abs(sh.cpu().numpy() - want_sh) / np.maximum(want_sh, 1e-300)) <= 1e-15
+
+
 def test_mode_power_spectrum_matches_oracle():
     N, L, m, a_t = 32, 25.6, 1.3, 1.7
     x, _ = make_inputs(N, L, 1, 9)
