@@ -619,10 +619,13 @@ def run_product(args):
                 "time_share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()
                                if v[0]}}
     if args.quick:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "config": WORKLOAD,
+                "roofline": roofline, "gpu_launches": launches, "clocks": clocks}
+        if args.spectrum:
+            line["spectrum"] = spectrum_bench(ctx, st, W["t0"] + (args.steps + args.warmup) * W["dt"], reps=2)
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                              "warmup": args.warmup, "ms_per_step": ms / args.steps, "config": WORKLOAD,
-                              "roofline": roofline, "gpu_launches": launches, "clocks": clocks}))
+            print(json.dumps(line))
         if pg is not None:
             pg.destroy_process_group()
         return
@@ -802,6 +805,8 @@ def main():
                     help="lattice size override (profiling a smaller case of the same workload)")
     ap.add_argument("--quick", action="store_true",
                     help="headline measurement only (no accuracy check, variants, e2e or CPU baseline)")
+    ap.add_argument("--spectrum", action="store_true",
+                    help="with --quick: also time the observer's density spectrum on the stepped state")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
