@@ -31,6 +31,7 @@ FLAG_FULL_PSI_FFT = 1
 FLAG_STAGE_KERNELS = 2
 FLAG_PAIR_KERNELS = 4
 FLAG_PSI_CTA_PASS_C = 8
+FLAG_PSI_SERIAL = 16
 PSI_NONE, PSI_FULL, PSI_PRUNED, PSI_PRUNED_FUSED = 0, 1, 2, 3
 
 

@@ -220,7 +220,8 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     set_error("stencil must be 7 or 13, got %d", p.stencil);
     return CF_ERR_INVALID;
   }
-  if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS | CF_FLAG_PAIR_KERNELS | CF_FLAG_PSI_CTA_PASS_C)) {
+  if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS | CF_FLAG_PAIR_KERNELS | CF_FLAG_PSI_CTA_PASS_C |
+                  CF_FLAG_PSI_SERIAL)) {
     set_error("unknown flags 0x%x", (unsigned)p.flags);
     return CF_ERR_INVALID;
   }
@@ -282,7 +283,17 @@ int cf_destroy(cf_ctx *ctx) {
   cudaFree(ctx->R_fft);
   cudaFree(ctx->psi_hc);
   cudaFree(ctx->psi_table);
-  for (auto &s : ctx->slot) cudaFree(s.psi);
+  for (auto &s : ctx->slot) {
+    cudaFree(s.psi);
+    if (s.ready) cudaEventDestroy(s.ready);
+  }
+  if (ctx->psi_side) {
+    cudaStreamSynchronize(ctx->psi_side);
+    cudaStreamDestroy(ctx->psi_side);
+    cudaEventDestroy(ctx->psi_fork);
+    cudaEventDestroy(ctx->psi_join);
+    cudaEventDestroy(ctx->psi_stepdone);
+  }
   if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
   psi_release(ctx);
   approx_release(ctx);

@@ -59,7 +59,12 @@ struct PsiSlot {
   void *psi = nullptr;   // N^3 of the storage type
   void *dpsi = nullptr;  // N^3 of the storage type
   uint64_t stamp = 0;
+  cudaEvent_t ready = nullptr;  // recorded after the slot's last refresh, on the stream that ran it
 };
+// 3 for a step's stage times t, t + dt/2, t + dt and 3 for the next step's, synthesised
+// beside it: the next step starts at t0 + (n + 1) dt, which can differ from t + dt in
+// the last bit (odeint's integrate_const forms its times the same way)
+constexpr int kPsiSlots = 6;
 
 // One cached coarse curvature table at a stage time (approximate comoving
 // equation): M^3 x 4 words of the storage type.
@@ -83,12 +88,17 @@ struct cf_ctx {
   void *acc = nullptr, *ya = nullptr, *yb = nullptr;
 
   // Comoving curvature: R_fft in the storage type's complex HC, the transfer
-  // outputs (2 HC arrays) and three cached (Psi, dPsi) slots.
+  // outputs (2 HC arrays) and the cached (Psi, dPsi) slots: three allocated with the
+  // buffers, three more when cf_rk4_steps first synthesises the next step's slots on
+  // the side stream while a step runs (psi_pipe_*).
   void *R_fft = nullptr;
   void *psi_hc = nullptr;  // 2 consecutive HC arrays (Psi_k, dPsi_k), storage type
   double *psi_table = nullptr;  // (T_Psi, T_dPsi) per s^2
-  cfb::PsiSlot slot[3];
+  cfb::PsiSlot slot[cfb::kPsiSlots];
+  int slots_alloc = 0;
   uint64_t slot_clock = 0;
+  cudaStream_t psi_side = nullptr;  // refreshes that overlap the stepping
+  cudaEvent_t psi_fork = nullptr, psi_join = nullptr, psi_stepdone = nullptr;
   cufftHandle plan_psi = 0;  // batched (2) C2R/Z2D into dense N^3
   bool have_plan_psi = false;
   // Pruned synthesis when R_fft is exactly zero outside |i|, |j| <= Ka, Kb and
@@ -165,6 +175,18 @@ int ensure_psi(cf_ctx *ctx);
 // Returns the cached Psi / dPsi/dt slot for stage time t, refreshing one slot
 // (transfer kernel + batched C2R on `stream`) if t is not cached.
 int psi_at(cf_ctx *ctx, double t, cudaStream_t stream, const void **psi, const void **dpsi);
+// Refreshes beside the stepping (comoving-curvature equation).  A stepping loop on
+// `stream` forks the side stream (begin; *on = false when the extra slots do not fit,
+// and the loop then refreshes in turn), has the slots of a step filled there (fill: a
+// no-op for a cached time; the victim is a slot whose time is not in keep[0..nkeep)),
+// takes them after their refresh (use: `stream` waits on the slot's event), marks
+// each step's kernels done (step_done: later fills wait on it before they overwrite a
+// slot that step read) and joins the side stream at the end (end).
+int psi_pipe_begin(cf_ctx *ctx, cudaStream_t stream, bool *on);
+int psi_pipe_fill(cf_ctx *ctx, double t, const double *keep, int nkeep);
+int psi_pipe_use(cf_ctx *ctx, double t, cudaStream_t stream, const void **psi, const void **dpsi);
+int psi_pipe_step_done(cf_ctx *ctx, cudaStream_t stream);
+int psi_pipe_end(cf_ctx *ctx, cudaStream_t stream);
 // Psi and dPsi at t, widened to FP64, into d_out (2 N^3 doubles).
 int psi_fields(cf_ctx *ctx, double t, double *d_out, cudaStream_t stream);
 // CF_PSI_* route the next Psi refresh takes.

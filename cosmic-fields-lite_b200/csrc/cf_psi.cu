@@ -1027,6 +1027,24 @@ __global__ void k_copy_convert(const double *__restrict__ in, S *__restrict__ ou
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (S)in[i];
 }
 
+// Slots [slots_alloc, n): 2 N^3 words each and their ready events.
+static int alloc_psi_slots(cf_ctx *ctx, int n) {
+  const size_t w = ctx->word;
+  for (; ctx->slots_alloc < n; ++ctx->slots_alloc) {
+    PsiSlot &s = ctx->slot[ctx->slots_alloc];
+    if (cudaMalloc(&s.psi, 2 * (size_t)ctx->N3 * w) != cudaSuccess) {
+      s.psi = nullptr;
+      (void)cudaGetLastError();
+      set_error("cudaMalloc Psi slot failed");
+      return CF_ERR_NOMEM;
+    }
+    s.dpsi = (char *)s.psi + (size_t)ctx->N3 * w;
+    s.valid = false;
+    CF_TRY_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
+  }
+  return CF_OK;
+}
+
 int ensure_psi(cf_ctx *ctx) {
   if (ctx->psi_table) return CF_OK;  // buffers in place
   const size_t w = ctx->word;
@@ -1042,15 +1060,7 @@ int ensure_psi(cf_ctx *ctx) {
     set_error("cudaMalloc transfer table failed");
     return CF_ERR_NOMEM;
   }
-  for (auto &s : ctx->slot) {
-    if (cudaMalloc(&s.psi, 2 * (size_t)ctx->N3 * w) != cudaSuccess) {
-      set_error("cudaMalloc Psi slot failed");
-      return CF_ERR_NOMEM;
-    }
-    s.dpsi = (char *)s.psi + (size_t)ctx->N3 * w;
-    s.valid = false;
-  }
-  return CF_OK;
+  return alloc_psi_slots(ctx, 3);
 }
 
 // The two padded HC arrays (Psi_k, dPsi_k) that the cuFFT C2R routes read:
@@ -1252,24 +1262,13 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
   return psi_to_e2m1(ctx, out, st);
 }
 
-int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void **dpsi) {
-  CF_TRY(ensure_psi(ctx));
-  for (auto &s : ctx->slot) {
-    if (s.valid && s.t == t) {
-      s.stamp = ++ctx->slot_clock;
-      *psi = s.psi;
-      *dpsi = s.dpsi;
-      return CF_OK;
-    }
-  }
-  // refresh the least recently used slot
-  PsiSlot *v = &ctx->slot[0];
-  for (auto &s : ctx->slot)
-    if (!s.valid || s.stamp < v->stamp) v = &s;
+// Synthesises Psi, dPsi/dt at t into slot v on stream st and records the slot's event.
+static int refresh_slot(cf_ctx *ctx, PsiSlot *v, double t, cudaStream_t st) {
   const double eta_t = cosmo_eta(ctx->p, t);
   const double H_t = cosmo_H(ctx->p, t);
   const double factor = (2 * 3.14159265358979323846 / ctx->p.L) * eta_t / sqrt(3);
   const long long pairs = ctx->hc_count / 2;
+  v->valid = false;
   {
     ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
     unsigned tb = (unsigned)std::min<long long>((ctx->s2_bins + 255) / 256, 148LL * 8);
@@ -1282,41 +1281,122 @@ int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void 
       CF_TRY(refresh_pruned<double>(ctx, v->psi, st));
     else
       CF_TRY(refresh_pruned<float>(ctx, v->psi, st));
-    v->t = t;
-    v->valid = true;
-    v->stamp = ++ctx->slot_clock;
-    *psi = v->psi;
-    *dpsi = v->dpsi;
-    return CF_OK;
+  } else {
+    CF_TRY(ensure_psi_hc(ctx));
+    CF_TRY(ensure_full_plan(ctx));
+    CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
+    {
+      ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
+      const int nh = (int)ctx->N / 2 + 1;
+      const dim3 tg((unsigned)((nh + 255) / 256), (unsigned)ctx->N, (unsigned)ctx->N);
+      if (ctx->word == 8)
+        k_transfer<double><<<tg, 256, 0, st>>>((const double *)ctx->R_fft, (double *)ctx->psi_hc, ctx->psi_table,
+                                               (int)ctx->N, pairs);
+      else
+        k_transfer<float><<<tg, 256, 0, st>>>((const float *)ctx->R_fft, (float *)ctx->psi_hc, ctx->psi_table,
+                                              (int)ctx->N, pairs);
+      CF_LAUNCHED(ctx);
+    }
+    {
+      ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
+      if (ctx->word == 8)
+        CF_TRY_CUFFT(cufftExecZ2D(ctx->plan_psi, (cufftDoubleComplex *)ctx->psi_hc, (cufftDoubleReal *)v->psi));
+      else
+        CF_TRY_CUFFT(cufftExecC2R(ctx->plan_psi, (cufftComplex *)ctx->psi_hc, (cufftReal *)v->psi));
+    }
+    CF_TRY(psi_to_e2m1(ctx, v->psi, st));
   }
-  CF_TRY(ensure_psi_hc(ctx));
-  CF_TRY(ensure_full_plan(ctx));
-  CF_TRY_CUFFT(cufftSetStream(ctx->plan_psi, st));
-  {
-    ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
-    const int nh = (int)ctx->N / 2 + 1;
-    const dim3 tg((unsigned)((nh + 255) / 256), (unsigned)ctx->N, (unsigned)ctx->N);
-    if (ctx->word == 8)
-      k_transfer<double><<<tg, 256, 0, st>>>((const double *)ctx->R_fft, (double *)ctx->psi_hc, ctx->psi_table,
-                                             (int)ctx->N, pairs);
-    else
-      k_transfer<float><<<tg, 256, 0, st>>>((const float *)ctx->R_fft, (float *)ctx->psi_hc, ctx->psi_table,
-                                            (int)ctx->N, pairs);
-    CF_LAUNCHED(ctx);
-  }
-  {
-    ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
-    if (ctx->word == 8)
-      CF_TRY_CUFFT(cufftExecZ2D(ctx->plan_psi, (cufftDoubleComplex *)ctx->psi_hc, (cufftDoubleReal *)v->psi));
-    else
-      CF_TRY_CUFFT(cufftExecC2R(ctx->plan_psi, (cufftComplex *)ctx->psi_hc, (cufftReal *)v->psi));
-  }
-  CF_TRY(psi_to_e2m1(ctx, v->psi, st));
+  CF_TRY_CUDA(cudaEventRecord(v->ready, st));
   v->t = t;
   v->valid = true;
   v->stamp = ++ctx->slot_clock;
+  return CF_OK;
+}
+
+static PsiSlot *cached_slot(cf_ctx *ctx, double t) {
+  for (int i = 0; i < ctx->slots_alloc; ++i)
+    if (ctx->slot[i].valid && ctx->slot[i].t == t) return &ctx->slot[i];
+  return nullptr;
+}
+
+int psi_at(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void **dpsi) {
+  CF_TRY(ensure_psi(ctx));
+  PsiSlot *v = cached_slot(ctx, t);
+  if (!v) {  // refresh the least recently used slot
+    v = &ctx->slot[0];
+    for (int i = 0; i < ctx->slots_alloc; ++i)
+      if (!ctx->slot[i].valid || ctx->slot[i].stamp < v->stamp) v = &ctx->slot[i];
+    CF_TRY(refresh_slot(ctx, v, t, st));
+  }
+  v->stamp = ++ctx->slot_clock;
   *psi = v->psi;
   *dpsi = v->dpsi;
+  return CF_OK;
+}
+
+// ---- refreshes beside the stepping ----------------------------------------
+// Psi depends on t only, so the new slots of step j + 1 (two, or three when its start
+// time differs from t + dt in the last bit) can be synthesised on a side stream while
+// step j's passes run: the refreshes (passes A-C, about a third of a step at N = 512)
+// fill the SMs the step's last wave leaves idle.  Six slots: step j reads three, the
+// side stream fills the next step's, and a fill overwrites a slot only after the step
+// that last read it has finished (psi_stepdone).  The fork and the join are events on
+// the caller's stream, so work enqueued after cf_rk4_steps sees every slot complete.
+int psi_pipe_begin(cf_ctx *ctx, cudaStream_t st, bool *on) {
+  CF_TRY(ensure_psi(ctx));
+  *on = false;
+  if (alloc_psi_slots(ctx, kPsiSlots) != CF_OK) return CF_OK;  // no room: the caller refreshes in turn
+  if (!ctx->psi_side) {
+    // default priority: the refreshes take the SMs the step's last wave leaves idle.
+    // At the highest priority they displaced the step's CTAs as they retired: N = 256
+    // 0.457 -> 0.393 ms per step, but N = 512 2.63 -> 2.68 (the step pass 1.69 ->
+    // 2.48 ms) against 2.57 at default priority.
+    CF_TRY_CUDA(cudaStreamCreateWithFlags(&ctx->psi_side, cudaStreamNonBlocking));
+    CF_TRY_CUDA(cudaEventCreateWithFlags(&ctx->psi_fork, cudaEventDisableTiming));
+    CF_TRY_CUDA(cudaEventCreateWithFlags(&ctx->psi_join, cudaEventDisableTiming));
+    CF_TRY_CUDA(cudaEventCreateWithFlags(&ctx->psi_stepdone, cudaEventDisableTiming));
+  }
+  // the side stream starts behind everything enqueued on st (slots read earlier)
+  CF_TRY_CUDA(cudaEventRecord(ctx->psi_fork, st));
+  CF_TRY_CUDA(cudaStreamWaitEvent(ctx->psi_side, ctx->psi_fork, 0));
+  *on = true;
+  return CF_OK;
+}
+
+int psi_pipe_fill(cf_ctx *ctx, double t, const double *keep, int nkeep) {
+  if (cached_slot(ctx, t)) return CF_OK;
+  PsiSlot *v = nullptr;
+  for (int i = 0; i < ctx->slots_alloc; ++i) {
+    PsiSlot *s = &ctx->slot[i];
+    bool kept = false;
+    for (int k = 0; k < nkeep; ++k) kept = kept || (s->valid && s->t == keep[k]);
+    if (kept) continue;
+    if (!v || !s->valid || (v->valid && s->stamp < v->stamp)) v = s;
+    if (!v->valid) break;
+  }
+  if (!v) return set_error("Psi slots: no slot outside the kept stage times"), CF_ERR_INVALID;
+  return refresh_slot(ctx, v, t, ctx->psi_side);
+}
+
+int psi_pipe_use(cf_ctx *ctx, double t, cudaStream_t st, const void **psi, const void **dpsi) {
+  PsiSlot *v = cached_slot(ctx, t);
+  if (!v) return set_error("Psi slot for t = %g not filled", t), CF_ERR_INVALID;
+  CF_TRY_CUDA(cudaStreamWaitEvent(st, v->ready, 0));
+  v->stamp = ++ctx->slot_clock;
+  *psi = v->psi;
+  *dpsi = v->dpsi;
+  return CF_OK;
+}
+
+int psi_pipe_step_done(cf_ctx *ctx, cudaStream_t st) {
+  CF_TRY_CUDA(cudaEventRecord(ctx->psi_stepdone, st));
+  CF_TRY_CUDA(cudaStreamWaitEvent(ctx->psi_side, ctx->psi_stepdone, 0));
+  return CF_OK;
+}
+
+int psi_pipe_end(cf_ctx *ctx, cudaStream_t st) {
+  CF_TRY_CUDA(cudaEventRecord(ctx->psi_join, ctx->psi_side));
+  CF_TRY_CUDA(cudaStreamWaitEvent(st, ctx->psi_join, 0));
   return CF_OK;
 }
 
@@ -1394,7 +1474,7 @@ int set_R_fft(cf_ctx *ctx, const double *R_fft, int on_device, cudaStream_t st) 
     }
   }
   if (tmp) CF_TRY_CUDA(cudaFreeAsync(tmp, st));
-  for (auto &s : ctx->slot) s.valid = false;
+  for (int i = 0; i < ctx->slots_alloc; ++i) ctx->slot[i].valid = false;
   // support of the new R_fft: decides between the pruned and the full synthesis
   int *d_box = nullptr;
   CF_TRY_CUDA(cudaMallocAsync((void **)&d_box, 3 * sizeof(int), st));

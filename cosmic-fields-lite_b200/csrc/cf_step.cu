@@ -266,12 +266,15 @@ static void eq_consts(const cf_ctx *ctx, double *q1, double *q2, const int **cma
 
 // The curvature input of a stage at time t: the comoving Psi slot, the fixed Psi
 // plane or the approximate equation's coarse table (none for the others).
+// pipe: the comoving slot was filled on the side stream (psi_pipe_fill_step); st waits for it.
 template <typename S>
-static int curvature_at(cf_ctx *ctx, double t, const S **psi, const S **dpsi, cudaStream_t st) {
+static int curvature_at(cf_ctx *ctx, double t, const S **psi, const S **dpsi, cudaStream_t st, bool pipe = false) {
   *psi = *dpsi = nullptr;
   const void *ps = nullptr, *dps = nullptr;
   switch (ctx->p.equation) {
-    case CF_EQ_COMOVING_FRW: CF_TRY(psi_at(ctx, t, st, &ps, &dps)); break;
+    case CF_EQ_COMOVING_FRW:
+      CF_TRY(pipe ? psi_pipe_use(ctx, t, st, &ps, &dps) : psi_at(ctx, t, st, &ps, &dps));
+      break;
     case CF_EQ_FIXED_CURVATURE_FRW: ps = ctx->fixed_e2m1; break;
     case CF_EQ_APPROX_COMOVING_FRW: CF_TRY(approx_at(ctx, t, st, &ps)); break;
     default: break;
@@ -284,11 +287,29 @@ static int curvature_at(cf_ctx *ctx, double t, const S **psi, const S **dpsi, cu
 // Stage-time coefficients and curvature input of a paired pass.
 template <typename S>
 static int pair_coeffs(cf_ctx *ctx, double t, double *inv, double *hub3, const S **psi, const S **dpsi,
-                       cudaStream_t st) {
+                       cudaStream_t st, bool pipe = false) {
   double H;
   stage_coeffs(ctx->p, t, inv, &H);
   *hub3 = 3.0 * H;
-  return curvature_at<S>(ctx, t, psi, dpsi, st);
+  return curvature_at<S>(ctx, t, psi, dpsi, st, pipe);
+}
+
+// Comoving curvature: cf_rk4_steps synthesises the next step's new Psi slots on the
+// context's side stream while the current step's passes run (psi_pipe_*); the same
+// slots and kernels, so the same bits as CF_FLAG_PSI_SERIAL.
+static bool psi_pipelined(const cf_ctx *ctx, int64_t nsteps) {
+  return ctx->p.equation == CF_EQ_COMOVING_FRW && !(ctx->p.flags & CF_FLAG_PSI_SERIAL) && nsteps >= 2;
+}
+// Before step j: the slots of step j's stage times (present after step 0) and, but
+// for the last step, those of step j + 1, on the side stream.  The times are the
+// ones the passes read: t, t + dt/2, t + dt with t = t0 + n dt.
+static int psi_pipe_fill_step(cf_ctx *ctx, double t0, double dt, int64_t step0, int64_t j, int64_t nsteps) {
+  const double t = t0 + (double)(step0 + j) * dt, tn = t0 + (double)(step0 + j + 1) * dt;
+  const double keep[6] = {t, t + dt / 2.0, t + dt, tn, tn + dt / 2.0, tn + dt};
+  for (int k = 0; k < 3; ++k) CF_TRY(psi_pipe_fill(ctx, keep[k], keep, 3));
+  if (j + 1 < nsteps)
+    for (int k = 3; k < 6; ++k) CF_TRY(psi_pipe_fill(ctx, keep[k], keep, 6));
+  return CF_OK;
 }
 
 // nsteps RK4 steps as paired-stage passes.  The new phi of pass B alternates
@@ -313,12 +334,15 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
   A.yb = (S *)ctx->yb;
   const double dh = dt / 2.0;
   A.dt6 = dt / 6.0;
+  bool pipe = psi_pipelined(ctx, nsteps);
+  if (pipe) CF_TRY(psi_pipe_begin(ctx, st, &pipe));
   for (int64_t j = 0; j < nsteps; ++j) {
     const double t = t0 + (double)(step0 + j) * dt;
     const double th = t + dh;
+    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps));
     // pass A: stages 1 (t) and 2 (t + dt/2)
-    CF_TRY(pair_coeffs<S>(ctx, t, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st));
-    CF_TRY(pair_coeffs<S>(ctx, th, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st));
+    CF_TRY(pair_coeffs<S>(ctx, t, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st, pipe));
+    CF_TRY(pair_coeffs<S>(ctx, th, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st, pipe));
     A.uphi = phi[cur];
     A.upi = x + N3;
     A.xphi = phi[cur];
@@ -327,16 +351,18 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
     A.cy = dh;
     CF_TRY(launch_pair<S, 1>(ctx, A, st));
     // pass B: stages 3 (t + dt/2) and 4 (t + dt)
-    CF_TRY(pair_coeffs<S>(ctx, th, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st));
-    CF_TRY(pair_coeffs<S>(ctx, t + dt, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st));
+    CF_TRY(pair_coeffs<S>(ctx, th, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st, pipe));
+    CF_TRY(pair_coeffs<S>(ctx, t + dt, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st, pipe));
     A.uphi = A.yb;
     A.upi = A.yb + N3;
     A.xphi = phi[cur];
     A.xphi_out = phi[cur ^ 1];
     A.cw = dt;
     CF_TRY(launch_pair<S, 2>(ctx, A, st));
+    if (pipe) CF_TRY(psi_pipe_step_done(ctx, st));
     cur ^= 1;
   }
+  if (pipe) CF_TRY(psi_pipe_end(ctx, st));
   if (cur) CF_TRY_CUDA(cudaMemcpyAsync(x, phi[1], N3 * sizeof(S), cudaMemcpyDeviceToDevice, st));
   return CF_OK;
 }
@@ -494,22 +520,27 @@ static int rk4_steps_fused_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
   A.dt2 = dt / 2.0;
   A.dt = dt;
   A.dt6 = dt / 6.0;
+  bool pipe = psi_pipelined(ctx, nsteps);
+  if (pipe) CF_TRY(psi_pipe_begin(ctx, st, &pipe));
   for (int64_t j = 0; j < nsteps; ++j) {
     const double t = t0 + (double)(step0 + j) * dt;
     const double ts[3] = {t, t + dt / 2.0, t + dt};
+    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps));
     for (int k = 0; k < 3; ++k) {
       double H;
       stage_coeffs(ctx->p, ts[k], &A.inv[k], &H);
       A.hub3[k] = 3.0 * H;
-      CF_TRY(curvature_at<S>(ctx, ts[k], &A.psi[k], &A.dpsi[k], st));
+      CF_TRY(curvature_at<S>(ctx, ts[k], &A.psi[k], &A.dpsi[k], st, pipe));
     }
     A.xphi = buf[cur];
     A.xpi = buf[cur] + N3;
     A.ophi = buf[cur ^ 1];
     A.opi = buf[cur ^ 1] + N3;
     CF_TRY(launch_step<S>(ctx, A, st));
+    if (pipe) CF_TRY(psi_pipe_step_done(ctx, st));
     cur ^= 1;
   }
+  if (pipe) CF_TRY(psi_pipe_end(ctx, st));
   if (cur) CF_TRY_CUDA(cudaMemcpyAsync(x, buf[1], 2 * N3 * sizeof(S), cudaMemcpyDeviceToDevice, st));
   return CF_OK;
 }

@@ -117,6 +117,12 @@ typedef struct cf_params {
  * runs as the CTA-per-tile kernel instead of the default warp-per-row-group kernel
  * (N = 256, 512, 1024); both compute the same values. */
 #define CF_FLAG_PSI_CTA_PASS_C 8
+/* Comoving-curvature equation: cf_rk4_steps synthesises each step's Psi slots
+ * before the step's passes on the caller's stream, instead of synthesising the next
+ * step's slots on a side stream of the context while the current step runs (the
+ * default; three more N^3 slot pairs, or the serial order when they do not fit);
+ * both give bit-identical states. */
+#define CF_FLAG_PSI_SERIAL 16
 
 typedef struct cf_ctx cf_ctx;
 

@@ -143,6 +143,41 @@ def test_psi_fields_each_route_matches_full_c2r_and_oracle(prec, tol_pf, tol_or,
         assert rel(b[sl], want) <= tol
 
 
+@pytest.mark.parametrize("route,stencil", [(0, 7), (cfb200.FLAG_PAIR_KERNELS, 7), (0, 13)])
+@pytest.mark.parametrize("prec", [cfb200.FP64, cfb200.FP32_COMP])
+@pytest.mark.parametrize("N,k_max", [(64, 1.0),    # pruned, passes B and C as own kernels (FP32)
+                                     (96, 1.0),    # pruned, cuFFT pass C
+                                     (64, 2.5)])   # full 3-D C2R
+def test_psi_side_stream_equals_serial(prec, N, k_max, route, stencil):
+    """By default cf_rk4_steps synthesises the next step's Psi slots on a side
+    stream while the current step runs (six slots); CF_FLAG_PSI_SERIAL synthesises
+    each step's slots before its passes on the caller's stream.  Same slots, same
+    kernels: bit-identical states for the whole-step and the paired route, over one
+    step, over several (dt = 0.05 from t = 1, where t + dt and the next step's start
+    differ in the last bit at some steps), and over calls that continue from cached
+    slots."""
+    L = float(N)
+    x, _ = make_inputs(N, L, 1, 41)
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=43)
+    got = {}
+    for flags in (route, route | cfb200.FLAG_PSI_SERIAL):
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=prec, stencil=stencil, flags=flags, **FRW)
+        c.set_R_fft(Rf, on_device=False)
+        st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+        c.upload(st, x)
+        outs = []
+        for step0, n in ((0, 1), (1, 5), (6, 2)):
+            c.rk4_steps(st, 1.0, 0.05, n, step0=step0)
+            rho = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
+            c.energy_density(st, 1.0 + 0.05 * (step0 + n), rho)  # reads the cached slot at the end time
+            outs.append((st.clone(), rho))
+        got[flags] = outs
+        c.close()
+    for (a, ra), (b, rb) in zip(got[route], got[route | cfb200.FLAG_PSI_SERIAL]):
+        assert torch.equal(a, b)
+        assert torch.equal(ra, rb)
+
+
 @pytest.mark.parametrize("N,k_max", [(256, 0.3), (256, 0.6), (512, 0.5), (1024, 0.5)])
 def test_warp_pass_c_equals_cta_pass_c(N, k_max):
     """FP32 storage, N = 256, 512, 1024: the last pass of the pruned synthesis as
