@@ -32,6 +32,7 @@ FLAG_STAGE_KERNELS = 2
 FLAG_PAIR_KERNELS = 4
 FLAG_PSI_CTA_PASS_C = 8
 FLAG_PSI_SERIAL = 16
+FLAG_PSI_NO_TMA = 32
 PSI_NONE, PSI_FULL, PSI_PRUNED, PSI_PRUNED_FUSED = 0, 1, 2, 3
 
 

@@ -221,7 +221,7 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     return CF_ERR_INVALID;
   }
   if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS | CF_FLAG_PAIR_KERNELS | CF_FLAG_PSI_CTA_PASS_C |
-                  CF_FLAG_PSI_SERIAL)) {
+                  CF_FLAG_PSI_SERIAL | CF_FLAG_PSI_NO_TMA)) {
     set_error("unknown flags 0x%x", (unsigned)p.flags);
     return CF_ERR_INVALID;
   }
@@ -296,6 +296,7 @@ int cf_destroy(cf_ctx *ctx) {
   }
   if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
   psi_release(ctx);
+  if (ctx->psi_err_h) cudaFreeHost(ctx->psi_err_h);
   approx_release(ctx);
   if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);
   if (ctx->have_z2d1) cufftDestroy(ctx->plan_z2d1);

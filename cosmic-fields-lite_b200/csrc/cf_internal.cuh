@@ -114,6 +114,13 @@ struct cf_ctx {
   bool pc_fused = false;
   void *pr_wN = nullptr;
   void *pr_twM = nullptr;  // pass-1 twiddles e^{2 pi i k2 m1 / (N/2)}, [m1][k2]
+  // The warp pass C's band tiles by TMA: a tensor map over pass B's lines (a
+  // CUtensorMap, 64-byte aligned, encoded when the pruned buffers are made), and a
+  // mapped host word its bounded waits set when they give up (read on the host
+  // without a synchronisation at the next refresh).
+  alignas(64) unsigned char pc_tmap[128] = {};
+  bool have_pc_tmap = false;
+  int *psi_err_h = nullptr, *psi_err_d = nullptr;
   // Pass B as one kernel (FP32, power-of-two N, 32..1024): its four-step twiddles
   // e^{2 pi i k2 m1 / N}, [m1][k2]; no plan_pb then.
   bool pb_fused = false;

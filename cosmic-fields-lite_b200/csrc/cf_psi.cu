@@ -19,10 +19,12 @@
 // small part of e^{2 Psi} (|Psi| ~ 1e-2) at full relative precision.
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "cf_internal.cuh"
@@ -567,80 +569,173 @@ __global__ void __launch_bounds__(256) k_prune_c_fft_p(const S *__restrict__ pb,
 // ---- pass C, one warp per row group (FP32, N = 256, 512, 1024) --------------
 // The same four-step arithmetic as k_prune_c_fft without a CTA barrier: a warp owns
 // RW = 32 / R2 consecutive rows of one (f, a) plane and does everything for them --
-// copies the rows' Kc + 1 band entries into its own shared memory by cp.async (one
-// tile ahead, double-buffered), runs pass 1 with one lane per (row, k2) -- every lane
-// busy -- forming X + i X w^k from the staged X as it loads, then pass 2 with RW R1 / 32
+// brings the rows' Kc + 1 band entries into its own shared memory (one tile ahead,
+// double-buffered), runs pass 1 with one lane per (row, k2) -- every lane busy --
+// forming X + i X w^k from the staged X as it loads, then pass 2 with RW R1 / 32
 // (row, m1) tasks per lane through a warp-private transpose, with only __syncwarp
 // between them, and stores along the output rows.  Persistent: warps walk the tiles
 // (f, a, row group) with stride = warps in the grid, adjacent warps on adjacent rows.
 //
-// Shared layout per warp: X[buf][r][XPP] (XPP = 8 mod 16 complex, so the two rows a
-// half-warp reads when R2 = 8 sit on disjoint banks) and T[r][RP] with T[r] = [m1][TP],
-// TP = R2 + 1 odd (pass-2 reads free of bank conflicts) and RP = R2 mod 16 where R2 < 16.
+// TMA (the default where the tensor map exists): one lane copies a tile's band as one
+// 3-D box {RW rows of b, one a, Kc + 1 k} of pass B's lines with cp.async.bulk.tensor,
+// completing on the buffer's mbarrier; the gather no longer occupies the LSU pipe
+// (each of its 8-byte cp.async took a line of its own).  The box lands as X[k][r].
+// Every mbarrier wait is bounded: when one gives up the warp sets the mapped error
+// word, waits (bounded again) for its copies still in flight and leaves the loop.
+// Otherwise X[r][XPP] by per-lane cp.async (XPP = 8 mod 16 complex, so the two rows a
+// half-warp reads sit on disjoint banks).
+//
+// T[r][RP] with T[r] = [m1][TP], TP = R2 + 1 odd (pass-2 reads free of bank
+// conflicts) and RP = R2 mod 16 where R2 < 16.
 __host__ __device__ constexpr int pc_xpp(int kn) { return ((kn + 7) & ~15) + 8; }
 __host__ __device__ constexpr int pc_rp(int R1, int R2) {
   return R2 >= 16 ? R1 * (R2 + 1) : R1 * (R2 + 1) + ((R2 - (R1 * (R2 + 1)) % 16) + 16) % 16;
 }
+__host__ __device__ constexpr int pc_up16(int n) { return (n + 15) & ~15; }  // complex: 128 bytes
+// Complex words per X buffer and per warp.
+__host__ __device__ constexpr int pc_xw(int kn, int RW, bool tma) { return tma ? pc_up16(kn * RW) : RW * pc_xpp(kn); }
+__host__ __device__ constexpr int pc_warp_words(int kn, int R1, int R2, bool tma) {
+  return tma ? pc_up16(2 * pc_xw(kn, 32 / R2, true) + (32 / R2) * pc_rp(R1, R2))
+             : 2 * pc_xw(kn, 32 / R2, false) + (32 / R2) * pc_rp(R1, R2);
+}
 
-template <int R1, int R2, int B>
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const void *tmap, int x, int y, int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+          "r"(dst),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+// try_wait suspends the thread for a while between tests: 2^20 tests are seconds.
+constexpr long long kPcSpinLimit = 1LL << 20;
+
+template <int R1, int R2, int B, bool TMA>
 __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict__ pb, float *__restrict__ out,
                                                      const float2 *__restrict__ wN, const float2 *__restrict__ twM,
                                                      int N, int Kc, int tile0, int ntiles, int log2_groups,
-                                                     int log2_n, const __grid_constant__ Tw32<float> tw) {
+                                                     int log2_n, const __grid_constant__ Tw32<float> tw,
+                                                     const __grid_constant__ CUtensorMap tmap, int *err) {
   constexpr int M = R1 * R2;  // N == 2 M
   constexpr int RW = 32 / R2;
   constexpr int TP = R2 + 1;
   constexpr int RP = pc_rp(R1, R2);
   constexpr int P2 = RW * R1 / 32;  // pass-2 tasks per lane
   static_assert(R2 <= R1 && 32 % R2 == 0 && (RW * R1) % 32 == 0, "shape");
-  extern __shared__ __align__(16) unsigned char smraw[];
-  float2 *TW = reinterpret_cast<float2 *>(smraw);  // [R1][R2]: e^{2 pi i k2 m1 / M}
-  float2 *WK = TW + M;                             // [Kc+1]: w^k
+  extern __shared__ __align__(128) unsigned char pcw_smem[];  // TMA boxes land on 128-byte boundaries
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kn = Kc + 1;
-  const int xpp = pc_xpp(kn), xw = RW * xpp;  // complex per X buffer
-  float2 *W = WK + ((kn + 1) & ~1) + (size_t)warp * (2 * xw + RW * RP);
+  // [mbarriers: 2 per warp, 128 bytes] [TW: M] [WK: kn, to 128 bytes] [per warp: X0, X1, T]
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(pcw_smem);
+  float2 *TW = reinterpret_cast<float2 *>(pcw_smem + 128);  // [R1][R2]: e^{2 pi i k2 m1 / M}
+  float2 *WK = TW + M;                                      // [Kc+1]: w^k
+  const int xw = pc_xw(kn, RW, TMA);
+  float2 *W = WK + pc_up16(kn) + (size_t)warp * pc_warp_words(kn, R1, R2, TMA);
   float2 *X0 = W, *T = W + 2 * xw;
   for (int i = threadIdx.x; i < M; i += blockDim.x) TW[i] = twM[i];
   for (int i = threadIdx.x; i < kn; i += blockDim.x) WK[i] = wN[i];
-  __syncthreads();  // the only CTA barrier: the shared twiddles
+  const unsigned bar0 = (unsigned)__cvta_generic_to_shared(bars + 2 * warp);
+  if constexpr (TMA) {
+    if (lane == 0) {
+      mbar_init(bar0, 1);
+      mbar_init(bar0 + 8, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+  }
+  __syncthreads();  // the only CTA barrier: the shared twiddles and the initialised mbarriers
 
   // tile t = (f N + a) groups + g, groups = N / RW row groups per plane (powers of two)
   const int gmask = (1 << log2_groups) - 1, nmask = (1 << log2_n) - 1;
   const long long NN = (long long)N * N;
   const int stride = gridDim.x * (blockDim.x >> 5);
   int tile = tile0 + blockIdx.x * (blockDim.x >> 5) + warp;  // tiles [tile0, ntiles)
-  auto issue = [&](int t, float2 *dst) {
+  auto issue = [&](int t, int b) {
     const int g = t & gmask, fa = t >> log2_groups;
     const int a = fa & nmask, f = fa >> log2_n;
-    const float2 *src = reinterpret_cast<const float2 *>(pb) + ((long long)f * kn * N + a) * N + g * RW + lane * NN;
-    const unsigned d0 = (unsigned)__cvta_generic_to_shared(dst + lane);
-    for (int k = lane; k < kn; k += 32, src += 32 * NN) {
-      const unsigned d = d0 + (unsigned)((k - lane) * sizeof(float2));
+    float2 *dst = X0 + b * xw;
+    if constexpr (TMA) {
+      if (lane == 0) {
+        // the warp's generic reads of this buffer (ordered by the __syncwarp that ended
+        // its last tile) before the async proxy overwrites it
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        const unsigned bar = bar0 + 8 * b;
+        mbar_expect_tx(bar, (unsigned)(kn * RW * sizeof(float2)));
+        tma_load_3d((unsigned)__cvta_generic_to_shared(dst), &tmap, 2 * g * RW, a, f * kn, bar);
+      }
+    } else {
+      const int xpp = pc_xpp(kn);
+      const float2 *src = reinterpret_cast<const float2 *>(pb) + ((long long)f * kn * N + a) * N + g * RW + lane * NN;
+      const unsigned d0 = (unsigned)__cvta_generic_to_shared(dst + lane);
+      for (int k = lane; k < kn; k += 32, src += 32 * NN) {
+        const unsigned d = d0 + (unsigned)((k - lane) * sizeof(float2));
 #pragma unroll
-      for (int r = 0; r < RW; ++r)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d + (unsigned)(r * xpp * sizeof(float2))),
-                     "l"(src + r)
-                     : "memory");
+        for (int r = 0; r < RW; ++r)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d + (unsigned)(r * xpp * sizeof(float2))),
+                       "l"(src + r)
+                       : "memory");
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  unsigned phase[2] = {0u, 0u};
+  bool pending[2] = {false, false};
+  auto wait_buf = [&](int b) -> bool {  // TMA: the buffer's copy has landed (bounded, per lane)
+    const unsigned bar = bar0 + 8 * b;
+    for (long long i = 0; i < kPcSpinLimit; ++i)
+      if (mbar_try_wait(bar, phase[b])) {
+        phase[b] ^= 1u;
+        pending[b] = false;
+        return true;
+      }
+    return false;
   };
   int buf = 0;
-  if (tile < ntiles) issue(tile, X0);
+  bool ok = true;
+  if (tile < ntiles) {
+    issue(tile, 0);
+    pending[0] = true;
+  }
   for (; tile < ntiles; tile += stride) {
-    if (tile + stride < ntiles) {
-      issue(tile + stride, X0 + (buf ^ 1) * xw);
-      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    const bool more = tile + stride < ntiles;
+    if (more) {
+      issue(tile + stride, buf ^ 1);
+      pending[buf ^ 1] = true;
+    }
+    if constexpr (TMA) {
+      // every lane tests the barrier itself; the warp gives up together if any lane did
+      if (!__all_sync(0xffffffffu, wait_buf(buf))) {
+        ok = false;
+        break;
+      }
     } else {
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      if (more)
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      else
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      pending[buf] = false;
     }
     __syncwarp();  // the tile's band entries (every lane's copies)
     const float2 *X = X0 + buf * xw;
+    // X[k][r] (TMA box) or X[r][XPP] (per-lane copies)
+    auto xat = [&](int r, int k) -> float2 { return TMA ? X[k * RW + r] : X[r * pc_xpp(kn) + k]; };
     const int g = tile & gmask, fa = tile >> log2_groups;
     // pass 1: lane (r, k2), an R1-point DFT over the band rows k1, times e^{2 pi i k2 m1 / M}
     {
       const int r = lane / R2, k2 = lane % R2;
-      const float2 *Xr = X + r * xpp;
       float2 v[R1];
 #pragma unroll
       for (int k1 = 0; k1 < R1; ++k1) {
@@ -650,14 +745,14 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
         float2 z = make_float2(0.0f, 0.0f);
         if (k1 < B) {
           if (k <= Kc) {
-            float2 x = Xr[k];
+            float2 x = xat(r, k);
             if (k == 0) x.y = 0.0f;  // X[0] by its real part: the Hermitian projection of every C2R
             z = c_add(x, c_mul_i(c_mul(x, WK[k])));  // X + i X w^k
           }
         } else if (k1 >= R1 - B) {
           const int j = M - k;
           if (j <= Kc) {
-            const float2 x = Xr[j];
+            const float2 x = xat(r, j);
             const float2 d = c_sub(x, c_mul_i(c_mul(x, WK[j])));  // conj(X - i X w^j)
             z = make_float2(d.x, -d.y);
           }
@@ -706,6 +801,16 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
     __syncwarp();  // T and this X buffer are free for the next tile
     buf ^= 1;
   }
+  if constexpr (TMA) {
+    if (!ok) {  // a copy did not land in time: report it, and let the copies in flight finish
+      if (lane == 0) {
+        *reinterpret_cast<volatile int *>(err) = 1;
+        __threadfence_system();
+      }
+      for (int b = 0; b < 2; ++b)
+        if (pending[b]) (void)wait_buf(b);
+    }
+  }
 }
 
 static bool pc_warp_shape(long long N, size_t word, int *R1, int *R2) {
@@ -717,20 +822,25 @@ static bool pc_warp_shape(long long N, size_t word, int *R1, int *R2) {
     default: return false;
   }
 }
-static size_t pc_warp_smem(int Kc, int R1, int R2) {
-  const int RW = 32 / R2, kn = Kc + 1;
-  return ((size_t)R1 * R2 + ((kn + 1) & ~1) + 8 * (size_t)(2 * RW * pc_xpp(kn) + RW * pc_rp(R1, R2))) * sizeof(float2);
+static size_t pc_warp_smem(int Kc, int R1, int R2, bool tma) {
+  const int kn = Kc + 1;
+  return 128 + ((size_t)R1 * R2 + pc_up16(kn) + 8 * (size_t)pc_warp_words(kn, R1, R2, tma)) * sizeof(float2);
 }
+// Whether the warp pass C takes its band tiles by TMA (a tensor map exists).
+static bool pc_warp_tma(const cf_ctx *ctx) { return ctx->have_pc_tmap; }
 
-template <int R1, int R2, int B>
+template <int R1, int R2, int B, bool TMA>
 static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st, int f0, int nf) {
-  auto kern = k_prune_c_warp<R1, R2, B>;
+  auto kern = k_prune_c_warp<R1, R2, B, TMA>;
   if (smem > 48 * 1024) CF_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Tw32<float> tw;
   for (int e = 0; e < 16; ++e) {
     const double ang = 2.0 * 3.14159265358979323846 * e / 32.0;
     tw.w[e] = float2{(float)std::cos(ang), (float)std::sin(ang)};
   }
+  CUtensorMap tmap;
+  static_assert(sizeof(tmap) == sizeof(ctx->pc_tmap), "tensor map size");
+  std::memcpy(&tmap, ctx->pc_tmap, sizeof(tmap));
   int sms = 0, per_sm = 0;
   CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
   CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
@@ -742,29 +852,81 @@ static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st
   const int grid = std::max(1, std::min((ntiles - tile0 + 7) / 8, sms * std::max(per_sm, 1)));
   kern<<<(unsigned)grid, 256, smem, st>>>((const float *)ctx->pz_b, (float *)out, (const float2 *)ctx->pr_wN,
                                           (const float2 *)ctx->pr_twM, N, ctx->Kc, tile0, ntiles, log2_g, log2_n,
-                                          tw);
+                                          tw, tmap, ctx->psi_err_d);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
 
 // The smallest compiled band B >= ceil((Kc+1)/R2).
-template <int R1, int R2>
+template <int R1, int R2, bool TMA>
 static int launch_pc_warp_t(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st, int f0, int nf) {
   const int need = (ctx->Kc + 1 + R2 - 1) / R2;
-  if (need <= 2) return launch_pc_warp_b<R1, R2, 2>(ctx, out, smem, st, f0, nf);
-  if (need <= 3) return launch_pc_warp_b<R1, R2, 3>(ctx, out, smem, st, f0, nf);
-  if (need <= 4) return launch_pc_warp_b<R1, R2, 4>(ctx, out, smem, st, f0, nf);
-  if (need <= 6) return launch_pc_warp_b<R1, R2, 6>(ctx, out, smem, st, f0, nf);
-  return launch_pc_warp_b<R1, R2, R1 / 2>(ctx, out, smem, st, f0, nf);
+  if (need <= 2) return launch_pc_warp_b<R1, R2, 2, TMA>(ctx, out, smem, st, f0, nf);
+  if (need <= 3) return launch_pc_warp_b<R1, R2, 3, TMA>(ctx, out, smem, st, f0, nf);
+  if (need <= 4) return launch_pc_warp_b<R1, R2, 4, TMA>(ctx, out, smem, st, f0, nf);
+  if (need <= 6) return launch_pc_warp_b<R1, R2, 6, TMA>(ctx, out, smem, st, f0, nf);
+  return launch_pc_warp_b<R1, R2, R1 / 2, TMA>(ctx, out, smem, st, f0, nf);
+}
+
+template <bool TMA>
+static int launch_pc_warp_m(cf_ctx *ctx, void *out, size_t smem, int R1, int R2, cudaStream_t st, int f0, int nf) {
+  if (R1 == 16 && R2 == 8) return launch_pc_warp_t<16, 8, TMA>(ctx, out, smem, st, f0, nf);
+  if (R1 == 16 && R2 == 16) return launch_pc_warp_t<16, 16, TMA>(ctx, out, smem, st, f0, nf);
+  return launch_pc_warp_t<32, 16, TMA>(ctx, out, smem, st, f0, nf);
 }
 
 static int launch_pc_warp(cf_ctx *ctx, void *out, cudaStream_t st, int f0 = 0, int nf = 2) {
   int R1 = 0, R2 = 0;
   if (!pc_warp_shape(ctx->N, ctx->word, &R1, &R2)) return set_error("warp pass C: unsupported N"), CF_ERR_INVALID;
-  const size_t smem = pc_warp_smem(ctx->Kc, R1, R2);
-  if (R1 == 16 && R2 == 8) return launch_pc_warp_t<16, 8>(ctx, out, smem, st, f0, nf);
-  if (R1 == 16 && R2 == 16) return launch_pc_warp_t<16, 16>(ctx, out, smem, st, f0, nf);
-  return launch_pc_warp_t<32, 16>(ctx, out, smem, st, f0, nf);
+  const bool tma = pc_warp_tma(ctx);
+  const size_t smem = pc_warp_smem(ctx->Kc, R1, R2, tma);
+  return tma ? launch_pc_warp_m<true>(ctx, out, smem, R1, R2, st, f0, nf)
+             : launch_pc_warp_m<false>(ctx, out, smem, R1, R2, st, f0, nf);
+}
+
+// The tensor map of the warp pass C's band tiles: pass B's lines pz_b[f][k][a][b]
+// (FP32 complex) as a 3-D array of floats {2N (b, re / im), N (a), 2 (Kc + 1) (f, k)}
+// with boxes {2 RW, 1, Kc + 1}.  The x coordinate 2 g RW of a box is 8 g RW bytes
+// (a multiple of 16 with RW >= 2), the box's inner extent 8 RW bytes.  Without a
+// driver entry point, or for Kc + 1 > 256 (a box dimension's limit), the kernel
+// copies with cp.async instead, and at N = 1024, where the boxes measured slower: Psi
+// synthesis per RK4 step 0.851 -> 0.771 ms at N = 512, but 7.44 -> 8.56 ms at N = 1024
+// (82-row boxes, 2 CTAs per SM, one tile of lookahead per warp).
+static int encode_pc_tmap(cf_ctx *ctx) {
+  ctx->have_pc_tmap = false;
+  int R1 = 0, R2 = 0;
+  if (!ctx->pc_fused || !pc_warp_shape(ctx->N, ctx->word, &R1, &R2) || ctx->N > 512) return CF_OK;
+  const int RW = 32 / R2, kn = ctx->Kc + 1;
+  if (kn > 256 || RW < 2) return CF_OK;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      (void)cudaGetLastError();
+      return CF_OK;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  if (!ctx->psi_err_h) {
+    CF_TRY_CUDA(cudaHostAlloc((void **)&ctx->psi_err_h, sizeof(int), cudaHostAllocMapped));
+    *ctx->psi_err_h = 0;
+    CF_TRY_CUDA(cudaHostGetDevicePointer((void **)&ctx->psi_err_d, ctx->psi_err_h, 0));
+  }
+  const cuuint64_t N = (cuuint64_t)ctx->N;
+  const cuuint64_t dims[3] = {2 * N, N, 2 * (cuuint64_t)kn};
+  const cuuint64_t strides[2] = {2 * N * sizeof(float), 2 * N * N * sizeof(float)};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * RW), 1u, (cuuint32_t)kn};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  CUtensorMap m;
+  if (encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->pz_b, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return CF_OK;
+  std::memcpy(ctx->pc_tmap, &m, sizeof(m));
+  ctx->have_pc_tmap = true;
+  return CF_OK;
 }
 
 // ---- pass B as one kernel: pruned lines -> full lines -----------------------
@@ -1106,6 +1268,7 @@ static void free_pruned(cf_ctx *ctx) {
   if (!ctx->pb_fused) cufftDestroy(ctx->plan_pb);
   if (!ctx->pc_fused) cufftDestroy(ctx->plan_pc);
   ctx->pz_a = ctx->pz_b = ctx->pr_wN = ctx->pr_twM = ctx->pr_twB = nullptr;
+  ctx->have_pc_tmap = false;
   ctx->have_pruned = false;
 }
 
@@ -1191,6 +1354,7 @@ static int ensure_pruned(cf_ctx *ctx) {
     CF_TRY_CUFFT(cufftMakePlanMany64(ctx->plan_pc, 1, n1, ie, 1, nh, oe, 1, N, dp ? CUFFT_Z2D : CUFFT_C2R,
                                      2 * N * N, &work));
   }
+  if (!(ctx->p.flags & CF_FLAG_PSI_NO_TMA)) CF_TRY(encode_pc_tmap(ctx));
   ctx->have_pruned = true;
   ctx->pr_Ka = ctx->Ka;
   ctx->pr_Kb = ctx->Kb;
@@ -1219,7 +1383,7 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
   }
   int R1w = 0, R2w = 0;
   const bool warp_c = ctx->pc_fused && !(ctx->p.flags & CF_FLAG_PSI_CTA_PASS_C) &&
-                      pc_warp_shape(ctx->N, ctx->word, &R1w, &R2w) && pc_warp_smem(ctx->Kc, R1w, R2w) <= kPcFusedSmemMax;
+                      pc_warp_shape(ctx->N, ctx->word, &R1w, &R2w) && pc_warp_smem(ctx->Kc, R1w, R2w, pc_warp_tma(ctx)) <= kPcFusedSmemMax;
   if (ctx->pb_fused) {
     ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
     CF_TRY(launch_pb_fused(ctx, st));
@@ -1264,6 +1428,8 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
 
 // Synthesises Psi, dPsi/dt at t into slot v on stream st and records the slot's event.
 static int refresh_slot(cf_ctx *ctx, PsiSlot *v, double t, cudaStream_t st) {
+  if (ctx->psi_err_h && *reinterpret_cast<volatile int *>(ctx->psi_err_h))
+    return set_error("Psi synthesis: a band copy of pass C did not land within its wait limit"), CF_ERR_TIMEOUT;
   const double eta_t = cosmo_eta(ctx->p, t);
   const double H_t = cosmo_H(ctx->p, t);
   const double factor = (2 * 3.14159265358979323846 / ctx->p.L) * eta_t / sqrt(3);

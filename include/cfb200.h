@@ -123,6 +123,11 @@ typedef struct cf_params {
  * default; three more N^3 slot pairs, or the serial order when they do not fit);
  * both give bit-identical states. */
 #define CF_FLAG_PSI_SERIAL 16
+/* FP32 storage: the warp-per-row-group pass C brings its band tiles into shared
+ * memory with per-lane cp.async instead of one TMA box per tile (the default at
+ * N = 256 and 512 where the driver provides cuTensorMapEncodeTiled; N = 1024 always
+ * uses cp.async); both compute the same values. */
+#define CF_FLAG_PSI_NO_TMA 32
 
 typedef struct cf_ctx cf_ctx;
 

@@ -181,13 +181,15 @@ def test_psi_side_stream_equals_serial(prec, N, k_max, route, stencil):
 @pytest.mark.parametrize("N,k_max", [(256, 0.3), (256, 0.6), (512, 0.5), (1024, 0.5)])
 def test_warp_pass_c_equals_cta_pass_c(N, k_max):
     """FP32 storage, N = 256, 512, 1024: the last pass of the pruned synthesis as
-    one warp per row group (the default) and as one CTA per tile
+    one warp per row group taking its band tiles by TMA (the default up to N = 512),
+    the same with per-lane cp.async copies (CF_FLAG_PSI_NO_TMA; the default at
+    N = 1024), and one CTA per tile
     (CF_FLAG_PSI_CTA_PASS_C) do the same arithmetic in the same order, so Psi and
     dPsi/dt are bit-identical."""
     L = float(N)
     Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=37, use_torch=True)
     got = {}
-    for flags in (0, cfb200.FLAG_PSI_CTA_PASS_C):
+    for flags in (0, cfb200.FLAG_PSI_NO_TMA, cfb200.FLAG_PSI_CTA_PASS_C):
         c = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, flags=flags, **FRW)
         c.set_R_fft(Rf, on_device=True)
         assert c.info.psi_route == cfb200.PSI_PRUNED_FUSED
@@ -197,6 +199,7 @@ def test_warp_pass_c_equals_cta_pass_c(N, k_max):
         got[flags] = out
         c.close()
     assert torch.equal(got[0], got[cfb200.FLAG_PSI_CTA_PASS_C])
+    assert torch.equal(got[0], got[cfb200.FLAG_PSI_NO_TMA])
     del got
     torch.cuda.empty_cache()
 
