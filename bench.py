@@ -617,7 +617,10 @@ def run_product(args):
                 "traffic_unit": "bytes per launch",
                 "algorithmic_bytes_per_site_update": bps,
                 "time_share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()
-                               if v[0]}}
+                               if v[0]},
+                "time_share_note": "per-kind CUDA-event intervals; the Psi refreshes run on a side stream beside "
+                                   "the step passes, so their intervals overlap the step's and include time "
+                                   "queued behind it"}
     if args.quick:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "config": WORKLOAD,

@@ -691,14 +691,16 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
       asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
   };
-  unsigned phase[2] = {0u, 0u};
-  bool pending[2] = {false, false};
+  // bit b: the parity buffer b's barrier completes next / a copy into buffer b is in
+  // flight (bit masks rather than arrays indexed by the buffer, which would live in
+  // local memory)
+  unsigned phase = 0u, pending = 0u;
   auto wait_buf = [&](int b) -> bool {  // TMA: the buffer's copy has landed (bounded, per lane)
     const unsigned bar = bar0 + 8 * b;
     for (long long i = 0; i < kPcSpinLimit; ++i)
-      if (mbar_try_wait(bar, phase[b])) {
-        phase[b] ^= 1u;
-        pending[b] = false;
+      if (mbar_try_wait(bar, (phase >> b) & 1u)) {
+        phase ^= 1u << b;
+        pending &= ~(1u << b);
         return true;
       }
     return false;
@@ -707,13 +709,13 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
   bool ok = true;
   if (tile < ntiles) {
     issue(tile, 0);
-    pending[0] = true;
+    pending |= 1u;
   }
   for (; tile < ntiles; tile += stride) {
     const bool more = tile + stride < ntiles;
     if (more) {
       issue(tile + stride, buf ^ 1);
-      pending[buf ^ 1] = true;
+      pending |= 1u << (buf ^ 1);
     }
     if constexpr (TMA) {
       // every lane tests the barrier itself; the warp gives up together if any lane did
@@ -726,7 +728,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
       else
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-      pending[buf] = false;
+      pending &= ~(1u << buf);
     }
     __syncwarp();  // the tile's band entries (every lane's copies)
     const float2 *X = X0 + buf * xw;
@@ -808,7 +810,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
         __threadfence_system();
       }
       for (int b = 0; b < 2; ++b)
-        if (pending[b]) (void)wait_buf(b);
+        if ((pending >> b) & 1u) (void)wait_buf(b);
     }
   }
 }
