@@ -943,61 +943,90 @@ static int encode_pc_tmap(cf_ctx *ctx) {
 // A CTA takes LINES consecutive a of one (f, k): the input tile Y[jj][line] is
 // read with the lines fastest (coalesced along a), the intermediate sits in
 // shared memory as T[m1][k2][line] (odd m1 stride), and pass 2 stores along b.
+//
+// Persistent: a CTA stages the twiddles once and walks the tiles (f, k, a-range) with
+// stride = CTAs in the grid, a fastest (adjacent CTAs read adjacent pieces of the same
+// pass-A rows); the next tile's band lines come into the other Ys buffer by cp.async
+// while the current tile runs, so no tile waits on its gathered loads.
 template <typename S, int R1, int R2, int LINES, int B>
 __global__ void __launch_bounds__(R2 *LINES) k_pass_b_fft(const S *__restrict__ pa, S *__restrict__ pb,
                                                          const typename Cplx<S>::T *__restrict__ twN, int N, int Kb,
-                                                         int Kc, int f0, const __grid_constant__ Tw32<S> tw) {
+                                                         int Kc, int f0, int ntiles,
+                                                         const __grid_constant__ Tw32<S> tw) {
   using C = typename Cplx<S>::T;
   constexpr int TS = R2 * LINES + 1;
+  constexpr int CPC = 16 / (int)sizeof(C);  // complex per 16-byte copy
+  constexpr int CH = LINES / CPC;           // 16-byte copies per band line of a tile
+  static_assert(LINES % CPC == 0, "lines");
   extern __shared__ __align__(16) unsigned char smraw[];
   C *T = reinterpret_cast<C *>(smraw);  // [R1][TS]
   C *TW = T + R1 * TS;                  // [R1][R2]: e^{2 pi i k2 m1 / N}
-  C *Ys = TW + R1 * R2;                 // [2Kb+1][LINES]
+  C *Ys = TW + R1 * R2;                 // 2 buffers [2Kb+1][LINES] (R1 R2 is even: 16-byte aligned)
   const int nj = 2 * Kb + 1;
-  const int a0 = blockIdx.x * LINES, k = blockIdx.y, f = f0 + (int)blockIdx.z;
-  const long long fk = (long long)f * (Kc + 1) + k;
-  const C *src = reinterpret_cast<const C *>(pa) + fk * nj * N + a0;
+  const int atiles = N / LINES;
   for (int i = threadIdx.x; i < R1 * R2; i += blockDim.x) TW[i] = twN[i];
-  for (int i = threadIdx.x; i < nj * LINES; i += blockDim.x) {
-    const int jj = i / LINES, l = i - jj * LINES;
-    Ys[i] = src[(long long)jj * N + l];
-  }
-  __syncthreads();
-  for (int task = threadIdx.x; task < R2 * LINES; task += blockDim.x) {
-    const int k2 = task / LINES, l = task - k2 * LINES;
-    C v[R1];
+  auto issue = [&](int t, int b) {
+    const long long fk = (long long)f0 * (Kc + 1) + t / atiles;
+    const C *src = reinterpret_cast<const C *>(pa) + fk * nj * N + (t % atiles) * LINES;
+    C *dst = Ys + b * nj * LINES;
+    for (int i = threadIdx.x; i < nj * CH; i += blockDim.x) {
+      const int jj = i / CH, c = i - jj * CH;
+      const unsigned d = (unsigned)__cvta_generic_to_shared(dst + jj * LINES + c * CPC);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + (long long)jj * N + c * CPC)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int b = 0;
+  if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if (t + (int)gridDim.x < ntiles) {
+      issue(t + gridDim.x, b ^ 1);  // buffer b ^ 1 was last read before the previous tile's second barrier
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();  // this tile's band lines; the previous tile's pass 2 is done with T
+    const C *Y = Ys + b * nj * LINES;
+    const long long fk = (long long)f0 * (Kc + 1) + t / atiles;
+    const int a0 = (t % atiles) * LINES;
+    for (int task = threadIdx.x; task < R2 * LINES; task += blockDim.x) {
+      const int k2 = task / LINES, l = task - k2 * LINES;
+      C v[R1];
 #pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) {
-      const int kk = k2 + R2 * k1;
-      C z{(S)0, (S)0};
-      if (k1 >= B && k1 < R1 - B) {
-        // outside the band's rows: zero
-      } else if (kk <= Kb) {
-        z = Ys[kk * LINES + l];  // b-frequency kk
-      } else if (kk >= N - Kb) {
-        z = Ys[(kk - N + nj) * LINES + l];  // b-frequency kk - N
+      for (int k1 = 0; k1 < R1; ++k1) {
+        const int kk = k2 + R2 * k1;
+        C z{(S)0, (S)0};
+        if (k1 >= B && k1 < R1 - B) {
+          // outside the band's rows: zero
+        } else if (kk <= Kb) {
+          z = Y[kk * LINES + l];  // b-frequency kk
+        } else if (kk >= N - Kb) {
+          z = Y[(kk - N + nj) * LINES + l];  // b-frequency kk - N
+        }
+        v[k1] = z;
       }
-      v[k1] = z;
+      dft_inv<S, R1, band_mask(R1, B)>(v, tw);
+#pragma unroll
+      for (int m1 = 0; m1 < R1; ++m1) {
+        C y = v[m1];
+        if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
+        T[m1 * TS + k2 * LINES + l] = y;
+      }
     }
-    dft_inv<S, R1, band_mask(R1, B)>(v, tw);
+    __syncthreads();
+    C *dst = reinterpret_cast<C *>(pb) + (fk * N + a0) * N;
+    for (int task = threadIdx.x; task < R1 * LINES; task += blockDim.x) {
+      const int l = task / R1, m1 = task - l * R1;
+      C u[R2];
 #pragma unroll
-    for (int m1 = 0; m1 < R1; ++m1) {
-      C y = v[m1];
-      if (m1 > 0) y = c_mul(y, TW[m1 * R2 + k2]);
-      T[m1 * TS + k2 * LINES + l] = y;
+      for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[m1 * TS + k2 * LINES + l];
+      dft_inv<S, R2>(u, tw);
+      C *row = dst + (long long)l * N;
+#pragma unroll
+      for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
     }
-  }
-  __syncthreads();
-  C *dst = reinterpret_cast<C *>(pb) + (fk * N + a0) * N;
-  for (int task = threadIdx.x; task < R1 * LINES; task += blockDim.x) {
-    const int l = task / R1, m1 = task - l * R1;
-    C u[R2];
-#pragma unroll
-    for (int k2 = 0; k2 < R2; ++k2) u[k2] = T[m1 * TS + k2 * LINES + l];
-    dft_inv<S, R2>(u, tw);
-    C *row = dst + (long long)l * N;
-#pragma unroll
-    for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
+    b ^= 1;
   }
 }
 
@@ -1017,9 +1046,9 @@ static bool pb_shape(long long N, size_t word, PbShape *sh) {
   }
   return true;
 }
-static size_t pb_fused_smem(const cf_ctx *ctx, const PbShape &sh) {
-  return ((size_t)sh.R1 * (sh.R2 * sh.lines + 1) + (size_t)sh.R1 * sh.R2 + (size_t)(2 * ctx->Kb + 1) * sh.lines) * 2 *
-         ctx->word;
+static size_t pb_fused_smem(const cf_ctx *ctx, const PbShape &sh) {  // T, TW, 2 Ys buffers
+  return ((size_t)sh.R1 * (sh.R2 * sh.lines + 1) + (size_t)sh.R1 * sh.R2 + 2 * (size_t)(2 * ctx->Kb + 1) * sh.lines) *
+         2 * ctx->word;
 }
 
 template <typename S, int R1, int R2, int LINES, int B>
@@ -1033,8 +1062,13 @@ static int launch_pb_fused_b(cf_ctx *ctx, size_t smem, cudaStream_t st, int f0, 
     tw.w[e] = C{(S)std::cos(ang), (S)std::sin(ang)};
   }
   const int N = (int)ctx->N;
-  kern<<<dim3(N / LINES, ctx->Kc + 1, nf), R2 * LINES, smem, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b,
-                                                                    (const C *)ctx->pr_twB, N, ctx->Kb, ctx->Kc, f0, tw);
+  const int ntiles = nf * (ctx->Kc + 1) * (N / LINES);
+  int sms = 0, per_sm = 0;
+  CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, R2 * LINES, smem));
+  const int grid = std::max(1, std::min(ntiles, sms * std::max(per_sm, 1)));
+  kern<<<(unsigned)grid, R2 * LINES, smem, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b, (const C *)ctx->pr_twB, N,
+                                                 ctx->Kb, ctx->Kc, f0, ntiles, tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
