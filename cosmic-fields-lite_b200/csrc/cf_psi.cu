@@ -592,12 +592,14 @@ __host__ __device__ constexpr int pc_rp(int R1, int R2) {
   return R2 >= 16 ? R1 * (R2 + 1) : R1 * (R2 + 1) + ((R2 - (R1 * (R2 + 1)) % 16) + 16) % 16;
 }
 __host__ __device__ constexpr int pc_up16(int n) { return (n + 15) & ~15; }  // complex: 128 bytes
-// Complex words per X buffer and per warp.
+// X buffers per warp (TMA: boxes two tiles ahead), complex words per X buffer and per warp.
+__host__ __device__ constexpr int pc_nbuf(bool tma) { return tma ? 3 : 2; }
 __host__ __device__ constexpr int pc_xw(int kn, int RW, bool tma) { return tma ? pc_up16(kn * RW) : RW * pc_xpp(kn); }
 __host__ __device__ constexpr int pc_warp_words(int kn, int R1, int R2, bool tma) {
-  return tma ? pc_up16(2 * pc_xw(kn, 32 / R2, true) + (32 / R2) * pc_rp(R1, R2))
-             : 2 * pc_xw(kn, 32 / R2, false) + (32 / R2) * pc_rp(R1, R2);
+  return tma ? pc_up16(pc_nbuf(true) * pc_xw(kn, 32 / R2, true) + (32 / R2) * pc_rp(R1, R2))
+             : pc_nbuf(false) * pc_xw(kn, 32 / R2, false) + (32 / R2) * pc_rp(R1, R2);
 }
+constexpr int kPcBarBytes = 256;  // 8 warps x 3 mbarriers, rounded to 128 bytes
 
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
@@ -636,23 +638,23 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
   constexpr int RP = pc_rp(R1, R2);
   constexpr int P2 = RW * R1 / 32;  // pass-2 tasks per lane
   static_assert(R2 <= R1 && 32 % R2 == 0 && (RW * R1) % 32 == 0, "shape");
+  constexpr int NB = pc_nbuf(TMA);
   extern __shared__ __align__(128) unsigned char pcw_smem[];  // TMA boxes land on 128-byte boundaries
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kn = Kc + 1;
-  // [mbarriers: 2 per warp, 128 bytes] [TW: M] [WK: kn, to 128 bytes] [per warp: X0, X1, T]
+  // [mbarriers: NB per warp] [TW: M] [WK: kn, to 128 bytes] [per warp: NB X buffers, T]
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(pcw_smem);
-  float2 *TW = reinterpret_cast<float2 *>(pcw_smem + 128);  // [R1][R2]: e^{2 pi i k2 m1 / M}
-  float2 *WK = TW + M;                                      // [Kc+1]: w^k
+  float2 *TW = reinterpret_cast<float2 *>(pcw_smem + kPcBarBytes);  // [R1][R2]: e^{2 pi i k2 m1 / M}
+  float2 *WK = TW + M;                                              // [Kc+1]: w^k
   const int xw = pc_xw(kn, RW, TMA);
   float2 *W = WK + pc_up16(kn) + (size_t)warp * pc_warp_words(kn, R1, R2, TMA);
-  float2 *X0 = W, *T = W + 2 * xw;
+  float2 *X0 = W, *T = W + NB * xw;
   for (int i = threadIdx.x; i < M; i += blockDim.x) TW[i] = twM[i];
   for (int i = threadIdx.x; i < kn; i += blockDim.x) WK[i] = wN[i];
-  const unsigned bar0 = (unsigned)__cvta_generic_to_shared(bars + 2 * warp);
+  const unsigned bar0 = (unsigned)__cvta_generic_to_shared(bars + NB * warp);
   if constexpr (TMA) {
     if (lane == 0) {
-      mbar_init(bar0, 1);
-      mbar_init(bar0 + 8, 1);
+      for (int b = 0; b < NB; ++b) mbar_init(bar0 + 8 * b, 1);
       asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
   }
@@ -707,15 +709,19 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
   };
   int buf = 0;
   bool ok = true;
-  if (tile < ntiles) {
-    issue(tile, 0);
-    pending |= 1u;
-  }
+  // prologue: the first NB - 1 tiles' copies; each iteration then issues the tile NB - 1
+  // strides ahead into the buffer the previous iteration finished with
+  for (int d = 0; d < NB - 1; ++d)
+    if (tile + d * stride < ntiles) {
+      issue(tile + d * stride, d);
+      pending |= 1u << d;
+    }
   for (; tile < ntiles; tile += stride) {
     const bool more = tile + stride < ntiles;
-    if (more) {
-      issue(tile + stride, buf ^ 1);
-      pending |= 1u << (buf ^ 1);
+    const int ahead = tile + (NB - 1) * stride, abuf = buf == 0 ? NB - 1 : buf - 1;
+    if (ahead < ntiles) {
+      issue(ahead, abuf);
+      pending |= 1u << abuf;
     }
     if constexpr (TMA) {
       // every lane tests the barrier itself; the warp gives up together if any lane did
@@ -800,8 +806,8 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
 #pragma unroll
       for (int m2 = 0; m2 < R2; ++m2) row[m1 + R1 * m2] = u[m2];
     }
-    __syncwarp();  // T and this X buffer are free for the next tile
-    buf ^= 1;
+    __syncwarp();  // T and this X buffer are free for the next tiles
+    buf = buf + 1 == NB ? 0 : buf + 1;
   }
   if constexpr (TMA) {
     if (!ok) {  // a copy did not land in time: report it, and let the copies in flight finish
@@ -809,7 +815,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
         *reinterpret_cast<volatile int *>(err) = 1;
         __threadfence_system();
       }
-      for (int b = 0; b < 2; ++b)
+      for (int b = 0; b < NB; ++b)
         if ((pending >> b) & 1u) (void)wait_buf(b);
     }
   }
@@ -826,7 +832,7 @@ static bool pc_warp_shape(long long N, size_t word, int *R1, int *R2) {
 }
 static size_t pc_warp_smem(int Kc, int R1, int R2, bool tma) {
   const int kn = Kc + 1;
-  return 128 + ((size_t)R1 * R2 + pc_up16(kn) + 8 * (size_t)pc_warp_words(kn, R1, R2, tma)) * sizeof(float2);
+  return kPcBarBytes + ((size_t)R1 * R2 + pc_up16(kn) + 8 * (size_t)pc_warp_words(kn, R1, R2, tma)) * sizeof(float2);
 }
 // Whether the warp pass C takes its band tiles by TMA (a tensor map exists).
 static bool pc_warp_tma(const cf_ctx *ctx) { return ctx->have_pc_tmap; }
@@ -892,8 +898,10 @@ static int launch_pc_warp(cf_ctx *ctx, void *out, cudaStream_t st, int f0 = 0, i
 // (a multiple of 16 with RW >= 2), the box's inner extent 8 RW bytes.  Without a
 // driver entry point, or for Kc + 1 > 256 (a box dimension's limit), the kernel
 // copies with cp.async instead, and at N = 1024, where the boxes measured slower: Psi
-// synthesis per RK4 step 0.851 -> 0.771 ms at N = 512, but 7.44 -> 8.56 ms at N = 1024
-// (82-row boxes, 2 CTAs per SM, one tile of lookahead per warp).
+// synthesis per RK4 step at N = 512 0.851 -> 0.771 ms with boxes one tile ahead, 0.726
+// -> 0.702 with boxes two tiles ahead (three buffers); at N = 1024 (82-row boxes,
+// 2 CTAs per SM) 7.44 -> 8.56 ms one tile ahead and 6.98 -> 7.17 two tiles ahead
+// (with registers up to 128 there, the per-lane copies took 7.06).
 static int encode_pc_tmap(cf_ctx *ctx) {
   ctx->have_pc_tmap = false;
   int R1 = 0, R2 = 0;
