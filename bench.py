@@ -98,8 +98,12 @@ class ClockSampler:
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # the timed region starts once the sampler is running (its first line is out)
+            t_end = time.time() + 3.0
+            while time.time() < t_end and os.path.getsize(self.f.name) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
