@@ -440,11 +440,15 @@ static int launch_step_t(cf_ctx *ctx, const StepArgs<S> &A0, cudaStream_t st) {
 }
 
 // ---- whole-step passes, 13-point stencil (FP32 storage) -------------------
-// 64 x 8 sites per CTA, two ring warps, 108 KB of shared memory: 2 CTAs per SM.
-constexpr int S13_TX = 32, S13_TY = 8;
+// 64 x 16 sites per CTA, two ring warps, 177 KB of shared memory: 1 CTA per SM.  The
+// 2-site ring makes phase 1 form 20 x 68 sites per 1024 own sites (1.33x) against 12 x
+// 68 per 512 (1.59x) at 64 x 8 (108 KB, 2 CTAs per SM): KG-FRW at N = 512 2.165 -> 2.076
+// ms per step.  For the comoving equation, which the paired passes serve (3.54 ms),
+// the whole-step pass measured 3.59 at 64 x 8 and 3.84 at 64 x 16.
+constexpr int S13_TX = 32, S13_TY = 16;
 
 template <int EQ, bool FULL>
-__global__ void __launch_bounds__(S13_TX *(S13_TY + 2), 2) k_step13(const StepArgs<float> A) {
+__global__ void __launch_bounds__(S13_TX *(S13_TY + 2), 1) k_step13(const StepArgs<float> A) {
   extern __shared__ __align__(16) unsigned char step13_smem[];
   using SM = Step13Smem<S13_TX, S13_TY>;
   const int a_begin = blockIdx.z * A.a_chunk;

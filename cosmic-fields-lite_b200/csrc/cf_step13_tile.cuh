@@ -12,7 +12,7 @@
 //
 // HBM moves the state once, like the 7-point pass: 8 (+6) words per site-update
 // against 18 (+8) for the paired passes.  A thread owns 2 consecutive sites of a row
-// -- one FP32 lane pair of cf_f32x2.cuh -- so the tile is 64 x 8 sites, and two ring
+// -- one FP32 lane pair of cf_f32x2.cuh -- so the tile is 64 x TY sites, and two ring
 // warps form the 2-site ring (its rows as lane pairs, its columns one site at a
 // time).  Every value is formed and rounded as the paired (cf_pair_tile.cuh) and the
 // single-stage (cf_stage_tile.cuh) 13-point passes form it, so all three routes give
@@ -21,7 +21,8 @@
 // Shared memory: x_phi, x_pi of six planes with a 4-site ring (the one being loaded
 // and the five phase 1 reads), yb_phi, yc_phi of five planes with a 2-site ring, and
 // what phase 1 hands to phase 2 at a thread's own sites two planes later (yb_pi and
-// the accumulator) for three planes: 108 KB at 64 x 8, two CTAs per SM.  The plane
+// the accumulator) for three planes: 177 KB at 64 x 16 (one CTA per SM), 108 KB at
+// 64 x 8 (two).  The plane
 // copies are spread over all threads (16-byte cp.async, the ring columns included),
 // so they are issued after the plane's barrier: by then no thread still reads the
 // slot they fill.  That barrier is the only one per plane: phase 2 reads the planes
