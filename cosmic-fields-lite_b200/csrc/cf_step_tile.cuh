@@ -215,6 +215,10 @@ __device__ __forceinline__ void step_tile(const StepArgs<S> &A, int c0, int b0, 
   using SM = StepSmem<S, TXv, TYv>;
   using T = typename Arith<S>::T;
   constexpr int V = SM::V, TW = SM::TW, O = SM::O, SP = SM::SP, NT = TXv * (TYv + (RINGW ? 2 : 0)), PD = SM::PD;
+  // With ring warps, the threads that form plane q's ring columns (the last 2 (TY + 2))
+  // and those that copy the next planes' ring columns (the last 2 (TY + 4)) read and
+  // refill the same slot columns ordered by __syncwarp alone: they must share one warp.
+  static_assert(!RINGW || (2 * (TYv + 4) <= 32 && NT % 32 == 0), "ring columns outside the last warp");
   S *XF = smem;               // x_phi, 4 planes of P2
   S *XP = XF + 4 * SM::P2;    // x_pi,  4 planes of P2
   S *YB = XP + 4 * SM::P2;    // yb_phi, 3 planes of P1
