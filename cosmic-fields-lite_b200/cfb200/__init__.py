@@ -74,6 +74,7 @@ _SIGS = {
     "cf_set_R_fft": ([_vp, _vp, _i, _vp], _i),
     "cf_set_psi": ([_vp, _vp, _i, _vp], _i),
     "cf_psi_fields": ([_vp, _d, _vp, _vp], _i),
+    "cf_psi_set_wait_test": ([_vp, _i, _i64], _i),
     "cf_rk4_steps": ([_vp, _vp, _d, _d, _i64, _i64, _vp], _i),
     "cf_rhs": ([_vp, _vp, _vp, _d, _vp], _i),
     "cf_scale_sum": ([_vp, _vp, _i, _vp, _vp, _i64, _vp], _i),
@@ -252,6 +253,10 @@ class Context:
     def psi_fields(self, t, d_out, stream=None):
         """Psi and dPsi/dt at time t into d_out (2 N^3 doubles on the device)."""
         check(lib().cf_psi_fields(self.h, float(t), _ptr(d_out), _stream(stream)))
+
+    def psi_set_wait_test(self, extra_bytes, spin_limit=1 << 20):
+        """Test hook: pass C's band-copy waits give up (cf_psi_set_wait_test)."""
+        check(lib().cf_psi_set_wait_test(self.h, int(extra_bytes), int(spin_limit)))
 
     # ---- hot path
     def rk4_steps(self, d_state, t0, dt, nsteps, step0=0, stream=None):

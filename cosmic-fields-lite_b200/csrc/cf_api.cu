@@ -404,6 +404,20 @@ int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream) {
   return psi_fields(ctx, t, d_out, (cudaStream_t)stream);
 }
 
+int cf_psi_set_wait_test(cf_ctx *ctx, int extra_bytes, int64_t spin_limit) {
+  CF_TRY(check_ctx(ctx));
+  if (extra_bytes < 0 || extra_bytes % 16 || spin_limit < 1) {
+    set_error("cf_psi_set_wait_test: extra_bytes must be a non-negative multiple of 16, spin_limit >= 1");
+    return CF_ERR_INVALID;
+  }
+  CF_TRY(use_device(ctx));
+  CF_TRY_CUDA(cudaDeviceSynchronize());  // no refresh of this context still running
+  ctx->pc_tx_extra = extra_bytes;
+  ctx->pc_spin_limit = spin_limit;
+  if (ctx->psi_err_h) *ctx->psi_err_h = 0;
+  return CF_OK;
+}
+
 int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps, void *stream) {
   CF_TRY(check_ctx(ctx));
   CF_TRY(check_ptr(d_state, "d_state"));

@@ -121,6 +121,8 @@ struct cf_ctx {
   alignas(64) unsigned char pc_tmap[128] = {};
   bool have_pc_tmap = false;
   int *psi_err_h = nullptr, *psi_err_d = nullptr;
+  long long pc_spin_limit = 1LL << 20;  // tests per bounded wait (cf_psi_set_wait_test)
+  int pc_tx_extra = 0;                  // bytes armed beyond each box (cf_psi_set_wait_test)
   // Pass B as one kernel (FP32, power-of-two N, 32..1024): its four-step twiddles
   // e^{2 pi i k2 m1 / N}, [m1][k2]; no plan_pb then.
   bool pb_fused = false;

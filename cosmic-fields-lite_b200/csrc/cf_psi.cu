@@ -623,15 +623,22 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const void *tmap, int 
       "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(bar)
       : "memory");
 }
-// try_wait suspends the thread for a while between tests: 2^20 tests are seconds.
-constexpr long long kPcSpinLimit = 1LL << 20;
+// The bounded waits of the warp pass C: tests per wait (by default 2^20: try_wait
+// suspends the thread for a while between tests, so seconds), and bytes armed on each
+// box's barrier beyond what the box delivers (0; cf_psi_set_wait_test sets it so that
+// the waits give up, to test that path).
+struct PcWait {
+  long long spin_limit;
+  int tx_extra;
+};
 
 template <int R1, int R2, int B, bool TMA>
 __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict__ pb, float *__restrict__ out,
                                                      const float2 *__restrict__ wN, const float2 *__restrict__ twM,
                                                      int N, int Kc, int tile0, int ntiles, int log2_groups,
                                                      int log2_n, const __grid_constant__ Tw32<float> tw,
-                                                     const __grid_constant__ CUtensorMap tmap, int *err) {
+                                                     const __grid_constant__ CUtensorMap tmap, int *err,
+                                                     const PcWait wt) {
   constexpr int M = R1 * R2;  // N == 2 M
   constexpr int RW = 32 / R2;
   constexpr int TP = R2 + 1;
@@ -675,7 +682,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
         // its last tile) before the async proxy overwrites it
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         const unsigned bar = bar0 + 8 * b;
-        mbar_expect_tx(bar, (unsigned)(kn * RW * sizeof(float2)));
+        mbar_expect_tx(bar, (unsigned)(kn * RW * sizeof(float2)) + (unsigned)wt.tx_extra);
         tma_load_3d((unsigned)__cvta_generic_to_shared(dst), &tmap, 2 * g * RW, a, f * kn, bar);
       }
     } else {
@@ -699,7 +706,7 @@ __global__ void __launch_bounds__(256, 3) k_prune_c_warp(const float *__restrict
   unsigned phase = 0u, pending = 0u;
   auto wait_buf = [&](int b) -> bool {  // TMA: the buffer's copy has landed (bounded, per lane)
     const unsigned bar = bar0 + 8 * b;
-    for (long long i = 0; i < kPcSpinLimit; ++i)
+    for (long long i = 0; i < wt.spin_limit; ++i)
       if (mbar_try_wait(bar, (phase >> b) & 1u)) {
         phase ^= 1u << b;
         pending &= ~(1u << b);
@@ -860,7 +867,7 @@ static int launch_pc_warp_b(cf_ctx *ctx, void *out, size_t smem, cudaStream_t st
   const int grid = std::max(1, std::min((ntiles - tile0 + 7) / 8, sms * std::max(per_sm, 1)));
   kern<<<(unsigned)grid, 256, smem, st>>>((const float *)ctx->pz_b, (float *)out, (const float2 *)ctx->pr_wN,
                                           (const float2 *)ctx->pr_twM, N, ctx->Kc, tile0, ntiles, log2_g, log2_n,
-                                          tw, tmap, ctx->psi_err_d);
+                                          tw, tmap, ctx->psi_err_d, PcWait{ctx->pc_spin_limit, ctx->pc_tx_extra});
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
@@ -1472,8 +1479,11 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st) {
 
 // Synthesises Psi, dPsi/dt at t into slot v on stream st and records the slot's event.
 static int refresh_slot(cf_ctx *ctx, PsiSlot *v, double t, cudaStream_t st) {
-  if (ctx->psi_err_h && *reinterpret_cast<volatile int *>(ctx->psi_err_h))
+  if (ctx->psi_err_h && *reinterpret_cast<volatile int *>(ctx->psi_err_h)) {
+    // some earlier refresh left its slot incomplete: none of the cached slots is trusted
+    for (int i = 0; i < kPsiSlots; ++i) ctx->slot[i].valid = false;
     return set_error("Psi synthesis: a band copy of pass C did not land within its wait limit"), CF_ERR_TIMEOUT;
+  }
   const double eta_t = cosmo_eta(ctx->p, t);
   const double H_t = cosmo_H(ctx->p, t);
   const double factor = (2 * 3.14159265358979323846 / ctx->p.L) * eta_t / sqrt(3);

@@ -186,6 +186,14 @@ int cf_set_psi(cf_ctx *ctx, const double *Psi, int on_device, void *stream);
  * (the reference computes them inside Equation::operator(),
  * src/equations_cuda.cu:678-731, and exposes no call of its own). */
 int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream);
+/* Failure-detection test hook (no counterpart in the reference): the warp pass C's
+ * TMA barriers are armed for `extra_bytes` (a multiple of 16) more than each band box
+ * delivers, so every bounded wait gives up after `spin_limit` tests (default 2^20).
+ * The kernel then sets the context's error word and leaves; the next refresh returns
+ * CF_ERR_TIMEOUT.  A call also clears the error word; (0, 1048576) restores normal
+ * operation.  Only for N = 256 and 512 in FP32 storage with the pruned synthesis (the
+ * TMA route); elsewhere it changes nothing. */
+int cf_psi_set_wait_test(cf_ctx *ctx, int extra_bytes, int64_t spin_limit);
 
 /* ---- the hot path -----------------------------------------------------------
  * nsteps classic RK4 steps in place; step j runs at t = t0 + (step0 + j) * dt

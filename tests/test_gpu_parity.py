@@ -204,6 +204,41 @@ def test_warp_pass_c_equals_cta_pass_c(N, k_max):
     torch.cuda.empty_cache()
 
 
+def test_pass_c_copy_wait_timeout_is_reported_and_recoverable():
+    """Failure detection without a GPU fault: pass C's band-copy barriers are armed
+    for 16 bytes more than each TMA box delivers, so every bounded wait runs out
+    (the copies themselves land).  The warps set the context's error word and leave;
+    the next refresh returns CF_ERR_TIMEOUT and drops every cached slot; with the
+    hook reset the same context gives Psi bit-identical to a fresh context's, at the
+    failed refresh's time too."""
+    N, L = 256, 256.0
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=0.5, seed=41, use_torch=True)
+    out = torch.empty(2, 2 * N ** 3, dtype=torch.float64, device="cuda")
+    want = torch.empty_like(out)
+    c = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, **FRW)
+    c.set_R_fft(Rf, on_device=True)
+    assert c.info.psi_route == cfb200.PSI_PRUNED_FUSED
+    c.psi_fields(1.1, out[0])  # builds the pruned route and its tensor map
+    c.psi_set_wait_test(16, spin_limit=1 << 12)
+    c.psi_fields(1.2, out[0])
+    torch.cuda.synchronize()
+    with pytest.raises(cfb200.CfError) as e:
+        c.psi_fields(1.3, out[1])
+    assert e.value.code == -6
+    c.psi_set_wait_test(0)
+    c.psi_fields(1.2, out[0])
+    c.psi_fields(1.3, out[1])
+    torch.cuda.synchronize()
+    c.close()
+    f = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, **FRW)
+    f.set_R_fft(Rf, on_device=True)
+    f.psi_fields(1.2, want[0])
+    f.psi_fields(1.3, want[1])
+    torch.cuda.synchronize()
+    f.close()
+    assert torch.equal(out, want)
+
+
 @pytest.mark.parametrize("N,K,prec,tol", [(512, 41, cfb200.FP32_COMP, 2e-6), (1024, 40, cfb200.FP32_COMP, 2e-6),
                                           (512, 41, cfb200.FP64, 1e-12)])
 def test_pruned_psi_at_full_size_equals_full_c2r(N, K, prec, tol):
