@@ -33,6 +33,7 @@ FLAG_PAIR_KERNELS = 4
 FLAG_PSI_CTA_PASS_C = 8
 FLAG_PSI_SERIAL = 16
 FLAG_PSI_NO_TMA = 32
+FLAG_PSI_NO_REUSE = 64
 PSI_NONE, PSI_FULL, PSI_PRUNED, PSI_PRUNED_FUSED = 0, 1, 2, 3
 
 
@@ -75,6 +76,7 @@ _SIGS = {
     "cf_set_psi": ([_vp, _vp, _i, _vp], _i),
     "cf_psi_fields": ([_vp, _d, _vp, _vp], _i),
     "cf_psi_set_wait_test": ([_vp, _i, _i64], _i),
+    "cf_psi_stats": ([_vp, _vp, _vp], _i),
     "cf_rk4_steps": ([_vp, _vp, _d, _d, _i64, _i64, _vp], _i),
     "cf_rhs": ([_vp, _vp, _vp, _d, _vp], _i),
     "cf_scale_sum": ([_vp, _vp, _i, _vp, _vp, _i64, _vp], _i),
@@ -253,6 +255,12 @@ class Context:
     def psi_fields(self, t, d_out, stream=None):
         """Psi and dPsi/dt at time t into d_out (2 N^3 doubles on the device)."""
         check(lib().cf_psi_fields(self.h, float(t), _ptr(d_out), _stream(stream)))
+
+    def psi_stats(self):
+        """(slots synthesised, stage times that reused a refresh with identical pass-A inputs)."""
+        r, u = ctypes.c_int64(0), ctypes.c_int64(0)
+        check(lib().cf_psi_stats(self.h, ctypes.byref(r), ctypes.byref(u)))
+        return r.value, u.value
 
     def psi_set_wait_test(self, extra_bytes, spin_limit=1 << 20):
         """Test hook: pass C's band-copy waits give up (cf_psi_set_wait_test)."""

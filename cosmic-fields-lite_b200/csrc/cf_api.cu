@@ -221,7 +221,7 @@ int cf_create(const cf_params *params, cf_ctx **out) {
     return CF_ERR_INVALID;
   }
   if (p.flags & ~(CF_FLAG_FULL_PSI_FFT | CF_FLAG_STAGE_KERNELS | CF_FLAG_PAIR_KERNELS | CF_FLAG_PSI_CTA_PASS_C |
-                  CF_FLAG_PSI_SERIAL | CF_FLAG_PSI_NO_TMA)) {
+                  CF_FLAG_PSI_SERIAL | CF_FLAG_PSI_NO_TMA | CF_FLAG_PSI_NO_REUSE)) {
     set_error("unknown flags 0x%x", (unsigned)p.flags);
     return CF_ERR_INVALID;
   }
@@ -297,6 +297,8 @@ int cf_destroy(cf_ctx *ctx) {
   if (ctx->have_plan_psi) cufftDestroy(ctx->plan_psi);
   psi_release(ctx);
   if (ctx->psi_err_h) cudaFreeHost(ctx->psi_err_h);
+  if (ctx->pa_diff_h) cudaFreeHost(ctx->pa_diff_h);
+  if (ctx->pa_check) cudaEventDestroy(ctx->pa_check);
   approx_release(ctx);
   if (ctx->have_d2z1) cufftDestroy(ctx->plan_d2z1);
   if (ctx->have_z2d1) cufftDestroy(ctx->plan_z2d1);
@@ -402,6 +404,13 @@ int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream) {
   }
   CF_TRY(use_device(ctx));
   return psi_fields(ctx, t, d_out, (cudaStream_t)stream);
+}
+
+int cf_psi_stats(const cf_ctx *ctx, int64_t *refreshes, int64_t *reused) {
+  CF_TRY(check_ctx(ctx));
+  if (refreshes) *refreshes = ctx->psi_refreshes;
+  if (reused) *reused = ctx->psi_reuses;
+  return CF_OK;
 }
 
 int cf_psi_set_wait_test(cf_ctx *ctx, int extra_bytes, int64_t spin_limit) {

@@ -56,6 +56,10 @@ const char *get_error();
 struct PsiSlot {
   double t = 0;
   bool valid = false;
+  // A second stage time whose refresh would have given these same bits: its pass-A
+  // inputs (FP32) were compared with this slot's on the device and found identical.
+  double t_alt = 0;
+  bool has_alt = false;
   void *psi = nullptr;   // N^3 of the storage type
   void *dpsi = nullptr;  // N^3 of the storage type
   uint64_t stamp = 0;
@@ -123,6 +127,17 @@ struct cf_ctx {
   int *psi_err_h = nullptr, *psi_err_d = nullptr;
   long long pc_spin_limit = 1LL << 20;  // tests per bounded wait (cf_psi_set_wait_test)
   int pc_tx_extra = 0;                  // bytes armed beyond each box (cf_psi_set_wait_test)
+  // FP32 pruned synthesis: the band of pass A's inputs (R_k times the transfer factors,
+  // [f][k][jj][ii], ii over the 2 Ka + 1 non-zero a-frequencies) of the latest refresh,
+  // at time pa_last_t; a refresh for a time a few ulp away compares its inputs with it
+  // (a mapped host word records a difference) and, when they are identical, takes the
+  // slot of pa_last_t instead of synthesising the same bits again.
+  void *pa_last = nullptr;
+  bool pa_last_valid = false;
+  double pa_last_t = 0;
+  int *pa_diff_h = nullptr, *pa_diff_d = nullptr;
+  cudaEvent_t pa_check = nullptr;
+  int64_t psi_refreshes = 0, psi_reuses = 0;  // cf_psi_stats
   // Pass B as one kernel (FP32, power-of-two N, 32..1024): its four-step twiddles
   // e^{2 pi i k2 m1 / N}, [m1][k2]; no plan_pb then.
   bool pb_fused = false;

@@ -303,11 +303,16 @@ static bool psi_pipelined(const cf_ctx *ctx, int64_t nsteps) {
 // Before step j: the slots of step j's stage times (present after step 0) and, but
 // for the last step, those of step j + 1, on the side stream.  The times are the
 // ones the passes read: t, t + dt/2, t + dt with t = t0 + n dt.
-static int psi_pipe_fill_step(cf_ctx *ctx, double t0, double dt, int64_t step0, int64_t j, int64_t nsteps) {
+// next = false: step j's own slots (already there but at a call's first step), before
+// its passes are enqueued; next = true: step j + 1's, after them, so that the host's
+// wait for a pass-A comparison (psi_pipe_fill) finds step j queued on the GPU.
+static int psi_pipe_fill_step(cf_ctx *ctx, double t0, double dt, int64_t step0, int64_t j, int64_t nsteps,
+                              bool next) {
   const double t = t0 + (double)(step0 + j) * dt, tn = t0 + (double)(step0 + j + 1) * dt;
   const double keep[6] = {t, t + dt / 2.0, t + dt, tn, tn + dt / 2.0, tn + dt};
-  for (int k = 0; k < 3; ++k) CF_TRY(psi_pipe_fill(ctx, keep[k], keep, 3));
-  if (j + 1 < nsteps)
+  if (!next)
+    for (int k = 0; k < 3; ++k) CF_TRY(psi_pipe_fill(ctx, keep[k], keep, 3));
+  else if (j + 1 < nsteps)
     for (int k = 3; k < 6; ++k) CF_TRY(psi_pipe_fill(ctx, keep[k], keep, 6));
   return CF_OK;
 }
@@ -339,7 +344,7 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
   for (int64_t j = 0; j < nsteps; ++j) {
     const double t = t0 + (double)(step0 + j) * dt;
     const double th = t + dh;
-    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps));
+    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps, false));
     // pass A: stages 1 (t) and 2 (t + dt/2)
     CF_TRY(pair_coeffs<S>(ctx, t, &A.inv1, &A.hub3_1, &A.psi1, &A.dpsi1, st, pipe));
     CF_TRY(pair_coeffs<S>(ctx, th, &A.inv2, &A.hub3_2, &A.psi2, &A.dpsi2, st, pipe));
@@ -359,6 +364,7 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
     A.xphi_out = phi[cur ^ 1];
     A.cw = dt;
     CF_TRY(launch_pair<S, 2>(ctx, A, st));
+    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps, true));
     if (pipe) CF_TRY(psi_pipe_step_done(ctx, st));
     cur ^= 1;
   }
@@ -529,7 +535,7 @@ static int rk4_steps_fused_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
   for (int64_t j = 0; j < nsteps; ++j) {
     const double t = t0 + (double)(step0 + j) * dt;
     const double ts[3] = {t, t + dt / 2.0, t + dt};
-    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps));
+    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps, false));
     for (int k = 0; k < 3; ++k) {
       double H;
       stage_coeffs(ctx->p, ts[k], &A.inv[k], &H);
@@ -541,6 +547,7 @@ static int rk4_steps_fused_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
     A.ophi = buf[cur ^ 1];
     A.opi = buf[cur ^ 1] + N3;
     CF_TRY(launch_step<S>(ctx, A, st));
+    if (pipe) CF_TRY(psi_pipe_fill_step(ctx, t0, dt, step0, j, nsteps, true));
     if (pipe) CF_TRY(psi_pipe_step_done(ctx, st));
     cur ^= 1;
   }

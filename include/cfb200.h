@@ -128,6 +128,12 @@ typedef struct cf_params {
  * N = 256 and 512 where the driver provides cuTensorMapEncodeTiled; N = 1024 always
  * uses cp.async); both compute the same values. */
 #define CF_FLAG_PSI_NO_TMA 32
+/* FP32 storage, pruned synthesis, side-stream refreshes: always synthesise a stage
+ * time's slot.  By default a time a few ulp from the latest refresh's (the next step's
+ * t0 + (n + 1) dt against this step's t + dt) first has its pass-A inputs compared bit
+ * for bit with that refresh's, and takes its slot when they are identical (passes A-C
+ * are deterministic in those inputs alone); both give bit-identical states. */
+#define CF_FLAG_PSI_NO_REUSE 64
 
 typedef struct cf_ctx cf_ctx;
 
@@ -194,6 +200,9 @@ int cf_psi_fields(cf_ctx *ctx, double t, double *d_out, void *stream);
  * operation.  Only for N = 256 and 512 in FP32 storage with the pruned synthesis (the
  * TMA route); elsewhere it changes nothing. */
 int cf_psi_set_wait_test(cf_ctx *ctx, int extra_bytes, int64_t spin_limit);
+/* Psi slots synthesised, and stage times that took the slot of a refresh with
+ * bit-identical pass-A inputs instead (CF_FLAG_PSI_NO_REUSE), since the context was made. */
+int cf_psi_stats(const cf_ctx *ctx, int64_t *refreshes, int64_t *reused);
 
 /* ---- the hot path -----------------------------------------------------------
  * nsteps classic RK4 steps in place; step j runs at t = t0 + (step0 + j) * dt

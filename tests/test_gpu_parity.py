@@ -155,12 +155,15 @@ def test_psi_side_stream_equals_serial(prec, N, k_max, route, stencil):
     kernels: bit-identical states for the whole-step and the paired route, over one
     step, over several (dt = 0.05 from t = 1, where t + dt and the next step's start
     differ in the last bit at some steps), and over calls that continue from cached
-    slots."""
+    slots.  At those steps the FP32 pruned synthesis compares the new time's pass-A
+    inputs with the latest refresh's and takes its slot when they are identical
+    (CF_FLAG_PSI_NO_REUSE synthesises every time): the same bits again, with fewer
+    refreshes."""
     L = float(N)
     x, _ = make_inputs(N, L, 1, 41)
     Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=k_max, seed=43)
-    got = {}
-    for flags in (route, route | cfb200.FLAG_PSI_SERIAL):
+    got, stats = {}, {}
+    for flags in (route, route | cfb200.FLAG_PSI_SERIAL, route | cfb200.FLAG_PSI_NO_REUSE):
         c = cfb200.Context(N, L, m=1.0, equation=2, precision=prec, stencil=stencil, flags=flags, **FRW)
         c.set_R_fft(Rf, on_device=False)
         st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
@@ -172,10 +175,45 @@ def test_psi_side_stream_equals_serial(prec, N, k_max, route, stencil):
             c.energy_density(st, 1.0 + 0.05 * (step0 + n), rho)  # reads the cached slot at the end time
             outs.append((st.clone(), rho))
         got[flags] = outs
+        stats[flags] = c.psi_stats()
         c.close()
-    for (a, ra), (b, rb) in zip(got[route], got[route | cfb200.FLAG_PSI_SERIAL]):
-        assert torch.equal(a, b)
-        assert torch.equal(ra, rb)
+    for other in (route | cfb200.FLAG_PSI_SERIAL, route | cfb200.FLAG_PSI_NO_REUSE):
+        for (a, ra), (b, rb) in zip(got[route], got[other]):
+            assert torch.equal(a, b)
+            assert torch.equal(ra, rb)
+    (r0, u0), (r1, u1) = stats[route], stats[route | cfb200.FLAG_PSI_NO_REUSE]
+    assert u1 == 0 and stats[route | cfb200.FLAG_PSI_SERIAL][1] == 0
+    assert r0 + u0 == r1
+    if prec == cfb200.FP32_COMP and k_max < 2.0:  # the pruned synthesis
+        assert u0 >= 1
+    else:
+        assert u0 == 0
+
+
+def test_psi_reuse_at_benchmark_shape_is_bit_identical():
+    """N = 256, FP32 storage, whole-step route, 20 steps of dt = 0.05 from t = 1 in
+    one call: seven steps start a few ulp from the previous step's t + dt.  With
+    the default reuse the states equal those with every slot synthesised, and
+    those seven times take the previous refresh's slot (or a few fewer, where a
+    pass-A input rounds differently)."""
+    N, L = 256, 256.0
+    x, _ = make_inputs(N, L, 1, 47)
+    Rf = fields.curvature_R_fft(N, L, 2.0, 1e-2, k_max=0.5, seed=49, use_torch=True)
+    got, stats = {}, {}
+    for flags in (0, cfb200.FLAG_PSI_NO_REUSE):
+        c = cfb200.Context(N, L, m=1.0, equation=2, precision=cfb200.FP32_COMP, flags=flags, **FRW)
+        c.set_R_fft(Rf, on_device=True)
+        st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
+        c.upload(st, x)
+        c.rk4_steps(st, 1.0, 0.05, 20)
+        torch.cuda.synchronize()
+        got[flags] = st
+        stats[flags] = c.psi_stats()
+        c.close()
+    assert torch.equal(got[0], got[cfb200.FLAG_PSI_NO_REUSE])
+    (r0, u0), (r1, u1) = stats[0], stats[cfb200.FLAG_PSI_NO_REUSE]
+    assert (r1, u1) == (48, 0)
+    assert r0 + u0 == 48 and 5 <= u0 <= 7
 
 
 @pytest.mark.parametrize("N,k_max", [(256, 0.3), (256, 0.6), (512, 0.5), (1024, 0.5)])
