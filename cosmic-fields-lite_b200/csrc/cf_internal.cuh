@@ -110,7 +110,9 @@ struct cf_ctx {
   bool pruned = false;
   int Ka = -1, Kb = -1, Kc = -1;
   int pr_Ka = -1, pr_Kb = -1, pr_Kc = -1;  // box the pruned plans / buffers were built for
-  void *pz_a = nullptr, *pz_b = nullptr;
+  // pz_a: pass A's input lines, zero outside the band (written once) and the band
+  // entries of the latest refresh; pz_a2: their C2C along a (out of place)
+  void *pz_a = nullptr, *pz_a2 = nullptr, *pz_b = nullptr;
   cufftHandle plan_pa = 0, plan_pb = 0, plan_pc = 0;
   bool have_pruned = false;
   // Pass C as one kernel (power-of-two N, 32..2048): twiddles e^{2 pi i j / N},
@@ -127,12 +129,11 @@ struct cf_ctx {
   int *psi_err_h = nullptr, *psi_err_d = nullptr;
   long long pc_spin_limit = 1LL << 20;  // tests per bounded wait (cf_psi_set_wait_test)
   int pc_tx_extra = 0;                  // bytes armed beyond each box (cf_psi_set_wait_test)
-  // FP32 pruned synthesis: the band of pass A's inputs (R_k times the transfer factors,
-  // [f][k][jj][ii], ii over the 2 Ka + 1 non-zero a-frequencies) of the latest refresh,
-  // at time pa_last_t; a refresh for a time a few ulp away compares its inputs with it
-  // (a mapped host word records a difference) and, when they are identical, takes the
-  // slot of pa_last_t instead of synthesising the same bits again.
-  void *pa_last = nullptr;
+  // Pruned synthesis: pz_a holds the band of pass A's inputs (R_k times the transfer
+  // factors) of the latest refresh, at time pa_last_t; an FP32 refresh for a time a few
+  // ulp away compares its inputs with them (a mapped host word records a difference)
+  // and, when they are identical, takes the slot of pa_last_t instead of synthesising
+  // the same bits again.
   bool pa_last_valid = false;
   double pa_last_t = 0;
   int *pa_diff_h = nullptr, *pa_diff_d = nullptr;

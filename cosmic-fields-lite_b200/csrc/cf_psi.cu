@@ -136,20 +136,20 @@ __global__ void k_support(const S *__restrict__ R, int N, int *__restrict__ box)
 }
 
 // Pass-A input: pz_a[f][k][jj][a] (f = Psi / dPsi, k <= Kc, jj indexes j in
-// -Kb..Kb as 0..Kb, then N-Kb..N-1), zero where |i| > Ka.
-// last (FP32, may be null): the non-zero entries are also kept there as
-// last[f][k][jj][ii], ii = a for a <= Ka and a - (N - 2 Ka - 1) for a >= N - Ka; with
-// `diff` set, each is first compared bit for bit with the value it replaces, and
-// *diff = 1 marks a difference.  Passes A-C are a fixed sequence of deterministic
-// kernels on these entries alone (the zeros and the twiddles do not change), so
-// identical entries give a bit-identical synthesis.
+// -Kb..Kb as 0..Kb, then N-Kb..N-1), zero where |i| > Ka.  Only the band |i| <= Ka is
+// written (the zeros stay from the allocation: pass A's C2C runs out of place), one
+// thread per a = ii for ii <= Ka and a = ii + N - (2 Ka + 1) above.  With `diff` set,
+// each new entry is first compared bit for bit with the one it replaces (the latest
+// refresh's) and *diff = 1 marks a difference.  Passes A-C are a fixed sequence of
+// deterministic kernels on these entries alone (the zeros and the twiddles do not
+// change), so identical entries give a bit-identical synthesis.
 __device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_uint(a) == __float_as_uint(b); }
 __device__ __forceinline__ bool same_bits(double a, double b) {
   return __double_as_longlong(a) == __double_as_longlong(b);
 }
 template <typename S>
 __global__ void k_prune_a(const S *__restrict__ R, const double *__restrict__ table, S *__restrict__ pz, int N, int Ka,
-                          int Kb, int Kc, S *__restrict__ last, int *__restrict__ diff) {
+                          int Kb, int Kc, int *__restrict__ diff) {
   using C = typename Cplx<S>::T;
   const int nh = N / 2 + 1, nj = 2 * Kb + 1, na = 2 * Ka + 1;
   const int jj = blockIdx.y, k = blockIdx.z;
@@ -158,37 +158,28 @@ __global__ void k_prune_a(const S *__restrict__ R, const double *__restrict__ ta
   const long long fstride = (long long)(Kc + 1) * nj * N;
   C *o0 = reinterpret_cast<C *>(pz) + ((long long)k * nj + jj) * N;
   C *o1 = o0 + fstride;
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < N; a += gridDim.x * blockDim.x) {
-    const int as = (a <= N / 2) ? a : N - a;
+  for (int ii = blockIdx.x * blockDim.x + threadIdx.x; ii < na; ii += gridDim.x * blockDim.x) {
+    const int a = ii <= Ka ? ii : ii + (N - na);
+    const int as = ii <= Ka ? ii : na - ii;  // |i| of a
+    const int s2 = as * as + bs * bs + k * k;
+    const double tp = table[2 * s2], td = table[2 * s2 + 1];
+    const C r = reinterpret_cast<const C *>(R)[((long long)a * N + b) * nh + k];
     C p, d;
-    p.x = p.y = d.x = d.y = (S)0;
-    if (as <= Ka) {
-      const int s2 = as * as + bs * bs + k * k;
-      const double tp = table[2 * s2], td = table[2 * s2 + 1];
-      const C r = reinterpret_cast<const C *>(R)[((long long)a * N + b) * nh + k];
-      p.x = (S)((double)r.x * tp);
-      p.y = (S)((double)r.y * tp);
-      d.x = (S)((double)r.x * td);
-      d.y = (S)((double)r.y * td);
-      if (last) {
-        const int ii = a <= Ka ? a : a - (N - na);
-        C *l0 = reinterpret_cast<C *>(last) + ((long long)k * nj + jj) * na + ii;
-        C *l1 = l0 + (long long)(Kc + 1) * nj * na;
-        if (diff) {
-          const C q0 = *l0, q1 = *l1;
-          if (!(same_bits(p.x, q0.x) && same_bits(p.y, q0.y) && same_bits(d.x, q1.x) && same_bits(d.y, q1.y)))
-            *reinterpret_cast<volatile int *>(diff) = 1;
-        }
-        *l0 = p;
-        *l1 = d;
-      }
+    p.x = (S)((double)r.x * tp);
+    p.y = (S)((double)r.y * tp);
+    d.x = (S)((double)r.x * td);
+    d.y = (S)((double)r.y * td);
+    if (diff) {
+      const C q0 = o0[a], q1 = o1[a];
+      if (!(same_bits(p.x, q0.x) && same_bits(p.y, q0.y) && same_bits(d.x, q1.x) && same_bits(d.y, q1.y)))
+        *reinterpret_cast<volatile int *>(diff) = 1;
     }
     o0[a] = p;
     o1[a] = d;
   }
 }
 
-// Pass-B input: pz_b[f][k][a][b] = pz_a[f][k][jj(b)][a] for b in the box, else 0.
+// Pass-B input: pz_b[f][k][a][b] = pz_a2[f][k][jj(b)][a] for b in the box, else 0.
 template <typename S>
 __global__ void k_prune_b(const S *__restrict__ pa, S *__restrict__ pb, int N, int Kb, int Kc) {
   using C = typename Cplx<S>::T;
@@ -970,7 +961,7 @@ static int encode_pc_tmap(cf_ctx *ctx) {
 
 // ---- pass B as one kernel: pruned lines -> full lines -----------------------
 // For FP32 storage and power-of-two N (32..1024) the C2C of pass B reads the
-// pass-A lines at their 2Kb+1 non-zero b-frequencies only (pz_a[f][k][jj][a]) and
+// pass-A lines at their 2Kb+1 non-zero b-frequencies only (pz_a2[f][k][jj][a]) and
 // writes the full lines pz_b[f][k][a][b] once: no zero-padded copy (k_prune_b)
 // and no library pass over the zeros.  The N-point inverse DFT is split
 // N = R1 x R2 as in pass C (k = k2 + R2 k1, m = m1 + R1 m2):
@@ -1104,7 +1095,7 @@ static int launch_pb_fused_b(cf_ctx *ctx, size_t smem, cudaStream_t st, int f0, 
   CF_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
   CF_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, R2 * LINES, smem));
   const int grid = std::max(1, std::min(ntiles, sms * std::max(per_sm, 1)));
-  kern<<<(unsigned)grid, R2 * LINES, smem, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b, (const C *)ctx->pr_twB, N,
+  kern<<<(unsigned)grid, R2 * LINES, smem, st>>>((const S *)ctx->pz_a2, (S *)ctx->pz_b, (const C *)ctx->pr_twB, N,
                                                  ctx->Kb, ctx->Kc, f0, ntiles, tw);
   CF_LAUNCHED(ctx);
   return CF_OK;
@@ -1333,6 +1324,7 @@ static int ensure_full_plan(cf_ctx *ctx) {
 static void free_pruned(cf_ctx *ctx) {
   if (!ctx->have_pruned) return;
   cudaFree(ctx->pz_a);
+  cudaFree(ctx->pz_a2);
   cudaFree(ctx->pz_b);
   cudaFree(ctx->pr_wN);
   cudaFree(ctx->pr_twM);
@@ -1340,8 +1332,7 @@ static void free_pruned(cf_ctx *ctx) {
   cufftDestroy(ctx->plan_pa);
   if (!ctx->pb_fused) cufftDestroy(ctx->plan_pb);
   if (!ctx->pc_fused) cufftDestroy(ctx->plan_pc);
-  cudaFree(ctx->pa_last);
-  ctx->pz_a = ctx->pz_b = ctx->pr_wN = ctx->pr_twM = ctx->pr_twB = ctx->pa_last = nullptr;
+  ctx->pz_a = ctx->pz_a2 = ctx->pz_b = ctx->pr_wN = ctx->pr_twM = ctx->pr_twB = nullptr;
   ctx->pa_last_valid = false;
   ctx->have_pc_tmap = false;
   ctx->have_pruned = false;
@@ -1349,20 +1340,21 @@ static void free_pruned(cf_ctx *ctx) {
 
 void psi_release(cf_ctx *ctx) { free_pruned(ctx); }
 
-static int ensure_pruned(cf_ctx *ctx) {
+static int ensure_pruned(cf_ctx *ctx, cudaStream_t st) {
   if (ctx->have_pruned && ctx->pr_Ka == ctx->Ka && ctx->pr_Kb == ctx->Kb && ctx->pr_Kc == ctx->Kc) return CF_OK;
   free_pruned(ctx);
   const long long N = ctx->N, nh = N / 2 + 1;
   const long long nj = 2 * ctx->Kb + 1, nk = ctx->Kc + 1;
   const size_t cb = 2 * ctx->word;  // bytes per complex
-  const long long na = 2 * ctx->Ka + 1;
   if (cudaMalloc(&ctx->pz_a, 2 * nk * nj * N * cb) != cudaSuccess ||
-      cudaMalloc(&ctx->pz_b, 2 * nk * N * N * cb) != cudaSuccess ||
-      (ctx->word == 4 && cudaMalloc(&ctx->pa_last, 2 * nk * nj * na * cb) != cudaSuccess)) {
+      cudaMalloc(&ctx->pz_a2, 2 * nk * nj * N * cb) != cudaSuccess ||
+      cudaMalloc(&ctx->pz_b, 2 * nk * N * N * cb) != cudaSuccess) {
     cudaGetLastError();
     set_error("cudaMalloc of the pruned Psi buffers failed");
     return CF_ERR_NOMEM;
   }
+  // the zeros of pass A's input lines outside the band (k_prune_a writes the band only)
+  CF_TRY_CUDA(cudaMemsetAsync(ctx->pz_a, 0, 2 * nk * nj * N * cb, st));
   const bool dp = ctx->word == 8;
   long long n1[1] = {N};
   size_t work = 0;
@@ -1446,7 +1438,7 @@ static int ensure_pruned(cf_ctx *ctx) {
   return CF_OK;
 }
 
-// check: compare pass A's inputs with those of the latest refresh (pa_last) and, when
+// check: compare pass A's inputs with those of the latest refresh (in pz_a) and, when
 // they are identical, set *same and stop there (the caller takes that refresh's slot).
 // The host waits for the comparison, so the caller issues it where the GPU has other
 // work queued (the side stream of cf_rk4_steps, behind an enqueued step).
@@ -1454,13 +1446,13 @@ template <typename S>
 static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st, bool check = false, bool *same = nullptr) {
   const int N = (int)ctx->N, Ka = ctx->Ka, Kb = ctx->Kb, Kc = ctx->Kc;
   const int nj = 2 * Kb + 1;
-  check = check && ctx->pa_last_valid && ctx->pa_last;
+  check = check && ctx->pa_last_valid;
   if (check) *reinterpret_cast<volatile int *>(ctx->pa_diff_h) = 0;  // no kernel holds it: the last check was waited for
   {
     ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
-    k_prune_a<S><<<dim3((N + 255) / 256, nj, Kc + 1), 256, 0, st>>>(
-        (const S *)ctx->R_fft, ctx->psi_table, (S *)ctx->pz_a, N, Ka, Kb, Kc, (S *)ctx->pa_last,
-        check ? ctx->pa_diff_d : nullptr);
+    const int na = 2 * Ka + 1;
+    k_prune_a<S><<<dim3((na + 127) / 128, nj, Kc + 1), 128, 0, st>>>(
+        (const S *)ctx->R_fft, ctx->psi_table, (S *)ctx->pz_a, N, Ka, Kb, Kc, check ? ctx->pa_diff_d : nullptr);
     CF_LAUNCHED(ctx);
   }
   if (check) {
@@ -1475,10 +1467,10 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st, bool check = 
     ProfScope ps(ctx, CF_PROF_PSI_FFT, st);
     CF_TRY_CUFFT(cufftSetStream(ctx->plan_pa, st));
     if (ctx->word == 8)
-      CF_TRY_CUFFT(cufftExecZ2Z(ctx->plan_pa, (cufftDoubleComplex *)ctx->pz_a, (cufftDoubleComplex *)ctx->pz_a,
+      CF_TRY_CUFFT(cufftExecZ2Z(ctx->plan_pa, (cufftDoubleComplex *)ctx->pz_a, (cufftDoubleComplex *)ctx->pz_a2,
                                 CUFFT_INVERSE));
     else
-      CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pa, (cufftComplex *)ctx->pz_a, (cufftComplex *)ctx->pz_a, CUFFT_INVERSE));
+      CF_TRY_CUFFT(cufftExecC2C(ctx->plan_pa, (cufftComplex *)ctx->pz_a, (cufftComplex *)ctx->pz_a2, CUFFT_INVERSE));
   }
   int R1w = 0, R2w = 0;
   const bool warp_c = ctx->pc_fused && !(ctx->p.flags & CF_FLAG_PSI_CTA_PASS_C) &&
@@ -1489,7 +1481,7 @@ static int refresh_pruned(cf_ctx *ctx, void *out, cudaStream_t st, bool check = 
   } else {
     {
       ProfScope ps(ctx, CF_PROF_PSI_TRANSFER, st);
-      k_prune_b<S><<<dim3((N + 255) / 256, N, 2 * (Kc + 1)), 256, 0, st>>>((const S *)ctx->pz_a, (S *)ctx->pz_b, N,
+      k_prune_b<S><<<dim3((N + 255) / 256, N, 2 * (Kc + 1)), 256, 0, st>>>((const S *)ctx->pz_a2, (S *)ctx->pz_b, N,
                                                                            Kb, Kc);
       CF_LAUNCHED(ctx);
     }
@@ -1548,7 +1540,7 @@ static int refresh_slot(cf_ctx *ctx, PsiSlot *v, double t, cudaStream_t st, PsiS
     CF_LAUNCHED(ctx);
   }
   if (ctx->pruned) {
-    CF_TRY(ensure_pruned(ctx));
+    CF_TRY(ensure_pruned(ctx, st));
     if (ctx->word == 8) {
       CF_TRY(refresh_pruned<double>(ctx, v->psi, st));
     } else {
