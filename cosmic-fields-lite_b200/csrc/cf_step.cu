@@ -378,34 +378,39 @@ static int rk4_steps_pairs_t(cf_ctx *ctx, void *d_state, double t0, double dt, i
 // step kernel): FP32 32 x 8 threads (128 x 8 sites, 2 CTAs/SM) 1.34 / 2.13 against
 // 16 x 16 1.41 / 2.22 and 16 x 8 (3 CTAs/SM) 1.59 / 2.41; FP64 16 x 8 threads (32 x 8
 // sites, 3 CTAs/SM) 1.71 / 3.14 against 32 x 8 1.85 / 3.19 and 16 x 16 1.81 / 3.32.
-template <typename S>
+template <typename S, int EQ>
 struct StepShape;
 // RW: two ring warps beside the own rows (step_tile RINGW), measured at N = 512
 // (ms per step, step kernel, comoving / KG-FRW): FP32 1.876 / 1.191 against 1.975 /
 // 1.195 without; FP64 2.883 / 1.731 against 2.942 / 1.721; bit-identical.
-template <>
-struct StepShape<float> {
+template <int EQ>
+struct StepShape<float, EQ> {
   static constexpr int TX = 32, TY = 8, MB = 2;
   static constexpr bool RW = true;
 };
-template <>
-struct StepShape<double> {
-  static constexpr int TX = 16, TY = 8, MB = 3;
+// FP64: 32 x 8 sites (57 KB, 3 CTAs per SM), or for the equations with a curvature
+// input 64 x 8 (109 KB, 2 CTAs of 10 warps, at most 102 registers, no spills): N = 512
+// step kernel, comoving 2.81 -> 2.56 ms, KG-FRW 1.69 -> 1.74 (so it keeps 32 x 8);
+// every tile shape forms the same values, so the bits do not change.
+template <int EQ>
+struct StepShape<double, EQ> {
+  static constexpr bool wide = EqOf<EQ>::coupled;
+  static constexpr int TX = wide ? 32 : 16, TY = 8, MB = wide ? 2 : 3;
   static constexpr bool RW = true;
 };
-template <typename S>
+template <typename S, int EQ>
 constexpr int step_threads_y() {
-  return StepShape<S>::TY + (StepShape<S>::RW ? 2 : 0);
+  return StepShape<S, EQ>::TY + (StepShape<S, EQ>::RW ? 2 : 0);
 }
 
 template <typename S, int EQ, bool FULL>
-__global__ void __launch_bounds__(StepShape<S>::TX *step_threads_y<S>(), StepShape<S>::MB)
+__global__ void __launch_bounds__(StepShape<S, EQ>::TX *step_threads_y<S, EQ>(), StepShape<S, EQ>::MB)
     k_step(const StepArgs<S> A) {
   extern __shared__ __align__(16) unsigned char step_smem[];
-  constexpr int TXs = StepShape<S>::TX, TYs = StepShape<S>::TY;
+  constexpr int TXs = StepShape<S, EQ>::TX, TYs = StepShape<S, EQ>::TY;
   using SM = StepSmem<S, TXs, TYs>;
   const int a_begin = blockIdx.z * A.a_chunk;
-  step_tile<S, EQ, TXs, TYs, FULL, StepShape<S>::RW>(A, blockIdx.x * SM::TW, blockIdx.y * TYs, a_begin,
+  step_tile<S, EQ, TXs, TYs, FULL, StepShape<S, EQ>::RW>(A, blockIdx.x * SM::TW, blockIdx.y * TYs, a_begin,
                                                      min(a_begin + A.a_chunk, A.N), reinterpret_cast<S *>(step_smem));
 }
 
@@ -419,7 +424,7 @@ static int step_a_chunk(int N, int tiles_xy) {
 
 template <typename S, int EQ, bool FULL>
 static int launch_step_k(cf_ctx *ctx, const StepArgs<S> &A, dim3 grid, cudaStream_t st) {
-  using SM = StepSmem<S, StepShape<S>::TX, StepShape<S>::TY>;
+  using SM = StepSmem<S, StepShape<S, EQ>::TX, StepShape<S, EQ>::TY>;
   constexpr size_t bytes = (size_t)SM::count * sizeof(S);
   static unsigned long long attr_set = 0;  // devices on which this instantiation may use > 48 KB
   const unsigned long long bit = 1ull << (ctx->device & 63);
@@ -427,15 +432,15 @@ static int launch_step_k(cf_ctx *ctx, const StepArgs<S> &A, dim3 grid, cudaStrea
     CF_TRY_CUDA(cudaFuncSetAttribute(k_step<S, EQ, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     attr_set |= bit;
   }
-  k_step<S, EQ, FULL><<<grid, dim3(StepShape<S>::TX, step_threads_y<S>()), bytes, st>>>(A);
+  k_step<S, EQ, FULL><<<grid, dim3(StepShape<S, EQ>::TX, step_threads_y<S, EQ>()), bytes, st>>>(A);
   CF_LAUNCHED(ctx);
   return CF_OK;
 }
 
 template <typename S, int EQ>
 static int launch_step_t(cf_ctx *ctx, const StepArgs<S> &A0, cudaStream_t st) {
-  using SM = StepSmem<S, StepShape<S>::TX, StepShape<S>::TY>;
-  constexpr int TYs = StepShape<S>::TY;
+  using SM = StepSmem<S, StepShape<S, EQ>::TX, StepShape<S, EQ>::TY>;
+  constexpr int TYs = StepShape<S, EQ>::TY;
   StepArgs<S> A = A0;
   unsigned gx = ceil_div(A.N, SM::TW), gy = ceil_div(A.N, TYs);
   A.a_chunk = step_a_chunk(A.N, (int)(gx * gy));
