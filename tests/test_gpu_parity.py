@@ -155,7 +155,7 @@ def test_psi_side_stream_equals_serial(prec, N, k_max, route, stencil):
     kernels: bit-identical states for the whole-step and the paired route, over one
     step, over several (dt = 0.05 from t = 1, where t + dt and the next step's start
     differ in the last bit at some steps), and over calls that continue from cached
-    slots.  At those steps the FP32 pruned synthesis compares the new time's pass-A
+    slots, two of them at such a step.  At those steps the FP32 pruned synthesis compares the new time's pass-A
     inputs with the latest refresh's and takes its slot when they are identical
     (CF_FLAG_PSI_NO_REUSE synthesises every time): the same bits again, with fewer
     refreshes."""
@@ -169,10 +169,14 @@ def test_psi_side_stream_equals_serial(prec, N, k_max, route, stencil):
         st = torch.empty(c.info.state_bytes // 8, dtype=torch.float64, device="cuda")
         c.upload(st, x)
         outs = []
-        for step0, n in ((0, 1), (1, 5), (6, 2)):
+        # steps 3 and 8 start a few ulp from the previous step's end: there the check
+        # runs at a call's first step, before its pass is enqueued
+        for step0, n in ((0, 1), (1, 2), (3, 5), (8, 2)):
             c.rk4_steps(st, 1.0, 0.05, n, step0=step0)
             rho = torch.empty(N ** 3, dtype=torch.float64, device="cuda")
-            c.energy_density(st, 1.0 + 0.05 * (step0 + n), rho)  # reads the cached slot at the end time
+            # the last stage time, t + dt of the call's last step: a cached slot (the end
+            # time t0 + (step0 + n) dt itself would be synthesised here at steps 3 and 8)
+            c.energy_density(st, 1.0 + 0.05 * (step0 + n - 1) + 0.05, rho)
             outs.append((st.clone(), rho))
         got[flags] = outs
         stats[flags] = c.psi_stats()
