@@ -597,8 +597,9 @@ def run_product(args):
     N, L = W["N"], W["L"]
     peak, peak_kind = load_peaks()
 
-    # ---- headline: FP32-comp comoving, 7-point
-    ctx, st = make_case(N, L, "fp32comp", 7, True)
+    # ---- headline: FP32-comp comoving, 7-point (--quick --fp64: the FP64 stepper on it)
+    prec = "fp64" if args.quick and args.fp64 else "fp32comp"
+    ctx, st = make_case(N, L, prec, 7, True)
     barrier(pg)
     with ClockSampler(local) as clk:
         ms, launches, prof = time_steps(ctx, st, args.steps, args.warmup, profile=True)
@@ -609,12 +610,14 @@ def run_product(args):
     import cfb200
     stage_ms = sum(prof[k][1] for k in cfb200.STEP_KINDS)
     stage_launches = sum(prof[k][0] for k in cfb200.STEP_KINDS)
-    bps = stage_bytes_per_site("fp32comp", True, "step")
+    bps = stage_bytes_per_site(prec, True, "step")
     achieved = bps * N ** 3 * args.steps / (stage_ms * 1e-3) / 1e9
     # DRAM bytes per site-update of the whole-step pass from an ncu capture at N = 256
     # (inputs 10x L2), scaled by the sites a launch processes
-    traffic = traffic_from_profiles("step_kernel_n256.md")
-    roofline = {"bound": "hbm", "kernel": "k_step (one pass per RK4 step, FP32-comp, comoving, 7-point)",
+    traffic = traffic_from_profiles("step_kernel_n256.md") if prec == "fp32comp" else None
+    roofline = {"bound": "hbm",
+                "kernel": f"k_step (one pass per RK4 step, {'FP32-comp' if prec == 'fp32comp' else 'FP64'}, "
+                          "comoving, 7-point)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
                 "traffic": (traffic * N ** 3 * args.steps / stage_launches) if traffic else None,
@@ -627,7 +630,7 @@ def run_product(args):
                                    "queued behind it"}
     if args.quick:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / args.steps, "config": WORKLOAD,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "config": WORKLOAD, "storage": prec,
                 "roofline": roofline, "gpu_launches": launches, "clocks": clocks}
         if args.spectrum:
             line["spectrum"] = spectrum_bench(ctx, st, W["t0"] + (args.steps + args.warmup) * W["dt"], reps=2)
@@ -814,9 +817,15 @@ def main():
                     help="headline measurement only (no accuracy check, variants, e2e or CPU baseline)")
     ap.add_argument("--spectrum", action="store_true",
                     help="with --quick: also time the observer's density spectrum on the stepped state")
+    ap.add_argument("--fp64", action="store_true",
+                    help="with --quick: the FP64 stepper on the headline workload instead of FP32-comp")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.fp64 and not args.quick:
+        ap.error("--fp64 goes with --quick")
+    if args.fp64:
+        WORKLOAD["workload"] = WORKLOAD["workload"].replace("FP32-comp", "FP64")
     if args.n:
         WORKLOAD["N"] = args.n
         WORKLOAD["L"] = float(args.n)
