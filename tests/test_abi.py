@@ -54,6 +54,19 @@ def test_calls_reject_null_context():
     L = cfb200.lib()
     assert L.cf_rk4_steps(None, None, 0.0, 0.1, 0, 1, None) == -1
     assert b"NULL context" in L.cf_last_error()
+    r, u = ctypes.c_int64(7), ctypes.c_int64(7)
+    assert L.cf_psi_stats(None, ctypes.byref(r), ctypes.byref(u)) == -1
+    assert (r.value, u.value) == (7, 7)
+    assert L.cf_psi_set_wait_test(None, 16, 1 << 10) == -1
+    assert b"NULL context" in L.cf_last_error()
+
+
+def test_unknown_flags_are_rejected_on_host():
+    args = dict(N=16, L=16.0, m=1.0, equation=2, precision=1, stencil=7, a1=1.0, H1=0.5, t1=1.0)
+    assert cfb200.FLAG_PSI_NO_REUSE == 64
+    with pytest.raises(cfb200.CfError) as e:
+        cfb200.Context(**args, flags=128)
+    assert e.value.code == -1 and "unknown flags" in str(e.value)
 
 
 def test_gaussian_field_contract():
