@@ -210,7 +210,11 @@ int cf_psi_stats(const cf_ctx *ctx, int64_t *refreshes, int64_t *reused);
  * stage times t, t+dt/2, t+dt/2, t+dt (stepper/runge_kutta4_classic.hpp:88-138).
  * Replaces 4 x Equation::operator() + 3 x scale_sum2 + scale_sum5 per step
  * (src/equations_cuda.cu:522-534, :678-731; src/odeint_thrust/thrust_operations.cu:238-313)
- * by one HBM pass per step (7-point stencil) or two (13-point); see CF_FLAG_*. */
+ * by one HBM pass per step (7-point stencil; 13-point for the equations without a
+ * curvature input) or two (13-point with one); see CF_FLAG_*.  Comoving curvature: the
+ * next step's Psi slots are synthesised on a side stream of the context, joined by an
+ * event on `stream` before the call returns; the host waits only for a pass-A
+ * comparison at a step start a few ulp from the previous step's end (CF_FLAG_PSI_NO_REUSE). */
 int cf_rk4_steps(cf_ctx *ctx, void *d_state, double t0, double dt, int64_t step0, int64_t nsteps,
                  void *stream);
 
